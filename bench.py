@@ -1,0 +1,313 @@
+"""Benchmark: fused hillshade (python/hill.py) on a 16384 x 16384 float32 fBm DEM.
+
+One step = one pass of the hot path over one batch: the hillshade program
+(one fused focal kernel) over the whole DEM. Per rank the DEM is its own
+independent raster (weak scaling, no data-path collective).
+
+  value  -- Gcells/s with the DEM and the output resident in HBM (all ranks,
+            units / max-over-ranks device time), CUDA events on the engine's stream;
+  e2e    -- the same metric through the public C ABI with pinned HOST buffers:
+            every step uploads the DEM, runs the program and downloads the result;
+  roofline -- algorithmic 8 B/cell (4 B read + 4 B written) per launch over the
+            measured kernel duration, against the measured HBM copy bandwidth;
+  cpu_baseline -- the C oracle (restatement of the reference semantics) on the
+            host cores, on a bounded window of the same DEM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size S]
+"""
+import argparse
+import concurrent.futures as cf
+import ctypes as ct
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = 8          # fused hillshade: read 4 B + write 4 B per cell
+METRIC = "hillshade Gcells/s & %HBM peak (fused/batched vs plain); tile p50/p99 ms"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--size", type=int, default=16384)
+    p.add_argument("--block", type=int, default=256)
+    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--no-clocks", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------- CPU baseline
+
+def cpu_baseline(dem_window, seconds_budget=12.0, threads=None):
+    """Times the C oracle over horizontal strips of `dem_window` on all host
+    cores (ctypes releases the GIL), repeating whole passes up to the budget."""
+    import numpy as np
+    from oracle import oracle as O
+    threads = threads or os.cpu_count() or 1
+    h = dem_window.shape[0]
+    strips = [dem_window[max(0, i - 1):min(h, i + h // threads + 2)] for i in range(0, h, max(1, h // threads))]
+    strips = [np.ascontiguousarray(s) for s in strips]
+    cells = sum(s.size for s in strips)
+
+    def one(s):
+        O.hillshade_f32(s, (256, 256), 0)
+
+    passes, t0 = 0, time.perf_counter()
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        while True:
+            list(ex.map(one, strips))
+            passes += 1
+            if time.perf_counter() - t0 > seconds_budget or passes >= 50:
+                break
+    dt = time.perf_counter() - t0
+    return {"value": round(cells * passes / dt / 1e9, 6), "unit": "Gcells/s", "cores": threads, "kind": "port",
+            "sample": "%dx%d window of the DEM x %d passes, oracle/oracle.c hillshade on %d threads" % (
+                dem_window.shape[1], dem_window.shape[0], passes, threads)}
+
+
+# ---------------------------------------------------------------- clocks
+
+class Clocks:
+    def __init__(self, index, enabled=True):
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_rank%d.csv" % index) if enabled else None
+        self.index = index
+
+    def __enter__(self):
+        if self.path is None:
+            return self
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+                 "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_power_cap", "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or self.path is None:
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------------- reference arm
+
+def run_reference(args, rank, world):
+    """The reference's CPU implementation of the path: its OpenCL pipeline cannot
+    be built here, so the oracle port (a C restatement of its semantics) runs on
+    the host cores, one bounded window of the workload per step."""
+    if rank != 0:
+        return
+    import numpy as np
+    from map_b200 import synth
+    from oracle import build_oracle
+    build_oracle.build_oracle()
+    win = 2048
+    dem = synth.fbm_dem(win, win, seed=1234)
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = cpu_baseline(dem, seconds_budget=0.0)
+        if i >= args.warmup:
+            times.append(r)
+    v = statistics.median([t["value"] for t in times])
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gcells/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(win * win / (v * 1e9) * 1e3, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "fused hillshade (hill.py), %dx%d F32 fBm DEM, 256x256 blocks" % (args.size, args.size),
+                       "sample": "%dx%d window per step" % (win, win)},
+            "cpu_baseline": {"value": v, "unit": "Gcells/s", "cores": times[0]["cores"], "kind": "port",
+                             "sample": times[0]["sample"]},
+            "e2e": {"value": v, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(local)
+
+    from map_b200 import map as M
+    from map_b200 import synth
+    from map_b200 import workloads as W
+    M._lib.ma_setDevice(local)
+
+    S = args.size
+    cells = S * S
+    dev = torch.device("cuda", local)
+    dem_t = synth.fbm_dem(S, S, seed=1000 + rank, xp=torch, device=dev).contiguous()
+    out_t = torch.empty_like(dem_t)
+    torch.cuda.synchronize()
+    pitch = S * 4
+    dem = M.from_device(dem_t.data_ptr(), pitch, [S, S], M.F32, [args.block, args.block])
+    hs = W.hillshade(dem)
+    stream = torch.cuda.ExternalStream(M.stream(), device=dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    # warm-up (compiles and loads the kernel)
+    for _ in range(args.warmup):
+        M.to_device(hs, out_t.data_ptr(), pitch, sync=False)
+    M.sync()
+    torch.cuda.synchronize()
+
+    # timed: K steps, inputs resident in HBM, events on the engine's stream
+    launches0 = M._lib.ma_totalLaunchCount()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize()
+    with Clocks(local, enabled=not args.no_clocks) as clk:
+        ev0.record(stream)
+        for _ in range(args.steps):
+            M.to_device(hs, out_t.data_ptr(), pitch, sync=False)
+        ev1.record(stream)
+        ev1.synchronize()
+    M.sync()
+    torch.cuda.synchronize()
+    barrier()
+    launches = M._lib.ma_totalLaunchCount() - launches0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if dist is not None:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * world / (ms * 1e-3) / 1e9
+
+    # parity spot check on a window against the oracle (cells away from the window edge)
+    parity = None
+    if rank == 0:
+        from oracle import oracle as O
+        win = 512
+        y0, x0 = S // 2 - win // 2, S // 3
+        dem_win = dem_t[y0:y0 + win, x0:x0 + win].cpu().numpy()
+        ref = O.hillshade_f32(dem_win, (args.block, args.block), 0)[1:-1, 1:-1]
+        got = out_t[y0 + 1:y0 + win - 1, x0 + 1:x0 + win - 1].cpu().numpy()
+        d = np.abs(got.astype(np.float64) - ref)
+        parity = {"cells_checked": int(d.size), "max_abs_diff_vs_oracle": float(d.max()),
+                  "bit_identical_fraction": float((got == ref).mean())}
+
+    # end to end through the public API with pinned host buffers
+    nbytes = cells * 4
+    h_in = M._lib.ma_hostAlloc(nbytes)
+    h_out = M._lib.ma_hostAlloc(nbytes)
+    ct.memmove(h_in, dem_t.cpu().numpy().ctypes.data, nbytes)
+    dem_h = M.Raster(M._lib.ma_fromHost(ct.c_void_p(h_in), M.Array([S, S]), M.F32, M.Array([args.block, args.block]), 0))
+    hs_h = W.hillshade(dem_h)
+    M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)  # warm
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
+    M._lib.ma_hostFree(ct.c_void_p(h_in))
+    M._lib.ma_hostFree(ct.c_void_p(h_out))
+
+    if rank == 0:
+        peak, peak_kind = peaks()
+        achieved = cells * BYTES_PER_CELL / (ms * 1e-3) / 1e9
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "hillshade_focal_traffic.json")
+        if os.path.exists(tpath):
+            try:
+                with open(tpath) as f:
+                    tj = json.load(f)
+                traffic = tj.get("dram_bytes_per_launch_scaled_to_%d" % S)
+            except Exception:
+                traffic = None
+        cpu_win = dem_t[:2048, :2048].cpu().numpy()
+        cpu = cpu_baseline(cpu_win, seconds_budget=10.0)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "fused hillshade (hill.py), %dx%d F32 fBm DEM (8 octaves, persistence 0.5, "
+                                   "0-3000 m) per GPU, %dx%d blocks, block-mirror border" % (S, S, args.block, args.block),
+                       "l2": "inputs larger than L2 (%.2f GiB in + %.2f GiB out per step)" % (nbytes / 2 ** 30, nbytes / 2 ** 30),
+                       "parallelism": "independent raster per GPU (weak scaling)"},
+            "e2e": {"value": round(e2e_value, 3), "unit": "Gcells/s", "h2d_bytes_per_step": nbytes,
+                    "d2h_bytes_per_step": nbytes},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "note": "achieved = 8 B/cell x cells / kernel time; peak %s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind},
+            "cpu_baseline": cpu,
+            "parity": parity,
+        }
+        ck = clk.summary()
+        if ck:
+            line["clocks"] = ck
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,163 @@
+/*
+ * map_b200.h -- C ABI of the B200 map-algebra engine (libmap_b200.so).
+ *
+ * The first block of functions is the reference's C ABI, same names, argument
+ * order and by-value POD structs, so that its ctypes bindings (python/map.py)
+ * and C/C++ callers bind unchanged. Each declaration cites the reference
+ * declaration it replaces (front/bindings.hpp:<line>).
+ *
+ * Error behaviour: the reference asserts; this library never aborts on bad input.
+ * A function that fails returns NULL (node constructors), a non-zero int
+ * (ma_write) or an empty value, and records a message readable through
+ * ma_lastError(); ma_errorCode() is non-zero after a failure and is cleared by
+ * the next successful call.
+ */
+#ifndef MAP_B200_H_
+#define MAP_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Scalar value + data type tag, 16 bytes, by value (util/VariantType.hpp:20-40). */
+typedef struct ma_Variant {
+  union {
+    float f32; double f64; uint8_t b8; uint8_t u8; uint16_t u16; uint32_t u32; uint64_t u64;
+    int8_t s8; int16_t s16; int32_t s32; int64_t s64;
+  } u;
+  int dtype;
+} ma_Variant;
+
+/* Two ints + count, 12 bytes, by value (util/Array4.hpp:42-45): data sizes,
+ * block sizes and coordinates. An empty array (n == 0) denotes D0. */
+typedef struct ma_Array {
+  int arr[2];
+  int n;
+} ma_Array;
+
+typedef struct ma_Node ma_Node; /* opaque IR node owned by the runtime */
+
+/* ---- reference ABI ---------------------------------------------------- */
+
+void ma_setupDevices(const char *plat_name, int dev_type, const char *dev_name); /* front/bindings.hpp:27 */
+void ma_increaseRef(ma_Node *node);                                              /* front/bindings.hpp:29 */
+void ma_decreaseRef(ma_Node *node);                                              /* front/bindings.hpp:30 */
+void ma_eval(ma_Node **vec, int num);                                            /* front/bindings.hpp:32 */
+ma_Variant ma_value(ma_Node *node);                                              /* front/bindings.hpp:33 */
+int ma_nodeid(ma_Node *node);                                                    /* front/bindings.hpp:36 */
+int ma_datatype(ma_Node *node);                                                  /* front/bindings.hpp:38 */
+int ma_numdim(ma_Node *node);                                                    /* front/bindings.hpp:39 */
+int ma_memorder(ma_Node *node);                                                  /* front/bindings.hpp:40 */
+ma_Array ma_datasize(ma_Node *node);                                             /* front/bindings.hpp:41 */
+ma_Array ma_blocksize(ma_Node *node);                                            /* front/bindings.hpp:42 */
+ma_Node *ma_read(const char *file_path);                                         /* front/bindings.hpp:48 */
+int ma_write(ma_Node *node, const char *file_path);                              /* front/bindings.hpp:49 */
+ma_Node *ma_constant(ma_Variant var, ma_Array ds, int dt, int mo, ma_Array bs);  /* front/bindings.hpp:55 */
+ma_Node *ma_rand(ma_Node *seed, int dt, int mo);                                 /* front/bindings.hpp:56 */
+ma_Node *ma_cast(ma_Node *node, int type);                                       /* front/bindings.hpp:57 */
+ma_Node *ma_index(ma_Node *node, int dim);                                       /* front/bindings.hpp:58 */
+ma_Node *ma_conditional(ma_Node *cond, ma_Node *lhs, ma_Node *rhs);              /* front/bindings.hpp:59 */
+ma_Node *ma_unary(ma_Node *node, int type);                                      /* front/bindings.hpp:61 */
+ma_Node *ma_binary(ma_Node *lhs, ma_Node *rhs, int type);                        /* front/bindings.hpp:62 */
+ma_Node *ma_diversity(ma_Node **vec, int num, int type);                         /* front/bindings.hpp:63 */
+ma_Node *ma_access(ma_Node *node, ma_Array coord);                               /* front/bindings.hpp:65 */
+ma_Node *ma_lhsAccess(ma_Node *lhs, ma_Node *rhs, ma_Array coord);               /* front/bindings.hpp:66 */
+ma_Node *ma_neighbor(ma_Node *node, ma_Array coord);                             /* front/bindings.hpp:68 */
+ma_Node *ma_boundedNbh(ma_Node *node, ma_Node *cx, ma_Node *cy);                 /* front/bindings.hpp:69 */
+ma_Node *ma_spreadNeighbor(ma_Node *node, ma_Node *dir, int type);               /* front/bindings.hpp:70 */
+ma_Node *ma_convolution(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds);           /* :71 */
+ma_Node *ma_focalFunc(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds, int type);   /* :72 */
+ma_Node *ma_focalPercent(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds, int type); /* :73 */
+ma_Node *ma_zonalReduc(ma_Node *node, int type);                                 /* front/bindings.hpp:75 */
+ma_Node *ma_radialScan(ma_Node *node, int type, ma_Array coord);                 /* front/bindings.hpp:76 */
+ma_Node *ma_spreadScan(ma_Node *node, ma_Node *dir, int type);                   /* front/bindings.hpp:77 */
+ma_Node *ma_stats(ma_Node *node);                                                /* front/bindings.hpp:79 */
+ma_Node *ma_barrier(ma_Node *node);                                              /* front/bindings.hpp:80 */
+/* Symbolic loops: the reference declares them but has no task to run them
+ * (runtime/task/Task.cpp:38-84); here they record an "unsupported" error. */
+void ma_loopStart(void);                                                         /* front/bindings.hpp:86 */
+void ma_loopCond(ma_Node *cond);                                                 /* front/bindings.hpp:87 */
+void ma_loopBody(void);                                                          /* front/bindings.hpp:88 */
+void ma_loopAgain(void);                                                         /* front/bindings.hpp:89 */
+ma_Node *ma_loopAssemble(void);                                                  /* front/bindings.hpp:90 */
+void ma_loopEnd(void);                                                           /* front/bindings.hpp:91 */
+void ma_loopAgainTail(ma_Node *loop, ma_Node ***agains, ma_Node ***tails, int *num); /* front/bindings.hpp:92 */
+
+/* Called by python/map.py (Raster.streamdir / Raster.numblock) but absent from
+ * the reference library; provided so those methods work. */
+int ma_streamdir(ma_Node *node);
+ma_Array ma_numblock(ma_Node *node);
+
+/* ---- extensions (no counterpart in the reference) ------------------------ */
+
+const char *ma_lastError(void);   /* message of the last failure on this thread */
+int ma_errorCode(void);           /* 0 after a successful call, non-zero after a failure */
+void ma_clearError(void);
+
+/* Border rule of focal reads outside the raster: 0 block mirror (reference),
+ * 1 raster-edge mirror, 2 dead (zero). Applies to evaluations that follow. */
+void ma_setBorder(int mode);
+int ma_getBorder(void);
+/* Launch granularity: 0 one launch per group over the whole raster (default),
+ * 1 one launch per group per block in the scheduler's order (reference granularity). */
+void ma_setExecMode(int mode);
+int ma_getExecMode(void);
+/* Block size given to rasters created without one (default 256 x 256). */
+void ma_setDefaultBlockSize(ma_Array bs);
+void ma_setDevice(int device);
+
+/* D8 steepest-descent flow direction (U8 codes 1 << dir, dir in E, SE, S, SW,
+ * W, NW, N, NE order; 0 for pits and flats). The reference builds the node in
+ * C++ only (front/Raster.cpp:485-557, FocalFlow::Factory) with no C binding. */
+ma_Node *ma_focalFlow(ma_Node *node);
+
+/* Raster inputs from caller memory. `data` is dense row-major (ds.arr[0]
+ * columns, ds.arr[1] rows). ma_fromHost copies the cells when copy != 0,
+ * otherwise it keeps the pointer, which must stay valid while the node is used
+ * (pinned memory from ma_hostAlloc makes the upload asynchronous). */
+ma_Node *ma_fromHost(const void *data, ma_Array ds, int dt, ma_Array bs, int copy);
+/* Device-resident raster input (pitch in bytes); the memory is not copied. */
+ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs);
+
+/* Evaluate `node` and copy the raster to dense row-major host memory of
+ * `bytes` bytes. Returns 0 on success. */
+int ma_toHost(ma_Node *node, void *dst, size_t bytes);
+/* Evaluate `node` into device memory (written in place when possible).
+ * With async != 0 the call returns once the work is enqueued on the library's
+ * stream (see ma_stream / ma_sync). Returns 0 on success. */
+int ma_toDevice(ma_Node *node, void *dptr, long long pitch, int async);
+/* Evaluate several nodes; async as above (scalar results always synchronise). */
+int ma_evalAsync(ma_Node **vec, int num);
+int ma_sync(void);
+void *ma_stream(void);            /* the cudaStream_t all work is enqueued on */
+
+void *ma_hostAlloc(size_t bytes); /* pinned host memory */
+void ma_hostFree(void *p);
+void *ma_devAlloc(size_t bytes);
+void ma_devFree(void *p);
+int ma_memcpy(void *dst, const void *src, size_t bytes, int kind); /* kind as cudaMemcpyKind */
+
+/* Introspection for tests and tools. */
+int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
+int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */
+int ma_totalLaunchCount(void);
+/* Fusion + code generation (+ NVRTC compilation when compile != 0) of the
+ * program that evaluates `vec`, without a device. Returns the number of
+ * kernels, or -1 on error. */
+int ma_compileOnly(ma_Node **vec, int num, int compile);
+/* Writes a text description of the fusion groups / the generated sources /
+ * the plain-mode launch order into buf; returns the length needed. */
+size_t ma_describeGroups(ma_Node **vec, int num, char *buf, size_t len);
+size_t ma_generatedSource(ma_Node **vec, int num, char *buf, size_t len);
+size_t ma_plainSchedule(ma_Node **vec, int num, char *buf, size_t len);
+int ma_nodeCount(void);
+void ma_collectGarbage(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MAP_B200_H_ */

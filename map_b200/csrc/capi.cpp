@@ -1,0 +1,506 @@
+// C ABI (include/map_b200.h): the reference's ma_* entry points
+// (front/bindings.cpp:14-273) plus the extensions documented in the header.
+// Every entry point converts C++ exceptions into a recorded error.
+#include "../../include/map_b200.h"
+#include "codegen.hpp"
+#include "cuda_env.hpp"
+#include "executor.hpp"
+#include "graph.hpp"
+
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <sstream>
+#include <string>
+
+using namespace mapb;
+
+static_assert(sizeof(ma_Variant) == sizeof(Variant), "ma_Variant layout");
+static_assert(sizeof(ma_Array) == sizeof(Arr2), "ma_Array layout");
+
+namespace {
+
+thread_local std::string t_err;
+thread_local int t_code = 0;
+
+void ok() { t_code = 0; }
+void fail(const std::string &m) {
+  t_err = m;
+  t_code = 1;
+}
+
+Variant V(ma_Variant v) {
+  Variant r;
+  std::memcpy(&r, &v, sizeof r);
+  return r;
+}
+ma_Variant MV(const Variant &v) {
+  ma_Variant r;
+  std::memcpy(&r, &v, sizeof r);
+  return r;
+}
+Arr2 A(ma_Array a) {
+  Arr2 r;
+  std::memcpy(&r, &a, sizeof r);
+  return r;
+}
+ma_Array MA(const Arr2 &a) {
+  ma_Array r;
+  std::memcpy(&r, &a, sizeof r);
+  return r;
+}
+Node *N(ma_Node *n) { return reinterpret_cast<Node *>(n); }
+ma_Node *MN(Node *n) { return reinterpret_cast<ma_Node *>(n); }
+
+Node *checked(ma_Node *n) {
+  if (n == nullptr) throw MapError("null node");
+  Node *p = N(n);
+  if (!Runtime::get().owns(p)) throw MapError("node handle does not belong to the runtime");
+  return p;
+}
+
+template <class F> ma_Node *node_call(F f) {
+  try {
+    Node *n = f();
+    ok();
+    return MN(n);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+
+template <class F> int int_call(F f) {
+  try {
+    int r = f();
+    ok();
+    return r;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return -1;
+  }
+}
+
+template <class F> void void_call(F f) {
+  try {
+    f();
+    ok();
+  } catch (const std::exception &e) {
+    fail(e.what());
+  }
+}
+
+size_t copy_out(const std::string &s, char *buf, size_t len) {
+  if (buf && len) {
+    size_t n = std::min(len - 1, s.size());
+    std::memcpy(buf, s.data(), n);
+    buf[n] = '\0';
+  }
+  return s.size() + 1;
+}
+
+std::vector<Node *> node_vec(ma_Node **vec, int num) {
+  if (num <= 0 || vec == nullptr) throw MapError("empty node list");
+  std::vector<Node *> v;
+  for (int i = 0; i < num; i++) v.push_back(checked(vec[i]));
+  return v;
+}
+
+}  // namespace
+
+#pragma GCC visibility push(default)
+extern "C" {
+
+void ma_setupDevices(const char *plat_name, int dev_type, const char *dev_name) {
+  // The platform / device strings select an OpenCL platform in the reference
+  // (runtime/Runtime.cpp:100-154); here the device is the CUDA device set by
+  // ma_setDevice (default 0), initialised lazily on first use.
+  (void)plat_name;
+  (void)dev_type;
+  (void)dev_name;
+  ok();
+}
+
+void ma_increaseRef(ma_Node *node) {
+  void_call([&] {
+    if (node) checked(node)->ref++;
+  });
+}
+
+void ma_decreaseRef(ma_Node *node) {
+  void_call([&] {
+    if (node && Runtime::get().owns(N(node)) && N(node)->ref > 0) N(node)->ref--;
+  });
+}
+
+void ma_eval(ma_Node **vec, int num) {
+  void_call([&] { Executor::get().evaluate(node_vec(vec, num), {}); });
+}
+
+ma_Variant ma_value(ma_Node *node) {
+  try {
+    Node *n = checked(node);
+    if (n->meta.numdim != D0) throw MapError("value: node is not a scalar (D0)");
+    if (!n->has_value) throw MapError("value: node has not been evaluated");
+    ok();
+    return MV(n->value);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    ma_Variant v;
+    std::memset(&v, 0, sizeof v);
+    return v;
+  }
+}
+
+int ma_nodeid(ma_Node *node) {
+  return int_call([&] { return checked(node)->id; });
+}
+int ma_datatype(ma_Node *node) {
+  return int_call([&] { return checked(node)->meta.dtype; });
+}
+int ma_numdim(ma_Node *node) {
+  return int_call([&] { return checked(node)->meta.numdim; });
+}
+int ma_memorder(ma_Node *node) {
+  return int_call([&] { return checked(node)->meta.memorder; });
+}
+int ma_streamdir(ma_Node *node) {
+  return int_call([&] {
+    checked(node);
+    return 0;
+  });
+}
+ma_Array ma_datasize(ma_Node *node) {
+  try {
+    ma_Array r = MA(checked(node)->meta.ds);
+    ok();
+    return r;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return ma_Array{{-1, -1}, 0};
+  }
+}
+ma_Array ma_blocksize(ma_Node *node) {
+  try {
+    ma_Array r = MA(checked(node)->meta.bs);
+    ok();
+    return r;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return ma_Array{{-1, -1}, 0};
+  }
+}
+ma_Array ma_numblock(ma_Node *node) {
+  try {
+    const Meta &m = checked(node)->meta;
+    ma_Array r{{-1, -1}, 0};
+    if (m.numdim == D2) r = ma_Array{{(m.W() + m.BS0() - 1) / m.BS0(), (m.H() + m.BS1() - 1) / m.BS1()}, 2};
+    ok();
+    return r;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return ma_Array{{-1, -1}, 0};
+  }
+}
+
+ma_Node *ma_read(const char *file_path) {
+  return node_call([&] {
+    if (!file_path) throw MapError("read: null path");
+    return Runtime::get().read(file_path);
+  });
+}
+
+// Evaluates eagerly, as the reference does (front/bindings.cpp:99-106).
+int ma_write(ma_Node *node, const char *file_path) {
+  try {
+    if (!file_path) throw MapError("write: null path");
+    Node *w = Runtime::get().write(checked(node), file_path);
+    w->ref++;
+    try {
+      Executor::get().evaluate({w}, {});
+    } catch (...) {
+      w->ref--;
+      throw;
+    }
+    w->ref--;
+    ok();
+    return 0;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 1;
+  }
+}
+
+ma_Node *ma_constant(ma_Variant var, ma_Array ds, int dt, int mo, ma_Array bs) {
+  return node_call([&] { return Runtime::get().constant(V(var), A(ds), dt, mo, A(bs)); });
+}
+ma_Node *ma_rand(ma_Node *seed, int dt, int mo) {
+  return node_call([&] { return Runtime::get().rand(checked(seed), dt, mo); });
+}
+ma_Node *ma_cast(ma_Node *node, int type) {
+  return node_call([&] { return Runtime::get().cast(checked(node), type); });
+}
+ma_Node *ma_index(ma_Node *node, int dim) {
+  return node_call([&] { return Runtime::get().index(checked(node), dim); });
+}
+ma_Node *ma_conditional(ma_Node *c, ma_Node *l, ma_Node *r) {
+  return node_call([&] { return Runtime::get().conditional(checked(c), checked(l), checked(r)); });
+}
+ma_Node *ma_unary(ma_Node *node, int type) {
+  return node_call([&] { return Runtime::get().unary(checked(node), type); });
+}
+ma_Node *ma_binary(ma_Node *l, ma_Node *r, int type) {
+  return node_call([&] { return Runtime::get().binary(checked(l), checked(r), type); });
+}
+ma_Node *ma_diversity(ma_Node **, int, int) {
+  return node_call([&]() -> Node * { throw MapError("diversity is not supported by this engine"); });
+}
+ma_Node *ma_access(ma_Node *, ma_Array) {
+  return node_call([&]() -> Node * { throw MapError("access is not supported by this engine"); });
+}
+ma_Node *ma_lhsAccess(ma_Node *, ma_Node *, ma_Array) {
+  return node_call([&]() -> Node * { throw MapError("lhsAccess is not supported by this engine"); });
+}
+ma_Node *ma_neighbor(ma_Node *node, ma_Array coord) {
+  return node_call([&] { return Runtime::get().neighbor(checked(node), A(coord)); });
+}
+ma_Node *ma_boundedNbh(ma_Node *, ma_Node *, ma_Node *) {
+  return node_call([&]() -> Node * { throw MapError("boundedNbh is not supported by this engine"); });
+}
+ma_Node *ma_spreadNeighbor(ma_Node *, ma_Node *, int) {
+  return node_call([&]() -> Node * { throw MapError("spreadNeighbor is not supported by this engine"); });
+}
+ma_Node *ma_convolution(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds) {
+  return node_call([&] {
+    return Runtime::get().convolution(checked(node), reinterpret_cast<Variant *>(mask_v), mask_s, A(mask_ds));
+  });
+}
+ma_Node *ma_focalFunc(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds, int type) {
+  return node_call([&] {
+    return Runtime::get().focal_func(checked(node), reinterpret_cast<Variant *>(mask_v), mask_s, A(mask_ds), type);
+  });
+}
+ma_Node *ma_focalPercent(ma_Node *, ma_Variant *, int, ma_Array, int) {
+  return node_call([&]() -> Node * { throw MapError("focalPercent is not supported by this engine"); });
+}
+ma_Node *ma_zonalReduc(ma_Node *node, int type) {
+  return node_call([&] { return Runtime::get().zonal_reduc(checked(node), type); });
+}
+ma_Node *ma_radialScan(ma_Node *node, int type, ma_Array coord) {
+  return node_call([&] { return Runtime::get().radial_scan(checked(node), type, A(coord)); });
+}
+ma_Node *ma_spreadScan(ma_Node *node, ma_Node *dir, int type) {
+  return node_call([&] { return Runtime::get().spread_scan(checked(node), checked(dir), type); });
+}
+ma_Node *ma_focalFlow(ma_Node *node) {
+  return node_call([&] { return Runtime::get().focal_flow(checked(node)); });
+}
+ma_Node *ma_stats(ma_Node *) {
+  return node_call([&]() -> Node * { throw MapError("stats is not supported by this engine"); });
+}
+ma_Node *ma_barrier(ma_Node *node) {
+  return node_call([&] { return Runtime::get().barrier(checked(node)); });
+}
+
+static void loops_unsupported() { fail("symbolic loops are not supported (the reference cannot execute them either)"); }
+void ma_loopStart(void) { loops_unsupported(); }
+void ma_loopCond(ma_Node *) { loops_unsupported(); }
+void ma_loopBody(void) { loops_unsupported(); }
+void ma_loopAgain(void) { loops_unsupported(); }
+ma_Node *ma_loopAssemble(void) {
+  loops_unsupported();
+  return nullptr;
+}
+void ma_loopEnd(void) { loops_unsupported(); }
+void ma_loopAgainTail(ma_Node *, ma_Node ***agains, ma_Node ***tails, int *num) {
+  if (agains) *agains = nullptr;
+  if (tails) *tails = nullptr;
+  if (num) *num = 0;
+  loops_unsupported();
+}
+
+// ---- extensions
+
+const char *ma_lastError(void) { return t_err.c_str(); }
+int ma_errorCode(void) { return t_code; }
+void ma_clearError(void) {
+  t_err.clear();
+  t_code = 0;
+}
+
+void ma_setBorder(int mode) {
+  void_call([&] {
+    if (mode < BORDER_BLOCK_MIRROR || mode > BORDER_DEAD) throw MapError("setBorder: invalid mode");
+    Runtime::get().border = mode;
+  });
+}
+int ma_getBorder(void) { return Runtime::get().border; }
+void ma_setExecMode(int mode) {
+  void_call([&] {
+    if (mode != EXEC_FUSED && mode != EXEC_PLAIN) throw MapError("setExecMode: invalid mode");
+    Runtime::get().exec_mode = mode;
+  });
+}
+int ma_getExecMode(void) { return Runtime::get().exec_mode; }
+void ma_setDefaultBlockSize(ma_Array bs) {
+  void_call([&] {
+    if (bs.n != 2 || bs.arr[0] <= 0 || bs.arr[1] <= 0) throw MapError("setDefaultBlockSize: invalid size");
+    Runtime::get().default_bs = A(bs);
+  });
+}
+void ma_setDevice(int device) {
+  void_call([&] { CudaEnv::get().set_device(device); });
+}
+
+ma_Node *ma_fromHost(const void *data, ma_Array ds, int dt, ma_Array bs, int copy) {
+  return node_call([&] { return Runtime::get().host_input(data, A(ds), dt, A(bs), copy != 0); });
+}
+ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs) {
+  return node_call([&] { return Runtime::get().dev_input(dptr, pitch, A(ds), dt, A(bs)); });
+}
+
+int ma_toHost(ma_Node *node, void *dst, size_t bytes) {
+  return int_call([&] {
+    Node *n = checked(node);
+    if (!dst) throw MapError("toHost: null destination");
+    if (n->meta.numdim != D2) throw MapError("toHost: node is not a 2-D raster");
+    size_t need = (size_t)n->meta.W() * n->meta.H() * dt_size(n->meta.dtype);
+    if (bytes < need) throw MapError("toHost: destination holds " + std::to_string(bytes) + " bytes, " + std::to_string(need) + " needed");
+    Sink s;
+    s.node = n;
+    s.host = dst;
+    Executor::get().evaluate({}, {s});
+    return 0;
+  });
+}
+
+int ma_toDevice(ma_Node *node, void *dptr, long long pitch, int async) {
+  return int_call([&] {
+    Node *n = checked(node);
+    if (!dptr) throw MapError("toDevice: null destination");
+    if (n->meta.numdim != D2) throw MapError("toDevice: node is not a 2-D raster");
+    if (pitch < (long long)n->meta.W() * (long long)dt_size(n->meta.dtype)) throw MapError("toDevice: pitch smaller than a row");
+    Sink s;
+    s.node = n;
+    s.dev = dptr;
+    s.dev_pitch = pitch;
+    Executor::get().evaluate({}, {s}, async != 0);
+    return 0;
+  });
+}
+
+int ma_evalAsync(ma_Node **vec, int num) {
+  return int_call([&] {
+    Executor::get().evaluate(node_vec(vec, num), {}, true);
+    return 0;
+  });
+}
+
+int ma_sync(void) {
+  return int_call([&] {
+    Executor::get().sync();
+    return 0;
+  });
+}
+
+void *ma_stream(void) {
+  try {
+    CudaEnv::get().ensure_device();
+    ok();
+    return (void *)CudaEnv::get().stream();
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+
+void *ma_hostAlloc(size_t bytes) {
+  try {
+    CudaEnv::get().ensure_device();
+    void *p = nullptr;
+    cuda_check(cudaMallocHost(&p, bytes), "cudaMallocHost");
+    ok();
+    return p;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+void ma_hostFree(void *p) {
+  if (p) cudaFreeHost(p);
+}
+void *ma_devAlloc(size_t bytes) {
+  try {
+    CudaEnv::get().ensure_device();
+    void *p = nullptr;
+    cuda_check(cudaMalloc(&p, bytes), "cudaMalloc");
+    ok();
+    return p;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+void ma_devFree(void *p) {
+  if (p) cudaFree(p);
+}
+int ma_memcpy(void *dst, const void *src, size_t bytes, int kind) {
+  return int_call([&] {
+    CudaEnv::get().ensure_device();
+    cuda_check(cudaMemcpy(dst, src, bytes, (cudaMemcpyKind)kind), "cudaMemcpy");
+    return 0;
+  });
+}
+
+int ma_lastLaunchCount(void) { return Executor::get().last.launches; }
+int ma_lastGroupCount(void) { return Executor::get().last.groups; }
+int ma_totalLaunchCount(void) { return CudaEnv::get().launches(); }
+
+int ma_compileOnly(ma_Node **vec, int num, int compile) {
+  return int_call([&] { return (int)Executor::get().compile_only(node_vec(vec, num), compile != 0).size(); });
+}
+
+size_t ma_describeGroups(ma_Node **vec, int num, char *buf, size_t len) {
+  try {
+    std::string s = Executor::get().describe_groups(node_vec(vec, num));
+    ok();
+    return copy_out(s, buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+size_t ma_generatedSource(ma_Node **vec, int num, char *buf, size_t len) {
+  try {
+    auto srcs = Executor::get().compile_only(node_vec(vec, num), false);
+    std::string s;
+    for (auto &x : srcs) s += x + "\n//----\n";
+    ok();
+    return copy_out(s, buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+size_t ma_plainSchedule(ma_Node **vec, int num, char *buf, size_t len) {
+  try {
+    auto jobs = Executor::get().schedule_for(node_vec(vec, num));
+    std::ostringstream s;
+    for (auto &j : jobs) s << j.group << " " << j.bx << " " << j.by << " " << j.kind << "\n";
+    ok();
+    return copy_out(s.str(), buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+int ma_nodeCount(void) { return (int)Runtime::get().nodes.size(); }
+void ma_collectGarbage(void) {
+  void_call([&] { Runtime::get().collect_garbage(); });
+}
+
+}  // extern "C"
+#pragma GCC visibility pop

@@ -1,0 +1,574 @@
+// Kernel generation for the Local, Focal and Zonal skeletons (see codegen.hpp).
+// The Radiating and Spreading skeletons are generated in codegen_scan.cpp.
+#include "codegen.hpp"
+
+#include <cstdlib>
+#include <map>
+#include <set>
+#include <sstream>
+
+namespace mapb {
+
+std::string codegen_scan(const Group &g, KernelPlan &plan);   // codegen_scan.cpp
+
+Variant reference_literal_value(const Variant &v) {
+  if (v.dtype == F32) {
+    std::string s = std::to_string(v.u.f32);
+    Variant r = v;
+    r.u.f32 = (float)std::strtod(s.c_str(), nullptr);
+    return r;
+  }
+  if (v.dtype == F64) {
+    std::string s = std::to_string(v.u.f64);
+    Variant r = v;
+    r.u.f64 = std::strtod(s.c_str(), nullptr);
+    return r;
+  }
+  return v;
+}
+
+namespace {
+
+const char *scalar_field(int dt) {
+  switch (dt) {
+    case F32: return "f32"; case F64: return "f64"; case B8: return "b8"; case U8: return "vu8";
+    case U16: return "vu16"; case U32: return "vu32"; case U64: return "vu64"; case S8: return "vs8";
+    case S16: return "vs16"; case S32: return "vs32"; case S64: return "vs64";
+    default: throw MapError("invalid data type");
+  }
+}
+
+std::string float_fn(int dt, const char *base) {
+  // float variants carry the 'f' suffix, double ones do not
+  return dt == F32 ? std::string(base) + "f" : std::string(base);
+}
+
+// C-level name of a unary function as used in device code
+const char *unary_fn(int op) {
+  switch (op) {
+    case SIN: return "sin"; case COS: return "cos"; case TAN: return "tan"; case ASIN: return "asin";
+    case ACOS: return "acos"; case ATAN: return "atan"; case SINH: return "sinh"; case COSH: return "cosh";
+    case TANH: return "tanh"; case ASINH: return "asinh"; case ACOSH: return "acosh"; case ATANH: return "atanh";
+    case EXP: return "exp"; case EXP2: return "exp2"; case EXP10: return "exp10"; case LOG: return "log";
+    case LOG2: return "log2"; case LOG10: return "log10"; case SQRT: return "sqrt"; case CBRT: return "cbrt";
+    case ABS: return "fabs"; case CEIL: return "ceil"; case FLOOR: return "floor"; case TRUNC: return "trunc";
+    case ROUND: return "round";
+    default: return nullptr;
+  }
+}
+
+const char *binary_sym(int op) {
+  switch (op) {
+    case ADD: return "+"; case SUB: return "-"; case MUL: return "*"; case DIV: return "/"; case MOD: return "%";
+    case EQ: return "=="; case NE: return "!="; case LT: return "<"; case GT: return ">"; case LE: return "<=";
+    case GE: return ">="; case AND: return "&&"; case OR: return "||"; case bAND: return "&"; case bOR: return "|";
+    case bXOR: return "^"; case SHL: return "<<"; case SHR: return ">>";
+    default: return nullptr;
+  }
+}
+
+struct Layout {
+  size_t off = 0;
+  std::ostringstream decl;
+  // Appends a field; `count` > 0 declares an array of that many elements, 0 a scalar.
+  size_t add(const std::string &type, const std::string &name, size_t size, size_t align, int count) {
+    off = (off + align - 1) / align * align;
+    size_t at = off;
+    decl << "  " << type << " " << name;
+    if (count > 0) decl << "[" << count << "]";
+    decl << ";  // offset " << at << "\n";
+    off += size * (count > 0 ? count : 1);
+    return at;
+  }
+  std::string finish(const std::string &sname, size_t &total) {
+    total = (off + 63) / 64 * 64;
+    std::ostringstream s;
+    s << "struct __align__(64) " << sname << " {\n" << decl.str() << "};\n";
+    s << "static_assert(sizeof(" << sname << ") == " << total << ", \"argument layout\");\n";
+    return s.str();
+  }
+};
+
+struct Gen {
+  const Group &g;
+  KernelPlan &plan;
+  std::map<Node *, int> member;   // node -> local index
+  std::map<Node *, int> rin;      // raster input -> a.in[k]
+  std::map<Node *, int> sca;      // scalar input -> a.s[k]
+  std::map<Node *, int> staged;   // focal-read raster input -> staging slot
+  std::map<Node *, int> outk;     // output raster -> a.out[k]
+  std::set<Node *> center_read;   // raster inputs read at the centre cell
+
+  Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
+
+  std::string T(Node *n) const { return dt_ctype(n->meta.dtype); }
+
+  std::string val(Node *p) const {
+    auto m = member.find(p);
+    if (m != member.end()) return "v" + std::to_string(m->second);
+    auto s = sca.find(p);
+    if (s != sca.end()) return "a.s[" + std::to_string(s->second) + "]." + scalar_field(p->meta.dtype);
+    auto r = rin.find(p);
+    if (r != rin.end()) return "i" + std::to_string(r->second);
+    throw MapError(std::string("codegen: value of node ") + kind_name(p->kind) + " is not available in its group");
+  }
+
+  std::string tap(Node *in, int dx, int dy) const {
+    auto s = staged.find(in);
+    if (s == staged.end()) throw MapError("codegen: focal read of a raster that is not staged");
+    return "f" + std::to_string(s->second) + ".tap(x, y, lx, ly, " + std::to_string(dx) + ", " + std::to_string(dy) + ")";
+  }
+
+  void classify() {
+    for (size_t i = 0; i < g.nodes.size(); i++) member[g.nodes[i]] = (int)i;
+    for (Node *in : g.inputs) {
+      if (in->meta.numdim == D0) {
+        sca[in] = (int)plan.scalars.size();
+        plan.scalars.push_back(in);
+      } else {
+        rin[in] = (int)plan.in_rasters.size();
+        plan.in_rasters.push_back(in);
+      }
+    }
+    for (Node *n : g.nodes) {
+      bool focal = n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW;
+      for (size_t j = 0; j < n->prev.size(); j++) {
+        Node *p = n->prev[j];
+        if (!rin.count(p)) continue;
+        if (focal && j == 0) {
+          if (!staged.count(p)) {
+            int k = (int)staged.size();
+            staged[p] = k;
+          }
+          plan.halo_x = std::max(plan.halo_x, n->halo_x());
+          plan.halo_y = std::max(plan.halo_y, n->halo_y());
+        } else {
+          center_read.insert(p);
+        }
+      }
+    }
+    for (Node *o : g.outputs) {
+      if (o->meta.numdim == D0) continue;
+      outk[o] = (int)plan.out_rasters.size();
+      plan.out_rasters.push_back(o);
+    }
+  }
+
+  // ---- per-node statements
+
+  std::string stmt(Node *n, bool zonal_acc) const {
+    std::ostringstream s;
+    const std::string t = T(n);
+    const std::string v = "v" + std::to_string(member.at(n));
+    const int dt = n->meta.dtype;
+    switch (n->kind) {
+      case K_CONSTANT:
+        s << "const " << t << " " << v << " = " << var_literal(reference_literal_value(n->cnst)) << ";";
+        break;
+      case K_INDEX:
+        s << "const " << t << " " << v << " = (" << t << ")(" << (n->op == D1 ? "x" : "y") << ");";
+        break;
+      case K_RAND: {
+        std::string c0 = v + "_c0", c1 = v + "_c1", k = v + "_k";
+        s << "u32 " << c0 << " = (u32)(" << val(n->prev[0]) << "), " << c1 << " = 0u; ";
+        s << "u32 " << k << " = (u32)(a.g.BS1 * (y / a.g.BS1) + a.g.BS0 * (x / a.g.BS0) + (y % a.g.BS1) * a.g.BS0 + (x % a.g.BS0)); ";
+        s << "philox2x32_10(" << c0 << ", " << c1 << ", " << k << "); ";
+        if (dt == F32) s << "const float " << v << " = (float)" << c0 << " / 4294967296.0f;";
+        else if (dt_size(dt) <= 4 && dt != B8)
+          s << t << " " << v << "; __builtin_memcpy(&" << v << ", &" << c0 << ", sizeof(" << t << "));";
+        else throw MapError("rand: unsupported output type");
+        break;
+      }
+      case K_CAST:
+        s << "const " << t << " " << v << " = (" << t << ")(" << val(n->prev[0]) << ");";
+        break;
+      case K_BARRIER:
+        s << "const " << t << " " << v << " = " << val(n->prev[0]) << ";";
+        break;
+      case K_UNARY: {
+        std::string p = val(n->prev[0]);
+        int pdt = n->prev[0]->meta.dtype;
+        switch (n->op) {
+          case POS: s << "const " << t << " " << v << " = (" << t << ")(+" << p << ");"; break;
+          case NEG: s << "const " << t << " " << v << " = (" << t << ")(-" << p << ");"; break;
+          case NOT: s << "const " << t << " " << v << " = (" << t << ")(!" << p << ");"; break;
+          case bNOT: s << "const " << t << " " << v << " = (" << t << ")(~" << p << ");"; break;
+          default: {
+            const char *fn = unary_fn(n->op);
+            if (!fn) throw MapError("codegen: invalid unary op");
+            if (dt_is_float(pdt)) {
+              s << "const " << t << " " << v << " = " << float_fn(pdt, fn) << "(" << p << ");";
+            } else if (n->op == ABS) {
+              s << "const " << t << " " << v << " = (" << t << ")(" << p << " < 0 ? -" << p << " : " << p << ");";
+            } else if (n->op == CEIL || n->op == FLOOR || n->op == TRUNC || n->op == ROUND) {
+              s << "const " << t << " " << v << " = " << p << ";";
+            } else {
+              s << "const " << t << " " << v << " = (" << t << ")" << fn << "((double)(" << p << "));";
+            }
+          }
+        }
+        break;
+      }
+      case K_BINARY: {
+        std::string l = val(n->prev[0]), r = val(n->prev[1]);
+        int pt = dt_promote(n->prev[0]->meta.dtype, n->prev[1]->meta.dtype);
+        std::string pts = dt_ctype(pt);
+        if (const char *sym = binary_sym(n->op)) {
+          if (dt_is_float(pt) && (n->op == MOD || binary_is_bitwise(n->op)))
+            throw MapError(std::string("binary op ") + binary_name(n->op) + " is not defined on floating types");
+          s << "const " << t << " " << v << " = (" << t << ")(" << l << " " << sym << " " << r << ");";
+        } else {
+          std::string L = "(" + pts + ")(" + l + ")", R = "(" + pts + ")(" + r + ")";
+          switch (n->op) {
+            case MAX2: s << "const " << t << " " << v << " = red_max<" << pts << ">(" << L << ", " << R << ");"; break;
+            case MIN2: s << "const " << t << " " << v << " = red_min<" << pts << ">(" << L << ", " << R << ");"; break;
+            case ATAN2: case POW: case HYPOT: case FMOD: {
+              const char *fn = n->op == ATAN2 ? "atan2" : n->op == POW ? "pow" : n->op == HYPOT ? "hypot" : "fmod";
+              if (dt_is_float(pt)) s << "const " << t << " " << v << " = " << float_fn(pt, fn) << "(" << L << ", " << R << ");";
+              else s << "const " << t << " " << v << " = (" << t << ")" << fn << "((double)" << L << ", (double)" << R << ");";
+              break;
+            }
+            default: throw MapError("codegen: invalid binary op");
+          }
+        }
+        break;
+      }
+      case K_CONDITIONAL:
+        s << "const " << t << " " << v << " = (" << val(n->prev[0]) << ") ? (" << t << ")(" << val(n->prev[1]) << ") : ("
+          << t << ")(" << val(n->prev[2]) << ");";
+        break;
+      case K_NEIGHBOR:
+        s << "const " << t << " " << v << " = " << tap(n->prev[0], n->coord.arr[0], n->coord.arr[1]) << ";";
+        break;
+      case K_CONVOLUTION: {
+        // runtime/skeleton/FocalSkeleton.cpp:300-336: var = 0; var += in(y+i1, x+i0) * mask[i1+h1][i0+h0],
+        // i1 outer, i0 inner; the mask is a correlation kernel (no flip).
+        int hx = n->halo_x(), hy = n->halo_y(), mw = n->mask_ds.arr[0];
+        s << t << " " << v << " = (" << t << ")0;";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++) {
+            const Variant &m = n->mask[(i1 + hy) * mw + (i0 + hx)];
+            s << "\n    " << v << " = (" << t << ")(" << v << " + " << tap(n->prev[0], i0, i1) << " * "
+              << var_literal(reference_literal_value(m)) << ");";
+          }
+        break;
+      }
+      case K_FOCALFUNC: {
+        // FocalSkeleton.cpp:338-373: var = neutral; var = var OP in(y+i1, x+i0) over the window
+        int hx = n->halo_x(), hy = n->halo_y();
+        s << t << " " << v << " = " << var_literal(reduction_neutral(n->op, dt)) << ";";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++)
+            s << "\n    " << v << " = RedOp<" << n->op << ", " << t << ">::f(" << v << ", (" << t << ")"
+              << tap(n->prev[0], i0, i1) << ");";
+        break;
+      }
+      case K_FOCALFLOW: {
+        // FocalSkeleton.cpp:405-443: steepest descent among the 8 neighbours in the order
+        // E, SE, S, SW, W, NW, N, NE; drop = (self - nbh) / dist with dist 1 or 1.414213f;
+        // strictly greater than the running max (initially 0); code 1 << dir, 0 for none.
+        static const int ox[8] = {1, 1, 0, -1, -1, -1, 0, 1}, oy[8] = {0, 1, 1, 1, 0, -1, -1, -1};
+        std::string it = T(n->prev[0]);
+        s << it << " " << v << "_m = (" << it << ")0; int " << v << "_p = -1; const " << it << " " << v << "_s = "
+          << tap(n->prev[0], 0, 0) << ";";
+        for (int d = 0; d < 8; d++) {
+          s << "\n    { const " << it << " zd = (" << it << ")(" << v << "_s - " << tap(n->prev[0], ox[d], oy[d]) << "); ";
+          s << "const " << it << " ds = " << (d % 2 == 0 ? "(" + it + ")1" : "(" + it + ")1.414213f") << "; ";
+          s << "const " << it << " dr = (" << it << ")(zd / ds); ";
+          s << "if (dr > " << v << "_m) { " << v << "_m = dr; " << v << "_p = " << d << "; } }";
+        }
+        s << "\n    const u8 " << v << " = (" << v << "_p == -1) ? (u8)0 : (u8)(1 << " << v << "_p);";
+        break;
+      }
+      case K_ZONALREDUC: {
+        if (!zonal_acc) throw MapError("codegen: zonal reduction outside a zonal group");
+        int z = -1;
+        for (size_t i = 0; i < plan.zonal.size(); i++)
+          if (plan.zonal[i] == n) z = (int)i;
+        s << "acc" << z << " = RedOp<" << n->op << ", " << t << ">::f(acc" << z << ", (" << t << ")(" << val(n->prev[0])
+          << "));";
+        break;
+      }
+      default:
+        throw MapError(std::string("codegen: node kind ") + kind_name(n->kind) + " cannot be computed per cell");
+    }
+    return s.str();
+  }
+
+  std::string stores() const {
+    std::ostringstream s;
+    for (auto &kv : outk) {
+      Node *o = kv.first;
+      s << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y, " << val(o) << ");\n";
+    }
+    return s.str();
+  }
+
+  std::string center_loads(bool from_struct) const {
+    std::ostringstream s;
+    for (Node *p : plan.in_rasters) {
+      if (!center_read.count(p)) continue;
+      int k = rin.at(p);
+      std::string t = T(p);
+      if (from_struct) s << "    const " << t << " i" << k << " = in.i" << k << ";\n";
+      else if (staged.count(p)) s << "    const " << t << " i" << k << " = " << tap(p, 0, 0) << ";\n";
+      else s << "    const " << t << " i" << k << " = ldr<" << t << ">(a.in[" << k << "], x, y);\n";
+    }
+    return s.str();
+  }
+
+  std::string body(bool zonal_acc) const {
+    std::ostringstream s;
+    for (Node *n : g.nodes) s << "    " << stmt(n, zonal_acc) << "\n";
+    return s.str();
+  }
+
+  std::string args_struct(int ntma, bool with_part) {
+    // Every field is naturally aligned in declaration order, so these offsets
+    // are the ones the device compiler assigns (checked by the size assertion).
+    Layout L;
+    plan.off_tm = ntma > 0 ? L.add("TmaDesc", "tm", 128, 64, ntma) : 0;
+    if (!plan.in_rasters.empty()) plan.off_in = L.add("RasterArg", "in", 16, 8, (int)plan.in_rasters.size());
+    if (!plan.out_rasters.empty()) plan.off_out = L.add("RasterArg", "out", 16, 8, (int)plan.out_rasters.size());
+    if (!plan.scalars.empty()) plan.off_s = L.add("Scalar8", "s", 8, 8, (int)plan.scalars.size());
+    plan.off_geom = L.add("Geom", "g", 48, 8, 0);
+    plan.off_err = L.add("u32*", "err", 8, 8, 0);
+    plan.off_aux = L.add("u64", "aux", 8, 8, 4);
+    plan.aux_count = 4;
+    (void)with_part;
+    return L.finish("Args", plan.args_size);
+  }
+};
+
+std::string fnv_hex(const std::string &s) {
+  uint64_t h = 1469598103934665603ull;
+  for (unsigned char c : s) { h ^= c; h *= 1099511628211ull; }
+  char b[17];
+  snprintf(b, sizeof b, "%016llx", (unsigned long long)h);
+  return b;
+}
+
+const int TW = 64, TH = 32, NT = 256;
+
+}  // namespace
+
+static std::string gen_local(Gen &G) {
+  KernelPlan &P = G.plan;
+  std::ostringstream s;
+  s << "#include \"map_common.cuh\"\n";
+  s << G.args_struct(0, false);
+  s << "struct In {\n";
+  for (Node *p : P.in_rasters) s << "  " << G.T(p) << " i" << G.rin.at(p) << ";\n";
+  s << "  int dummy;\n};\n";
+  s << "__device__ __forceinline__ void load_cell(const Args &a, In &in, int x, int y) {\n";
+  for (Node *p : P.in_rasters) {
+    int k = G.rin.at(p);
+    s << "  in.i" << k << " = ldr<" << G.T(p) << ">(a.in[" << k << "], x, y);\n";
+  }
+  s << "}\n";
+  s << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
+  s << G.center_loads(true) << G.body(false) << G.stores() << "}\n";
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+    << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, blockIdx.x);\n"
+    << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+    << "  const int x = t.x0 + lx;\n"
+    << "  In in[" << TH * TW / NT << "];\n"
+    << "#pragma unroll\n"
+    << "  for (int k = 0; k < " << TH * TW / NT << "; ++k) {\n"
+    << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
+    << "    if (x < t.xe && y < t.ye) load_cell(a, in[k], x, y);\n"
+    << "  }\n"
+    << "#pragma unroll\n"
+    << "  for (int k = 0; k < " << TH * TW / NT << "; ++k) {\n"
+    << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
+    << "    if (x < t.xe && y < t.ye) compute_cell(a, in[k], x, y);\n"
+    << "  }\n"
+    << "}\n";
+  return s.str();
+}
+
+static std::string gen_focal(Gen &G) {
+  KernelPlan &P = G.plan;
+  const int hx = P.halo_x, hy = P.halo_y;
+  std::ostringstream s;
+  s << "#include \"map_common.cuh\"\n";
+  const int nst = (int)G.staged.size();
+  std::vector<Node *> staged_nodes(nst);
+  for (auto &kv : G.staged) staged_nodes[kv.second] = kv.first;
+  // staging geometry: the box starts at x0 - pad_x, pad_x = halo rounded up to 16 bytes of elements
+  size_t off = 0;
+  for (int k = 0; k < nst; k++) {
+    Node *in = staged_nodes[k];
+    TmaSpec t;
+    t.in_index = G.rin.at(in);
+    t.dtype = in->meta.dtype;
+    int es = (int)dt_size(t.dtype);
+    int align_e = 16 / es;
+    t.pad_x = ((hx + align_e - 1) / align_e) * align_e;
+    if (t.pad_x == 0) t.pad_x = 0;
+    t.box_w = TW + 2 * t.pad_x;
+    t.box_h = TH + 2 * hy;
+    off = (off + 127) / 128 * 128;
+    t.smem_off = off;
+    off += (size_t)t.box_w * t.box_h * es;
+    t.halo_y = hy;
+    P.tma.push_back(t);
+  }
+  off = (off + 15) / 16 * 16;
+  const size_t bar_off = off;
+  P.smem_bytes = off + 16;
+  const bool use_tma = nst > 0 && hx <= 16 && hy <= 16;
+  s << G.args_struct(nst, false);
+  // cell function, templated on the tap providers of the staged rasters
+  s << "template <";
+  for (int k = 0; k < nst; k++) s << (k ? ", " : "") << "class F" << k;
+  s << ">\n__device__ __forceinline__ void focal_cell(const Args &a";
+  for (int k = 0; k < nst; k++) s << ", const F" << k << " &f" << k;
+  s << ", int x, int y, int lx, int ly) {\n";
+  s << G.center_loads(false) << G.body(false) << G.stores() << "}\n";
+  auto call = [&](void) {
+    std::ostringstream c;
+    c << "focal_cell(a";
+    for (int k = 0; k < nst; k++) c << ", f" << k;
+    c << ", x, y, lx, ly)";
+    return c.str();
+  };
+  const int rows = TH * TW / NT, rstep = NT / TW;
+  std::ostringstream loop;
+  loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+       << "    const int x = t.x0 + lx;\n"
+       << "#pragma unroll 2\n"
+       << "    for (int k = 0; k < " << rows << "; ++k) {\n"
+       << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
+       << "      if (x < t.xe && y < t.ye) " << call() << ";\n"
+       << "    }\n";
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+    << "  extern __shared__ __align__(128) unsigned char smem[];\n"
+    << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, blockIdx.x);\n";
+  if (use_tma) {
+    s << "  if (tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ")) {\n"
+      << "    u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
+      << "    if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
+      << "    __syncthreads();\n"
+      << "    if (threadIdx.x == 0) {\n";
+    size_t total = 0;
+    for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
+    s << "      mbar_arrive_expect_tx(bar, " << total << "u);\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      s << "      tma_load_2d(smem + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
+        << ");\n";
+    }
+    s << "    }\n"
+      << "    if (!mbar_wait_bounded(bar, 0, 1u << 26)) {\n"
+      << "      skel_fail(a.err, ERR_TMA_TIMEOUT);\n"
+      << "      mbar_wait_bounded(bar, 0, 1u << 26);\n"
+      << "      return;\n"
+      << "    }\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      std::string ty = dt_ctype(t.dtype);
+      s << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
+        << " *)(smem + " << t.smem_off << ")};\n";
+    }
+    s << loop.str() << "  } else {\n";
+  } else {
+    s << "  {\n";
+  }
+  for (int k = 0; k < nst; k++) {
+    std::string ty = G.T(staged_nodes[k]);
+    s << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
+  }
+  s << loop.str() << "  }\n}\n";
+  if (!use_tma) { P.tma.clear(); P.smem_bytes = 0; }
+  return s.str();
+}
+
+static std::string gen_zonal(Gen &G) {
+  KernelPlan &P = G.plan;
+  std::ostringstream s;
+  s << "#include \"map_common.cuh\"\n";
+  s << G.args_struct(0, true);
+  for (Node *n : G.g.nodes)
+    if (n->kind == K_ZONALREDUC) P.zonal.push_back(n);
+  const int nz = (int)P.zonal.size();
+  // cell: updates the accumulators
+  s << "__device__ __forceinline__ void zonal_cell(const Args &a, int x, int y";
+  for (int z = 0; z < nz; z++) s << ", " << G.T(P.zonal[z]) << " &acc" << z;
+  s << ") {\n" << G.center_loads(false) << G.body(true) << G.stores() << "}\n";
+  // main kernel: tiles strided over the grid, per-thread accumulation, CTA reduction, one partial per CTA.
+  // aux[0] = partials (Scalar8[slot * nz + z]), aux[1] = first slot of this launch
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+    << "  __shared__ Scalar8 scratch[" << NT / 32 << "];\n";
+  for (int z = 0; z < nz; z++) {
+    Node *n = P.zonal[z];
+    s << "  " << G.T(n) << " acc" << z << " = " << var_literal(reduction_neutral(n->op, n->meta.dtype)) << ";\n";
+  }
+  s << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+    << "  for (int ti = blockIdx.x; ti < a.g.tiles; ti += gridDim.x) {\n"
+    << "    const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, ti);\n"
+    << "    const int x = t.x0 + lx;\n"
+    << "#pragma unroll 4\n"
+    << "    for (int k = 0; k < " << TH * TW / NT << "; ++k) {\n"
+    << "      const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
+    << "      if (x < t.xe && y < t.ye) zonal_cell(a, x, y";
+  for (int z = 0; z < nz; z++) s << ", acc" << z;
+  s << ");\n    }\n  }\n"
+    << "  Scalar8 *part = (Scalar8 *)a.aux[0];\n"
+    << "  const u64 slot = a.aux[1] + blockIdx.x;\n";
+  for (int z = 0; z < nz; z++) {
+    Node *n = P.zonal[z];
+    s << "  { const " << G.T(n) << " r = block_reduce<" << n->op << ", " << G.T(n) << ">(acc" << z << ", scratch);\n"
+      << "    if (threadIdx.x == 0) put_scalar<" << G.T(n) << ">(&part[slot * " << nz << " + " << z << "], r); }\n";
+  }
+  s << "}\n";
+  // finalisation: one CTA folds every partial in slot order, deterministically
+  s << "struct FinalArgs { u64 part; s64 nslots; u64 res; u64 pad; };\n";
+  P.final_args_size = 32;
+  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME_final(const __grid_constant__ FinalArgs f) {\n"
+    << "  __shared__ Scalar8 scratch[" << NT / 32 << "];\n"
+    << "  const Scalar8 *part = (const Scalar8 *)f.part;\n"
+    << "  Scalar8 *res = (Scalar8 *)f.res;\n";
+  for (int z = 0; z < nz; z++) {
+    Node *n = P.zonal[z];
+    std::string t = G.T(n);
+    s << "  { " << t << " acc = " << var_literal(reduction_neutral(n->op, n->meta.dtype)) << ";\n"
+      << "    for (s64 i = threadIdx.x; i < f.nslots; i += blockDim.x) acc = RedOp<" << n->op << ", " << t
+      << ">::f(acc, get_scalar<" << t << ">(part[i * " << nz << " + " << z << "]));\n"
+      << "    const " << t << " r = block_reduce<" << n->op << ", " << t << ">(acc, scratch);\n"
+      << "    if (threadIdx.x == 0) put_scalar<" << t << ">(&res[" << z << "], r); }\n";
+  }
+  s << "}\n";
+  return s.str();
+}
+
+KernelPlan generate_kernel(const Group &g) {
+  KernelPlan P;
+  P.skeleton = g.skeleton;
+  P.threads = NT;
+  P.tile_w = TW;
+  P.tile_h = TH;
+  Gen G(g, P);
+  G.classify();
+  std::string src;
+  const char *prefix = "map_local";
+  switch (g.skeleton) {
+    case SK_LOCAL: src = gen_local(G); prefix = "map_local"; break;
+    case SK_FOCAL: src = gen_focal(G); prefix = "map_focal"; break;
+    case SK_ZONAL: src = gen_zonal(G); prefix = "map_zonal"; break;
+    case SK_RADIAL: case SK_SPREAD:
+      src = codegen_scan(g, P);
+      prefix = g.skeleton == SK_RADIAL ? "map_radial" : "map_spread";
+      break;
+    default: throw MapError("codegen: group has no device skeleton");
+  }
+  std::string name = std::string(prefix) + "_" + fnv_hex(src).substr(0, 12);
+  size_t pos;
+  while ((pos = src.find("KNAME")) != std::string::npos) src.replace(pos, 5, name);
+  P.kname = name;
+  if (g.skeleton == SK_ZONAL) P.kname_final = name + "_final";
+  P.source = src;
+  return P;
+}
+
+}  // namespace mapb

@@ -1,0 +1,58 @@
+// Kernel generation: turns one fusion group into CUDA C++ source that
+// instantiates the hand-written skeleton building blocks (skeleton/*.cuh), plus
+// the launch plan the executor needs (argument layout, tiles, TMA boxes).
+//
+// This replaces the reference's OpenCL code generators (runtime/skeleton/*.cpp):
+// the per-cell expression of the group is emitted as straight-line code with
+// canonical (position-based) names, so groups with equal structure produce
+// identical source and share one compiled module, as the reference's Version
+// cache shares one program per signature (runtime/Program.cpp:64).
+#pragma once
+
+#include "fusion.hpp"
+
+#include <string>
+#include <vector>
+
+namespace mapb {
+
+struct TmaSpec {
+  int in_index = 0;     // index into the plan's raster inputs
+  int dtype = 0;
+  int box_w = 0, box_h = 0;
+  int pad_x = 0;        // tile column 0 is raster column (x0 - pad_x)
+  int halo_y = 0;
+  size_t smem_off = 0;  // offset of the staged tile in dynamic shared memory
+};
+
+struct KernelPlan {
+  int skeleton = SK_LOCAL;
+  std::string source;
+  std::string kname;        // main kernel
+  std::string kname_final;  // zonal finalisation kernel (empty otherwise)
+  size_t args_size = 0;
+  // argument layout (byte offsets inside the kernel's argument struct)
+  size_t off_tm = 0, off_in = 0, off_out = 0, off_s = 0, off_geom = 0, off_err = 0, off_part = 0, off_aux = 0;
+  size_t final_args_size = 0;
+  std::vector<Node *> in_rasters;   // a.in[k]
+  std::vector<Node *> out_rasters;  // a.out[k]
+  std::vector<Node *> scalars;      // a.s[k]
+  std::vector<Node *> zonal;        // reductions, in partial-slot order
+  std::vector<TmaSpec> tma;
+  int threads = 256;
+  int tile_w = 64, tile_h = 32;
+  int halo_x = 0, halo_y = 0;
+  size_t smem_bytes = 0;
+  int aux_count = 0;
+  // radial / spreading specifics
+  Node *core = nullptr;
+};
+
+KernelPlan generate_kernel(const Group &g);
+
+// Reference float-constant rounding: constants written into kernel text by the
+// reference go through std::to_string ("%f", six decimals) before the device
+// compiler parses them (util/VariantType.cpp:89-104, runtime/skeleton/util.cpp mask_decl).
+Variant reference_literal_value(const Variant &v);
+
+}  // namespace mapb

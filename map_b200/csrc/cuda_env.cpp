@@ -1,0 +1,266 @@
+// CUDA device layer: NVRTC compilation with a cubin cache, module loading and
+// launches through driver entry points (see cuda_env.hpp).
+#include "cuda_env.hpp"
+#include "types.hpp"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <dlfcn.h>
+#include <nvrtc.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#include <cstdio>
+#include <cstdlib>
+#include <fstream>
+#include <map>
+#include <mutex>
+#include <sstream>
+
+namespace mapb {
+
+namespace {
+
+#include "skeleton_embed.inc"   // kSkeletonHeaders[] = {name, source}
+
+typedef CUresult (*PFN_ModuleLoadData)(CUmodule *, const void *);
+typedef CUresult (*PFN_ModuleGetFunction)(CUfunction *, CUmodule, const char *);
+typedef CUresult (*PFN_LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
+                                     void **, void **);
+typedef CUresult (*PFN_FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
+typedef CUresult (*PFN_TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                             const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                             CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+typedef CUresult (*PFN_GetErrorString)(CUresult, const char **);
+
+struct Driver {
+  PFN_ModuleLoadData moduleLoadData = nullptr;
+  PFN_ModuleGetFunction moduleGetFunction = nullptr;
+  PFN_LaunchKernel launchKernel = nullptr;
+  PFN_FuncSetAttribute funcSetAttribute = nullptr;
+  PFN_TensorMapEncodeTiled tensorMapEncodeTiled = nullptr;
+  PFN_GetErrorString getErrorString = nullptr;
+};
+
+Driver g_drv;
+std::mutex g_mtx;
+std::map<std::string, std::vector<unsigned char>> g_cubins;   // key: source hash
+std::map<std::string, CUmodule> g_modules;                   // key: source hash
+std::map<std::string, KernelHandle> g_kernels;               // key: source hash + name
+
+std::string hash_hex(const std::string &s) {
+  uint64_t h = 1469598103934665603ull;
+  for (unsigned char c : s) { h ^= c; h *= 1099511628211ull; }
+  char b[17];
+  std::snprintf(b, sizeof b, "%016llx", (unsigned long long)h);
+  return b;
+}
+
+const char *kNvrtcOpts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-lineinfo", "-DMAPB_NVRTC=1"};
+
+std::string options_key() {
+  std::string k;
+  for (const char *o : kNvrtcOpts) k += std::string(o) + " ";
+  int maj = 0, min = 0;
+  nvrtcVersion(&maj, &min);
+  k += std::to_string(maj) + "." + std::to_string(min);
+  for (auto &h : kSkeletonHeaders) k += hash_hex(h.source);
+  return k;
+}
+
+void drv_check(CUresult r, const char *what) {
+  if (r == CUDA_SUCCESS) return;
+  const char *s = "unknown";
+  if (g_drv.getErrorString) g_drv.getErrorString(r, &s);
+  throw MapError(std::string(what) + " failed: " + s + " (" + std::to_string((int)r) + ")");
+}
+
+template <class F> void load_entry(F &fp, const char *name) {
+  void *p = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  cudaError_t e = cudaGetDriverEntryPoint(name, &p, cudaEnableDefault, &q);
+  if (e != cudaSuccess || p == nullptr || q != cudaDriverEntryPointSuccess)
+    throw MapError(std::string("driver entry point ") + name + " unavailable");
+  fp = reinterpret_cast<F>(p);
+}
+
+}  // namespace
+
+void cuda_check(int err, const char *what) {
+  if (err != cudaSuccess)
+    throw MapError(std::string(what) + " failed: " + cudaGetErrorString((cudaError_t)err));
+}
+
+CudaEnv &CudaEnv::get() {
+  static CudaEnv env;
+  return env;
+}
+
+std::string CudaEnv::cache_dir() {
+  if (const char *e = std::getenv("MAP_B200_KCACHE")) return e;
+  Dl_info info;
+  if (dladdr((void *)&CudaEnv::get, &info) && info.dli_fname) {
+    std::string p = info.dli_fname;
+    size_t s = p.rfind('/');
+    if (s != std::string::npos) return p.substr(0, s) + "/_kcache";
+  }
+  return "/tmp/map_b200_kcache";
+}
+
+const std::vector<unsigned char> &CudaEnv::compile(const std::string &source) {
+  const std::string key = hash_hex(source + "\n//" + options_key());
+  {
+    std::lock_guard<std::mutex> lk(g_mtx);
+    auto it = g_cubins.find(key);
+    if (it != g_cubins.end()) return it->second;
+  }
+  // disk cache
+  const std::string dir = cache_dir();
+  const std::string file = dir + "/" + key + ".cubin";
+  {
+    std::ifstream f(file, std::ios::binary);
+    if (f) {
+      std::vector<unsigned char> buf((std::istreambuf_iterator<char>(f)), std::istreambuf_iterator<char>());
+      if (!buf.empty()) {
+        std::lock_guard<std::mutex> lk(g_mtx);
+        return g_cubins[key] = std::move(buf);
+      }
+    }
+  }
+  // NVRTC runs outside the lock so that several groups compile in parallel
+  nvrtcProgram prog;
+  std::vector<const char *> hsrc, hname;
+  for (auto &h : kSkeletonHeaders) {
+    hsrc.push_back(h.source);
+    hname.push_back(h.name);
+  }
+  nvrtcResult r = nvrtcCreateProgram(&prog, source.c_str(), "map_kernel.cu", (int)hsrc.size(), hsrc.data(), hname.data());
+  if (r != NVRTC_SUCCESS) throw MapError(std::string("nvrtcCreateProgram: ") + nvrtcGetErrorString(r));
+  r = nvrtcCompileProgram(prog, (int)(sizeof(kNvrtcOpts) / sizeof(kNvrtcOpts[0])), kNvrtcOpts);
+  size_t logn = 0;
+  nvrtcGetProgramLogSize(prog, &logn);
+  std::string log(logn, '\0');
+  if (logn) nvrtcGetProgramLog(prog, &log[0]);
+  if (r != NVRTC_SUCCESS) {
+    nvrtcDestroyProgram(&prog);
+    throw MapError("kernel compilation failed: " + log + "\n--- source ---\n" + source);
+  }
+  size_t n = 0;
+  nvrtcGetCUBINSize(prog, &n);
+  std::vector<unsigned char> cubin(n);
+  nvrtcGetCUBIN(prog, (char *)cubin.data());
+  nvrtcDestroyProgram(&prog);
+  // best-effort disk cache write (atomic rename)
+  ::mkdir(dir.c_str(), 0755);
+  const std::string tmp = file + ".tmp" + std::to_string(::getpid()) + "_" + std::to_string((uintptr_t)&cubin);
+  {
+    std::ofstream f(tmp, std::ios::binary);
+    if (f) f.write((const char *)cubin.data(), (std::streamsize)cubin.size());
+  }
+  if (std::rename(tmp.c_str(), file.c_str()) != 0) std::remove(tmp.c_str());
+  std::lock_guard<std::mutex> lk(g_mtx);
+  last_log_ = log;
+  return g_cubins[key] = std::move(cubin);
+}
+
+void CudaEnv::set_device(int d) {
+  if (device_ready_ && d != device_) throw MapError("the device cannot change after it has been set up");
+  device_ = d;
+}
+
+void CudaEnv::ensure_device() {
+  if (device_ready_) return;
+  std::lock_guard<std::mutex> lk(g_mtx);
+  if (device_ready_) return;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0)
+    throw MapError(std::string("no CUDA device available: ") + (e != cudaSuccess ? cudaGetErrorString(e) : "0 devices"));
+  if (device_ >= n) throw MapError("device index out of range");
+  cuda_check(cudaSetDevice(device_), "cudaSetDevice");
+  cuda_check(cudaFree(0), "context creation");
+  cudaDeviceProp prop;
+  cuda_check(cudaGetDeviceProperties(&prop, device_), "cudaGetDeviceProperties");
+  if (prop.major != 10 || prop.minor != 0)
+    throw MapError(std::string("this build targets sm_100a (B200); found ") + prop.name + " sm_" +
+                   std::to_string(prop.major) + std::to_string(prop.minor));
+  sm_count_ = prop.multiProcessorCount;
+  device_name_ = prop.name;
+  load_entry(g_drv.moduleLoadData, "cuModuleLoadData");
+  load_entry(g_drv.moduleGetFunction, "cuModuleGetFunction");
+  load_entry(g_drv.launchKernel, "cuLaunchKernel");
+  load_entry(g_drv.funcSetAttribute, "cuFuncSetAttribute");
+  load_entry(g_drv.tensorMapEncodeTiled, "cuTensorMapEncodeTiled");
+  load_entry(g_drv.getErrorString, "cuGetErrorString");
+  cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
+  cuda_check(cudaMalloc(&err_word_, sizeof(uint32_t)), "cudaMalloc(error word)");
+  cuda_check(cudaMemset(err_word_, 0, sizeof(uint32_t)), "cudaMemset");
+  device_ready_ = true;
+}
+
+KernelHandle CudaEnv::kernel(const std::string &source, const std::string &name, size_t dyn_smem) {
+  ensure_device();
+  const auto &cubin = compile(source);
+  std::lock_guard<std::mutex> lk(g_mtx);
+  const std::string key = hash_hex(source) + "/" + name;
+  auto it = g_kernels.find(key);
+  if (it != g_kernels.end() && it->second.max_dyn_smem >= dyn_smem) return it->second;
+  const std::string mkey = hash_hex(source);
+  CUmodule mod;
+  auto mit = g_modules.find(mkey);
+  if (mit == g_modules.end()) {
+    drv_check(g_drv.moduleLoadData(&mod, cubin.data()), "cuModuleLoadData");
+    g_modules[mkey] = mod;
+  } else {
+    mod = mit->second;
+  }
+  KernelHandle h;
+  CUfunction fn;
+  drv_check(g_drv.moduleGetFunction(&fn, mod, name.c_str()), ("cuModuleGetFunction(" + name + ")").c_str());
+  h.fn = reinterpret_cast<CUfunc_st *>(fn);
+  if (dyn_smem > 48 * 1024)
+    drv_check(g_drv.funcSetAttribute(fn, CU_FUNC_ATTRIBUTE_MAX_DYNAMIC_SHARED_SIZE_BYTES, (int)dyn_smem),
+              "cuFuncSetAttribute");
+  h.max_dyn_smem = dyn_smem;
+  g_kernels[key] = h;
+  return h;
+}
+
+void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args, size_t) {
+  if (grid <= 0) return;
+  void *params[] = {args};
+  drv_check(g_drv.launchKernel(reinterpret_cast<CUfunction>(k.fn), (unsigned)grid, 1, 1, (unsigned)block, 1, 1, (unsigned)smem,
+                               reinterpret_cast<CUstream>(stream), params, nullptr),
+            "cuLaunchKernel");
+  launches_++;
+}
+
+void CudaEnv::encode_tma_2d(void *desc128, int dtype, const void *base, uint64_t width, uint64_t height, uint64_t pitch_bytes,
+                            uint32_t box_w, uint32_t box_h) {
+  ensure_device();
+  CUtensorMapDataType t;
+  switch (dtype) {
+    case U8: case S8: case B8: t = CU_TENSOR_MAP_DATA_TYPE_UINT8; break;
+    case U16: case S16: t = CU_TENSOR_MAP_DATA_TYPE_UINT16; break;
+    case U32: t = CU_TENSOR_MAP_DATA_TYPE_UINT32; break;
+    case S32: t = CU_TENSOR_MAP_DATA_TYPE_INT32; break;
+    case F32: t = CU_TENSOR_MAP_DATA_TYPE_FLOAT32; break;
+    case U64: t = CU_TENSOR_MAP_DATA_TYPE_UINT64; break;
+    case S64: t = CU_TENSOR_MAP_DATA_TYPE_INT64; break;
+    case F64: t = CU_TENSOR_MAP_DATA_TYPE_FLOAT64; break;
+    default: throw MapError("TMA: unsupported data type");
+  }
+  if (((uintptr_t)base & 15) != 0) throw MapError("TMA: base address not 16-byte aligned");
+  if ((pitch_bytes & 15) != 0) throw MapError("TMA: pitch not a multiple of 16 bytes");
+  if ((box_w * dt_size(dtype)) % 16 != 0) throw MapError("TMA: box row not a multiple of 16 bytes");
+  cuuint64_t dims[2] = {width, height};
+  cuuint64_t strides[1] = {pitch_bytes};
+  cuuint32_t box[2] = {box_w, box_h};
+  cuuint32_t estr[2] = {1, 1};
+  drv_check(g_drv.tensorMapEncodeTiled(reinterpret_cast<CUtensorMap *>(desc128), t, 2, const_cast<void *>(base), dims, strides,
+                                       box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                       CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE),
+            "cuTensorMapEncodeTiled");
+}
+
+}  // namespace mapb

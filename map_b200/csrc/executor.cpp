@@ -1,0 +1,575 @@
+// Evaluation engine (see executor.hpp).
+#include "executor.hpp"
+#include "binfile.hpp"
+#include "cuda_env.hpp"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <functional>
+#include <cstring>
+#include <future>
+#include <queue>
+#include <sstream>
+#include <unordered_map>
+#include <unordered_set>
+
+namespace mapb {
+
+void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node *, DevRaster> &bufs,
+                    const std::function<DevRaster &(Node *)> &get, const std::function<DevRaster(Node *)> &alloc_out);
+
+namespace {
+
+long long pitch_for(int W, int dt) {
+  long long b = (long long)W * (long long)dt_size(dt);
+  return (b + 127) / 128 * 128;
+}
+
+uint64_t spread_bits(uint32_t v) {
+  uint64_t x = v & 0x1fffff;
+  x = (x | x << 32) & 0x1f00000000ffffull;
+  x = (x | x << 16) & 0x1f0000ff0000ffull;
+  x = (x | x << 8) & 0x100f00f00f00f00full;
+  x = (x | x << 4) & 0x10c30c30c30c30c3ull;
+  x = (x | x << 2) & 0x1249249249249249ull;
+  return x;
+}
+// Morton interleave of (x, y, group): x bits highest in each triple, as the
+// reference's Order interleaves (h, t, y, x) with x highest (runtime/Job.cpp:22-45).
+uint64_t morton3(uint32_t x, uint32_t y, uint32_t t) { return spread_bits(x) << 2 | spread_bits(y) << 1 | spread_bits(t); }
+
+std::vector<Node *> collect(const std::vector<Node *> &targets) {
+  std::unordered_set<Node *> seen;
+  std::vector<Node *> st(targets.begin(), targets.end()), out;
+  while (!st.empty()) {
+    Node *n = st.back();
+    st.pop_back();
+    if (!seen.insert(n).second) continue;
+    out.push_back(n);
+    for (Node *p : n->prev) st.push_back(p);
+  }
+  std::sort(out.begin(), out.end(), [](Node *a, Node *b) { return a->id < b->id; });
+  return out;
+}
+
+bool per_block(int sk) { return sk == SK_LOCAL || sk == SK_FOCAL || sk == SK_ZONAL; }
+
+bool reads_focal(const Group &g, Node *in) {
+  for (Node *n : g.nodes)
+    if ((n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW) &&
+        n->prev[0] == in)
+      return true;
+  return false;
+}
+
+Variant host_eval(Node *n) {
+  for (Node *p : n->prev)
+    if (!p->has_value) throw MapError(std::string("scalar input of ") + kind_name(n->kind) + " has no value");
+  switch (n->kind) {
+    case K_UNARY: return var_convert(host_unary(n->op, n->prev[0]->value), n->meta.dtype);
+    case K_BINARY: return var_convert(host_binary(n->op, n->prev[0]->value, n->prev[1]->value), n->meta.dtype);
+    case K_CAST: return var_convert(n->prev[0]->value, n->meta.dtype);
+    case K_BARRIER: return n->prev[0]->value;
+    case K_CONDITIONAL: {
+      bool c = var_as_f64(n->prev[0]->value) != 0.0;
+      return var_convert(c ? n->prev[1]->value : n->prev[2]->value, n->meta.dtype);
+    }
+    default: throw MapError(std::string("cannot evaluate ") + kind_name(n->kind) + " on the host");
+  }
+}
+
+double now_ms() {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+}  // namespace
+
+std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &groups, const std::vector<KernelPlan> &plans) {
+  (void)plans;
+  struct J { PlainJob j; std::vector<int> succ; int indeg = 0; uint64_t key = 0; };
+  std::vector<J> jobs;
+  std::unordered_map<Node *, const Group *> owner;
+  for (auto &g : groups)
+    for (Node *o : g->outputs) owner[o] = g.get();
+  for (auto &g : groups)
+    for (Node *n : g->nodes) if (!owner.count(n)) owner[n] = g.get();
+  // job index tables
+  std::vector<std::vector<int>> block_job(groups.size());
+  std::vector<int> single_job(groups.size(), -1);
+  std::vector<int> nbx(groups.size(), 1), nby(groups.size(), 1);
+  for (auto &gp : groups) {
+    const Group &g = *gp;
+    if (per_block(g.skeleton)) {
+      nbx[g.id] = (g.W + g.BS0 - 1) / g.BS0;
+      nby[g.id] = (g.H + g.BS1 - 1) / g.BS1;
+      for (int by = 0; by < nby[g.id]; by++)
+        for (int bx = 0; bx < nbx[g.id]; bx++) {
+          J j;
+          j.j = PlainJob{g.id, bx, by, 0};
+          j.key = morton3(bx, by, g.id);
+          block_job[g.id].push_back((int)jobs.size());
+          jobs.push_back(j);
+        }
+      if (g.skeleton == SK_ZONAL) {
+        J j;
+        j.j = PlainJob{g.id, -1, -1, 2};
+        j.key = morton3(nbx[g.id], nby[g.id], g.id);
+        single_job[g.id] = (int)jobs.size();
+        jobs.push_back(j);
+        for (int b : block_job[g.id]) { jobs[b].succ.push_back(single_job[g.id]); jobs[single_job[g.id]].indeg++; }
+      }
+    } else {
+      J j;
+      j.j = PlainJob{g.id, -1, -1, g.skeleton == SK_HOST ? 3 : 1};
+      j.key = morton3(0, 0, g.id);
+      single_job[g.id] = (int)jobs.size();
+      jobs.push_back(j);
+    }
+  }
+  auto dep = [&](int from, int to) {
+    jobs[from].succ.push_back(to);
+    jobs[to].indeg++;
+  };
+  for (auto &gp : groups) {
+    const Group &g = *gp;
+    for (Node *in : g.inputs) {
+      auto it = owner.find(in);
+      if (it == owner.end()) continue;
+      const Group &src = *it->second;
+      const bool scalar = in->meta.numdim == D0;
+      const bool src_blocks = per_block(src.skeleton) && !scalar;
+      auto whole_of = [&](const Group &s) -> std::vector<int> {
+        if (single_job[s.id] >= 0 && (s.skeleton != SK_ZONAL || scalar)) return {single_job[s.id]};
+        return block_job[s.id];
+      };
+      if (per_block(g.skeleton)) {
+        for (int b : block_job[g.id]) {
+          const PlainJob &pj = jobs[b].j;
+          if (src_blocks && src.W == g.W && src.H == g.H && src.BS0 == g.BS0 && src.BS1 == g.BS1) {
+            const int r = reads_focal(g, in) ? 1 : 0;
+            for (int dy = -r; dy <= r; dy++)
+              for (int dx = -r; dx <= r; dx++) {
+                int bx = pj.bx + dx, by = pj.by + dy;
+                if (bx < 0 || by < 0 || bx >= nbx[src.id] || by >= nby[src.id]) continue;
+                dep(block_job[src.id][by * nbx[src.id] + bx], b);
+              }
+          } else {
+            for (int s : whole_of(src)) dep(s, b);
+          }
+        }
+      } else {
+        for (int s : whole_of(src)) dep(s, single_job[g.id]);
+      }
+    }
+  }
+  // ready queue: smallest key first, ties by creation order
+  typedef std::pair<uint64_t, int> KI;
+  std::priority_queue<KI, std::vector<KI>, std::greater<KI>> ready;
+  for (int i = 0; i < (int)jobs.size(); i++)
+    if (jobs[i].indeg == 0) ready.push({jobs[i].key, i});
+  std::vector<PlainJob> out;
+  while (!ready.empty()) {
+    int i = ready.top().second;
+    ready.pop();
+    out.push_back(jobs[i].j);
+    for (int s : jobs[i].succ)
+      if (--jobs[s].indeg == 0) ready.push({jobs[s].key, s});
+  }
+  if (out.size() != jobs.size()) throw MapError("plain schedule: dependency cycle");
+  return out;
+}
+
+Executor &Executor::get() {
+  static Executor e;
+  return e;
+}
+
+Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const std::set<Node *> &tset, bool compile) {
+  Prepared P;
+  P.order = collect(targets);
+  P.fr = fuse(P.order, tset);
+  P.plans.resize(P.fr.groups.size());
+  std::vector<std::future<void>> jobs;
+  std::set<std::string> seen;
+  for (auto &g : P.fr.groups) {
+    if (g->skeleton == SK_HOST) { P.plans[g->id].skeleton = SK_HOST; continue; }
+    P.plans[g->id] = generate_kernel(*g);
+    if (compile && seen.insert(P.plans[g->id].source).second) {
+      const std::string *src = &P.plans[g->id].source;
+      jobs.push_back(std::async(std::launch::async, [src]() { CudaEnv::get().compile(*src); }));
+    }
+  }
+  for (auto &f : jobs) f.get();
+  return P;
+}
+
+std::vector<std::string> Executor::compile_only(const std::vector<Node *> &targets, bool compile) {
+  std::lock_guard<std::recursive_mutex> lk(Runtime::get().mtx);
+  std::set<Node *> tset(targets.begin(), targets.end());
+  Prepared P = prepare(targets, tset, compile);
+  std::vector<std::string> srcs;
+  for (auto &p : P.plans)
+    if (!p.source.empty()) srcs.push_back(p.source);
+  return srcs;
+}
+
+std::string Executor::describe_groups(const std::vector<Node *> &targets) {
+  std::lock_guard<std::recursive_mutex> lk(Runtime::get().mtx);
+  std::set<Node *> tset(targets.begin(), targets.end());
+  FusionResult fr = fuse(collect(targets), tset);
+  std::ostringstream s;
+  for (auto &g : fr.groups) {
+    s << skeleton_name(g->skeleton) << " in=[";
+    for (Node *n : g->inputs) s << kind_name(n->kind) << ":" << n->id << " ";
+    s << "] nodes=[";
+    for (Node *n : g->nodes) s << kind_name(n->kind) << ":" << n->id << " ";
+    s << "] out=[";
+    for (Node *n : g->outputs) s << kind_name(n->kind) << ":" << n->id << " ";
+    s << "]\n";
+  }
+  return s.str();
+}
+
+std::vector<PlainJob> Executor::schedule_for(const std::vector<Node *> &targets) {
+  std::lock_guard<std::recursive_mutex> lk(Runtime::get().mtx);
+  std::set<Node *> tset(targets.begin(), targets.end());
+  Prepared P = prepare(targets, tset, false);
+  return plain_schedule(P.fr.groups, P.plans);
+}
+
+void Executor::sync() {
+  CudaEnv &env = CudaEnv::get();
+  if (!env.device_ready()) return;
+  cuda_check(cudaStreamSynchronize((cudaStream_t)env.stream()), "stream synchronize");
+  uint32_t err = 0;
+  cuda_check(cudaMemcpy(&err, env.err_word(), sizeof err, cudaMemcpyDeviceToHost), "error word read");
+  if (err) {
+    cuda_check(cudaMemset(env.err_word(), 0, sizeof err), "error word reset");
+    std::string m = "device kernel reported an error:";
+    if (err & 1) m += " shared-memory staging timed out;";
+    if (err & 2) m += " invalid launch shape;";
+    if (err & 4) m += " iteration limit reached before convergence;";
+    if (err & 8) m += " spin-wait limit reached;";
+    throw MapError(m);
+  }
+}
+
+void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector<Sink> &sinks, bool async) {
+  const double t0 = now_ms();
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  CudaEnv &env = CudaEnv::get();
+  std::vector<Node *> targets = targets_in;
+  for (auto &s : sinks) targets.push_back(s.node);
+  for (Node *t : targets)
+    if (!rt.owns(t)) throw MapError("evaluate: unknown node");
+  std::set<Node *> tset(targets.begin(), targets.end());
+  Prepared P = prepare(targets, tset, true);
+  last = EvalStats();
+  last.groups = (int)P.fr.groups.size();
+  const int launches0 = env.launches();
+
+  bool need_device = false;
+  for (auto &g : P.fr.groups) if (g->skeleton != SK_HOST) need_device = true;
+  for (Node *t : targets) if (t->meta.numdim != D0) need_device = true;
+  if (!need_device) {
+    for (auto &g : P.fr.groups) {
+      Node *n = g->nodes[0];
+      n->value = host_eval(n);
+      n->has_value = true;
+    }
+    last.host_ms = now_ms() - t0;
+    return;
+  }
+  env.ensure_device();
+  cudaStream_t st = (cudaStream_t)env.stream();
+  static bool pool_cfg = false;
+  if (!pool_cfg) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, env.device()) == cudaSuccess) {
+      uint64_t thr = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    pool_cfg = true;
+  }
+
+  std::unordered_map<Node *, DevRaster> bufs;
+  std::vector<void *> pinned;
+  bool must_sync = !async;
+  std::unordered_map<Node *, const Sink *> dev_sink;
+  for (auto &s : sinks)
+    if (s.dev) dev_sink[s.node] = &s;
+
+  auto alloc_raster = [&](int dtype, int W, int H) {
+    DevRaster r;
+    r.dtype = dtype;
+    r.W = W;
+    r.H = H;
+    r.pitch = pitch_for(W, dtype);
+    cuda_check(cudaMallocAsync(&r.ptr, (size_t)r.pitch * H, st), "cudaMallocAsync");
+    r.owned = true;
+    return r;
+  };
+  std::function<DevRaster &(Node *)> get = [&](Node *n) -> DevRaster & {
+    auto it = bufs.find(n);
+    if (it != bufs.end()) return it->second;
+    const int W = n->meta.W(), H = n->meta.H(), dt = n->meta.dtype;
+    const size_t row = (size_t)W * dt_size(dt);
+    if (n->kind == K_DEVIN) {
+      DevRaster r;
+      r.ptr = n->dev->ptr;
+      r.pitch = n->dev->pitch;
+      r.dtype = dt;
+      r.W = W;
+      r.H = H;
+      if (((uintptr_t)r.ptr & 127) != 0 || (r.pitch & 15) != 0) {   // realign for TMA and coalescing
+        DevRaster c = alloc_raster(dt, W, H);
+        cuda_check(cudaMemcpy2DAsync(c.ptr, c.pitch, r.ptr, r.pitch, row, H, cudaMemcpyDeviceToDevice, st), "realign copy");
+        return bufs[n] = c;
+      }
+      return bufs[n] = r;
+    }
+    if (n->kind == K_HOSTIN) {
+      DevRaster r = alloc_raster(dt, W, H);
+      cuda_check(cudaMemcpy2DAsync(r.ptr, r.pitch, n->host->ptr, row, row, H, cudaMemcpyHostToDevice, st), "upload");
+      return bufs[n] = r;
+    }
+    if (n->kind == K_READ) {
+      BinHeader h = bin_read_header(n->path);
+      void *pin = nullptr;
+      cuda_check(cudaMallocHost(&pin, row * H), "cudaMallocHost");
+      pinned.push_back(pin);
+      bin_read_dense(n->path, h, pin);
+      DevRaster r = alloc_raster(dt, W, H);
+      cuda_check(cudaMemcpy2DAsync(r.ptr, r.pitch, pin, row, row, H, cudaMemcpyHostToDevice, st), "upload");
+      must_sync = true;
+      return bufs[n] = r;
+    }
+    throw MapError(std::string("raster of ") + kind_name(n->kind) + " #" + std::to_string(n->id) + " was not computed");
+  };
+  std::function<DevRaster(Node *)> alloc_out = [&](Node *o) -> DevRaster {
+    auto ds = dev_sink.find(o);
+    if (ds != dev_sink.end()) {
+      const Sink *s = ds->second;
+      if (((uintptr_t)s->dev & 127) == 0 && (s->dev_pitch & 15) == 0 &&
+          s->dev_pitch >= (long long)o->meta.W() * (long long)dt_size(o->meta.dtype)) {
+        DevRaster r;
+        r.ptr = s->dev;
+        r.pitch = s->dev_pitch;
+        r.dtype = o->meta.dtype;
+        r.W = o->meta.W();
+        r.H = o->meta.H();
+        return r;
+      }
+    }
+    return alloc_raster(o->meta.dtype, o->meta.W(), o->meta.H());
+  };
+
+  // partial-result storage of zonal groups
+  struct ZonalState { void *part = nullptr; long long slots = 0; long long cap = 0; void *res = nullptr; };
+  std::unordered_map<int, ZonalState> zst;
+
+  auto build_args = [&](const Group &g, const KernelPlan &K, int rx0, int ry0, int rx1, int ry1, uint64_t aux0,
+                        uint64_t aux1) {
+    std::vector<unsigned char> a(K.args_size, 0);
+    for (size_t k = 0; k < K.tma.size(); k++) {
+      const TmaSpec &t = K.tma[k];
+      DevRaster &r = get(K.in_rasters[t.in_index]);
+      alignas(64) unsigned char desc[128];
+      env.encode_tma_2d(desc, r.dtype, r.ptr, (uint64_t)r.W, (uint64_t)r.H, (uint64_t)r.pitch, (uint32_t)t.box_w,
+                        (uint32_t)t.box_h);
+      std::memcpy(a.data() + K.off_tm + 128 * k, desc, 128);
+    }
+    for (size_t k = 0; k < K.in_rasters.size(); k++) {
+      DevRaster &r = get(K.in_rasters[k]);
+      uint64_t p = (uint64_t)(uintptr_t)r.ptr;
+      int64_t pitch = r.pitch;
+      std::memcpy(a.data() + K.off_in + 16 * k, &p, 8);
+      std::memcpy(a.data() + K.off_in + 16 * k + 8, &pitch, 8);
+    }
+    for (size_t k = 0; k < K.out_rasters.size(); k++) {
+      DevRaster &r = bufs.at(K.out_rasters[k]);
+      uint64_t p = (uint64_t)(uintptr_t)r.ptr;
+      int64_t pitch = r.pitch;
+      std::memcpy(a.data() + K.off_out + 16 * k, &p, 8);
+      std::memcpy(a.data() + K.off_out + 16 * k + 8, &pitch, 8);
+    }
+    for (size_t k = 0; k < K.scalars.size(); k++) {
+      Node *s = K.scalars[k];
+      if (!s->has_value) throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
+      Variant v = var_convert(s->value, s->meta.dtype);
+      std::memcpy(a.data() + K.off_s + 8 * k, &v.u, dt_size(v.dtype));
+    }
+    int32_t geom[12] = {g.W, g.H, g.BS0, g.BS1, rx0, ry0, rx1, ry1, 0, 0, rt.border, 0};
+    const int tx = (rx1 - rx0 + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+    geom[8] = tx;
+    geom[9] = tx * ty;
+    std::memcpy(a.data() + K.off_geom, geom, sizeof geom);
+    uint64_t errp = (uint64_t)(uintptr_t)env.err_word();
+    std::memcpy(a.data() + K.off_err, &errp, 8);
+    uint64_t aux[4] = {aux0, aux1, 0, 0};
+    std::memcpy(a.data() + K.off_aux, aux, sizeof aux);
+    return a;
+  };
+
+  auto ensure_outputs = [&](const Group &g, const KernelPlan &K) {
+    for (Node *o : K.out_rasters)
+      if (!bufs.count(o)) bufs[o] = alloc_out(o);
+    (void)g;
+  };
+
+  auto launch_region = [&](const Group &g, const KernelPlan &K, int rx0, int ry0, int rx1, int ry1) {
+    const int tx = (rx1 - rx0 + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+    const int tiles = tx * ty;
+    KernelHandle kh = env.kernel(K.source, K.kname, K.smem_bytes);
+    if (g.skeleton == SK_ZONAL) {
+      ZonalState &z = zst[g.id];
+      const int nz = (int)K.zonal.size();
+      const int grid = std::min(tiles, env.sm_count() * 8);
+      if (z.slots + grid > z.cap) throw MapError("zonal partial storage overflow");
+      auto a = build_args(g, K, rx0, ry0, rx1, ry1, (uint64_t)(uintptr_t)z.part, (uint64_t)z.slots);
+      env.launch(kh, grid, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+      z.slots += grid;
+      (void)nz;
+    } else {
+      auto a = build_args(g, K, rx0, ry0, rx1, ry1, 0, 0);
+      env.launch(kh, tiles, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+    }
+  };
+
+  auto zonal_begin = [&](const Group &g, const KernelPlan &K) {
+    ZonalState &z = zst[g.id];
+    if (z.part) return;
+    const int nz = (int)K.zonal.size();
+    long long cap;
+    if (rt.exec_mode == EXEC_PLAIN) {
+      const int nbx = (g.W + g.BS0 - 1) / g.BS0, nby = (g.H + g.BS1 - 1) / g.BS1;
+      const int tpb = ((g.BS0 + K.tile_w - 1) / K.tile_w) * ((g.BS1 + K.tile_h - 1) / K.tile_h);
+      cap = (long long)nbx * nby * std::min(tpb, env.sm_count() * 8);
+    } else {
+      cap = env.sm_count() * 8;
+    }
+    cuda_check(cudaMallocAsync(&z.part, (size_t)cap * nz * 8, st), "cudaMallocAsync(partials)");
+    cuda_check(cudaMallocAsync(&z.res, (size_t)nz * 8, st), "cudaMallocAsync(results)");
+    z.cap = cap;
+    z.slots = 0;
+  };
+
+  auto zonal_finish = [&](const Group &g, const KernelPlan &K) {
+    ZonalState &z = zst[g.id];
+    const int nz = (int)K.zonal.size();
+    KernelHandle kf = env.kernel(K.source, K.kname_final, 0);
+    struct { uint64_t part; int64_t nslots; uint64_t res; uint64_t pad; } fa{(uint64_t)(uintptr_t)z.part, z.slots,
+                                                                              (uint64_t)(uintptr_t)z.res, 0};
+    env.launch(kf, 1, K.threads, 0, (CUstream_st *)st, &fa, sizeof fa);
+    std::vector<uint64_t> res(nz);
+    cuda_check(cudaMemcpyAsync(res.data(), z.res, (size_t)nz * 8, cudaMemcpyDeviceToHost, st), "result read-back");
+    cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+    for (int i = 0; i < nz; i++) {
+      Node *n = K.zonal[i];
+      Variant v;
+      std::memset(&v, 0, sizeof v);
+      v.dtype = n->meta.dtype;
+      std::memcpy(&v.u, &res[i], dt_size(v.dtype));
+      n->value = v;
+      n->has_value = true;
+    }
+    cudaFreeAsync(z.part, st);
+    cudaFreeAsync(z.res, st);
+    z.part = z.res = nullptr;
+  };
+
+  auto run_host = [&](const Group &g) {
+    Node *n = g.nodes[0];
+    n->value = host_eval(n);
+    n->has_value = true;
+  };
+
+  try {
+    if (rt.exec_mode == EXEC_FUSED) {
+      for (auto &gp : P.fr.groups) {
+        const Group &g = *gp;
+        const KernelPlan &K = P.plans[g.id];
+        if (g.skeleton == SK_HOST) { run_host(g); continue; }
+        if (g.skeleton == SK_RADIAL || g.skeleton == SK_SPREAD) {
+          run_scan_group(g, K, bufs, get, alloc_out);
+          continue;
+        }
+        ensure_outputs(g, K);
+        if (g.skeleton == SK_ZONAL) zonal_begin(g, K);
+        launch_region(g, K, 0, 0, g.W, g.H);
+        if (g.skeleton == SK_ZONAL) zonal_finish(g, K);
+      }
+    } else {
+      std::vector<PlainJob> jobs = plain_schedule(P.fr.groups, P.plans);
+      for (const PlainJob &j : jobs) {
+        const Group &g = *P.fr.groups[j.group];
+        const KernelPlan &K = P.plans[g.id];
+        switch (j.kind) {
+          case 3: run_host(g); break;
+          case 1: run_scan_group(g, K, bufs, get, alloc_out); break;
+          case 2: zonal_finish(g, K); break;
+          default: {
+            ensure_outputs(g, K);
+            if (g.skeleton == SK_ZONAL) zonal_begin(g, K);
+            const int rx0 = j.bx * g.BS0, ry0 = j.by * g.BS1;
+            launch_region(g, K, rx0, ry0, std::min(rx0 + g.BS0, g.W), std::min(ry0 + g.BS1, g.H));
+          }
+        }
+      }
+    }
+    // sinks
+    for (const Sink &s : sinks) {
+      Node *n = s.node;
+      if (n->meta.numdim == D0) continue;
+      DevRaster &r = get(n);
+      const size_t row = (size_t)n->meta.W() * dt_size(n->meta.dtype);
+      if (s.host) {
+        cuda_check(cudaMemcpy2DAsync(s.host, row, r.ptr, r.pitch, row, n->meta.H(), cudaMemcpyDeviceToHost, st), "download");
+        must_sync = true;
+      }
+      if (s.dev && r.ptr != s.dev)
+        cuda_check(cudaMemcpy2DAsync(s.dev, s.dev_pitch, r.ptr, r.pitch, row, n->meta.H(), cudaMemcpyDeviceToDevice, st),
+                   "device copy");
+    }
+    // writes
+    for (Node *t : P.order) {
+      if (t->kind != K_WRITE) continue;
+      Node *src = t->prev[0];
+      DevRaster &r = get(src);
+      const size_t row = (size_t)src->meta.W() * dt_size(src->meta.dtype);
+      void *pin = nullptr;
+      cuda_check(cudaMallocHost(&pin, row * src->meta.H()), "cudaMallocHost");
+      pinned.push_back(pin);
+      cuda_check(cudaMemcpy2DAsync(pin, row, r.ptr, r.pitch, row, src->meta.H(), cudaMemcpyDeviceToHost, st), "download");
+      cuda_check(cudaStreamSynchronize(st), "stream synchronize");
+      BinHeader h;
+      h.dtype = src->meta.dtype;
+      h.numdim = D2;
+      h.ds0 = src->meta.W();
+      h.ds1 = src->meta.H();
+      h.memorder = (src->meta.memorder == ROW) ? ROW : ROW + BLK;
+      h.bs0 = src->meta.BS0();
+      h.bs1 = src->meta.BS1();
+      bin_write_dense(t->path, h, pin);
+    }
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    for (auto &kv : bufs) if (kv.second.owned) cudaFree(kv.second.ptr);
+    for (void *p : pinned) cudaFreeHost(p);
+    throw;
+  }
+  for (auto &kv : bufs)
+    if (kv.second.owned) cudaFreeAsync(kv.second.ptr, st);
+  if (must_sync || !pinned.empty()) {
+    sync();
+    for (void *p : pinned) cudaFreeHost(p);
+  }
+  last.launches = env.launches() - launches0;
+  last.host_ms = now_ms() - t0;
+}
+
+}  // namespace mapb

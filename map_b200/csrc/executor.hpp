@@ -1,0 +1,83 @@
+// Evaluation engine: runs the groups of one evaluation on the device.
+//
+// Replaces the reference's Program / Task / Scheduler / Worker / Cache / Block
+// runtime (runtime/Program.cpp, runtime/task/*, runtime/Scheduler.cpp,
+// runtime/Worker.cpp, runtime/Cache.cpp, runtime/Block.cpp) with an HBM-resident
+// design: every raster lives whole in device memory (row-major, 128-byte pitch),
+// allocated stream-ordered from the CUDA memory pool, and all work is enqueued on
+// one stream. Two launch granularities:
+//  * fused: one launch per group over the whole raster;
+//  * plain: one launch per group per block, issued in the order of a ready-queue
+//    of (group, block) jobs keyed by a Morton interleave of (x, y, group), with the
+//    focal 3x3 block dependencies of runtime/task/FocalTask.cpp:36-115.
+#pragma once
+
+#include "codegen.hpp"
+#include "fusion.hpp"
+
+#include <map>
+#include <memory>
+#include <set>
+#include <string>
+#include <vector>
+
+namespace mapb {
+
+struct DevRaster {
+  void *ptr = nullptr;
+  long long pitch = 0;   // bytes
+  bool owned = false;
+  int dtype = 0;
+  int W = 0, H = 0;
+};
+
+// Where a requested raster goes after evaluation.
+struct Sink {
+  Node *node = nullptr;
+  void *host = nullptr;      // dense row-major host destination (or null)
+  void *dev = nullptr;       // device destination (or null)
+  long long dev_pitch = 0;
+};
+
+// One job of the plain-mode schedule.
+struct PlainJob {
+  int group = 0;
+  int bx = -1, by = -1;   // block coordinate, -1 for whole-raster jobs
+  int kind = 0;           // 0 block launch, 1 whole-raster launch, 2 zonal finalisation, 3 host scalar step
+};
+
+// Plain-mode launch order for the given groups (pure host logic).
+std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &groups,
+                                     const std::vector<KernelPlan> &plans);
+
+struct EvalStats {
+  int launches = 0;
+  int groups = 0;
+  int compiled = 0;
+  double host_ms = 0;
+};
+
+class Executor {
+ public:
+  static Executor &get();
+  // Evaluates `targets` (and the sinks' nodes). Blocks until done unless `async`
+  // is set and nothing needs the host (no sinks with host memory, no writes,
+  // no scalar read-backs).
+  void evaluate(const std::vector<Node *> &targets, const std::vector<Sink> &sinks, bool async = false);
+  // Fusion + code generation + compilation only (no device needed).
+  std::vector<std::string> compile_only(const std::vector<Node *> &targets, bool compile);
+  std::string describe_groups(const std::vector<Node *> &targets);
+  std::vector<PlainJob> schedule_for(const std::vector<Node *> &targets);
+  EvalStats last;
+  void sync();
+
+ private:
+  struct Prepared {
+    FusionResult fr;
+    std::vector<KernelPlan> plans;
+    std::vector<Node *> order;
+  };
+  Prepared prepare(const std::vector<Node *> &targets, const std::set<Node *> &tset, bool compile);
+};
+
+}  // namespace mapb

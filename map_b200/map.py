@@ -1,0 +1,862 @@
+##
+# Python 3 interface of the B200 map-algebra engine over its C ABI (ctypes).
+#
+# Same module surface as the reference's Python bindings (python/map.py): the
+# enum tables, Variant / Array / Node / Raster, operator overloading, the
+# module functions (read, write, eval, value, convolve, zsum, rmax, con, ...)
+# and the compound helpers, so scripts written for it (`from map import *`)
+# run unchanged under Python 3 when this directory is on sys.path.
+#
+# Differences from the reference module:
+#  * Python 3: `/` maps to __truediv__, `__bool__` replaces `__nonzero__`;
+#  * errors raise MapError with the library's message instead of asserting;
+#  * symbolic while-loops (python/map.py:234-330) raise MapError, as the
+#    reference runtime cannot execute them either;
+#  * extensions at the end: NumPy in/out, border and launch-mode switches,
+#    device-resident inputs, flow direction / accumulation and viewshed helpers.
+##
+
+import builtins as _builtins
+import ctypes as ct
+import functools
+import math
+import operator
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIBPATH = os.environ.get("MAP_B200_LIB", os.path.join(_HERE, "libmap_b200.so"))
+if not os.path.exists(_LIBPATH):
+    raise ImportError("map: native library %s is missing; build it with `python -m map_b200.build`" % _LIBPATH)
+_lib = ct.CDLL(_LIBPATH)
+
+
+class MapError(RuntimeError):
+    pass
+
+
+## Enumerates / Constants (python/map.py:35-90)
+
+DataTypeId = ['NONE_DATATYPE', 'F32', 'F64', 'B8', 'U8', 'U16', 'U32', 'U64', 'S8', 'S16', 'S32', 'S64', 'N_DATATYPE']
+DataTypeVal = list(range(len(DataTypeId)))
+
+NumDimId = ['NONE_NUMDIM', 'TIME', 'D0', 'D1', 'D2', 'D3', 'N_NUMDIM']
+NumDimVal = [0x00, 0x01, 0x02, 0x04, 0x06, 0x08, 0x0A]
+
+MemOrderId = ['NONE_MEMORDER', 'BLK', 'ROW', 'COL', 'SFC', 'N_MEMORDER']
+MemOrderVal = [0x00, 0x01, 0x02, 0x04, 0x06, 0x08]
+
+DeviceTypeId = ['DEV_DEF', 'DEV_CPU', 'DEV_GPU', 'DEV_ACC', 'DEV_CUS', 'DEV_ALL']
+DeviceTypeVal = [0x01, 0x02, 0x04, 0x08, 0x16, 0xFFFFFFFF]
+
+UnaryTypeId = [
+    'NONE_UNARY', 'POS', 'NEG', 'NOT', 'bNOT', 'MARK_UNARY',
+    'SIN', 'COS', 'TAN', 'ASIN', 'ACOS', 'ATAN',
+    'SINH', 'COSH', 'TANH', 'ASINH', 'ACOSH', 'ATANH',
+    'EXP', 'EXP2', 'EXP10', 'LOG', 'LOG2', 'LOG10',
+    'SQRT', 'CBRT', 'ABS',
+    'CEIL', 'FLOOR', 'TRUNC', 'ROUND', 'N_UNARY'
+]
+UnaryTypeSym = [
+    '', '__pos__', '__neg__', '__not__', '__invert__', '',
+    'sin', 'cos', 'tan', 'asin', 'acos', 'atan',
+    'sinh', 'cosh', 'tanh', 'asinh', 'acosh', 'atanh',
+    'exp', 'exp2', 'exp10', 'log', 'log2', 'log10',
+    'sqrt', 'cbrt', 'abs',
+    'ceil', 'floor', 'trunc', 'round', ''
+]
+UnaryTypeVal = list(range(len(UnaryTypeId)))
+
+BinaryTypeId = [
+    'NONE_BINARY', 'ADD', 'SUB', 'MUL', 'DIV', 'MOD',
+    'EQ', 'NE', 'LT', 'GT', 'LE', 'GE', 'AND', 'OR',
+    'bAND', 'bOR', 'bXOR', 'SHL', 'SHR', 'MARK_BINARY',
+    'MAX2', 'MIN2', 'ATAN2', 'POW', 'HYPOT', 'FMOD', 'N_BINARY'
+]
+BinaryTypeSym = [
+    '', '__add__', '__sub__', '__mul__', '__truediv__', '__mod__',
+    '__eq__', '__ne__', '__lt__', '__gt__', '__le__', '__ge__', '', '',
+    '__and__', '__or__', '__xor__', '__lshift__', '__rshift__', '',
+    'max', 'min', 'atan2', 'pow', 'hypot', 'fmod', ''
+]
+BinaryTypeVal = list(range(len(BinaryTypeId)))
+
+ReductionTypeId = ['NONE_REDUCTION', 'SUM', 'PROD', 'rAND', 'rOR', 'MARK_REDUCTION', 'MAX', 'MIN', 'N_REDUCTION']
+ReductionTypeVal = list(range(len(ReductionTypeId)))
+
+EnumIds = [DataTypeId, NumDimId, MemOrderId, DeviceTypeId, UnaryTypeId, BinaryTypeId, ReductionTypeId]
+EnumVals = [DataTypeVal, NumDimVal, MemOrderVal, DeviceTypeVal, UnaryTypeVal, BinaryTypeVal, ReductionTypeVal]
+
+for _ids, _vals in zip(EnumIds, EnumVals):
+    for _i, _v in zip(_ids, _vals):
+        globals()[_i] = _v
+
+# border rules and launch modes (extensions)
+BORDER_BLOCK_MIRROR, BORDER_RASTER_MIRROR, BORDER_DEAD = 0, 1, 2
+EXEC_FUSED, EXEC_PLAIN = 0, 1
+
+## Wrapper classes
+
+
+class Variant(ct.Structure):
+    class Union(ct.Union):
+        _fields_ = [
+            ('b8', ct.c_bool), ('s8', ct.c_int8), ('s16', ct.c_int16), ('s32', ct.c_int32), ('s64', ct.c_int64),
+            ('u8', ct.c_uint8), ('u16', ct.c_uint16), ('u32', ct.c_uint32), ('u64', ct.c_uint64),
+            ('f16', ct.c_float), ('f32', ct.c_float), ('f64', ct.c_double)
+        ]
+    _fields_ = [('union', Union), ('dtype', ct.c_int)]
+
+    _field_of = {F32: 'f32', F64: 'f64', B8: 'b8', U8: 'u8', U16: 'u16', U32: 'u32', U64: 'u64',
+                 S8: 's8', S16: 's16', S32: 's32', S64: 's64'}
+
+    def __init__(self, val=None, dtype=None):
+        union = self.Union()
+        if val is None:
+            super().__init__(union, NONE_DATATYPE)
+            return
+        if dtype is not None:
+            setattr(union, self._field_of[dtype], val)
+            super().__init__(union, dtype)
+            return
+        if isinstance(val, float):
+            union.f32, dtype = val, F32
+        elif isinstance(val, bool):
+            union.b8, dtype = val, B8
+        elif isinstance(val, int):
+            union.s32, dtype = val, S32
+        elif isinstance(val, ct.c_uint8):
+            union.u8, dtype = val.value, U8
+        else:
+            raise MapError("Variant: unsupported value %r" % (val,))
+        super().__init__(union, dtype)
+
+    def datatype(self):
+        return self.dtype
+
+    def value(self):
+        f = self._field_of.get(self.dtype)
+        if f is None:
+            raise MapError("Variant has no value")
+        return getattr(self.union, f)
+
+    def convert(self, new_dt):
+        v = self.value()
+        if new_dt in (F32, F64):
+            return Variant(float(v), new_dt)
+        if new_dt == B8:
+            return Variant(bool(v), B8)
+        return Variant(int(v), new_dt)
+
+
+class Array(ct.Structure):
+    N = 2
+    T = ct.c_int * N
+    _fields_ = [('arr', T), ('n', ct.c_int)]
+
+    def __init__(self, arg=()):
+        if arg is None or (isinstance(arg, (list, tuple)) and len(arg) == 0):
+            super().__init__(self.T(-1, -1), 0)
+        elif isinstance(arg, (list, tuple)):
+            if len(arg) != self.N:
+                raise MapError("Array needs %d elements, got %d" % (self.N, len(arg)))
+            super().__init__(self.T(*[int(a) for a in arg]), self.N)
+        elif isinstance(arg, Array):
+            super().__init__(arg.arr, arg.n)
+        else:
+            raise MapError("Array: unsupported argument %r" % (arg,))
+
+    def isNone(self):
+        return all(e == -1 for e in self.arr)
+
+    def toList(self):
+        return [x for x in self.arr if x != -1]
+
+
+class Node(ct.c_void_p):  # distinct type so ctypes returns a handle, not an int
+    pass
+
+
+def _check(result, func, args):
+    if _lib.ma_errorCode():
+        raise MapError(_lib.ma_lastError().decode())
+    return result
+
+
+class Raster:
+    def __init__(self, node=None):
+        if isinstance(node, Node):
+            if not node.value:
+                raise MapError("null node")
+            self._node = node
+            _lib.ma_increaseRef(self)
+        elif node is None:
+            self._node = Node(None)
+        else:
+            raise MapError("Raster: expected a node handle")
+
+    def __del__(self):
+        try:
+            if getattr(self, "_node", None) is not None and self._node.value:
+                _lib.ma_decreaseRef(self)
+        except Exception:
+            pass
+
+    @classmethod
+    def from_param(cls, ins):  # lets ctypes take ._node from Rasters given as arguments
+        return ins._node
+
+    def __getitem__(self, key):
+        if isinstance(key, (list, tuple)):
+            return Raster(_lib.ma_access(self, Array(key)))
+        elif isinstance(key, Raster):
+            return Raster(_lib.ma_conditional(key, self, empty_like(self)))
+        raise MapError("unsupported index")
+
+    def __setitem__(self, key, other):
+        other = _const_to_raster(other).astype(self.datatype())
+        if isinstance(key, (list, tuple)):
+            node = _lib.ma_lhsAccess(self, other, Array(key))
+        elif isinstance(key, Raster):
+            node = _lib.ma_conditional(key, other, self)
+        else:
+            raise MapError("unsupported index")
+        _lib.ma_increaseRef(node)
+        _lib.ma_decreaseRef(self)
+        self._node = node
+
+    def __call__(self, ngb):
+        if isinstance(ngb, list):
+            return Raster(_lib.ma_neighbor(self, Array(ngb)))
+        elif isinstance(ngb, tuple):
+            if len(ngb) != 2 or not isinstance(ngb[0], Raster):
+                raise MapError("bounded neighbourhood needs two rasters")
+            return Raster(_lib.ma_boundedNbh(self, ngb[0], ngb[1]))
+        raise MapError("unsupported neighbour access")
+
+    def __bool__(self):
+        raise MapError("symbolic while-loops over rasters are not supported")
+
+    __hash__ = object.__hash__
+
+    ## Public methods
+
+    def nodeid(self):
+        return _lib.ma_nodeid(self)
+
+    def streamdir(self):
+        return _lib.ma_streamdir(self)
+
+    def datatype(self):
+        return _lib.ma_datatype(self)
+
+    def numdim(self):
+        return _lib.ma_numdim(self)
+
+    def memorder(self):
+        return _lib.ma_memorder(self)
+
+    def datasize(self):
+        return _lib.ma_datasize(self).toList()
+
+    def blocksize(self):
+        return _lib.ma_blocksize(self).toList()
+
+    def numblock(self):
+        return _lib.ma_numblock(self).toList()
+
+    def __pow__(self, other):
+        rhs = _const_to_raster(other)
+        return Raster(_lib.ma_binary(self, rhs, POW))
+
+    def __rpow__(self, other):
+        lhs = _const_to_raster(other)
+        return Raster(_lib.ma_binary(lhs, self, POW))
+
+    def no(self):
+        return Raster(_lib.ma_unary(self, NOT))
+
+    def astype(self, dt):
+        return astype(self, dt)
+
+    # extensions
+    def numpy(self):
+        return to_numpy(self)
+
+
+## Helper functions
+
+def _const_to_raster(arg):
+    if isinstance(arg, Raster):
+        return arg
+    elif isinstance(arg, (bool, int, float)):
+        var = Variant(arg)
+        return Raster(_lib.ma_constant(var, Array(), var.datatype(), ROW + BLK, Array()))
+    raise MapError("cannot convert %r to a raster" % (arg,))
+
+
+## Unary functions
+
+def _def_unary_op(symbol, utype):
+    def uop(self):
+        return Raster(_lib.ma_unary(self, utype))
+    setattr(Raster, symbol, uop)
+
+
+def _def_unary_fun(symbol, utype):
+    def ufun(raster):
+        if isinstance(raster, Raster):
+            return Raster(_lib.ma_unary(raster, utype))
+        if symbol == 'exp10':
+            return 10.0 ** raster
+        if symbol == 'round':
+            return _builtins.round(raster)
+        if symbol == 'abs':
+            return _builtins.abs(raster)
+        return getattr(math, symbol)(raster)
+    globals()[symbol] = ufun
+
+
+for _sym, _ut in zip(UnaryTypeSym, UnaryTypeVal):
+    if _sym and _ut < MARK_UNARY:
+        _def_unary_op(_sym, _ut)
+    elif _sym and _ut > MARK_UNARY:
+        _def_unary_fun(_sym, _ut)
+
+## Binary functions
+
+
+def _def_binary_op(symbol, bitype):
+    def biop(self, rhs):
+        rhs = _const_to_raster(rhs)
+        return Raster(_lib.ma_binary(self, rhs, bitype))
+    setattr(Raster, symbol, biop)
+
+    def rbiop(self, lhs):
+        lhs = _const_to_raster(lhs)
+        return Raster(_lib.ma_binary(lhs, self, bitype))
+    rsymbol = symbol[:2] + 'r' + symbol[2:]
+    setattr(Raster, rsymbol, rbiop)
+
+
+def _def_binary_fun(symbol, bitype):
+    def bifun(lhs, rhs):
+        if not isinstance(lhs, Raster) and not isinstance(rhs, Raster):
+            if symbol == 'max':
+                return _builtins.max(lhs, rhs)
+            if symbol == 'min':
+                return _builtins.min(lhs, rhs)
+            return getattr(math, symbol)(lhs, rhs)
+        lhs = _const_to_raster(lhs)
+        rhs = _const_to_raster(rhs)
+        return Raster(_lib.ma_binary(lhs, rhs, bitype))
+    globals()[symbol] = bifun
+
+
+for _sym, _bt in zip(BinaryTypeSym, BinaryTypeVal):
+    if _sym and _bt < MARK_BINARY:
+        _def_binary_op(_sym, _bt)
+    elif _sym and _bt > MARK_BINARY:
+        _def_binary_fun(_sym, _bt)
+
+# Python 2 spelling of the division operator, kept for callers that use it
+Raster.__div__ = Raster.__truediv__
+Raster.__rdiv__ = Raster.__rtruediv__
+
+## Standalone functions
+
+
+def setupDevices(plat_name, dev_type, dev_name):
+    _lib.ma_setupDevices(plat_name.encode(), dev_type, dev_name.encode())
+
+
+def eval(*args):
+    # Note: shadows the built-in eval, as the reference module does
+    cond = [isinstance(a, Raster) for a in args]
+    if len(args) and not all(cond):
+        if not any(cond):
+            return _builtins.eval(*args)
+        raise MapError("eval: mix of rasters and other arguments")
+    num = len(args)
+    NodeArr = Node * num
+    nodearr = NodeArr(*[r._node for r in args])
+    _lib.ma_eval(ct.cast(nodearr, ct.POINTER(Node)), num)
+
+
+def value(arg):
+    var = _lib.ma_value(arg)
+    return var.value()
+
+
+def read(file):
+    return Raster(_lib.ma_read(os.fsencode(file)))
+
+
+def write(raster, file):
+    return _lib.ma_write(raster, os.fsencode(file))
+
+
+def _cnst(cnst, ds, dt, mo, bs):
+    var = Variant(cnst).convert(dt)
+    return Raster(_lib.ma_constant(var, Array(ds), dt, mo, Array(bs)))
+
+
+def zeros(ds=[], dt=F32, mo=ROW + BLK, bs=[]):
+    return _cnst(0, ds, dt, mo, bs)
+
+
+def ones(ds=[], dt=F32, mo=ROW + BLK, bs=[]):
+    return _cnst(1, ds, dt, mo, bs)
+
+
+def trues(ds=[], dt=B8, mo=ROW + BLK, bs=[]):
+    return _cnst(True, ds, dt, mo, bs)
+
+
+def falses(ds=[], dt=B8, mo=ROW + BLK, bs=[]):
+    return _cnst(False, ds, dt, mo, bs)
+
+
+def full(cnst, ds=[], dt=F32, mo=ROW + BLK, bs=[]):
+    return _cnst(cnst, ds, dt, mo, bs)
+
+
+def empty(ds=[], dt=F32, mo=ROW + BLK, bs=[]):
+    return True
+
+
+def _like(cnst, raster, dt, mo):
+    dt = raster.datatype() if (dt == NONE_DATATYPE) else dt
+    mo = raster.memorder() if (mo == NONE_MEMORDER) else mo
+    var = Variant(cnst).convert(dt)
+    ds = Array(raster.datasize())
+    bs = Array(raster.blocksize())
+    return Raster(_lib.ma_constant(var, ds, dt, mo, bs))
+
+
+def zeros_like(raster, dt=NONE_DATATYPE, mo=NONE_MEMORDER):
+    return _like(0, raster, dt, mo)
+
+
+def ones_like(raster, dt=NONE_DATATYPE, mo=NONE_MEMORDER):
+    return _like(1, raster, dt, mo)
+
+
+def full_like(cnst, raster, dt=NONE_DATATYPE, mo=NONE_MEMORDER):
+    return _like(cnst, raster, dt, mo)
+
+
+def empty_like(raster, dt=NONE_DATATYPE, mo=NONE_MEMORDER):
+    return True
+
+
+def index(raster, dim):
+    return Raster(_lib.ma_index(raster, dim))
+
+
+def rand(seed, ds=[], dt=NONE_DATATYPE, mo=NONE_MEMORDER, bs=[]):
+    ds = seed.datasize() if isinstance(seed, Raster) else ds
+    dt = seed.datatype() if dt == NONE_DATATYPE else dt
+    mo = BLK + ROW if mo == NONE_DATATYPE else mo
+    bs = seed.blocksize() if isinstance(seed, Raster) else bs
+    if not isinstance(seed, Raster):
+        var = Variant(seed).convert(dt)
+        seed = Raster(_lib.ma_constant(var, Array(ds), dt, mo, Array(bs)))
+    return Raster(_lib.ma_rand(seed, dt, mo))
+
+
+def astype(raster, dt):
+    return Raster(_lib.ma_cast(raster, dt))
+
+
+def con(cond, lhs, rhs):
+    cond = _const_to_raster(cond)
+    lhs = _const_to_raster(lhs)
+    rhs = _const_to_raster(rhs)
+    return Raster(_lib.ma_conditional(cond, lhs, rhs))
+
+
+def _mask(lst):
+    if not all(len(e) == len(lst[0]) for e in lst):
+        raise MapError("mask rows differ in length")
+    ds = Array([len(lst[0]), len(lst)])
+    unroll = sum(lst, [])
+    size = len(unroll)
+    VarArr = Variant * size
+    vararr = VarArr(*[Variant(e) for e in unroll])
+    return ct.cast(vararr, ct.POINTER(Variant)), size, ds, vararr
+
+
+def convolve(raster, lst):
+    varptr, size, ds, _keep = _mask(lst)
+    return Raster(_lib.ma_convolution(raster, varptr, size, ds))
+
+
+def fsum(raster):
+    lst = [[1, 1, 1], [1, 1, 1], [1, 1, 1]]
+    return convolve(raster, lst)
+
+
+def fmin(raster, lst):
+    varptr, size, ds, _keep = _mask(lst)
+    return Raster(_lib.ma_focalFunc(raster, varptr, size, ds, MIN))
+
+
+def fmax(raster, lst):
+    varptr, size, ds, _keep = _mask(lst)
+    return Raster(_lib.ma_focalFunc(raster, varptr, size, ds, MAX))
+
+
+def zsum(raster):
+    return Raster(_lib.ma_zonalReduc(raster, SUM))
+
+
+def zprod(raster):
+    return Raster(_lib.ma_zonalReduc(raster, PROD))
+
+
+def zmax(raster):
+    return Raster(_lib.ma_zonalReduc(raster, MAX))
+
+
+def zmin(raster):
+    return Raster(_lib.ma_zonalReduc(raster, MIN))
+
+
+def rsum(raster, coord):
+    return Raster(_lib.ma_radialScan(raster, SUM, Array(coord)))
+
+
+def rprod(raster, coord):
+    return Raster(_lib.ma_radialScan(raster, PROD, Array(coord)))
+
+
+def rmax(raster, coord):
+    return Raster(_lib.ma_radialScan(raster, MAX, Array(coord)))
+
+
+def rmin(raster, coord):
+    return Raster(_lib.ma_radialScan(raster, MIN, Array(coord)))
+
+
+## Compound functions (python/map.py:592-706)
+
+def lmax(lst):
+    accu = lst[0]
+    for i in range(1, len(lst)):
+        accu = max(accu, lst[i])
+    return accu
+
+
+def lmin(lst):
+    accu = lst[0]
+    for i in range(1, len(lst)):
+        accu = min(accu, lst[i])
+    return accu
+
+
+def lmaxpos(lst):
+    maxim = lst[0]
+    idx = zeros_like(maxim, U8)
+    for i in range(1, len(lst)):
+        idx = con(lst[i] > maxim, full_like(i, idx), idx)
+        maxim = max(maxim, lst[i])
+    return idx
+
+
+def lminpos(lst):
+    minim = lst[0]
+    idx = zeros_like(minim, U8)
+    for i in range(1, len(lst)):
+        idx = con(lst[i] < minim, full_like(i, idx), idx)
+        minim = min(minim, lst[i])
+    return idx
+
+
+def lor(lst):
+    accu = lst[0]
+    for i in range(1, len(lst)):
+        accu = accu + lst[i]
+    return accu
+
+
+def pick(raster, lst):
+    acu = _const_to_raster(lst[0])
+    for i in range(len(lst)):
+        acu = con(raster == i, lst[i], acu)
+    return acu
+
+
+def degrees(raster):
+    return raster / (2 * PI) * 360
+
+
+def radians(raster):
+    return raster / 360 * (2 * PI)
+
+
+PI = 3.141593
+
+
+def distance(raster, coord):
+    x = coord[0] - index(raster, D1)
+    y = coord[1] - index(raster, D2)
+    return sqrt(x * x + y * y + 0.0)
+
+
+def mean(raster):
+    return zsum(raster) / prod(raster.datasize())
+
+
+def covariance(x, y):
+    if x.datasize() != y.datasize():
+        raise MapError("covariance: rasters differ in size")
+    xydif = (x - mean(x)) * (y - mean(y))
+    return zsum(xydif) / prod(x.datasize())
+
+
+def gradient(raster):
+    kx = [[-1, 0, 1], [-1, 0, 1], [-1, 0, 1]]
+    ky = [[-1, -1, -1], [0, 0, 0], [1, 1, 1]]
+    return convolve(raster, kx), convolve(raster, ky)
+
+
+def blur(raster, size=3):
+    if size == 3:
+        krnl = [[1, 2, 1], [2, 4, 2], [1, 2, 1]]
+        norm = 16
+    elif size == 5:
+        krnl = [[1, 4, 7, 4, 1], [4, 16, 26, 16, 4], [7, 26, 41, 26, 7], [4, 16, 26, 16, 4], [1, 4, 7, 4, 1]]
+        norm = 276
+    else:
+        raise MapError("blur: size must be 3 or 5")
+    return convolve(raster, krnl) / norm
+
+
+def harris(raster):
+    ix, iy = gradient(raster)
+    xx, yy, xy = blur(ix * ix), blur(iy * iy), blur(ix * iy)
+    return (xx * yy - xy) - 0.04 * (xx + yy) ** 2
+
+
+def prod(arg):
+    if isinstance(arg, (list, tuple)):
+        return functools.reduce(operator.mul, arg, 1)
+    elif isinstance(arg, Array):
+        return arg.arr[0] * arg.arr[1]
+    raise MapError("prod: unsupported argument")
+
+
+## Extensions (no counterpart in the reference module)
+
+_np_dtype = {F32: 'float32', F64: 'float64', B8: 'bool', U8: 'uint8', U16: 'uint16', U32: 'uint32',
+             U64: 'uint64', S8: 'int8', S16: 'int16', S32: 'int32', S64: 'int64'}
+_dt_of_np = {v: k for k, v in _np_dtype.items()}
+
+
+def from_numpy(arr, bs=None, copy=True):
+    """Raster input from a 2-D NumPy array (rows = y, columns = x)."""
+    import numpy as np
+    a = np.ascontiguousarray(arr)
+    if a.ndim != 2:
+        raise MapError("from_numpy: array must be 2-D")
+    dt = _dt_of_np.get(a.dtype.name)
+    if dt is None:
+        raise MapError("from_numpy: unsupported dtype %s" % a.dtype)
+    ds = Array([a.shape[1], a.shape[0]])
+    node = _lib.ma_fromHost(a.ctypes.data_as(ct.c_void_p), ds, dt, Array(bs or []), 1 if copy else 0)
+    r = Raster(node)
+    if not copy:
+        r._keep = a
+    return r
+
+
+def from_device(ptr, pitch, ds, dt, bs=None):
+    """Raster input from device memory (pointer as int, pitch in bytes, ds = [x, y])."""
+    return Raster(_lib.ma_fromDevice(ct.c_void_p(ptr), pitch, Array(ds), dt, Array(bs or [])))
+
+
+def to_numpy(raster, out=None):
+    """Evaluates a raster and returns it as a 2-D NumPy array."""
+    import numpy as np
+    w, h = raster.datasize()
+    dt = np.dtype(_np_dtype[raster.datatype()])
+    if out is None:
+        out = np.empty((h, w), dtype=dt)
+    _lib.ma_toHost(raster, out.ctypes.data_as(ct.c_void_p), out.nbytes)
+    return out
+
+
+def to_device(raster, ptr, pitch, sync=True):
+    _lib.ma_toDevice(raster, ct.c_void_p(ptr), pitch, 0 if sync else 1)
+
+
+def set_border(mode):
+    _lib.ma_setBorder(mode)
+
+
+def get_border():
+    return _lib.ma_getBorder()
+
+
+def set_exec_mode(mode):
+    _lib.ma_setExecMode(mode)
+
+
+def get_exec_mode():
+    return _lib.ma_getExecMode()
+
+
+def set_default_blocksize(bs):
+    _lib.ma_setDefaultBlockSize(Array(bs))
+
+
+def flow_direction(dem):
+    """D8 steepest-descent direction codes (U8, 1 << dir in E,SE,S,SW,W,NW,N,NE order)."""
+    return Raster(_lib.ma_focalFlow(dem))
+
+
+def flow_accumulation(water, dirs):
+    """Sum of `water` over every upstream cell along D8 directions (front/Raster.cpp:571-579)."""
+    return Raster(_lib.ma_spreadScan(water, dirs, SUM))
+
+
+def viewshed(dem, obs, h):
+    """Height above the line of sight from observer `obs` at height `h` (front/Raster.cpp:558-569)."""
+    shift = dem - h
+    dist = distance(dem, obs)
+    slope = shift / dist
+    maxr = rmax(slope, obs)
+    return (maxr * dist + h) - dem
+
+
+def sync():
+    _lib.ma_sync()
+
+
+def stream():
+    return _lib.ma_stream()
+
+
+def last_launch_count():
+    return _lib.ma_lastLaunchCount()
+
+
+def last_group_count():
+    return _lib.ma_lastGroupCount()
+
+
+def _node_array(rasters):
+    NodeArr = Node * len(rasters)
+    return NodeArr(*[r._node for r in rasters])
+
+
+def describe_groups(*rasters):
+    arr = _node_array(rasters)
+    n = _lib.ma_describeGroups(arr, len(rasters), None, 0)
+    buf = ct.create_string_buffer(n)
+    _lib.ma_describeGroups(arr, len(rasters), buf, n)
+    return buf.value.decode()
+
+
+def generated_source(*rasters):
+    arr = _node_array(rasters)
+    n = _lib.ma_generatedSource(arr, len(rasters), None, 0)
+    buf = ct.create_string_buffer(n)
+    _lib.ma_generatedSource(arr, len(rasters), buf, n)
+    return buf.value.decode()
+
+
+def plain_schedule(*rasters):
+    arr = _node_array(rasters)
+    n = _lib.ma_plainSchedule(arr, len(rasters), None, 0)
+    buf = ct.create_string_buffer(n)
+    _lib.ma_plainSchedule(arr, len(rasters), buf, n)
+    return [tuple(int(v) for v in line.split()) for line in buf.value.decode().splitlines() if line.strip()]
+
+
+def compile_only(*rasters, compile=True):
+    arr = _node_array(rasters)
+    return _lib.ma_compileOnly(arr, len(rasters), 1 if compile else 0)
+
+
+## CDLL interface: arguments & returns (python/map.py:723-830)
+
+def _sig(name, argtypes, restype, check=True):
+    f = getattr(_lib, name)
+    f.argtypes = argtypes
+    f.restype = restype
+    if check:
+        f.errcheck = _check
+
+
+_lib.ma_errorCode.argtypes = []
+_lib.ma_errorCode.restype = ct.c_int
+_lib.ma_lastError.argtypes = []
+_lib.ma_lastError.restype = ct.c_char_p
+
+_sig('ma_setupDevices', [ct.c_char_p, ct.c_int, ct.c_char_p], None)
+_sig('ma_increaseRef', [Raster], None)
+_sig('ma_decreaseRef', [Raster], None, check=False)
+_sig('ma_eval', [ct.POINTER(Node), ct.c_int], None)
+_sig('ma_nodeid', [Raster], ct.c_int)
+_sig('ma_streamdir', [Raster], ct.c_int)
+_sig('ma_value', [Raster], Variant)
+_sig('ma_datatype', [Raster], ct.c_int)
+_sig('ma_numdim', [Raster], ct.c_int)
+_sig('ma_memorder', [Raster], ct.c_int)
+_sig('ma_datasize', [Raster], Array)
+_sig('ma_blocksize', [Raster], Array)
+_sig('ma_numblock', [Raster], Array)
+_sig('ma_read', [ct.c_char_p], Node)
+_sig('ma_write', [Raster, ct.c_char_p], ct.c_int)
+_sig('ma_index', [Raster, ct.c_int], Node)
+_sig('ma_rand', [Raster, ct.c_int, ct.c_int], Node)
+_sig('ma_cast', [Raster, ct.c_int], Node)
+_sig('ma_conditional', [Raster, Raster, Raster], Node)
+_sig('ma_unary', [Raster, ct.c_int], Node)
+_sig('ma_binary', [Raster, Raster, ct.c_int], Node)
+_sig('ma_constant', [Variant, Array, ct.c_int, ct.c_int, Array], Node)
+_sig('ma_access', [Raster, Array], Node)
+_sig('ma_lhsAccess', [Raster, Raster, Array], Node)
+_sig('ma_neighbor', [Raster, Array], Node)
+_sig('ma_boundedNbh', [Raster, Raster, Raster], Node)
+_sig('ma_convolution', [Raster, ct.POINTER(Variant), ct.c_int, Array], Node)
+_sig('ma_focalFunc', [Raster, ct.POINTER(Variant), ct.c_int, Array, ct.c_int], Node)
+_sig('ma_zonalReduc', [Raster, ct.c_int], Node)
+_sig('ma_radialScan', [Raster, ct.c_int, Array], Node)
+_sig('ma_spreadScan', [Raster, Raster, ct.c_int], Node)
+_sig('ma_barrier', [Raster], Node)
+_sig('ma_loopStart', [], None)
+_sig('ma_loopCond', [Raster], None)
+_sig('ma_loopBody', [], None)
+_sig('ma_loopAgain', [], None)
+_sig('ma_loopAssemble', [], Node)
+_sig('ma_loopEnd', [], None)
+_sig('ma_loopAgainTail', [Raster, ct.POINTER(ct.POINTER(Node)), ct.POINTER(ct.POINTER(Node)), ct.POINTER(ct.c_int)], None)
+_sig('ma_setBorder', [ct.c_int], None)
+_sig('ma_getBorder', [], ct.c_int, check=False)
+_sig('ma_setExecMode', [ct.c_int], None)
+_sig('ma_getExecMode', [], ct.c_int, check=False)
+_sig('ma_setDefaultBlockSize', [Array], None)
+_sig('ma_fromHost', [ct.c_void_p, Array, ct.c_int, Array, ct.c_int], Node)
+_sig('ma_fromDevice', [ct.c_void_p, ct.c_longlong, Array, ct.c_int, Array], Node)
+_sig('ma_toHost', [Raster, ct.c_void_p, ct.c_size_t], ct.c_int)
+_sig('ma_toDevice', [Raster, ct.c_void_p, ct.c_longlong, ct.c_int], ct.c_int)
+_sig('ma_sync', [], ct.c_int)
+_sig('ma_stream', [], ct.c_void_p)
+_sig('ma_lastLaunchCount', [], ct.c_int, check=False)
+_sig('ma_lastGroupCount', [], ct.c_int, check=False)
+_sig('ma_compileOnly', [ct.POINTER(Node), ct.c_int, ct.c_int], ct.c_int)
+_sig('ma_describeGroups', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_generatedSource', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_plainSchedule', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+if hasattr(_lib, 'ma_focalFlow'):
+    _sig('ma_focalFlow', [Raster], Node)
+_sig('ma_devAlloc', [ct.c_size_t], ct.c_void_p)
+_sig('ma_devFree', [ct.c_void_p], None, check=False)
+_sig('ma_hostAlloc', [ct.c_size_t], ct.c_void_p)
+_sig('ma_hostFree', [ct.c_void_p], None, check=False)
+_sig('ma_memcpy', [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int], ct.c_int)
+_sig('ma_evalAsync', [ct.POINTER(Node), ct.c_int], ct.c_int)
+_sig('ma_totalLaunchCount', [], ct.c_int, check=False)
+_sig('ma_setDevice', [ct.c_int], None)

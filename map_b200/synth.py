@@ -1,0 +1,112 @@
+"""Seeded synthetic rasters for tests and benchmarks.
+
+No public dataset is used by the reference or its benchmark plan, so inputs are
+generated with the shapes and value distributions the workloads name:
+  * fBm DEM: `octaves` octaves of value noise (lattice values uniform in [0,1),
+    smoothstep-interpolated), persistence 0.5, rescaled to [lo, hi] metres;
+  * Bernoulli grids (U8 0/1);
+  * lognormal value rasters;
+  * uniform [0,1) layers;
+  * Voronoi zone rasters (nearest of `n` uniform seed points).
+All generators take an explicit seed. `xp` may be numpy or torch (arrays on the
+device the torch tensors live on) for large rasters.
+"""
+import numpy as np
+
+
+def _axis_weights(n, cells, xp, device=None):
+    if xp is np:
+        u = (np.arange(n, dtype=np.float64) + 0.5) * (cells / n)
+        i = np.minimum(np.floor(u).astype(np.int64), cells - 1)
+    else:
+        u = (xp.arange(n, dtype=xp.float64, device=device) + 0.5) * (cells / n)
+        i = xp.clamp(xp.floor(u).long(), max=cells - 1)
+    f = u - i
+    f = f * f * (3.0 - 2.0 * f)
+    return i, f
+
+
+def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cells=4, xp=np, device=None):
+    """float32 (h, w) fractal Brownian value-noise DEM rescaled to [lo, hi]."""
+    rng = np.random.default_rng(seed)
+    side = max(h, w)
+    total = None
+    amp = 1.0
+    for o in range(octaves):
+        cells = base_cells * (2 ** o)
+        cx = max(1, int(round(cells * w / side)))
+        cy = max(1, int(round(cells * h / side)))
+        lat = rng.random((cy + 1, cx + 1))
+        if xp is np:
+            L = lat
+        else:
+            L = xp.as_tensor(lat, dtype=xp.float64, device=device)
+        iy, fy = _axis_weights(h, cy, xp, device)
+        ix, fx = _axis_weights(w, cx, xp, device)
+        if xp is np:
+            top = L[iy][:, ix] * (1 - fx)[None, :] + L[iy][:, ix + 1] * fx[None, :]
+            bot = L[iy + 1][:, ix] * (1 - fx)[None, :] + L[iy + 1][:, ix + 1] * fx[None, :]
+            noise = top * (1 - fy)[:, None] + bot * fy[:, None]
+        else:
+            Ly0, Ly1 = L[iy], L[iy + 1]
+            top = Ly0[:, ix] * (1 - fx)[None, :] + Ly0[:, ix + 1] * fx[None, :]
+            del Ly0
+            bot = Ly1[:, ix] * (1 - fx)[None, :] + Ly1[:, ix + 1] * fx[None, :]
+            del Ly1
+            noise = top * (1 - fy)[:, None] + bot * fy[:, None]
+            del top, bot
+        total = noise * amp if total is None else total + noise * amp
+        del noise
+        amp *= persistence
+    mn, mx = total.min(), total.max()
+    out = (total - mn) / (mx - mn) * (hi - lo) + lo
+    return out.astype(np.float32) if xp is np else out.float()
+
+
+def bernoulli_u8(h, w, p, seed):
+    rng = np.random.default_rng(seed)
+    return (rng.random((h, w)) < p).astype(np.uint8)
+
+
+def lognormal_f32(h, w, seed, mu=0.0, sigma=1.0):
+    rng = np.random.default_rng(seed)
+    return rng.lognormal(mu, sigma, size=(h, w)).astype(np.float32)
+
+
+def uniform_f32(h, w, seed):
+    rng = np.random.default_rng(seed)
+    return rng.random((h, w), dtype=np.float32)
+
+
+def voronoi_s32(h, w, n, seed, xp=np, device=None, chunk_rows=256):
+    """int32 (h, w) zone ids: index of the nearest of n uniform seed points."""
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 2)) * np.array([w, h])
+    if xp is np:
+        out = np.empty((h, w), np.int32)
+        xs = np.arange(w) + 0.5
+        for y0 in range(0, h, chunk_rows):
+            ys = np.arange(y0, min(h, y0 + chunk_rows)) + 0.5
+            best = np.full((len(ys), w), np.inf)
+            arg = np.zeros((len(ys), w), np.int32)
+            for k in range(n):
+                d = (ys[:, None] - pts[k, 1]) ** 2 + (xs[None, :] - pts[k, 0]) ** 2
+                m = d < best
+                best[m] = d[m]
+                arg[m] = k
+            out[y0:y0 + len(ys)] = arg
+        return out
+    P = xp.as_tensor(pts, dtype=xp.float32, device=device)
+    out = xp.empty((h, w), dtype=xp.int32, device=device)
+    xs = xp.arange(w, device=device, dtype=xp.float32) + 0.5
+    for y0 in range(0, h, chunk_rows):
+        ys = xp.arange(y0, min(h, y0 + chunk_rows), device=device, dtype=xp.float32) + 0.5
+        best = xp.full((len(ys), w), float("inf"), device=device)
+        arg = xp.zeros((len(ys), w), dtype=xp.int32, device=device)
+        for k in range(n):
+            d = (ys[:, None] - P[k, 1]) ** 2 + (xs[None, :] - P[k, 0]) ** 2
+            m = d < best
+            best = xp.where(m, d, best)
+            arg = xp.where(m, xp.full_like(arg, k), arg)
+        out[y0:y0 + len(ys)] = arg
+    return out

@@ -1,0 +1,111 @@
+"""Fusion compiler and code generation on CPU: the reference scripts partition
+into the groups the reference's fusion rules give, the plain-mode schedule
+respects block dependencies, and every generated kernel compiles for sm_100a
+with NVRTC (no device needed)."""
+import numpy as np
+import pytest
+
+from map_b200 import workloads as W
+
+
+def groups(M, *rs):
+    return [l for l in M.describe_groups(*rs).splitlines() if l.strip()]
+
+
+def nodes_of(line):
+    return line.split("nodes=[")[1].split("]")[0]
+
+
+def test_hillshade_is_one_focal_group(M):
+    dem = M.from_numpy(np.zeros((64, 96), np.float32), bs=[32, 32])
+    hs = W.hillshade(dem)
+    g = groups(M, hs)
+    assert len(g) == 1 and g[0].startswith("Focal")
+    assert nodes_of(g[0]).count("Convolution") == 2          # both Sobel kernels share one staged tile
+    assert M.compile_only(hs) == 1
+
+
+def test_life_is_one_focal_group_per_generation(M):
+    st = M.from_numpy(np.zeros((64, 64), np.uint8), bs=[32, 32])
+    out = W.life(st, 5)
+    g = groups(M, out)
+    assert len(g) == 5 and all(x.startswith("Focal") for x in g)
+    # every generation has the same structure, hence the same kernel source
+    src = M.generated_source(out).split("//----")
+    assert len(set(s.strip() for s in src if s.strip())) == 1
+
+
+def test_stats_groups(M):
+    dem = M.from_numpy(np.ones((64, 64), np.float32), bs=[32, 32])
+    s = W.stats(dem)
+    g = groups(M, *s.values())
+    zonal = [x for x in g if x.startswith("Zonal")]
+    host = [x for x in g if x.startswith("Host")]
+    # all reductions of the raster itself flat-fuse into one pass; the deviation
+    # pass (needs the mean) is a second zonal pass
+    assert len(zonal) == 2
+    assert nodes_of(zonal[0]).count("ZonalReduc") == 7
+    assert nodes_of(zonal[1]).count("ZonalReduc") == 2
+    assert len(host) >= 8
+
+
+def test_wsum_is_one_local_group(M):
+    ls = [M.from_numpy(np.zeros((16, 16), np.float32)) for _ in range(6)]
+    out = W.wsum(ls, [0.1, 0.2, 0.3, 0.15, 0.15, 0.1])
+    g = groups(M, out)
+    assert len(g) == 1 and g[0].startswith("Local")
+
+
+def test_focal_of_local_is_not_fused(M):
+    d = M.from_numpy(np.zeros((16, 16), np.float32))
+    out = M.convolve(d * 2.0, [[1, 1, 1]] * 3) + 1.0
+    g = groups(M, out)
+    assert [x.split()[0] for x in g] == ["Local", "Focal"]   # PIPE(LOCAL, FOCAL) is not allowed
+
+
+def test_plain_schedule_respects_dependencies(M):
+    st = M.from_numpy(np.zeros((96, 64), np.uint8), bs=[32, 32])
+    out = W.life(st, 3)
+    jobs = M.plain_schedule(out)
+    nb = (2, 3)
+    assert len(jobs) == 3 * nb[0] * nb[1]
+    done = set()
+    for g, bx, by, kind in jobs:
+        if g > 0:
+            for dy in (-1, 0, 1):
+                for dx in (-1, 0, 1):
+                    x, y = bx + dx, by + dy
+                    if 0 <= x < nb[0] and 0 <= y < nb[1]:
+                        assert (g - 1, x, y) in done, (g, bx, by)
+        done.add((g, bx, by))
+    # the schedule interleaves generations (it is not group-major)
+    first_g1 = next(i for i, j in enumerate(jobs) if j[0] == 1)
+    last_g0 = max(i for i, j in enumerate(jobs) if j[0] == 0)
+    assert first_g1 < last_g0
+
+
+@pytest.mark.parametrize("dt", ["U8", "S16", "S32", "U32", "F32", "F64", "S64"])
+def test_generated_elementwise_kernels_compile(M, dt):
+    npdt = {"U8": np.uint8, "S16": np.int16, "S32": np.int32, "U32": np.uint32, "F32": np.float32,
+            "F64": np.float64, "S64": np.int64}[dt]
+    a = M.from_numpy(np.ones((16, 16), npdt))
+    b = M.from_numpy(np.ones((16, 16), npdt))
+    exprs = [a + b, a - b, a * b, a / (b + 1), M.max(a, b), M.min(a, 3), a < b, M.con(a > b, a, b),
+             M.astype(a, M.F32), (a == 1) * 2]
+    if dt in ("F32", "F64"):
+        exprs += [M.sin(a), M.atan2(a, b), M.sqrt(M.abs(a)), a ** b, M.exp(a) + M.log(b + 2)]
+    else:
+        exprs += [a % (b + 1)]
+    if dt in ("U8", "U32"):
+        one = M.full(1, [], a.datatype())
+        exprs += [a & b, a | b, a ^ b, a << one, ~a]
+    assert M.compile_only(*exprs) >= 1
+
+
+def test_focal_variants_compile(M):
+    d = M.from_numpy(np.zeros((40, 40), np.float32))
+    u = M.from_numpy(np.zeros((40, 40), np.uint8))
+    outs = [M.convolve(d, [[1.0 / 16, 1.0 / 8, 1.0 / 16], [1.0 / 8, 1.0 / 4, 1.0 / 8], [1.0 / 16, 1.0 / 8, 1.0 / 16]]),
+            M.convolve(d, [[1] * 5] * 5), M.fmin(d, [[1] * 3] * 3), M.fmax(u, [[1] * 5] * 3), d([1, -1]) - d([0, 2]),
+            M.flow_direction(d), M.convolve(u, [[1, 1, 1], [1, 0, 1], [1, 1, 1]])]
+    assert M.compile_only(*outs) >= 1
