@@ -17,6 +17,7 @@ independent raster (weak scaling, no data-path collective).
 """
 import argparse
 import concurrent.futures as cf
+import faulthandler
 import ctypes as ct
 import json
 import os
@@ -169,6 +170,7 @@ def run_reference(args, rank, world):
 # ---------------------------------------------------------------- our arm
 
 def main():
+    faulthandler.enable()
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -252,7 +254,9 @@ def main():
     nbytes = cells * 4
     h_in = M._lib.ma_hostAlloc(nbytes)
     h_out = M._lib.ma_hostAlloc(nbytes)
-    ct.memmove(h_in, dem_t.cpu().numpy().ctypes.data, nbytes)
+    dem_host = dem_t.cpu().numpy()          # keep the array alive while it is copied
+    ct.memmove(h_in, dem_host.ctypes.data, nbytes)
+    del dem_host
     dem_h = M.Raster(M._lib.ma_fromHost(ct.c_void_p(h_in), M.Array([S, S]), M.F32, M.Array([args.block, args.block]), 0))
     hs_h = W.hillshade(dem_h)
     M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)  # warm

@@ -114,6 +114,11 @@ void ma_setDevice(int device);
  * C++ only (front/Raster.cpp:485-557, FocalFlow::Factory) with no C binding. */
 ma_Node *ma_focalFlow(ma_Node *node);
 
+/* Radial scan limited to fronts within `radius` cells of the start along the
+ * octant's primary axis (radius <= 0: the whole raster). Cells not swept hold
+ * NaN (all-ones bytes) in every output of the scan's group. */
+ma_Node *ma_radialScanRadius(ma_Node *node, int type, ma_Array coord, double radius);
+
 /* Raster inputs from caller memory. `data` is dense row-major (ds.arr[0]
  * columns, ds.arr[1] rows). ma_fromHost copies the cells when copy != 0,
  * otherwise it keeps the pointer, which must stay valid while the node is used

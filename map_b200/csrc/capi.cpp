@@ -289,6 +289,9 @@ ma_Node *ma_zonalReduc(ma_Node *node, int type) {
 ma_Node *ma_radialScan(ma_Node *node, int type, ma_Array coord) {
   return node_call([&] { return Runtime::get().radial_scan(checked(node), type, A(coord)); });
 }
+ma_Node *ma_radialScanRadius(ma_Node *node, int type, ma_Array coord, double radius) {
+  return node_call([&] { return Runtime::get().radial_scan(checked(node), type, A(coord), radius); });
+}
 ma_Node *ma_spreadScan(ma_Node *node, ma_Node *dir, int type) {
   return node_call([&] { return Runtime::get().spread_scan(checked(node), checked(dir), type); });
 }

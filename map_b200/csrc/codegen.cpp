@@ -1,5 +1,5 @@
-// Kernel generation for the Local, Focal and Zonal skeletons (see codegen.hpp).
-// The Radiating and Spreading skeletons are generated in codegen_scan.cpp.
+// Kernel generation for the Local, Focal, Zonal, Radiating and Spreading
+// skeletons (see codegen.hpp); the scan skeletons run through codegen_scan.cpp.
 #include "codegen.hpp"
 
 #include <cstdlib>
@@ -9,7 +9,6 @@
 
 namespace mapb {
 
-std::string codegen_scan(const Group &g, KernelPlan &plan);   // codegen_scan.cpp
 
 Variant reference_literal_value(const Variant &v) {
   if (v.dtype == F32) {
@@ -542,6 +541,143 @@ static std::string gen_zonal(Gen &G) {
   return s.str();
 }
 
+// Radiating skeleton (runtime/skeleton/RadiatingSkeleton.cpp:32-323): one CTA per
+// octant sweeps the fronts d0 = 1, 2, ... in order; a front's cells are spread over
+// the CTA's threads. A cell's scan value is op(LIT(front d0-1 at d1, at d1-1), in)
+// when `in` is finite; the start cell holds the neutral value. The previous front
+// is read back (L1-bypassing loads) from the scan's own output raster, written by
+// this CTA one step earlier; cells on an octant boundary are written by both
+// adjacent octants with identical values. Local nodes before the scan produce
+// `in` per cell; those after it run right after the cell's scan value.
+static std::string gen_radial(Gen &G) {
+  KernelPlan &P = G.plan;
+  Node *scan = P.core;
+  const std::string T = G.T(scan);
+  const std::string v = G.val(scan);
+  const std::string nt = var_literal(reduction_neutral(scan->op, scan->meta.dtype));
+  std::ostringstream s;
+  s << "#include \"map_scan.cuh\"\n" << G.args_struct(0, false);
+  s << "__device__ __forceinline__ void radial_cell(const Args &a, int x, int y, " << T << " lit, bool observer) {\n"
+    << G.center_loads(false);
+  for (Node *n : G.g.nodes) {
+    if (n == scan) {
+      s << "    " << T << " " << v << " = lit;\n"
+        << "    if (observer) " << v << " = " << nt << ";\n"
+        << "    else if (isfinite((double)(" << G.val(scan->prev[0]) << "))) " << v << " = RedOp<" << scan->op << ", " << T
+        << ">::f(" << v << ", (" << T << ")(" << G.val(scan->prev[0]) << "));\n";
+    } else {
+      s << "    " << G.stmt(n, false) << "\n";
+    }
+  }
+  s << G.stores() << "}\n";
+  int ri = G.outk.at(scan);
+  // aux[0] start x, aux[1] start y, aux[2] last front (or -1 for all)
+  s << "extern \"C\" __global__ void __launch_bounds__(512) KNAME(const __grid_constant__ Args a) {\n"
+    << "  const int sx = (int)a.aux[0], sy = (int)a.aux[1];\n"
+    << "  const long long lim = (long long)a.aux[2];\n"
+    << "  const RasterArg R = a.out[" << ri << "];\n"
+    << "  const int W = a.g.W, H = a.g.H;\n"
+    << "  int p0, p1, q0, q1;\n"
+    << "  octant_units(blockIdx.x, p0, p1, q0, q1);\n"
+    << "  if (threadIdx.x == 0) radial_cell(a, sx, sy, (" << T << ")0, true);\n"
+    << "  const int ep = p0 > 0 ? W - 1 - sx : p0 < 0 ? sx : p1 > 0 ? H - 1 - sy : sy;\n"
+    << "  const int eq = q0 > 0 ? W - 1 - sx : q0 < 0 ? sx : q1 > 0 ? H - 1 - sy : sy;\n"
+    << "  const int dmax = (lim >= 0 && lim < ep) ? (int)lim : ep;\n"
+    << "  __syncthreads();\n"
+    << "  for (int d0 = 1; d0 <= dmax; ++d0) {\n"
+    << "    const int d1max = d0 < eq ? d0 : eq;\n"
+    << "    for (int d1 = threadIdx.x; d1 <= d1max; d1 += blockDim.x) {\n"
+    << "      const int x = sx + p0 * d0 + q0 * d1, y = sy + p1 * d0 + q1 * d1;\n"
+    << "      const " << T << " va = (d1 <= d0 - 1) ? ld_coherent<" << T
+    << ">(R, sx + p0 * (d0 - 1) + q0 * d1, sy + p1 * (d0 - 1) + q1 * d1) : (" << T << ")0;\n"
+    << "      const " << T << " vb = (d1 >= 1) ? ld_coherent<" << T
+    << ">(R, sx + p0 * (d0 - 1) + q0 * (d1 - 1), sy + p1 * (d0 - 1) + q1 * (d1 - 1)) : (" << T << ")0;\n"
+    << "      radial_cell(a, x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
+    << "    }\n"
+    << "    __syncthreads();\n"
+    << "  }\n"
+    << "}\n";
+  return s.str();
+}
+
+// Spreading skeleton (runtime/skeleton/SpreadingSkeleton.cpp:288-393). The
+// reference relaxes pending spread one neighbour per iteration, block by block,
+// until stable; the fixed point is, for every cell, the sum of the water of all
+// strictly-upstream cells. The same fixed point is reached here by a topological
+// (Kahn) sweep inside one CTA: in-degrees are counted by pulling from the 8
+// neighbours, cells with no pending upstream form the frontier, and each
+// frontier cell pushes (its accumulation + its water) to its downstream cell
+// with an atomic add; a cell joins the next frontier when its last upstream
+// neighbour has pushed. The sweep ends when the frontier is empty or after N+1
+// rounds (error flag). Integer sums are exact and independent of order.
+static std::string gen_spread(Gen &G) {
+  KernelPlan &P = G.plan;
+  Node *scan = P.core;
+  const int dt = scan->meta.dtype;
+  if (!(dt == S32 || dt == U32 || dt == F32 || dt == F64 || dt == S64 || dt == U64))
+    throw MapError("spreadScan: the accumulated raster must be a 32- or 64-bit type");
+  if (!G.rin.count(scan->prev[1])) throw MapError("spreadScan: the direction raster must be materialised");
+  const std::string T = G.T(scan);
+  std::ostringstream s;
+  s << "#include \"map_scan.cuh\"\n" << G.args_struct(0, false);
+  s << "__device__ __forceinline__ " << T << " water_at(const Args &a, int x, int y) {\n";
+  for (Node *p : P.in_rasters) {
+    if (p == scan->prev[1] || !G.center_read.count(p)) continue;
+    int k = G.rin.at(p);
+    s << "    const " << G.T(p) << " i" << k << " = ldr<" << G.T(p) << ">(a.in[" << k << "], x, y);\n";
+  }
+  for (Node *n : G.g.nodes)
+    if (n != scan) s << "    " << G.stmt(n, false) << "\n";
+  s << "    return (" << T << ")(" << G.val(scan->prev[0]) << ");\n}\n";
+  const int kd = G.rin.at(scan->prev[1]);
+  const int ko = G.outk.at(scan);
+  // aux[0] in-degree (s32[N]), aux[1] frontier A (s32[N]), aux[2] frontier B, aux[3] round limit
+  s << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME(const __grid_constant__ Args a) {\n"
+    << "  const int W = a.g.W, H = a.g.H;\n"
+    << "  const s64 N = (s64)W * H;\n"
+    << "  s32 *indeg = (s32 *)a.aux[0];\n"
+    << "  s32 *fa = (s32 *)a.aux[1], *fb = (s32 *)a.aux[2];\n"
+    << "  const long long limit = (long long)a.aux[3];\n"
+    << "  const RasterArg D = a.in[" << kd << "];\n"
+    << "  const RasterArg O = a.out[" << ko << "];\n"
+    << "  __shared__ int n_cur, n_next;\n"
+    << "  if (threadIdx.x == 0) { n_cur = 0; n_next = 0; }\n"
+    << "  __syncthreads();\n"
+    << "  for (s64 c = threadIdx.x; c < N; c += blockDim.x) {\n"
+    << "    const int x = (int)(c % W), y = (int)(c / W);\n"
+    << "    *cell_ptr<" << T << ">(O, x, y) = (" << T << ")0;\n"
+    << "    int cnt = 0;\n"
+    << "    for (int d = 0; d < 8; ++d) {\n"
+    << "      const int nx = x - d8_dx(d), ny = y - d8_dy(d);\n"
+    << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+    << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) cnt++;\n"
+    << "    }\n"
+    << "    indeg[c] = cnt;\n"
+    << "    if (cnt == 0) fa[atomicAdd(&n_cur, 1)] = (s32)c;\n"
+    << "  }\n"
+    << "  __syncthreads();\n"
+    << "  for (long long it = 0;; ++it) {\n"
+    << "    const int n = n_cur;\n"
+    << "    if (n == 0) break;\n"
+    << "    if (it > limit) { if (threadIdx.x == 0) skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
+    << "    for (int i = threadIdx.x; i < n; i += blockDim.x) {\n"
+    << "      const s32 c = fa[i];\n"
+    << "      const int x = c % W, y = c / W;\n"
+    << "      const s64 dn = d8_down(D, W, H, x, y);\n"
+    << "      if (dn < 0) continue;\n"
+    << "      const " << T << " v = (" << T << ")(ld_coherent<" << T << ">(O, x, y) + water_at(a, x, y));\n"
+    << "      atomic_add_any(cell_ptr<" << T << ">(O, (int)(dn % W), (int)(dn / W)), v);\n"
+    << "      if (atomicSub(&indeg[dn], 1) == 1) fb[atomicAdd(&n_next, 1)] = (s32)dn;\n"
+    << "    }\n"
+    << "    __syncthreads();\n"
+    << "    if (threadIdx.x == 0) { n_cur = n_next; n_next = 0; }\n"
+    << "    s32 *t = fa; fa = fb; fb = t;\n"
+    << "    __syncthreads();\n"
+    << "  }\n"
+    << "}\n";
+  return s.str();
+}
+
 KernelPlan generate_kernel(const Group &g) {
   KernelPlan P;
   P.skeleton = g.skeleton;
@@ -557,8 +693,10 @@ KernelPlan generate_kernel(const Group &g) {
     case SK_FOCAL: src = gen_focal(G); prefix = "map_focal"; break;
     case SK_ZONAL: src = gen_zonal(G); prefix = "map_zonal"; break;
     case SK_RADIAL: case SK_SPREAD:
-      src = codegen_scan(g, P);
-      prefix = g.skeleton == SK_RADIAL ? "map_radial" : "map_spread";
+      for (Node *n : g.nodes)
+        if (n->kind == K_RADIALSCAN || n->kind == K_SPREADSCAN) P.core = n;
+      if (g.skeleton == SK_RADIAL) { src = gen_radial(G); prefix = "map_radial"; }
+      else { src = gen_spread(G); prefix = "map_spread"; }
       break;
     default: throw MapError("codegen: group has no device skeleton");
   }

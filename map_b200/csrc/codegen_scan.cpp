@@ -1,22 +1,73 @@
-// Kernel generation and execution for the Radiating (viewshed-style radial
-// scans) and Spreading (flow accumulation) skeletons.
+// Execution of the Radiating (radial scan) and Spreading (flow accumulation)
+// skeletons; their kernels are generated in codegen.cpp (gen_radial, gen_spread).
+//
+// Radiating (runtime/skeleton/RadiatingSkeleton.cpp:32-323): one CTA per octant
+// sweeps the octant's fronts d0 = 1, 2, ... in order; the cells of a front are
+// independent and are spread over the CTA's threads. A cell's scan value is
+// op(LIT(prev front at d1, prev front at d1-1), in) when `in` is finite; the
+// start cell holds the neutral value. The previous front is read back from the
+// scan's own output raster (written by this CTA one step earlier; cells on an
+// octant boundary are written by both adjacent octants with identical values).
+// The group's local nodes before the scan are evaluated per cell to produce
+// `in`; those after it are evaluated right after the cell's scan value.
+//
+// Spreading (runtime/skeleton/SpreadingSkeleton.cpp:288-393): the reference
+// relaxes "pending spread" one neighbour per iteration, block by block, until
+// stable; the fixed point is, for every cell, the sum of the water of all
+// strictly-upstream cells. Here the same fixed point is reached by a
+// topological (Kahn) sweep on the device: in-degrees are counted by pulling
+// from the 8 neighbours, cells with no pending upstream form the frontier, and
+// each frontier cell pushes (its accumulation + its water) to its downstream
+// cell with an atomic add; a cell joins the next frontier when its last
+// upstream neighbour has pushed. Integer sums are exact and order-independent.
 #include "codegen.hpp"
+#include "cuda_env.hpp"
 #include "executor.hpp"
 
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <cstring>
 #include <functional>
 #include <unordered_map>
 
 namespace mapb {
 
-std::string codegen_scan(const Group &g, KernelPlan &plan) {
-  (void)plan;
-  throw MapError(std::string(skeleton_name(g.skeleton)) + " groups are not supported by this build yet");
-}
-
 void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node *, DevRaster> &bufs,
                     const std::function<DevRaster &(Node *)> &get, const std::function<DevRaster(Node *)> &alloc_out) {
-  (void)P; (void)bufs; (void)get; (void)alloc_out;
-  throw MapError(std::string(skeleton_name(g.skeleton)) + " groups are not supported by this build yet");
+  CudaEnv &env = CudaEnv::get();
+  cudaStream_t st = (cudaStream_t)env.stream();
+  for (Node *o : P.out_rasters)
+    if (!bufs.count(o)) bufs[o] = alloc_out(o);
+  Node *scan = P.core;
+  KernelHandle kh = env.kernel(P.source, P.kname, 0);
+  if (scan->kind == K_RADIALSCAN) {
+    int ri = -1;
+    for (size_t k = 0; k < P.out_rasters.size(); k++)
+      if (P.out_rasters[k] == scan) ri = (int)k;
+    if (ri < 0) throw MapError("radial scan output missing");
+    long long lim = -1;
+    if (scan->radius > 0) {
+      lim = (long long)scan->radius;
+      for (Node *o : P.out_rasters) {
+        DevRaster &r = bufs.at(o);
+        cuda_check(cudaMemset2DAsync(r.ptr, r.pitch, 0xFF, (size_t)r.W * dt_size(r.dtype), r.H, st), "memset");
+      }
+    }
+    uint64_t aux[4] = {(uint64_t)scan->coord.arr[0], (uint64_t)scan->coord.arr[1], (uint64_t)lim, (uint64_t)ri};
+    auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+    env.launch(kh, 8, 512, 0, (CUstream_st *)st, a.data(), a.size());
+    return;
+  }
+  const size_t N = (size_t)g.W * g.H;
+  if (N >= (size_t)1 << 31) throw MapError("spreadScan: raster too large");
+  void *work = nullptr;
+  cuda_check(cudaMallocAsync(&work, 3 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
+  uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
+                     (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
+  auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+  env.launch(kh, 1, 1024, 0, (CUstream_st *)st, a.data(), a.size());
+  cuda_check(cudaFreeAsync(work, st), "cudaFreeAsync");
 }
 
 }  // namespace mapb

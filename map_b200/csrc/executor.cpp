@@ -182,6 +182,50 @@ std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &
   return out;
 }
 
+std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
+                                     std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
+                                     const uint64_t aux[4]) {
+  CudaEnv &env = CudaEnv::get();
+  std::vector<unsigned char> a(K.args_size, 0);
+  for (size_t k = 0; k < K.tma.size(); k++) {
+    const TmaSpec &t = K.tma[k];
+    DevRaster &r = get(K.in_rasters[t.in_index]);
+    alignas(64) unsigned char desc[128];
+    env.encode_tma_2d(desc, r.dtype, r.ptr, (uint64_t)r.W, (uint64_t)r.H, (uint64_t)r.pitch, (uint32_t)t.box_w,
+                      (uint32_t)t.box_h);
+    std::memcpy(a.data() + K.off_tm + 128 * k, desc, 128);
+  }
+  for (size_t k = 0; k < K.in_rasters.size(); k++) {
+    DevRaster &r = get(K.in_rasters[k]);
+    uint64_t p = (uint64_t)(uintptr_t)r.ptr;
+    int64_t pitch = r.pitch;
+    std::memcpy(a.data() + K.off_in + 16 * k, &p, 8);
+    std::memcpy(a.data() + K.off_in + 16 * k + 8, &pitch, 8);
+  }
+  for (size_t k = 0; k < K.out_rasters.size(); k++) {
+    DevRaster &r = bufs.at(K.out_rasters[k]);
+    uint64_t p = (uint64_t)(uintptr_t)r.ptr;
+    int64_t pitch = r.pitch;
+    std::memcpy(a.data() + K.off_out + 16 * k, &p, 8);
+    std::memcpy(a.data() + K.off_out + 16 * k + 8, &pitch, 8);
+  }
+  for (size_t k = 0; k < K.scalars.size(); k++) {
+    Node *s = K.scalars[k];
+    if (!s->has_value) throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
+    Variant v = var_convert(s->value, s->meta.dtype);
+    std::memcpy(a.data() + K.off_s + 8 * k, &v.u, dt_size(v.dtype));
+  }
+  int32_t geom[12] = {g.W, g.H, g.BS0, g.BS1, rx0, ry0, rx1, ry1, 0, 0, Runtime::get().border, 0};
+  const int tx = (rx1 - rx0 + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+  geom[8] = tx;
+  geom[9] = tx * ty;
+  std::memcpy(a.data() + K.off_geom, geom, sizeof geom);
+  uint64_t errp = (uint64_t)(uintptr_t)env.err_word();
+  std::memcpy(a.data() + K.off_err, &errp, 8);
+  std::memcpy(a.data() + K.off_aux, aux, 4 * sizeof(uint64_t));
+  return a;
+}
+
 Executor &Executor::get() {
   static Executor e;
   return e;
@@ -374,45 +418,8 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
 
   auto build_args = [&](const Group &g, const KernelPlan &K, int rx0, int ry0, int rx1, int ry1, uint64_t aux0,
                         uint64_t aux1) {
-    std::vector<unsigned char> a(K.args_size, 0);
-    for (size_t k = 0; k < K.tma.size(); k++) {
-      const TmaSpec &t = K.tma[k];
-      DevRaster &r = get(K.in_rasters[t.in_index]);
-      alignas(64) unsigned char desc[128];
-      env.encode_tma_2d(desc, r.dtype, r.ptr, (uint64_t)r.W, (uint64_t)r.H, (uint64_t)r.pitch, (uint32_t)t.box_w,
-                        (uint32_t)t.box_h);
-      std::memcpy(a.data() + K.off_tm + 128 * k, desc, 128);
-    }
-    for (size_t k = 0; k < K.in_rasters.size(); k++) {
-      DevRaster &r = get(K.in_rasters[k]);
-      uint64_t p = (uint64_t)(uintptr_t)r.ptr;
-      int64_t pitch = r.pitch;
-      std::memcpy(a.data() + K.off_in + 16 * k, &p, 8);
-      std::memcpy(a.data() + K.off_in + 16 * k + 8, &pitch, 8);
-    }
-    for (size_t k = 0; k < K.out_rasters.size(); k++) {
-      DevRaster &r = bufs.at(K.out_rasters[k]);
-      uint64_t p = (uint64_t)(uintptr_t)r.ptr;
-      int64_t pitch = r.pitch;
-      std::memcpy(a.data() + K.off_out + 16 * k, &p, 8);
-      std::memcpy(a.data() + K.off_out + 16 * k + 8, &pitch, 8);
-    }
-    for (size_t k = 0; k < K.scalars.size(); k++) {
-      Node *s = K.scalars[k];
-      if (!s->has_value) throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
-      Variant v = var_convert(s->value, s->meta.dtype);
-      std::memcpy(a.data() + K.off_s + 8 * k, &v.u, dt_size(v.dtype));
-    }
-    int32_t geom[12] = {g.W, g.H, g.BS0, g.BS1, rx0, ry0, rx1, ry1, 0, 0, rt.border, 0};
-    const int tx = (rx1 - rx0 + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
-    geom[8] = tx;
-    geom[9] = tx * ty;
-    std::memcpy(a.data() + K.off_geom, geom, sizeof geom);
-    uint64_t errp = (uint64_t)(uintptr_t)env.err_word();
-    std::memcpy(a.data() + K.off_err, &errp, 8);
     uint64_t aux[4] = {aux0, aux1, 0, 0};
-    std::memcpy(a.data() + K.off_aux, aux, sizeof aux);
-    return a;
+    return pack_args(g, K, get, bufs, rx0, ry0, rx1, ry1, aux);
   };
 
   auto ensure_outputs = [&](const Group &g, const KernelPlan &K) {

@@ -15,7 +15,9 @@
 #include "codegen.hpp"
 #include "fusion.hpp"
 
+#include <functional>
 #include <map>
+#include <unordered_map>
 #include <memory>
 #include <set>
 #include <string>
@@ -49,6 +51,12 @@ struct PlainJob {
 // Plain-mode launch order for the given groups (pure host logic).
 std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &groups,
                                      const std::vector<KernelPlan> &plans);
+
+// Packs the kernel argument struct of plan K for a launch over region
+// [rx0,rx1) x [ry0,ry1); rasters are looked up with `get` (inputs) and in `bufs` (outputs).
+std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
+                                     std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
+                                     const uint64_t aux[4]);
 
 struct EvalStats {
   int launches = 0;

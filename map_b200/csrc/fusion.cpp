@@ -95,8 +95,13 @@ FusionResult fuse(const std::vector<Node *> &order, const std::set<Node *> &targ
   std::unordered_set<Node *> materialise;
   for (Node *n : order) {
     if (!needs_materialised_arg(n)) continue;
-    for (Node *p : n->prev)
+    for (size_t j = 0; j < n->prev.size(); j++) {
+      Node *p = n->prev[j];
+      // a spread scan reads its water at the cell itself; only the directions
+      // are read over the neighbourhood
+      if (n->pattern == P_SPREAD && j == 0) continue;
       if (is_free_raster(p)) materialise.insert(p);
+    }
   }
   for (Node *t : targets)
     if (is_free_raster(t)) materialise.insert(t);

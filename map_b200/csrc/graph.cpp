@@ -351,7 +351,7 @@ Node *Runtime::zonal_reduc(Node *arg, int red) {
   return add(std::move(n), "Z|" + std::to_string(red) + "|" + pid(arg));
 }
 
-Node *Runtime::radial_scan(Node *arg, int red, Arr2 start) {
+Node *Runtime::radial_scan(Node *arg, int red, Arr2 start, double radius) {
   check_focal_arg(arg, "radialScan");
   reduction_name(red);
   if (start.n != 2) throw MapError("radialScan: start must have 2 components");
@@ -362,10 +362,12 @@ Node *Runtime::radial_scan(Node *arg, int red, Arr2 start) {
   n->kind = K_RADIALSCAN;
   n->pattern = P_RADIAL;
   n->op = red;
+  if (radius < 0) throw MapError("radialScan: negative radius");
   n->coord = start;
+  n->radius = radius;
   n->meta = arg->meta;
   n->prev = {arg};
-  return add(std::move(n), "RAD|" + std::to_string(red) + "|" + arr_str(start) + "|" + pid(arg));
+  return add(std::move(n), "RAD|" + std::to_string(red) + "|" + arr_str(start) + "|" + std::to_string(radius) + "|" + pid(arg));
 }
 
 Node *Runtime::spread_scan(Node *arg, Node *dir, int red) {

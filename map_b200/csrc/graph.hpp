@@ -64,6 +64,7 @@ struct Node {
   std::vector<Variant> mask;   // focal mask, row-major (mask_ds.arr[0] columns)
   Arr2 mask_ds{{-1, -1}, 0};
   Arr2 coord{{0, 0}, 2};       // neighbour offset / radial start
+  double radius = 0;           // radial scan: fronts farther than this are not swept (0 = all)
   std::string path;            // read / write path
   std::shared_ptr<HostData> host;
   std::shared_ptr<DevData> dev;
@@ -106,7 +107,7 @@ struct Runtime {
   Node *focal_func(Node *arg, const Variant *mask, int n, Arr2 mask_ds, int red);
   Node *focal_flow(Node *arg);
   Node *zonal_reduc(Node *arg, int red);
-  Node *radial_scan(Node *arg, int red, Arr2 start);
+  Node *radial_scan(Node *arg, int red, Arr2 start, double radius = 0);
   Node *spread_scan(Node *arg, Node *dir, int red);
   Node *barrier(Node *arg);
   Node *write(Node *arg, const std::string &path);

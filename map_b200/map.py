@@ -522,19 +522,27 @@ def zmin(raster):
     return Raster(_lib.ma_zonalReduc(raster, MIN))
 
 
-def rsum(raster, coord):
+def rsum(raster, coord, radius=None):
+    if radius:
+        return Raster(_lib.ma_radialScanRadius(raster, SUM, Array(coord), float(radius)))
     return Raster(_lib.ma_radialScan(raster, SUM, Array(coord)))
 
 
-def rprod(raster, coord):
+def rprod(raster, coord, radius=None):
+    if radius:
+        return Raster(_lib.ma_radialScanRadius(raster, PROD, Array(coord), float(radius)))
     return Raster(_lib.ma_radialScan(raster, PROD, Array(coord)))
 
 
-def rmax(raster, coord):
+def rmax(raster, coord, radius=None):
+    if radius:
+        return Raster(_lib.ma_radialScanRadius(raster, MAX, Array(coord), float(radius)))
     return Raster(_lib.ma_radialScan(raster, MAX, Array(coord)))
 
 
-def rmin(raster, coord):
+def rmin(raster, coord, radius=None):
+    if radius:
+        return Raster(_lib.ma_radialScanRadius(raster, MIN, Array(coord), float(radius)))
     return Raster(_lib.ma_radialScan(raster, MIN, Array(coord)))
 
 
@@ -825,6 +833,7 @@ _sig('ma_focalFunc', [Raster, ct.POINTER(Variant), ct.c_int, Array, ct.c_int], N
 _sig('ma_zonalReduc', [Raster, ct.c_int], Node)
 _sig('ma_radialScan', [Raster, ct.c_int, Array], Node)
 _sig('ma_spreadScan', [Raster, Raster, ct.c_int], Node)
+_sig('ma_radialScanRadius', [Raster, ct.c_int, Array, ct.c_double], Node)
 _sig('ma_barrier', [Raster], Node)
 _sig('ma_loopStart', [], None)
 _sig('ma_loopCond', [Raster], None)

@@ -11,38 +11,45 @@ golden vectors; see oracle/oracle.c.
 """
 import ctypes as ct
 import os
+import threading
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _lib = None
 _ref = None
+_lock = threading.Lock()
 
 
 def lib():
     global _lib
-    if _lib is None:
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
         path = os.path.join(HERE, "_build", "liboracle.so")
         if not os.path.exists(path):
             raise RuntimeError("oracle library missing: run `python oracle/build_oracle.py`")
-        _lib = ct.CDLL(path)
+        L = ct.CDLL(path)
         f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
         f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
         u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
         i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
         I = ct.c_int
-        _lib.orc_conv_f32.argtypes = [f32p, I, I, I, I, I, f32p, I, I, f32p]
-        _lib.orc_hillshade_f32.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f32p, ct.c_void_p, ct.c_void_p]
-        _lib.orc_hillshade_f64.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f64p]
-        _lib.orc_life.argtypes = [u8p, I, I, I, I, I, I, u8p]
-        _lib.orc_rand_u8.argtypes = [ct.c_uint32, I, I, I, I, u8p]
-        _lib.orc_d8.argtypes = [f32p, I, I, I, I, I, u8p]
-        _lib.orc_flowacc_s32.argtypes = [i32p, u8p, I, I, i32p]
-        _lib.orc_flowacc_s32.restype = ct.c_int
-        _lib.orc_radial_f32.argtypes = [f32p, I, I, I, I, I, f32p]
-        _lib.orc_wsum_f32.argtypes = [ct.POINTER(ct.c_void_p), f32p, I, ct.c_size_t, f32p]
-        _lib.orc_focal_src.argtypes = [I, I, I, I, I, I, I, I, I, ct.POINTER(I), ct.POINTER(I)]
-        _lib.orc_focal_src.restype = I
+        L.orc_conv_f32.argtypes = [f32p, I, I, I, I, I, f32p, I, I, f32p]
+        L.orc_hillshade_f32.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f32p, ct.c_void_p, ct.c_void_p]
+        L.orc_hillshade_f64.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f64p]
+        L.orc_life.argtypes = [u8p, I, I, I, I, I, I, u8p]
+        L.orc_rand_u8.argtypes = [ct.c_uint32, I, I, I, I, u8p]
+        L.orc_d8.argtypes = [f32p, I, I, I, I, I, u8p]
+        L.orc_flowacc_s32.argtypes = [i32p, u8p, I, I, i32p]
+        L.orc_flowacc_s32.restype = ct.c_int
+        L.orc_radial_f32.argtypes = [f32p, I, I, I, I, I, f32p]
+        L.orc_wsum_f32.argtypes = [ct.POINTER(ct.c_void_p), f32p, I, ct.c_size_t, f32p]
+        L.orc_focal_src.argtypes = [I, I, I, I, I, I, I, I, I, ct.POINTER(I), ct.POINTER(I)]
+        L.orc_focal_src.restype = I
+        _lib = L
     return _lib
 
 

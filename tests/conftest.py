@@ -1,5 +1,6 @@
 """Shared test setup: builds the native library and the oracle (incremental),
 registers the `gpu` marker and puts the packages on sys.path."""
+import faulthandler
 import os
 import sys
 
@@ -9,6 +10,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 PKG = os.path.join(ROOT, "map_b200")
+
+
+faulthandler.enable()
 
 
 def pytest_configure(config):
