@@ -97,6 +97,9 @@ struct Gen {
   std::map<Node *, int> staged;   // focal-read raster input -> staging slot
   std::map<Node *, int> outk;     // output raster -> a.out[k]
   std::set<Node *> center_read;   // raster inputs read at the centre cell
+  std::map<Node *, std::string> literal;   // scalar constants written into the source
+  std::set<Node *> sincos_first;  // float sin/cos pairs on one argument: emitted once with sincosf
+  std::map<Node *, Node *> sincos_mate;
 
   Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
 
@@ -105,6 +108,8 @@ struct Gen {
   std::string val(Node *p) const {
     auto m = member.find(p);
     if (m != member.end()) return "v" + std::to_string(m->second);
+    auto l = literal.find(p);
+    if (l != literal.end()) return l->second;
     auto s = sca.find(p);
     if (s != sca.end()) return "a.s[" + std::to_string(s->second) + "]." + scalar_field(p->meta.dtype);
     auto r = rin.find(p);
@@ -121,7 +126,12 @@ struct Gen {
   void classify() {
     for (size_t i = 0; i < g.nodes.size(); i++) member[g.nodes[i]] = (int)i;
     for (Node *in : g.inputs) {
-      if (in->meta.numdim == D0) {
+      if (in->meta.numdim == D0 && in->kind == K_CONSTANT) {
+        // Scalar constants are part of the kernel's signature (as constant values
+        // are part of the reference's Version signature, runtime/dag/Constant.cpp),
+        // so the device compiler folds them (x / 8 becomes an exact multiply).
+        literal[in] = "((" + std::string(dt_ctype(in->meta.dtype)) + ")" + var_literal(in->cnst) + ")";
+      } else if (in->meta.numdim == D0) {
         sca[in] = (int)plan.scalars.size();
         plan.scalars.push_back(in);
       } else {
@@ -151,6 +161,20 @@ struct Gen {
       outk[o] = (int)plan.out_rasters.size();
       plan.out_rasters.push_back(o);
     }
+    // sin(x) and cos(x) of the same float argument share one sincosf call
+    for (Node *n : g.nodes) {
+      if (n->kind != K_UNARY || (n->op != SIN && n->op != COS) || n->meta.dtype != F32) continue;
+      if (sincos_mate.count(n)) continue;
+      for (Node *m : g.nodes) {
+        if (m == n || m->kind != K_UNARY || m->prev[0] != n->prev[0] || sincos_mate.count(m)) continue;
+        if ((n->op == SIN && m->op == COS) || (n->op == COS && m->op == SIN)) {
+          sincos_mate[n] = m;
+          sincos_mate[m] = n;
+          sincos_first.insert(n->id < m->id ? n : m);
+          break;
+        }
+      }
+    }
   }
 
   // ---- per-node statements
@@ -174,7 +198,7 @@ struct Gen {
         s << "philox2x32_10(" << c0 << ", " << c1 << ", " << k << "); ";
         if (dt == F32) s << "const float " << v << " = (float)" << c0 << " / 4294967296.0f;";
         else if (dt_size(dt) <= 4 && dt != B8)
-          s << t << " " << v << "; __builtin_memcpy(&" << v << ", &" << c0 << ", sizeof(" << t << "));";
+          s << "const " << t << " " << v << " = bit_cast8<" << t << ">(" << c0 << ");";
         else throw MapError("rand: unsupported output type");
         break;
       }
@@ -195,6 +219,15 @@ struct Gen {
           default: {
             const char *fn = unary_fn(n->op);
             if (!fn) throw MapError("codegen: invalid unary op");
+            auto mate = sincos_mate.find(n);
+            if (mate != sincos_mate.end()) {
+              if (sincos_first.count(n)) {
+                Node *sn = n->op == SIN ? n : mate->second, *cn = n->op == COS ? n : mate->second;
+                s << "float v" << member.at(sn) << ", v" << member.at(cn) << "; sincosf(" << p << ", &v" << member.at(sn)
+                  << ", &v" << member.at(cn) << ");";
+              }
+              break;
+            }
             if (dt_is_float(pdt)) {
               s << "const " << t << " " << v << " = " << float_fn(pdt, fn) << "(" << p << ");";
             } else if (n->op == ABS) {
@@ -347,54 +380,64 @@ std::string fnv_hex(const std::string &s) {
   return b;
 }
 
-const int TW = 64, TH = 32, NT = 256;
-
 }  // namespace
 
-static std::string gen_local(Gen &G) {
+// Local skeleton (runtime/skeleton/LocalSkeleton.cpp:31-180): a tile of TW x TH
+// cells per CTA of NT threads; each thread owns TH*TW/NT cells of one column,
+// issues all of its input loads first (memory-level parallelism), then
+// evaluates the fused expression and stores the outputs.
+static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap) {
   KernelPlan &P = G.plan;
-  std::ostringstream s;
-  s << "#include \"map_common.cuh\"\n";
-  s << G.args_struct(0, false);
-  s << "struct In {\n";
-  for (Node *p : P.in_rasters) s << "  " << G.T(p) << " i" << G.rin.at(p) << ";\n";
-  s << "  int dummy;\n};\n";
-  s << "__device__ __forceinline__ void load_cell(const Args &a, In &in, int x, int y) {\n";
+  const int TW = P.tile_w, TH = P.tile_h, NT = P.threads, R = TH * TW / NT;
+  body << G.args_struct(0, false);
+  body << "struct In {\n";
+  for (Node *p : P.in_rasters) body << "  " << G.T(p) << " i" << G.rin.at(p) << ";\n";
+  body << "  int dummy;\n};\n";
+  body << "__device__ __forceinline__ void load_cell(const Args &a, In &in, int x, int y) {\n";
   for (Node *p : P.in_rasters) {
     int k = G.rin.at(p);
-    s << "  in.i" << k << " = ldr<" << G.T(p) << ">(a.in[" << k << "], x, y);\n";
+    body << "  in.i" << k << " = ldr<" << G.T(p) << ">(a.in[" << k << "], x, y);\n";
   }
-  s << "}\n";
-  s << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
-  s << G.center_loads(true) << G.body(false) << G.stores() << "}\n";
-  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
-    << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, blockIdx.x);\n"
-    << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
-    << "  const int x = t.x0 + lx;\n"
-    << "  In in[" << TH * TW / NT << "];\n"
-    << "#pragma unroll\n"
-    << "  for (int k = 0; k < " << TH * TW / NT << "; ++k) {\n"
-    << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
-    << "    if (x < t.xe && y < t.ye) load_cell(a, in[k], x, y);\n"
-    << "  }\n"
-    << "#pragma unroll\n"
-    << "  for (int k = 0; k < " << TH * TW / NT << "; ++k) {\n"
-    << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
-    << "    if (x < t.xe && y < t.ye) compute_cell(a, in[k], x, y);\n"
-    << "  }\n"
-    << "}\n";
-  return s.str();
+  body << "}\n";
+  body << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
+  body << G.center_loads(true) << G.body(false) << G.stores() << "}\n";
+  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase) {\n"
+       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
+       << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+       << "  const int x = t.x0 + lx;\n"
+       << "  In in[" << R << "];\n"
+       << "#pragma unroll\n"
+       << "  for (int k = 0; k < " << R << "; ++k) {\n"
+       << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
+       << "    if (x < t.xe && y < t.ye) load_cell(a, in[k], x, y);\n"
+       << "  }\n"
+       << "#pragma unroll\n"
+       << "  for (int k = 0; k < " << R << "; ++k) {\n"
+       << "    const int y = t.y0 + ly0 + k * " << NT / TW << ";\n"
+       << "    if (x < t.xe && y < t.ye) compute_cell(a, in[k], x, y);\n"
+       << "  }\n"
+       << "  return true;\n"
+       << "}\n";
+  wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+       << "  u32 phase = 0;\n"
+       << "  run_tile(a, blockIdx.x, nullptr, nullptr, phase);\n"
+       << "}\n";
 }
 
-static std::string gen_focal(Gen &G) {
+// Focal skeleton (runtime/skeleton/FocalSkeleton.cpp:37-274). A tile whose halo
+// lies inside the raster is staged into shared memory by one 2-D TMA load per
+// focal input (box TW + 2*pad_x by TH + 2*halo, x start rounded down to a
+// 16-byte boundary), completion tracked by an mbarrier with a bounded wait; the
+// taps then read shared memory. Tiles that touch the raster edge read their taps
+// straight from global memory through the border rule (GatherTap), which also
+// carries the reference's block-relative mirror.
+static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap) {
   KernelPlan &P = G.plan;
+  const int TW = P.tile_w, TH = P.tile_h, NT = P.threads;
   const int hx = P.halo_x, hy = P.halo_y;
-  std::ostringstream s;
-  s << "#include \"map_common.cuh\"\n";
   const int nst = (int)G.staged.size();
   std::vector<Node *> staged_nodes(nst);
   for (auto &kv : G.staged) staged_nodes[kv.second] = kv.first;
-  // staging geometry: the box starts at x0 - pad_x, pad_x = halo rounded up to 16 bytes of elements
   size_t off = 0;
   for (int k = 0; k < nst; k++) {
     Node *in = staged_nodes[k];
@@ -404,7 +447,6 @@ static std::string gen_focal(Gen &G) {
     int es = (int)dt_size(t.dtype);
     int align_e = 16 / es;
     t.pad_x = ((hx + align_e - 1) / align_e) * align_e;
-    if (t.pad_x == 0) t.pad_x = 0;
     t.box_w = TW + 2 * t.pad_x;
     t.box_h = TH + 2 * hy;
     off = (off + 127) / 128 * 128;
@@ -415,23 +457,23 @@ static std::string gen_focal(Gen &G) {
   }
   off = (off + 15) / 16 * 16;
   const size_t bar_off = off;
-  P.smem_bytes = off + 16;
-  const bool use_tma = nst > 0 && hx <= 16 && hy <= 16;
-  s << G.args_struct(nst, false);
-  // cell function, templated on the tap providers of the staged rasters
-  s << "template <";
-  for (int k = 0; k < nst; k++) s << (k ? ", " : "") << "class F" << k;
-  s << ">\n__device__ __forceinline__ void focal_cell(const Args &a";
-  for (int k = 0; k < nst; k++) s << ", const F" << k << " &f" << k;
-  s << ", int x, int y, int lx, int ly) {\n";
-  s << G.center_loads(false) << G.body(false) << G.stores() << "}\n";
-  auto call = [&](void) {
-    std::ostringstream c;
-    c << "focal_cell(a";
-    for (int k = 0; k < nst; k++) c << ", f" << k;
-    c << ", x, y, lx, ly)";
-    return c.str();
-  };
+  bool use_tma = nst > 0 && hx <= 16 && hy <= 16;
+  for (auto &t : P.tma)
+    if (t.box_w > 256 || t.box_h > 256) use_tma = false;
+  if (use_tma && off + 16 > 200 * 1024) use_tma = false;
+  P.smem_bytes = use_tma ? off + 16 : 0;
+  P.bar_off = bar_off;
+  body << G.args_struct(use_tma ? nst : 0, false);
+  body << "template <";
+  for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
+  body << ">\n__device__ __forceinline__ void focal_cell(const Args &a";
+  for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
+  body << ", int x, int y, int lx, int ly) {\n";
+  body << G.center_loads(false) << G.body(false) << G.stores() << "}\n";
+  std::ostringstream call;
+  call << "focal_cell(a";
+  for (int k = 0; k < nst; k++) call << ", f" << k;
+  call << ", x, y, lx, ly)";
   const int rows = TH * TW / NT, rstep = NT / TW;
   std::ostringstream loop;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
@@ -439,52 +481,61 @@ static std::string gen_focal(Gen &G) {
        << "#pragma unroll 2\n"
        << "    for (int k = 0; k < " << rows << "; ++k) {\n"
        << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
-       << "      if (x < t.xe && y < t.ye) " << call() << ";\n"
+       << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n"
        << "    }\n";
-  s << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
-    << "  extern __shared__ __align__(128) unsigned char smem[];\n"
-    << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, blockIdx.x);\n";
+  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase) {\n"
+       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n";
   if (use_tma) {
-    s << "  if (tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ")) {\n"
-      << "    u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
-      << "    if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
-      << "    __syncthreads();\n"
-      << "    if (threadIdx.x == 0) {\n";
     size_t total = 0;
     for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
-    s << "      mbar_arrive_expect_tx(bar, " << total << "u);\n";
+    body << "  if (tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ")) {\n"
+         << "    __syncthreads();   // earlier readers of the staging buffer are done\n"
+         << "    if (threadIdx.x == 0) {\n"
+         << "      fence_proxy_async();\n"
+         << "      mbar_arrive_expect_tx(bar, " << total << "u);\n";
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
-      s << "      tma_load_2d(smem + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
-        << ");\n";
+      body << "      tma_load_2d(smem + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
+           << ");\n";
     }
-    s << "    }\n"
-      << "    if (!mbar_wait_bounded(bar, 0, 1u << 26)) {\n"
-      << "      skel_fail(a.err, ERR_TMA_TIMEOUT);\n"
-      << "      mbar_wait_bounded(bar, 0, 1u << 26);\n"
-      << "      return;\n"
-      << "    }\n";
+    body << "    }\n"
+         << "    if (!mbar_wait_bounded(bar, phase, 1u << 26)) {\n"
+         << "      skel_fail(a.err, ERR_TMA_TIMEOUT);\n"
+         << "      mbar_wait_bounded(bar, phase, 1u << 26);\n"
+         << "      return false;\n"
+         << "    }\n"
+         << "    phase ^= 1u;\n";
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
       std::string ty = dt_ctype(t.dtype);
-      s << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
-        << " *)(smem + " << t.smem_off << ")};\n";
+      body << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
+           << " *)(smem + " << t.smem_off << ")};\n";
     }
-    s << loop.str() << "  } else {\n";
-  } else {
-    s << "  {\n";
+    body << loop.str() << "    return true;\n  }\n";
   }
+  body << "  {\n";
   for (int k = 0; k < nst; k++) {
     std::string ty = G.T(staged_nodes[k]);
-    s << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
+    body << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
   }
-  s << loop.str() << "  }\n}\n";
-  if (!use_tma) { P.tma.clear(); P.smem_bytes = 0; }
-  return s.str();
+  body << loop.str() << "  }\n  return true;\n}\n";
+  wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+       << "  extern __shared__ __align__(128) unsigned char smem[];\n"
+       << "  u32 phase = 0;\n";
+  if (use_tma)
+    wrap << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
+         << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
+         << "  __syncthreads();\n"
+         << "  run_tile(a, blockIdx.x, smem, bar, phase);\n";
+  else
+    wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase);\n";
+  wrap << "}\n";
+  if (!use_tma) P.tma.clear();
 }
 
 static std::string gen_zonal(Gen &G) {
   KernelPlan &P = G.plan;
+  const int TW = P.tile_w, TH = P.tile_h, NT = P.threads;
   std::ostringstream s;
   s << "#include \"map_common.cuh\"\n";
   s << G.args_struct(0, true);
@@ -678,19 +729,26 @@ static std::string gen_spread(Gen &G) {
   return s.str();
 }
 
-KernelPlan generate_kernel(const Group &g) {
+bool tile_cfg_valid(const TileCfg &c) {
+  return c.tw > 0 && c.th > 0 && c.nt >= 32 && c.nt <= 1024 && c.nt % 32 == 0 && c.nt % c.tw == 0 &&
+         (c.tw * c.th) % c.nt == 0 && c.tw <= c.nt && c.tw <= 224 && c.th <= 224;
+}
+
+KernelPlan generate_kernel(const Group &g, TileCfg cfg) {
+  if (!tile_cfg_valid(cfg)) throw MapError("codegen: invalid tile configuration");
   KernelPlan P;
   P.skeleton = g.skeleton;
-  P.threads = NT;
-  P.tile_w = TW;
-  P.tile_h = TH;
+  P.threads = cfg.nt;
+  P.tile_w = cfg.tw;
+  P.tile_h = cfg.th;
   Gen G(g, P);
   G.classify();
   std::string src;
   const char *prefix = "map_local";
+  std::ostringstream body, wrap;
   switch (g.skeleton) {
-    case SK_LOCAL: src = gen_local(G); prefix = "map_local"; break;
-    case SK_FOCAL: src = gen_focal(G); prefix = "map_focal"; break;
+    case SK_LOCAL: gen_local(G, body, wrap); prefix = "map_local"; break;
+    case SK_FOCAL: gen_focal(G, body, wrap); prefix = "map_focal"; break;
     case SK_ZONAL: src = gen_zonal(G); prefix = "map_zonal"; break;
     case SK_RADIAL: case SK_SPREAD:
       for (Node *n : g.nodes)
@@ -699,6 +757,10 @@ KernelPlan generate_kernel(const Group &g) {
       else { src = gen_spread(G); prefix = "map_spread"; }
       break;
     default: throw MapError("codegen: group has no device skeleton");
+  }
+  if (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL) {
+    P.body = body.str();
+    src = "#include \"map_common.cuh\"\n" + P.body + wrap.str();
   }
   std::string name = std::string(prefix) + "_" + fnv_hex(src).substr(0, 12);
   size_t pos;

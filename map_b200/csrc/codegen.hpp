@@ -25,9 +25,17 @@ struct TmaSpec {
   size_t smem_off = 0;  // offset of the staged tile in dynamic shared memory
 };
 
+// Tile shape of the Local / Focal / Zonal skeletons: TW x TH cells per CTA of NT threads.
+struct TileCfg {
+  int tw = 64, th = 32, nt = 256;
+};
+bool tile_cfg_valid(const TileCfg &c);
+
 struct KernelPlan {
   int skeleton = SK_LOCAL;
   std::string source;
+  std::string body;         // group code without include and kernel wrapper (Local / Focal), for batching
+  size_t bar_off = 0;       // Focal: offset of the TMA mbarrier in dynamic shared memory
   std::string kname;        // main kernel
   std::string kname_final;  // zonal finalisation kernel (empty otherwise)
   size_t args_size = 0;
@@ -48,7 +56,7 @@ struct KernelPlan {
   Node *core = nullptr;
 };
 
-KernelPlan generate_kernel(const Group &g);
+KernelPlan generate_kernel(const Group &g, TileCfg cfg = TileCfg());
 
 // Reference float-constant rounding: constants written into kernel text by the
 // reference go through std::to_string ("%f", six decimals) before the device

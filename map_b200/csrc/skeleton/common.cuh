@@ -196,28 +196,25 @@ template <class T> struct RedOp<4, T> { __device__ static T f(T a, T b) { return
 template <class T> struct RedOp<6, T> { __device__ static T f(T a, T b) { return red_max<T>(a, b); } };
 template <class T> struct RedOp<7, T> { __device__ static T f(T a, T b) { return red_min<T>(a, b); } };
 
+// Reinterprets the bytes of a value as another type of at most 8 bytes.
+template <class To, class From> __device__ __forceinline__ To bit_cast8(From v) {
+  union { From f; To t; u64 raw; } u;
+  u.raw = 0;
+  u.f = v;
+  return u.t;
+}
+
 template <class T> __device__ __forceinline__ T shfl_xor_any(T v, int m) {
   if constexpr (sizeof(T) == 8) {
-    u64 b;
-    __builtin_memcpy(&b, &v, 8);
+    u64 b = bit_cast8<u64>(v);
     u32 lo = (u32)b, hi = (u32)(b >> 32);
     lo = __shfl_xor_sync(0xffffffffu, lo, m);
     hi = __shfl_xor_sync(0xffffffffu, hi, m);
-    b = ((u64)hi << 32) | lo;
-    __builtin_memcpy(&v, &b, 8);
-    return v;
-  } else if constexpr (sizeof(T) == 4) {
-    u32 b;
-    __builtin_memcpy(&b, &v, 4);
-    b = __shfl_xor_sync(0xffffffffu, b, m);
-    __builtin_memcpy(&v, &b, 4);
-    return v;
+    return bit_cast8<T>(((u64)hi << 32) | lo);
   } else {
-    u32 b = 0;
-    __builtin_memcpy(&b, &v, sizeof(T));
+    u32 b = bit_cast8<u32>(v);
     b = __shfl_xor_sync(0xffffffffu, b, m);
-    __builtin_memcpy(&v, &b, sizeof(T));
-    return v;
+    return bit_cast8<T>(b);
   }
 }
 
@@ -227,29 +224,15 @@ template <int OP, class T> __device__ __forceinline__ T block_reduce(T v, Scalar
   for (int m = 16; m > 0; m >>= 1) v = RedOp<OP, T>::f(v, shfl_xor_any<T>(v, m));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = (blockDim.x + 31) >> 5;
   __syncthreads();
-  if (lane == 0) __builtin_memcpy(&scratch[warp], &v, sizeof(T));
+  if (lane == 0) scratch[warp].raw = bit_cast8<u64>(v);
   __syncthreads();
-  T r;
-  __builtin_memcpy(&r, &scratch[0], sizeof(T));
-  for (int w = 1; w < nw; ++w) {
-    T o;
-    __builtin_memcpy(&o, &scratch[w], sizeof(T));
-    r = RedOp<OP, T>::f(r, o);
-  }
+  T r = bit_cast8<T>(scratch[0].raw);
+  for (int w = 1; w < nw; ++w) r = RedOp<OP, T>::f(r, bit_cast8<T>(scratch[w].raw));
   return r;
 }
 
-template <class T> __device__ __forceinline__ void put_scalar(Scalar8 *dst, T v) {
-  Scalar8 s;
-  s.raw = 0;
-  __builtin_memcpy(&s, &v, sizeof(T));
-  *dst = s;
-}
-template <class T> __device__ __forceinline__ T get_scalar(const Scalar8 &s) {
-  T v;
-  __builtin_memcpy(&v, &s, sizeof(T));
-  return v;
-}
+template <class T> __device__ __forceinline__ void put_scalar(Scalar8 *dst, T v) { dst->raw = bit_cast8<u64>(v); }
+template <class T> __device__ __forceinline__ T get_scalar(const Scalar8 &s) { return bit_cast8<T>(s.raw); }
 
 // ------------------------------------------------------------------ Philox2x32-10
 

@@ -109,3 +109,34 @@ def test_focal_variants_compile(M):
             M.convolve(d, [[1] * 5] * 5), M.fmin(d, [[1] * 3] * 3), M.fmax(u, [[1] * 5] * 3), d([1, -1]) - d([0, 2]),
             M.flow_direction(d), M.convolve(u, [[1, 1, 1], [1, 0, 1], [1, 1, 1]])]
     assert M.compile_only(*outs) >= 1
+
+
+def test_every_skeleton_compiles(M):
+    """Zonal, radiating, spreading, rand and host-scalar programs generate
+    kernels that NVRTC compiles for sm_100a."""
+    dem = M.from_numpy(np.ones((40, 50), np.float32), bs=[32, 32])
+    s = W.stats(dem)
+    assert M.compile_only(*s.values()) == 2
+    assert M.compile_only(W.life_initial([50, 40], [32, 32])) == 1
+    v = W.viewshed(dem, [10, 20], 5.0)
+    soft = M.convolve(v, [[1.0 / 16, 1.0 / 8, 1.0 / 16], [1.0 / 8, 1.0 / 4, 1.0 / 8], [1.0 / 16, 1.0 / 8, 1.0 / 16]])
+    out = M.con(soft < 0.1, dem, M.zeros_like(dem))
+    assert M.compile_only(out) >= 2
+    d = M.flow_direction(dem)
+    assert M.compile_only(M.flow_accumulation(M.ones_like(dem, M.S32), d)) == 2
+    i64 = M.from_numpy(np.ones((8, 8), np.int64))
+    assert M.compile_only(M.zsum(i64), M.zmax(M.from_numpy(np.ones((8, 8), np.uint8)))) == 2
+
+
+def test_scalar_constants_become_literals(M):
+    dem = M.from_numpy(np.zeros((16, 16), np.float32))
+    src = M.generated_source(dem / 8 + 1.5)
+    assert "a.s[" not in src and "/ ((s32)8)" in src
+
+
+def test_sin_cos_pairs_share_sincosf(M):
+    dem = M.from_numpy(np.zeros((16, 16), np.float32))
+    x = M.atan(dem)
+    src = M.generated_source(M.sin(x) * 2.0 + M.cos(x))
+    import re
+    assert "sincosf(" in src and not re.search(r"\bsinf\(", src) and not re.search(r"\bcosf\(", src)
