@@ -145,6 +145,23 @@ void *ma_devAlloc(size_t bytes);
 void ma_devFree(void *p);
 int ma_memcpy(void *dst, const void *src, size_t bytes, int kind); /* kind as cudaMemcpyKind */
 
+/* Batched persistent execution: many programs (e.g. one script over hundreds
+ * of rasters of uneven size) run as one persistent kernel per dependency level,
+ * driven by a device work-list of (kernel kind, instance, tile) items and
+ * replayed from a CUDA graph. Only Local and Focal groups can be batched; inputs
+ * must be device-resident, host or file rasters; outputs go to caller device
+ * buffers (16-byte aligned base and pitch).
+ * ma_batchAdd returns the instance index; ma_batchPrepare fuses, autotunes tile
+ * shapes (autotune != 0), compiles and captures the graph (called by the first
+ * ma_batchRun when omitted); ma_batchInfo writes a JSON description. */
+typedef struct ma_Batch ma_Batch;
+ma_Batch *ma_batchCreate(void);
+int ma_batchAdd(ma_Batch *b, ma_Node **outs, int num, void **dst, const long long *pitch);
+int ma_batchPrepare(ma_Batch *b, int autotune);
+int ma_batchRun(ma_Batch *b, int sync);
+size_t ma_batchInfo(ma_Batch *b, char *buf, size_t len);
+void ma_batchDestroy(ma_Batch *b);
+
 /* Introspection for tests and tools. */
 int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
 int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */

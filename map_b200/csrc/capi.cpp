@@ -2,6 +2,7 @@
 // (front/bindings.cpp:14-273) plus the extensions documented in the header.
 // Every entry point converts C++ exceptions into a recorded error.
 #include "../../include/map_b200.h"
+#include "batch.hpp"
 #include "codegen.hpp"
 #include "cuda_env.hpp"
 #include "executor.hpp"
@@ -498,6 +499,72 @@ size_t ma_plainSchedule(ma_Node **vec, int num, char *buf, size_t len) {
     fail(e.what());
     return 0;
   }
+}
+
+// ---- batches
+
+struct ma_Batch {
+  Batch b;
+  std::vector<Node *> held;   // output nodes kept alive while the batch exists
+};
+
+ma_Batch *ma_batchCreate(void) {
+  try {
+    ok();
+    return new ma_Batch();
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+
+int ma_batchAdd(ma_Batch *b, ma_Node **outs, int n, void **dst, const long long *pitch) {
+  return int_call([&] {
+    if (!b) throw MapError("batch: null handle");
+    std::vector<Node *> o = node_vec(outs, n);
+    std::vector<void *> d(dst, dst + n);
+    std::vector<long long> p(pitch, pitch + n);
+    b->b.add(o, d, p);
+    for (Node *x : o) {
+      x->ref++;
+      b->held.push_back(x);
+    }
+    return b->b.instances() - 1;
+  });
+}
+
+int ma_batchPrepare(ma_Batch *b, int autotune) {
+  return int_call([&] {
+    if (!b) throw MapError("batch: null handle");
+    b->b.prepare(autotune != 0);
+    return 0;
+  });
+}
+
+int ma_batchRun(ma_Batch *b, int sync) {
+  return int_call([&] {
+    if (!b) throw MapError("batch: null handle");
+    b->b.run(sync != 0);
+    return 0;
+  });
+}
+
+size_t ma_batchInfo(ma_Batch *b, char *buf, size_t len) {
+  try {
+    if (!b) throw MapError("batch: null handle");
+    ok();
+    return copy_out(b->b.info(), buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+void ma_batchDestroy(ma_Batch *b) {
+  if (!b) return;
+  for (Node *x : b->held)
+    if (Runtime::get().owns(x) && x->ref > 0) x->ref--;
+  delete b;
 }
 
 int ma_nodeCount(void) { return (int)Runtime::get().nodes.size(); }

@@ -32,6 +32,7 @@ typedef CUresult (*PFN_TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType,
                                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 typedef CUresult (*PFN_GetErrorString)(CUresult, const char **);
+typedef CUresult (*PFN_Occupancy)(int *, CUfunction, int, size_t);
 
 struct Driver {
   PFN_ModuleLoadData moduleLoadData = nullptr;
@@ -40,6 +41,7 @@ struct Driver {
   PFN_FuncSetAttribute funcSetAttribute = nullptr;
   PFN_TensorMapEncodeTiled tensorMapEncodeTiled = nullptr;
   PFN_GetErrorString getErrorString = nullptr;
+  PFN_Occupancy occupancy = nullptr;
 };
 
 Driver g_drv;
@@ -192,6 +194,7 @@ void CudaEnv::ensure_device() {
   load_entry(g_drv.funcSetAttribute, "cuFuncSetAttribute");
   load_entry(g_drv.tensorMapEncodeTiled, "cuTensorMapEncodeTiled");
   load_entry(g_drv.getErrorString, "cuGetErrorString");
+  load_entry(g_drv.occupancy, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaMalloc(&err_word_, sizeof(uint32_t)), "cudaMalloc(error word)");
   cuda_check(cudaMemset(err_word_, 0, sizeof(uint32_t)), "cudaMemset");
@@ -233,6 +236,12 @@ void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CU
                                reinterpret_cast<CUstream>(stream), params, nullptr),
             "cuLaunchKernel");
   launches_++;
+}
+
+int CudaEnv::occupancy(const KernelHandle &k, int block, size_t smem) {
+  int n = 0;
+  drv_check(g_drv.occupancy(&n, reinterpret_cast<CUfunction>(k.fn), block, smem), "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  return n;
 }
 
 void CudaEnv::encode_tma_2d(void *desc128, int dtype, const void *base, uint64_t width, uint64_t height, uint64_t pitch_bytes,

@@ -41,7 +41,9 @@ uint64_t spread_bits(uint32_t v) {
 // reference's Order interleaves (h, t, y, x) with x highest (runtime/Job.cpp:22-45).
 uint64_t morton3(uint32_t x, uint32_t y, uint32_t t) { return spread_bits(x) << 2 | spread_bits(y) << 1 | spread_bits(t); }
 
-std::vector<Node *> collect(const std::vector<Node *> &targets) {
+}  // namespace
+
+std::vector<Node *> collect_nodes(const std::vector<Node *> &targets) {
   std::unordered_set<Node *> seen;
   std::vector<Node *> st(targets.begin(), targets.end()), out;
   while (!st.empty()) {
@@ -54,6 +56,10 @@ std::vector<Node *> collect(const std::vector<Node *> &targets) {
   std::sort(out.begin(), out.end(), [](Node *a, Node *b) { return a->id < b->id; });
   return out;
 }
+
+namespace {
+
+std::vector<Node *> collect(const std::vector<Node *> &targets) { return collect_nodes(targets); }
 
 bool per_block(int sk) { return sk == SK_LOCAL || sk == SK_FOCAL || sk == SK_ZONAL; }
 

@@ -58,6 +58,9 @@ std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const 
                                      std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
                                      const uint64_t aux[4]);
 
+// Every node `targets` depend on (themselves included), in id (= topological) order.
+std::vector<Node *> collect_nodes(const std::vector<Node *> &targets);
+
 struct EvalStats {
   int launches = 0;
   int groups = 0;

@@ -869,3 +869,52 @@ _sig('ma_memcpy', [ct.c_void_p, ct.c_void_p, ct.c_size_t, ct.c_int], ct.c_int)
 _sig('ma_evalAsync', [ct.POINTER(Node), ct.c_int], ct.c_int)
 _sig('ma_totalLaunchCount', [], ct.c_int, check=False)
 _sig('ma_setDevice', [ct.c_int], None)
+
+
+class Batch:
+    """Batched persistent execution of many programs (see ma_batchAdd).
+
+    add(outputs, buffers) registers one program: `outputs` are rasters and
+    `buffers` (device pointer, pitch in bytes) receive them. run() launches
+    every registered program as one persistent kernel per dependency level."""
+
+    def __init__(self):
+        self._h = _lib.ma_batchCreate()
+        self._keep = []
+
+    def add(self, outputs, buffers):
+        n = len(outputs)
+        arr = _node_array(outputs)
+        dst = (ct.c_void_p * n)(*[b[0] for b in buffers])
+        pitch = (ct.c_longlong * n)(*[b[1] for b in buffers])
+        self._keep.append(outputs)
+        return _lib.ma_batchAdd(self._h, arr, n, dst, pitch)
+
+    def prepare(self, autotune=True):
+        _lib.ma_batchPrepare(self._h, 1 if autotune else 0)
+
+    def run(self, sync=True):
+        _lib.ma_batchRun(self._h, 1 if sync else 0)
+
+    def info(self):
+        import json
+        n = _lib.ma_batchInfo(self._h, None, 0)
+        buf = ct.create_string_buffer(n)
+        _lib.ma_batchInfo(self._h, buf, n)
+        return json.loads(buf.value.decode())
+
+    def __del__(self):
+        try:
+            if self._h:
+                _lib.ma_batchDestroy(self._h)
+                self._h = None
+        except Exception:
+            pass
+
+
+_sig('ma_batchCreate', [], ct.c_void_p)
+_sig('ma_batchAdd', [ct.c_void_p, ct.POINTER(Node), ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_longlong)], ct.c_int)
+_sig('ma_batchPrepare', [ct.c_void_p, ct.c_int], ct.c_int)
+_sig('ma_batchRun', [ct.c_void_p, ct.c_int], ct.c_int)
+_sig('ma_batchInfo', [ct.c_void_p, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_batchDestroy', [ct.c_void_p], None, check=False)

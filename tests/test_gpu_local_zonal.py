@@ -133,3 +133,24 @@ def test_device_resident_input_and_output(M):
     assert np.array_equal(out, a_np * np.float32(3.0) + np.float32(1.0))
     M._lib.ma_devFree(ct.c_void_p(d_in))
     M._lib.ma_devFree(ct.c_void_p(d_out))
+
+
+def test_sincos_pairing_is_bit_identical(M):
+    """sin(x) and cos(x) of one argument compile to one sincosf call; its
+    results equal separate sinf / cosf calls on every input."""
+    rng = np.random.default_rng(7)
+    x_np = np.concatenate([rng.uniform(-10, 10, 200000), rng.uniform(-1e4, 1e4, 50000),
+                           np.linspace(0, 1.5707964, 50000)]).astype(np.float32).reshape(300, 1000)
+    x = M.from_numpy(x_np)
+    pair_s = M.to_numpy(M.sin(x) + 0.0 * M.cos(x) + M.cos(x) * 0.0)
+    only_s = M.to_numpy(M.sin(x))
+    only_c = M.to_numpy(M.cos(x))
+    both = M.to_numpy(M.sin(x) * 1.0 + M.cos(x) * 0.0)   # same shape of program, paired
+    assert np.array_equal(M.to_numpy(M.sin(x) * 1.0), only_s)
+    s_pair = M.from_numpy(x_np)
+    a = M.sin(s_pair)
+    b = M.cos(s_pair)
+    src = M.generated_source(a + b)
+    assert "sincosf(" in src
+    ab = M.to_numpy(a + b)
+    assert np.array_equal(ab, only_s + only_c)
