@@ -623,13 +623,13 @@ static std::string gen_radial(Gen &G) {
   s << G.stores() << "}\n";
   int ri = G.outk.at(scan);
   // aux[0] start x, aux[1] start y, aux[2] last front (or -1 for all)
-  s << "extern \"C\" __global__ void __launch_bounds__(512) KNAME(const __grid_constant__ Args a) {\n"
+  s << "__device__ __forceinline__ void radial_run(const Args &a, int octant) {\n"
     << "  const int sx = (int)a.aux[0], sy = (int)a.aux[1];\n"
     << "  const long long lim = (long long)a.aux[2];\n"
     << "  const RasterArg R = a.out[" << ri << "];\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  int p0, p1, q0, q1;\n"
-    << "  octant_units(blockIdx.x, p0, p1, q0, q1);\n"
+    << "  octant_units(octant, p0, p1, q0, q1);\n"
     << "  if (threadIdx.x == 0) radial_cell(a, sx, sy, (" << T << ")0, true);\n"
     << "  const int ep = p0 > 0 ? W - 1 - sx : p0 < 0 ? sx : p1 > 0 ? H - 1 - sy : sy;\n"
     << "  const int eq = q0 > 0 ? W - 1 - sx : q0 < 0 ? sx : q1 > 0 ? H - 1 - sy : sy;\n"
@@ -647,6 +647,15 @@ static std::string gen_radial(Gen &G) {
     << "    }\n"
     << "    __syncthreads();\n"
     << "  }\n"
+    << "}\n";
+  // one scan: 8 CTAs (one per octant); many scans: 8 CTAs per Args of a device array
+  s << "extern \"C\" __global__ void __launch_bounds__(512) KNAME(const __grid_constant__ Args a) {\n"
+    << "  radial_run(a, blockIdx.x);\n"
+    << "}\n"
+    << "struct ManyArgs { u64 args; s64 n; };\n"
+    << "extern \"C\" __global__ void __launch_bounds__(512) KNAME_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  if ((s64)(blockIdx.x >> 3) >= m.n) return;\n"
+    << "  radial_run(((const Args *)m.args)[blockIdx.x >> 3], blockIdx.x & 7);\n"
     << "}\n";
   return s.str();
 }
@@ -683,7 +692,7 @@ static std::string gen_spread(Gen &G) {
   const int kd = G.rin.at(scan->prev[1]);
   const int ko = G.outk.at(scan);
   // aux[0] in-degree (s32[N]), aux[1] frontier A (s32[N]), aux[2] frontier B, aux[3] round limit
-  s << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME(const __grid_constant__ Args a) {\n"
+  s << "__device__ __forceinline__ void spread_run(const Args &a) {\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  const s64 N = (s64)W * H;\n"
     << "  s32 *indeg = (s32 *)a.aux[0];\n"
@@ -725,6 +734,14 @@ static std::string gen_spread(Gen &G) {
     << "    s32 *t = fa; fa = fb; fb = t;\n"
     << "    __syncthreads();\n"
     << "  }\n"
+    << "}\n";
+  s << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME(const __grid_constant__ Args a) {\n"
+    << "  spread_run(a);\n"
+    << "}\n"
+    << "struct ManyArgs { u64 args; s64 n; };\n"
+    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  if ((s64)blockIdx.x >= m.n) return;\n"
+    << "  spread_run(((const Args *)m.args)[blockIdx.x]);\n"
     << "}\n";
   return s.str();
 }
