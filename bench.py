@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--block", type=int, default=256)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-clocks", action="store_true")
+    p.add_argument("--no-mix", action="store_true", help="skip the batched-mix and serving sections")
     return p.parse_args()
 
 
@@ -165,6 +166,103 @@ def run_reference(args, rank, world):
                              "sample": times[0]["sample"]},
             "e2e": {"value": v, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- mixes
+
+def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
+    """512 rasters, sides log-uniform in [64, 2048], aspect uniform in [0.5, 2],
+    each running fused hillshade + a 6-layer weighted overlay: batched
+    persistent launch (graph replay) against the plain path (one launch per
+    group per 256x256 block, reference launch order). Raster-edge mirror border."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    weights = [0.1, 0.2, 0.3, 0.15, 0.15, 0.1]
+    M.set_border(M.BORDER_RASTER_MIRROR)
+    keep, progs = [], []
+    cells = 0
+    for i in range(n_rasters):
+        side = float(np.exp(rng.uniform(np.log(64), np.log(2048))))
+        asp = float(rng.uniform(0.5, 2.0))
+        w = max(8, int(round(side * np.sqrt(asp))))
+        h = max(8, int(round(side / np.sqrt(asp))))
+        pw = (w + 31) // 32 * 32
+        dem = torch.zeros((h, pw), dtype=torch.float32, device=dev)
+        dem[:, :w] = synth.fbm_dem(h, w, seed=seed * 1000 + i, xp=torch, device=dev)
+        lay = [torch.rand((h, pw), generator=gen, device=dev) for _ in range(6)]
+        hs_o = torch.empty((h, pw), dtype=torch.float32, device=dev)
+        ov_o = torch.empty((h, pw), dtype=torch.float32, device=dev)
+        bs = [256, 256]
+        dn = M.from_device(dem.data_ptr(), pw * 4, [w, h], M.F32, bs)
+        ln = [M.from_device(l.data_ptr(), pw * 4, [w, h], M.F32, bs) for l in lay]
+        progs.append((W.hillshade(dn), W.wsum(ln, weights), hs_o, ov_o, pw * 4))
+        keep.append((dem, lay, dn, ln))
+        cells += w * h
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(M.stream(), device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # plain path
+    M.set_exec_mode(M.EXEC_PLAIN)
+    for hs, ov, ho, oo, pitch in progs[:8]:
+        M.to_device(hs, ho.data_ptr(), pitch, sync=False)
+        M.to_device(ov, oo.data_ptr(), pitch, sync=False)
+    M.sync()
+    n0 = M._lib.ma_totalLaunchCount()
+    e0.record(stream)
+    for hs, ov, ho, oo, pitch in progs:
+        M.to_device(hs, ho.data_ptr(), pitch, sync=False)
+        M.to_device(ov, oo.data_ptr(), pitch, sync=False)
+    e1.record(stream)
+    e1.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    plain_launches = M._lib.ma_totalLaunchCount() - n0
+    plain_ref = [ho[:64, :64].clone() for _, _, ho, _, _ in progs[:16]]
+    M.set_exec_mode(M.EXEC_FUSED)
+    # batched path
+    b = M.Batch()
+    for hs, ov, ho, oo, pitch in progs:
+        b.add([hs, ov], [(ho.data_ptr(), pitch), (oo.data_ptr(), pitch)])
+    t0 = time.perf_counter()
+    b.prepare(autotune=True)
+    prep_s = time.perf_counter() - t0
+    b.run()
+    e0.record(stream)
+    for _ in range(steps):
+        b.run(sync=False)
+    e1.record(stream)
+    e1.synchronize()
+    M.sync()
+    batch_ms = e0.elapsed_time(e1) / steps
+    same = all(torch.equal(r, progs[i][2][:64, :64]) for i, r in enumerate(plain_ref))
+    M.set_border(M.BORDER_BLOCK_MIRROR)
+    info = b.info()
+    return {"rasters": n_rasters, "cells": cells, "value": round(cells / (batch_ms * 1e-3) / 1e9, 3),
+            "plain_value": round(cells / (plain_ms * 1e-3) / 1e9, 3), "unit": "Gcells/s",
+            "speedup_vs_plain": round(plain_ms / batch_ms, 2), "ms_per_step": round(batch_ms, 3),
+            "plain_ms": round(plain_ms, 3), "plain_launches": plain_launches, "batched_launches_per_step": info["phases"],
+            "prepare_s": round(prep_s, 2), "kinds": info["kinds"], "plain_equals_batched": same,
+            "programs": "fused hillshade + 6-layer weighted overlay per raster"}
+
+
+def bench_serving(M, synth, torch, dev, size=32768, rates=(200, 1000, 2000), seconds=3.0):
+    """Requests over a device-resident size^2 DEM: Poisson arrivals, windows
+    256^2/512^2/1024^2 at uniform offsets, mix 50% hillshade / 20% slope / 15%
+    viewshed (observer height 10 m, radius 167 cells = 5 km at 30 m) / 15% D8 +
+    flow accumulation; admission by an HBM budget of 8 GiB."""
+    dem = synth.fbm_dem(size, size, seed=4242, xp=torch, device=dev).contiguous()
+    torch.cuda.synchronize()
+    srv = M.Server(dem.data_ptr(), size * 4, size, size, budget_bytes=8 << 30, max_batch=512)
+    srv.load(rate=200, seconds=0.5, seed=99)            # warm-up: compiles every program kind
+    out = {"dem": "%dx%d F32 fBm, resident" % (size, size), "mix": [0.5, 0.2, 0.15, 0.15], "runs": []}
+    for r in rates:
+        res = srv.load(rate=r, seconds=seconds, seed=r)
+        out["runs"].append({k: res[k] for k in ("rate_req_s", "requests", "throughput_req_s", "gcells_s", "p50_ms",
+                                                "p99_ms", "by_window", "by_program")} | {"mean_batch": res["server"]["mean_batch"]})
+    srv.close()
+    del dem
+    return out
 
 
 # ---------------------------------------------------------------- our arm
@@ -307,6 +405,15 @@ def main():
         ck = clk.summary()
         if ck:
             line["clocks"] = ck
+        if world == 1 and not args.no_mix:
+            try:
+                line["batched"] = bench_batched(M, W, synth, torch, dev)
+            except Exception as e:   # reported, not fatal: the headline line still prints
+                line["batched"] = {"error": str(e)[:300]}
+            try:
+                line["serving"] = bench_serving(M, synth, torch, dev)
+            except Exception as e:
+                line["serving"] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

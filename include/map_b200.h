@@ -162,6 +162,29 @@ int ma_batchRun(ma_Batch *b, int sync);
 size_t ma_batchInfo(ma_Batch *b, char *buf, size_t len);
 void ma_batchDestroy(ma_Batch *b);
 
+/* Serving over a device-resident DEM (F32, `pitch` bytes per row) with
+ * continuous batching and admission by an HBM budget. Request types:
+ * 0 hillshade, 1 slope, 2 viewshed (observer inside the window, height obs_h,
+ * radius in cells, <= 0 for no limit), 3 D8 flow direction + flow accumulation
+ * (S32 upstream counts). A request's window is an independent raster.
+ * ma_serverSubmit returns the request id (-1 on error); results stay on the
+ * device until ma_serverResult (copies to host and releases) or
+ * ma_serverRelease. ma_serverLoad runs an open-loop Poisson load (rate req/s,
+ * program mix weights mix[4], windows 256/512/1024 squared) and writes
+ * latency percentiles and throughput as JSON. */
+typedef struct ma_Server ma_Server;
+ma_Server *ma_serverCreate(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch);
+long long ma_serverSubmit(ma_Server *s, int type, int x0, int y0, int w, int h, int obs_x, int obs_y, float obs_h,
+                          double radius);
+int ma_serverWait(ma_Server *s, long long id, double timeout_s);
+int ma_serverResult(ma_Server *s, long long id, void *dst, size_t bytes);
+int ma_serverRelease(ma_Server *s, long long id);
+double ma_serverLatency(ma_Server *s, long long id);
+size_t ma_serverStats(ma_Server *s, char *buf, size_t len);
+size_t ma_serverLoad(ma_Server *s, double rate, double seconds, const double *mix, unsigned seed, double obs_h,
+                     double radius, char *buf, size_t len);
+void ma_serverDestroy(ma_Server *s);
+
 /* Introspection for tests and tools. */
 int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
 int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */

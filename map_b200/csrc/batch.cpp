@@ -119,6 +119,53 @@ TileCfg autotune_group(const Group &g, const std::function<DevRaster &(Node *)> 
   return best;
 }
 
+// ------------------------------------------------------------------ persistent module
+
+PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &kinds) {
+  size_t bar_off = 16;
+  for (const KernelPlan *p : kinds) {
+    if (p->threads != 256) throw MapError("persistent module: tile configurations must use 256 threads");
+    if (!p->tma.empty()) bar_off = std::max(bar_off, (p->bar_off + 15) / 16 * 16);
+  }
+  PersistentModule pm;
+  pm.smem = bar_off + 16;
+  std::ostringstream src;
+  src << "#include \"map_common.cuh\"\n";
+  for (size_t k = 0; k < kinds.size(); k++) src << "namespace k" << k << " {\n" << kinds[k]->body << "}\n";
+  src << "struct BItem { u32 kind, inst, tile, pad; };\n"
+      << "struct BatchArgs { u64 items; s64 n; u64 counter; u64 err; u64 args[" << kinds.size() << "]; };\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ BatchArgs b) {\n"
+      << "  extern __shared__ __align__(128) unsigned char smem[];\n"
+      << "  __shared__ int item_s;\n"
+      << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
+      << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
+      << "  __syncthreads();\n"
+      << "  u32 phase = 0;\n"
+      << "  const BItem *items = (const BItem *)b.items;\n"
+      << "  for (;;) {\n"
+      << "    if (threadIdx.x == 0) item_s = atomicAdd((int *)b.counter, 1);\n"
+      << "    __syncthreads();\n"
+      << "    const int i = item_s;\n"
+      << "    __syncthreads();\n"
+      << "    if (i >= b.n) break;\n"
+      << "    const BItem w = items[i];\n"
+      << "    bool ok = true;\n"
+      << "    switch (w.kind) {\n";
+  for (size_t k = 0; k < kinds.size(); k++)
+    src << "      case " << k << ": ok = k" << k << "::run_tile(((const k" << k << "::Args *)b.args[" << k
+        << "])[w.inst], (int)w.tile, smem, bar, phase); break;\n";
+  src << "      default: skel_fail((u32 *)b.err, ERR_BAD_LAUNCH); ok = false;\n"
+      << "    }\n"
+      << "    if (!ok) break;\n"
+      << "  }\n"
+      << "}\n";
+  pm.source = src.str();
+  pm.kname = "map_batch_" + hex16(pm.source).substr(0, 12);
+  size_t pos;
+  while ((pos = pm.source.find("KNAME")) != std::string::npos) pm.source.replace(pos, 5, pm.kname);
+  return pm;
+}
+
 // ------------------------------------------------------------------ batch
 
 struct Batch::Kind {
@@ -302,44 +349,12 @@ void Batch::prepare(bool autotune) {
   }
 
   // batch module: every kind's tile function in its own namespace + a persistent dispatcher
-  size_t bar_off = 16;
-  for (auto &kd : I.kinds)
-    if (!kd.plan.tma.empty()) bar_off = std::max(bar_off, (kd.plan.bar_off + 15) / 16 * 16);
-  I.smem = bar_off + 16;
-  std::ostringstream src;
-  src << "#include \"map_common.cuh\"\n";
-  for (size_t k = 0; k < I.kinds.size(); k++) src << "namespace k" << k << " {\n" << I.kinds[k].plan.body << "}\n";
-  src << "struct BItem { u32 kind, inst, tile, pad; };\n"
-      << "struct BatchArgs { u64 items; s64 n; u64 counter; u64 err; u64 args[" << I.kinds.size() << "]; };\n"
-      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ BatchArgs b) {\n"
-      << "  extern __shared__ __align__(128) unsigned char smem[];\n"
-      << "  __shared__ int item_s;\n"
-      << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
-      << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
-      << "  __syncthreads();\n"
-      << "  u32 phase = 0;\n"
-      << "  const BItem *items = (const BItem *)b.items;\n"
-      << "  for (;;) {\n"
-      << "    if (threadIdx.x == 0) item_s = atomicAdd((int *)b.counter, 1);\n"
-      << "    __syncthreads();\n"
-      << "    const int i = item_s;\n"
-      << "    __syncthreads();\n"
-      << "    if (i >= b.n) break;\n"
-      << "    const BItem w = items[i];\n"
-      << "    bool ok = true;\n"
-      << "    switch (w.kind) {\n";
-  for (size_t k = 0; k < I.kinds.size(); k++)
-    src << "      case " << k << ": ok = k" << k << "::run_tile(((const k" << k << "::Args *)b.args[" << k
-        << "])[w.inst], (int)w.tile, smem, bar, phase); break;\n";
-  src << "      default: skel_fail((u32 *)b.err, ERR_BAD_LAUNCH); ok = false;\n"
-      << "    }\n"
-      << "    if (!ok) break;\n"
-      << "  }\n"
-      << "}\n";
-  I.source = src.str();
-  I.kname = "map_batch_" + hex16(I.source).substr(0, 12);
-  size_t pos;
-  while ((pos = I.source.find("KNAME")) != std::string::npos) I.source.replace(pos, 5, I.kname);
+  std::vector<const KernelPlan *> kp;
+  for (auto &kd : I.kinds) kp.push_back(&kd.plan);
+  PersistentModule pm = build_persistent_module(kp);
+  I.source = pm.source;
+  I.kname = pm.kname;
+  I.smem = pm.smem;
   I.kh = env.kernel(I.source, I.kname, I.smem);
   int occ = std::max(1, env.occupancy(I.kh, 256, I.smem));
   I.grid = env.sm_count() * occ;

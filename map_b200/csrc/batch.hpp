@@ -48,6 +48,16 @@ class Batch {
   std::unique_ptr<Impl> impl_;
 };
 
+// Persistent dispatcher over several kinds of tile function (Local / Focal
+// plans with 256 threads): one kernel `kname` taking
+//   struct { u64 items; s64 n; u64 counter; u64 err; u64 args[kinds]; }
+// that pulls (kind, instance, tile) items with an atomic counter.
+struct PersistentModule {
+  std::string source, kname;
+  size_t smem = 0;
+};
+PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &kinds);
+
 // Autotuned tile shape for group `g`, whose inputs/outputs are bound through
 // `get` / `bufs` (launches candidate kernels on the library stream).
 TileCfg autotune_group(const Group &g, const std::function<DevRaster &(Node *)> &get,

@@ -3,6 +3,7 @@
 // Every entry point converts C++ exceptions into a recorded error.
 #include "../../include/map_b200.h"
 #include "batch.hpp"
+#include "server.hpp"
 #include "codegen.hpp"
 #include "cuda_env.hpp"
 #include "executor.hpp"
@@ -565,6 +566,105 @@ void ma_batchDestroy(ma_Batch *b) {
   for (Node *x : b->held)
     if (Runtime::get().owns(x) && x->ref > 0) x->ref--;
   delete b;
+}
+
+// ---- serving
+
+struct ma_Server {
+  std::unique_ptr<Server> s;
+};
+
+ma_Server *ma_serverCreate(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch) {
+  try {
+    auto *h = new ma_Server();
+    h->s = std::make_unique<Server>(dem, pitch, W, H, budget_bytes, max_batch);
+    ok();
+    return h;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return nullptr;
+  }
+}
+
+long long ma_serverSubmit(ma_Server *h, int type, int x0, int y0, int w, int hh, int obs_x, int obs_y, float obs_h,
+                          double radius) {
+  try {
+    if (!h) throw MapError("server: null handle");
+    long long id = h->s->submit(type, x0, y0, w, hh, obs_x, obs_y, obs_h, radius, false);
+    ok();
+    return id;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return -1;
+  }
+}
+
+int ma_serverWait(ma_Server *h, long long id, double timeout_s) {
+  return int_call([&] {
+    if (!h) throw MapError("server: null handle");
+    return h->s->wait(id, timeout_s);
+  });
+}
+
+int ma_serverResult(ma_Server *h, long long id, void *dst, size_t bytes) {
+  return int_call([&] {
+    if (!h) throw MapError("server: null handle");
+    h->s->result(id, dst, bytes);
+    return 0;
+  });
+}
+
+int ma_serverRelease(ma_Server *h, long long id) {
+  return int_call([&] {
+    if (!h) throw MapError("server: null handle");
+    h->s->release(id);
+    return 0;
+  });
+}
+
+double ma_serverLatency(ma_Server *h, long long id) {
+  try {
+    if (!h) throw MapError("server: null handle");
+    double v = h->s->latency_ms(id);
+    ok();
+    return v;
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return -1;
+  }
+}
+
+size_t ma_serverStats(ma_Server *h, char *buf, size_t len) {
+  try {
+    if (!h) throw MapError("server: null handle");
+    ok();
+    return copy_out(h->s->stats_json(), buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+size_t ma_serverLoad(ma_Server *h, double rate, double seconds, const double *mix, unsigned seed, double obs_h,
+                     double radius, char *buf, size_t len) {
+  try {
+    if (!h || !mix) throw MapError("server: null argument");
+    std::string j = h->s->run_load(rate, seconds, mix, seed, obs_h, radius);
+    ok();
+    return copy_out(j, buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+void ma_serverDestroy(ma_Server *h) {
+  try {
+    delete h;
+    ok();
+  } catch (const std::exception &e) {
+    fail(e.what());
+  }
 }
 
 int ma_nodeCount(void) { return (int)Runtime::get().nodes.size(); }

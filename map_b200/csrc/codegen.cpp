@@ -126,7 +126,7 @@ struct Gen {
   void classify() {
     for (size_t i = 0; i < g.nodes.size(); i++) member[g.nodes[i]] = (int)i;
     for (Node *in : g.inputs) {
-      if (in->meta.numdim == D0 && in->kind == K_CONSTANT) {
+      if (in->meta.numdim == D0 && in->kind == K_CONSTANT && !in->as_param) {
         // Scalar constants are part of the kernel's signature (as constant values
         // are part of the reference's Version signature, runtime/dag/Constant.cpp),
         // so the device compiler folds them (x / 8 becomes an exact multiply).

@@ -5,6 +5,7 @@
 // dependency, so the library also loads on machines without a GPU driver).
 #pragma once
 
+#include <atomic>
 #include <cstddef>
 #include <cstdint>
 #include <string>
@@ -63,7 +64,7 @@ class CudaEnv {
   std::string device_name_;
   CUstream_st *stream_ = nullptr;
   uint32_t *err_word_ = nullptr;
-  int launches_ = 0;
+  std::atomic<int> launches_{0};
 };
 
 // CUDA runtime error check helper

@@ -72,15 +72,13 @@ Node *Runtime::add(std::unique_ptr<Node> n, const std::string &key) {
   n->id = next_id++;
   for (Node *p : n->prev) p->next.push_back(n.get());
   Node *raw = n.get();
+  live_set.insert(raw);
   nodes.push_back(std::move(n));
   if (!key.empty()) cse[key] = raw;
   return raw;
 }
 
-bool Runtime::owns(const Node *n) const {
-  for (auto &u : nodes) if (u.get() == n) return true;
-  return false;
-}
+bool Runtime::owns(const Node *n) const { return live_set.count(n) > 0; }
 
 static void check_node(Node *n, const char *what) {
   if (n == nullptr) throw MapError(std::string(what) + ": null node argument");
@@ -117,6 +115,20 @@ Node *Runtime::constant(Variant v, Arr2 ds, int dt, int mo, Arr2 bs) {
   n->value = n->cnst;
   std::string key = "C|" + meta_key(n->meta) + "|" + var_key(n->cnst);
   return add(std::move(n), key);
+}
+
+Node *Runtime::scalar_param(Variant v) {
+  dt_size(v.dtype);
+  auto n = std::make_unique<Node>();
+  n->kind = K_CONSTANT;
+  n->pattern = P_FREE;
+  n->meta.dtype = v.dtype;
+  n->meta.numdim = D0;
+  n->cnst = v;
+  n->as_param = true;
+  n->has_value = true;
+  n->value = v;
+  return add(std::move(n), "P|" + var_key(v));
 }
 
 Node *Runtime::read(const std::string &path) {
@@ -434,6 +446,8 @@ void Runtime::collect_garbage() {
     auto &nx = u->next;
     nx.erase(std::remove_if(nx.begin(), nx.end(), [&](Node *m) { return !live.count(m); }), nx.end());
   }
+  for (auto &u : nodes)
+    if (!live.count(u.get())) live_set.erase(u.get());
   nodes.erase(std::remove_if(nodes.begin(), nodes.end(), [&](const std::unique_ptr<Node> &u) { return !live.count(u.get()); }),
               nodes.end());
 }
@@ -441,6 +455,7 @@ void Runtime::collect_garbage() {
 void Runtime::reset() {
   std::lock_guard<std::recursive_mutex> lk(mtx);
   cse.clear();
+  live_set.clear();
   nodes.clear();
 }
 

@@ -13,6 +13,7 @@
 #include <mutex>
 #include <string>
 #include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 namespace mapb {
@@ -65,6 +66,7 @@ struct Node {
   Arr2 mask_ds{{-1, -1}, 0};
   Arr2 coord{{0, 0}, 2};       // neighbour offset / radial start
   double radius = 0;           // radial scan: fronts farther than this are not swept (0 = all)
+  bool as_param = false;       // scalar constant passed to kernels as an argument, not written into their source
   std::string path;            // read / write path
   std::shared_ptr<HostData> host;
   std::shared_ptr<DevData> dev;
@@ -84,6 +86,7 @@ struct Runtime {
   std::recursive_mutex mtx;
   std::vector<std::unique_ptr<Node>> nodes;
   std::unordered_map<std::string, Node *> cse;
+  std::unordered_set<const Node *> live_set;   // fast ownership test of node handles
   int next_id = 0;
 
   // configuration
@@ -94,6 +97,9 @@ struct Runtime {
   // factories (each returns a node owned by the runtime, possibly pre-existing)
   Node *constant(Variant v, Arr2 ds, int dt, int mo, Arr2 bs);
   Node *read(const std::string &path);
+  // A scalar whose value is a kernel argument rather than part of the kernel's
+  // source, so programs differing only in this value share compiled code.
+  Node *scalar_param(Variant v);
   Node *host_input(const void *ptr, Arr2 ds, int dt, Arr2 bs, bool copy);
   Node *dev_input(void *ptr, long long pitch, Arr2 ds, int dt, Arr2 bs);
   Node *index(Node *arg, int dim);

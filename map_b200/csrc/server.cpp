@@ -1,0 +1,658 @@
+// Serving with continuous batching (see server.hpp).
+#include "server.hpp"
+#include "batch.hpp"
+#include "codegen.hpp"
+#include "cuda_env.hpp"
+#include "executor.hpp"
+#include "fusion.hpp"
+#include "programs.hpp"
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <random>
+#include <set>
+#include <sstream>
+#include <thread>
+#include <unordered_map>
+
+namespace mapb {
+
+namespace {
+
+double now_s() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+long long pitch_for(int W, int dt) {
+  long long b = (long long)W * (long long)dt_size(dt);
+  return (b + 127) / 128 * 128;
+}
+
+struct Req {
+  long long id = 0;
+  int type = 0, x0 = 0, y0 = 0, w = 0, h = 0, ox = 0, oy = 0;
+  float oh = 0;
+  double radius = 0;
+  bool auto_release = false;
+  double t_submit = 0, t_done = 0;
+  int state = 0;   // 0 queued, 1 running, 2 done, 3 failed
+  std::string err;
+  size_t bytes = 0;
+  int stream = 0;
+  void *win = nullptr;
+  long long win_pitch = 0;
+  void *out = nullptr;
+  long long out_pitch = 0;
+  int out_dt = F32;
+  std::vector<void *> scratch;
+  Node *out_node = nullptr;
+};
+
+size_t request_bytes(int type, int w, int h) {
+  size_t b = (size_t)pitch_for(w, F32) * h * 2;   // window copy + output
+  if (type == REQ_FLOW) b += (size_t)pitch_for(w, U8) * h + (size_t)w * h * 12;
+  return b;
+}
+
+struct InFlight {
+  std::vector<Req *> reqs;
+  cudaEvent_t ev = nullptr;
+  int stream = 0;
+  std::vector<void *> dev_free;
+};
+
+}  // namespace
+
+struct Server::Impl {
+  void *dem = nullptr;
+  long long pitch = 0;
+  int W = 0, H = 0;
+  size_t budget = 0;
+  int max_batch = 0;
+
+  std::mutex m;
+  std::condition_variable cv_pending, cv_done, cv_inflight;
+  std::deque<Req *> pending;
+  std::map<long long, std::unique_ptr<Req>> reqs;
+  std::deque<InFlight> inflight;
+  size_t used = 0;
+  long long next_id = 1;
+  bool stop = false;
+  std::thread dispatcher, completer;
+  cudaStream_t streams[2] = {nullptr, nullptr};
+  cudaEvent_t last_ev[2] = {nullptr, nullptr};
+  int next_stream = 0;
+  // pinned staging for argument / work-list uploads, one per stream
+  void *stage[2] = {nullptr, nullptr};
+  size_t stage_cap[2] = {0, 0};
+  // statistics
+  long long batches = 0, completed = 0, failed = 0, max_batch_seen = 0, batched_requests = 0;
+  size_t peak_used = 0;
+  int gc_counter = 0;
+
+  void dispatch_loop();
+  void complete_loop();
+  void run_batch(std::vector<Req *> &batch);
+  void free_request(Req *r, cudaStream_t st);
+};
+
+void Server::Impl::free_request(Req *r, cudaStream_t st) {
+  if (r->win) cudaFreeAsync(r->win, st);
+  if (r->out) cudaFreeAsync(r->out, st);
+  for (void *p : r->scratch) cudaFreeAsync(p, st);
+  r->win = r->out = nullptr;
+  r->scratch.clear();
+}
+
+void Server::Impl::run_batch(std::vector<Req *> &batch) {
+  CudaEnv &env = CudaEnv::get();
+  const int si = next_stream;
+  next_stream ^= 1;
+  cudaStream_t st = streams[si];
+  // the staging buffer of this stream was last used by the batch recorded in last_ev
+  if (last_ev[si]) cuda_check(cudaEventSynchronize(last_ev[si]), "cudaEventSynchronize");
+
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  struct KindSet {
+    std::map<std::string, int> index;
+    std::vector<KernelPlan> plans;
+    std::vector<std::vector<unsigned char>> args;
+    std::vector<int> members;
+  } kinds;
+  struct Item { uint32_t kind, inst, tile, pad; };
+  std::vector<std::vector<Item>> levels(2);
+  struct Many { KernelPlan plan; std::vector<unsigned char> args; int n = 0; };
+  std::map<std::string, Many> radial, spread;
+  std::vector<FusionResult> keep;
+  std::vector<Req *> ok;
+
+  for (Req *r : batch) {
+    try {
+      r->stream = si;
+      r->win_pitch = pitch_for(r->w, F32);
+      cuda_check(cudaMallocAsync(&r->win, (size_t)r->win_pitch * r->h, st), "cudaMallocAsync(window)");
+      cuda_check(cudaMemcpy2DAsync(r->win, r->win_pitch, (char *)dem + (size_t)r->y0 * pitch + (size_t)r->x0 * 4, pitch,
+                                   (size_t)r->w * 4, r->h, cudaMemcpyDeviceToDevice, st),
+                 "window copy");
+      Node *win = rt.dev_input(r->win, r->win_pitch, Arr2{{r->w, r->h}, 2}, F32, Arr2{{r->w, r->h}, 2});
+      Node *out = nullptr;
+      switch (r->type) {
+        case REQ_HILLSHADE: out = prog_hillshade(rt, win); break;
+        case REQ_SLOPE: out = prog_slope(rt, win); break;
+        case REQ_VIEWSHED: out = prog_viewshed(rt, win, r->ox, r->oy, r->oh, r->radius); break;
+        case REQ_FLOW: out = prog_flow(rt, win); break;
+        default: throw MapError("unknown request type");
+      }
+      out->ref++;
+      r->out_node = out;
+      r->out_dt = out->meta.dtype;
+      r->out_pitch = pitch_for(r->w, r->out_dt);
+      cuda_check(cudaMallocAsync(&r->out, (size_t)r->out_pitch * r->h, st), "cudaMallocAsync(output)");
+      std::unordered_map<Node *, DevRaster> bufs;
+      DevRaster wr;
+      wr.ptr = r->win;
+      wr.pitch = r->win_pitch;
+      wr.dtype = F32;
+      wr.W = r->w;
+      wr.H = r->h;
+      bufs[win] = wr;
+      DevRaster orr;
+      orr.ptr = r->out;
+      orr.pitch = r->out_pitch;
+      orr.dtype = r->out_dt;
+      orr.W = r->w;
+      orr.H = r->h;
+      bufs[out] = orr;
+      std::function<DevRaster &(Node *)> get = [&](Node *n) -> DevRaster & {
+        auto it = bufs.find(n);
+        if (it == bufs.end()) throw MapError("serving: raster not bound");
+        return it->second;
+      };
+      keep.push_back(fuse(collect_nodes({out}), {out}));
+      std::map<const Group *, int> level;
+      for (auto &gp : keep.back().groups) {
+        const Group &g = *gp;
+        int lv = 0;
+        for (Group *p : g.prev) lv = std::max(lv, level[p] + 1);
+        level[&g] = lv;
+        if (g.skeleton == SK_HOST) {
+          Node *n = g.nodes[0];
+          throw MapError(std::string("serving: unexpected host step ") + kind_name(n->kind));
+        }
+        KernelPlan P = generate_kernel(g);
+        for (Node *o : P.out_rasters) {
+          if (bufs.count(o)) continue;
+          DevRaster t;
+          t.dtype = o->meta.dtype;
+          t.W = o->meta.W();
+          t.H = o->meta.H();
+          t.pitch = pitch_for(t.W, t.dtype);
+          cuda_check(cudaMallocAsync(&t.ptr, (size_t)t.pitch * t.H, st), "cudaMallocAsync(intermediate)");
+          r->scratch.push_back(t.ptr);
+          bufs[o] = t;
+        }
+        if (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL) {
+          if (lv > 1) throw MapError("serving: program too deep");
+          auto it = kinds.index.find(P.body);
+          int k;
+          if (it == kinds.index.end()) {
+            k = (int)kinds.plans.size();
+            kinds.index[P.body] = k;
+            kinds.plans.push_back(P);
+            kinds.args.emplace_back();
+            kinds.members.push_back(0);
+          } else {
+            k = it->second;
+          }
+          uint64_t aux[4] = {0, 0, 0, 0};
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          kinds.args[k].insert(kinds.args[k].end(), a.begin(), a.end());
+          const uint32_t idx = (uint32_t)kinds.members[k]++;
+          const int tiles = ((g.W + P.tile_w - 1) / P.tile_w) * ((g.H + P.tile_h - 1) / P.tile_h);
+          for (int t = 0; t < tiles; t++) levels[lv].push_back(Item{(uint32_t)k, idx, (uint32_t)t, 0});
+        } else if (g.skeleton == SK_RADIAL) {
+          Many &mn = radial[P.source];
+          if (mn.n == 0) mn.plan = P;
+          long long lim = P.core->radius > 0 ? (long long)P.core->radius : -1;
+          int ri = 0;
+          for (size_t k = 0; k < P.out_rasters.size(); k++)
+            if (P.out_rasters[k] == P.core) ri = (int)k;
+          if (lim >= 0)
+            for (Node *o : P.out_rasters) {
+              DevRaster &d = bufs.at(o);
+              cuda_check(cudaMemset2DAsync(d.ptr, d.pitch, 0xFF, (size_t)d.W * dt_size(d.dtype), d.H, st), "memset");
+            }
+          uint64_t aux[4] = {(uint64_t)P.core->coord.arr[0], (uint64_t)P.core->coord.arr[1], (uint64_t)lim, (uint64_t)ri};
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          mn.args.insert(mn.args.end(), a.begin(), a.end());
+          mn.n++;
+        } else if (g.skeleton == SK_SPREAD) {
+          Many &mn = spread[P.source];
+          if (mn.n == 0) mn.plan = P;
+          const size_t N = (size_t)g.W * g.H;
+          void *work = nullptr;
+          cuda_check(cudaMallocAsync(&work, 3 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
+          r->scratch.push_back(work);
+          uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
+                             (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          mn.args.insert(mn.args.end(), a.begin(), a.end());
+          mn.n++;
+        } else {
+          throw MapError("serving: zonal groups are not served");
+        }
+      }
+      ok.push_back(r);
+    } catch (const std::exception &e) {
+      r->state = 3;
+      r->err = e.what();
+    }
+  }
+  batch = ok;
+  // stage every upload into this stream's pinned buffer
+  std::vector<std::pair<const void *, size_t>> blobs;
+  for (auto &a : kinds.args) blobs.push_back({a.data(), a.size()});
+  for (auto &lv : levels) blobs.push_back({lv.data(), lv.size() * sizeof(Item)});
+  for (auto &kv : radial) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
+  for (auto &kv : spread) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
+  size_t total = 512;
+  for (auto &b : blobs) total += (b.second + 255) / 256 * 256;
+  if (total > stage_cap[si]) {
+    if (stage[si]) cudaFreeHost(stage[si]);
+    stage_cap[si] = std::max(total, (size_t)1 << 20);
+    cuda_check(cudaMallocHost(&stage[si], stage_cap[si]), "cudaMallocHost(staging)");
+  }
+  void *dbuf = nullptr;
+  cuda_check(cudaMallocAsync(&dbuf, total, st), "cudaMallocAsync(batch arrays)");
+  std::vector<void *> dptr;
+  size_t off = 256;   // first 256 bytes: work-list counters
+  std::memset(stage[si], 0, 256);
+  for (auto &b : blobs) {
+    std::memcpy((char *)stage[si] + off, b.first, b.second);
+    dptr.push_back((char *)dbuf + off);
+    off += (b.second + 255) / 256 * 256;
+  }
+  cuda_check(cudaMemcpyAsync(dbuf, stage[si], off, cudaMemcpyHostToDevice, st), "upload batch arrays");
+  size_t bi = 0;
+  std::vector<void *> d_kind_args;
+  for (size_t k = 0; k < kinds.args.size(); k++) d_kind_args.push_back(dptr[bi++]);
+  std::vector<void *> d_levels;
+  for (size_t l = 0; l < levels.size(); l++) d_levels.push_back(dptr[bi++]);
+
+  // persistent launch per level over the Local / Focal kinds; radial after level 0; spread after level 1
+  KernelHandle pk;
+  int grid = 0;
+  size_t smem = 0;
+  if (!kinds.plans.empty()) {
+    std::vector<const KernelPlan *> kp;
+    for (auto &p : kinds.plans) kp.push_back(&p);
+    PersistentModule pm = build_persistent_module(kp);
+    pk = env.kernel(pm.source, pm.kname, pm.smem);
+    smem = pm.smem;
+    grid = env.sm_count() * std::max(1, env.occupancy(pk, 256, smem));
+  }
+  auto launch_level = [&](int l) {
+    if (levels[l].empty()) return;
+    struct {
+      uint64_t items;
+      int64_t n;
+      uint64_t counter;
+      uint64_t err;
+      uint64_t args[64];
+    } ba;
+    if (kinds.plans.size() > 64) throw MapError("serving: too many kinds");
+    ba.items = (uint64_t)(uintptr_t)d_levels[l];
+    ba.n = (int64_t)levels[l].size();
+    ba.counter = (uint64_t)(uintptr_t)((char *)dbuf + 16 * l);
+    ba.err = (uint64_t)(uintptr_t)env.err_word();
+    for (size_t k = 0; k < kinds.plans.size(); k++) ba.args[k] = (uint64_t)(uintptr_t)d_kind_args[k];
+    env.launch(pk, std::min<int>(grid, (int)levels[l].size()), 256, smem, (CUstream_st *)st, &ba, 32 + 8 * kinds.plans.size());
+  };
+  launch_level(0);
+  for (auto &kv : radial) {
+    Many &mn = kv.second;
+    KernelHandle kh = env.kernel(mn.plan.source, mn.plan.kname + "_many", 0);
+    struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
+    env.launch(kh, 8 * mn.n, 512, 0, (CUstream_st *)st, &ma, sizeof ma);
+  }
+  launch_level(1);
+  for (auto &kv : spread) {
+    Many &mn = kv.second;
+    KernelHandle kh = env.kernel(mn.plan.source, mn.plan.kname + "_many", 0);
+    struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
+    env.launch(kh, mn.n, 1024, 0, (CUstream_st *)st, &ma, sizeof ma);
+  }
+  InFlight f;
+  f.reqs = batch;
+  f.stream = si;
+  f.dev_free.push_back(dbuf);
+  cuda_check(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventRecord(f.ev, st), "cudaEventRecord");
+  if (last_ev[si]) cudaEventDestroy(last_ev[si]);
+  cuda_check(cudaEventCreateWithFlags(&last_ev[si], cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventRecord(last_ev[si], st), "cudaEventRecord");
+  {
+    std::lock_guard<std::mutex> lk2(m);
+    batches++;
+    batched_requests += (long long)batch.size();
+    max_batch_seen = std::max<long long>(max_batch_seen, (long long)batch.size());
+    inflight.push_back(std::move(f));
+  }
+  cv_inflight.notify_all();
+}
+
+void Server::Impl::dispatch_loop() {
+  CudaEnv &env = CudaEnv::get();
+  cudaSetDevice(env.device());
+  while (true) {
+    std::vector<Req *> batch;
+    {
+      std::unique_lock<std::mutex> lk(m);
+      cv_pending.wait(lk, [&] { return stop || !pending.empty(); });
+      if (stop) return;
+      while (!pending.empty() && (int)batch.size() < max_batch) {
+        Req *r = pending.front();
+        if (used + r->bytes > budget && !(batch.empty() && inflight.empty() && used == 0)) break;
+        used += r->bytes;
+        peak_used = std::max(peak_used, used);
+        r->state = 1;
+        pending.pop_front();
+        batch.push_back(r);
+      }
+      if (batch.empty()) {
+        // memory is held by running batches: wait for a completion
+        cv_done.wait_for(lk, std::chrono::milliseconds(5));
+        continue;
+      }
+    }
+    try {
+      run_batch(batch);
+    } catch (const std::exception &e) {
+      std::lock_guard<std::mutex> lk(m);
+      for (Req *r : batch) {
+        r->state = 3;
+        r->err = e.what();
+      }
+      cv_done.notify_all();
+    }
+  }
+}
+
+void Server::Impl::complete_loop() {
+  CudaEnv &env = CudaEnv::get();
+  cudaSetDevice(env.device());
+  while (true) {
+    InFlight f;
+    {
+      std::unique_lock<std::mutex> lk(m);
+      cv_inflight.wait(lk, [&] { return stop || !inflight.empty(); });
+      if (inflight.empty() && stop) return;
+      f = std::move(inflight.front());
+      inflight.pop_front();
+    }
+    cudaError_t e = cudaEventSynchronize(f.ev);
+    const double t = now_s();
+    cudaEventDestroy(f.ev);
+    cudaStream_t st = streams[f.stream];
+    for (void *p : f.dev_free) cudaFreeAsync(p, st);
+    std::vector<Node *> unref;
+    {
+      std::lock_guard<std::mutex> lk(m);
+      for (Req *r : f.reqs) {
+        r->t_done = t;
+        if (e != cudaSuccess) {
+          r->state = 3;
+          r->err = cudaGetErrorString(e);
+          failed++;
+        } else {
+          r->state = 2;
+          completed++;
+        }
+        unref.push_back(r->out_node);
+        r->out_node = nullptr;
+        if (r->auto_release) {
+          free_request(r, st);
+          used -= r->bytes;
+          r->bytes = 0;
+        }
+      }
+    }
+    {
+      Runtime &rt = Runtime::get();
+      std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+      for (Node *n : unref)
+        if (n && rt.owns(n) && n->ref > 0) n->ref--;
+      if (++gc_counter % 64 == 0) rt.collect_garbage();
+    }
+    cv_done.notify_all();
+    cv_pending.notify_all();
+  }
+}
+
+Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch) : impl_(new Impl) {
+  if (!dem || W <= 0 || H <= 0 || pitch < (long long)W * 4) throw MapError("server: invalid DEM");
+  CudaEnv &env = CudaEnv::get();
+  env.ensure_device();
+  Impl &I = *impl_;
+  I.dem = dem;
+  I.pitch = pitch;
+  I.W = W;
+  I.H = H;
+  I.budget = budget_bytes;
+  I.max_batch = std::max(1, max_batch);
+  for (int i = 0; i < 2; i++) cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+  I.dispatcher = std::thread([&I] { I.dispatch_loop(); });
+  I.completer = std::thread([&I] { I.complete_loop(); });
+}
+
+Server::~Server() {
+  Impl &I = *impl_;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    I.stop = true;
+  }
+  I.cv_pending.notify_all();
+  I.cv_inflight.notify_all();
+  I.dispatcher.join();
+  // drain what is still running
+  {
+    std::unique_lock<std::mutex> lk(I.m);
+    I.stop = false;
+  }
+  I.cv_inflight.notify_all();
+  for (;;) {
+    std::unique_lock<std::mutex> lk(I.m);
+    if (I.inflight.empty()) break;
+    I.cv_done.wait_for(lk, std::chrono::milliseconds(5));
+  }
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    I.stop = true;
+  }
+  I.cv_inflight.notify_all();
+  I.completer.join();
+  for (int i = 0; i < 2; i++) {
+    cudaStreamSynchronize(I.streams[i]);
+    for (auto &kv : I.reqs) if (kv.second->stream == i) I.free_request(kv.second.get(), I.streams[i]);
+    cudaStreamSynchronize(I.streams[i]);
+    if (I.last_ev[i]) cudaEventDestroy(I.last_ev[i]);
+    cudaStreamDestroy(I.streams[i]);
+    if (I.stage[i]) cudaFreeHost(I.stage[i]);
+  }
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  for (auto &kv : I.reqs)
+    if (kv.second->out_node && rt.owns(kv.second->out_node) && kv.second->out_node->ref > 0) kv.second->out_node->ref--;
+}
+
+long long Server::submit(int type, int x0, int y0, int w, int h, int obs_x, int obs_y, float obs_h, double radius,
+                         bool auto_release) {
+  Impl &I = *impl_;
+  if (type < REQ_HILLSHADE || type > REQ_FLOW) throw MapError("server: unknown request type");
+  if (w <= 0 || h <= 0 || x0 < 0 || y0 < 0 || x0 + w > I.W || y0 + h > I.H) throw MapError("server: window outside the DEM");
+  if (type == REQ_VIEWSHED && (obs_x < 0 || obs_y < 0 || obs_x >= w || obs_y >= h))
+    throw MapError("server: observer outside the window");
+  auto r = std::make_unique<Req>();
+  r->type = type;
+  r->x0 = x0;
+  r->y0 = y0;
+  r->w = w;
+  r->h = h;
+  r->ox = obs_x;
+  r->oy = obs_y;
+  r->oh = obs_h;
+  r->radius = radius;
+  r->auto_release = auto_release;
+  r->bytes = request_bytes(type, w, h);
+  if (r->bytes > I.budget) throw MapError("server: request larger than the memory budget");
+  r->t_submit = now_s();
+  long long id;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    id = I.next_id++;
+    r->id = id;
+    I.pending.push_back(r.get());
+    I.reqs[id] = std::move(r);
+  }
+  I.cv_pending.notify_one();
+  return id;
+}
+
+int Server::wait(long long id, double timeout_s) {
+  Impl &I = *impl_;
+  std::unique_lock<std::mutex> lk(I.m);
+  auto it = I.reqs.find(id);
+  if (it == I.reqs.end()) throw MapError("server: unknown request");
+  Req *r = it->second.get();
+  auto done = [&] { return r->state >= 2; };
+  if (timeout_s < 0) I.cv_done.wait(lk, done);
+  else if (!I.cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), done)) return 1;
+  if (r->state == 3) throw MapError("server: request failed: " + r->err);
+  return 0;
+}
+
+void Server::result(long long id, void *dst, size_t bytes) {
+  wait(id, -1);
+  Impl &I = *impl_;
+  Req *r;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    r = I.reqs.at(id).get();
+    if (!r->out) throw MapError("server: result already released");
+  }
+  const size_t row = (size_t)r->w * dt_size(r->out_dt);
+  if (bytes < row * r->h) throw MapError("server: destination too small");
+  cuda_check(cudaMemcpy2D(dst, row, r->out, r->out_pitch, row, r->h, cudaMemcpyDeviceToHost), "result download");
+  release(id);
+}
+
+void Server::release(long long id) {
+  Impl &I = *impl_;
+  std::lock_guard<std::mutex> lk(I.m);
+  auto it = I.reqs.find(id);
+  if (it == I.reqs.end()) return;
+  Req *r = it->second.get();
+  if (r->state < 2) throw MapError("server: request still running");
+  I.free_request(r, I.streams[r->stream]);
+  I.used -= r->bytes;
+  r->bytes = 0;
+  I.cv_pending.notify_all();
+}
+
+double Server::latency_ms(long long id) {
+  Impl &I = *impl_;
+  std::lock_guard<std::mutex> lk(I.m);
+  Req *r = I.reqs.at(id).get();
+  return r->state == 2 ? (r->t_done - r->t_submit) * 1e3 : -1.0;
+}
+
+std::string Server::stats_json() {
+  Impl &I = *impl_;
+  std::lock_guard<std::mutex> lk(I.m);
+  std::ostringstream s;
+  s << "{\"batches\": " << I.batches << ", \"completed\": " << I.completed << ", \"failed\": " << I.failed
+    << ", \"mean_batch\": " << (I.batches ? (double)I.batched_requests / I.batches : 0.0)
+    << ", \"max_batch\": " << I.max_batch_seen << ", \"peak_bytes\": " << I.peak_used << ", \"budget_bytes\": " << I.budget
+    << "}";
+  return s.str();
+}
+
+namespace {
+double pct(std::vector<double> v, double p) {
+  if (v.empty()) return 0;
+  std::sort(v.begin(), v.end());
+  double idx = p / 100.0 * (v.size() - 1);
+  size_t lo = (size_t)std::floor(idx), hi = (size_t)std::ceil(idx);
+  return v[lo] + (v[hi] - v[lo]) * (idx - lo);
+}
+}  // namespace
+
+std::string Server::run_load(double rate, double seconds, const double *mix, unsigned seed, double obs_h, double radius) {
+  Impl &I = *impl_;
+  std::mt19937_64 rng(seed);
+  std::exponential_distribution<double> gap(rate);
+  std::discrete_distribution<int> pick(mix, mix + 4);
+  const int sizes[3] = {256, 512, 1024};
+  std::uniform_int_distribution<int> pick_size(0, 2);
+  std::vector<long long> ids;
+  std::vector<int> types, wsz;
+  const double t0 = now_s();
+  double t = 0;
+  long long cells = 0;
+  while (true) {
+    t += gap(rng);
+    if (t > seconds) break;
+    const int type = pick(rng);
+    const int w = sizes[pick_size(rng)];
+    const int h = w;
+    std::uniform_int_distribution<int> px(0, I.W - w), py(0, I.H - h), po(0, w - 1);
+    const int x0 = px(rng), y0 = py(rng), ox = po(rng), oy = po(rng);
+    const double target = t0 + t;
+    double dt = target - now_s();
+    if (dt > 0) std::this_thread::sleep_for(std::chrono::duration<double>(dt));
+    ids.push_back(submit(type, x0, y0, w, h, ox, oy, (float)obs_h, radius, true));
+    types.push_back(type);
+    wsz.push_back(w);
+    cells += (long long)w * h;
+  }
+  for (long long id : ids) wait(id, 120.0);
+  const double t_end = now_s();
+  std::vector<double> all, by_size[3], by_type[4];
+  for (size_t i = 0; i < ids.size(); i++) {
+    double l = latency_ms(ids[i]);
+    if (l < 0) continue;
+    all.push_back(l);
+    by_size[wsz[i] == 256 ? 0 : wsz[i] == 512 ? 1 : 2].push_back(l);
+    by_type[types[i]].push_back(l);
+  }
+  std::ostringstream s;
+  s.setf(std::ios::fixed);
+  s.precision(3);
+  const double wall = t_end - t0;
+  s << "{\"rate_req_s\": " << rate << ", \"seconds\": " << seconds << ", \"requests\": " << ids.size()
+    << ", \"completed\": " << all.size() << ", \"wall_s\": " << wall << ", \"throughput_req_s\": " << ids.size() / wall
+    << ", \"gcells_s\": " << cells / wall / 1e9 << ", \"p50_ms\": " << pct(all, 50) << ", \"p99_ms\": " << pct(all, 99)
+    << ", \"by_window\": {";
+  for (int k = 0; k < 3; k++)
+    s << (k ? ", " : "") << "\"" << sizes[k] << "\": {\"n\": " << by_size[k].size() << ", \"p50_ms\": " << pct(by_size[k], 50)
+      << ", \"p99_ms\": " << pct(by_size[k], 99) << "}";
+  const char *tn[4] = {"hillshade", "slope", "viewshed", "flow"};
+  s << "}, \"by_program\": {";
+  for (int k = 0; k < 4; k++)
+    s << (k ? ", " : "") << "\"" << tn[k] << "\": {\"n\": " << by_type[k].size() << ", \"p50_ms\": " << pct(by_type[k], 50)
+      << ", \"p99_ms\": " << pct(by_type[k], 99) << "}";
+  s << "}, \"server\": " << stats_json() << "}";
+  return s.str();
+}
+
+}  // namespace mapb

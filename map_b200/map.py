@@ -918,3 +918,68 @@ _sig('ma_batchPrepare', [ct.c_void_p, ct.c_int], ct.c_int)
 _sig('ma_batchRun', [ct.c_void_p, ct.c_int], ct.c_int)
 _sig('ma_batchInfo', [ct.c_void_p, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_batchDestroy', [ct.c_void_p], None, check=False)
+
+
+class Server:
+    """Serving over a device-resident DEM with continuous batching (ma_server*)."""
+    HILLSHADE, SLOPE, VIEWSHED, FLOW = 0, 1, 2, 3
+
+    def __init__(self, dem_ptr, pitch, width, height, budget_bytes, max_batch=256):
+        self._h = _lib.ma_serverCreate(ct.c_void_p(dem_ptr), pitch, width, height, budget_bytes, max_batch)
+
+    def submit(self, kind, x0, y0, w, h, obs=(0, 0), obs_h=10.0, radius=0.0):
+        return _lib.ma_serverSubmit(self._h, kind, x0, y0, w, h, obs[0], obs[1], obs_h, radius)
+
+    def wait(self, rid, timeout=-1.0):
+        return _lib.ma_serverWait(self._h, rid, timeout)
+
+    def result(self, rid, shape, dtype):
+        import numpy as np
+        out = np.empty(shape, dtype=dtype)
+        _lib.ma_serverResult(self._h, rid, out.ctypes.data_as(ct.c_void_p), out.nbytes)
+        return out
+
+    def release(self, rid):
+        _lib.ma_serverRelease(self._h, rid)
+
+    def latency_ms(self, rid):
+        return _lib.ma_serverLatency(self._h, rid)
+
+    def stats(self):
+        import json
+        n = _lib.ma_serverStats(self._h, None, 0)
+        buf = ct.create_string_buffer(n)
+        _lib.ma_serverStats(self._h, buf, n)
+        return json.loads(buf.value.decode())
+
+    def load(self, rate, seconds, mix=(0.5, 0.2, 0.15, 0.15), seed=0, obs_h=10.0, radius=167.0):
+        import json
+        m = (ct.c_double * 4)(*mix)
+        cap = 1 << 16
+        buf = ct.create_string_buffer(cap)
+        n = _lib.ma_serverLoad(self._h, rate, seconds, m, seed, obs_h, radius, buf, cap)
+        return json.loads(buf.value.decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.ma_serverDestroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_sig('ma_serverCreate', [ct.c_void_p, ct.c_longlong, ct.c_int, ct.c_int, ct.c_size_t, ct.c_int], ct.c_void_p)
+_sig('ma_serverSubmit', [ct.c_void_p, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_int, ct.c_float,
+                         ct.c_double], ct.c_longlong)
+_sig('ma_serverWait', [ct.c_void_p, ct.c_longlong, ct.c_double], ct.c_int)
+_sig('ma_serverResult', [ct.c_void_p, ct.c_longlong, ct.c_void_p, ct.c_size_t], ct.c_int)
+_sig('ma_serverRelease', [ct.c_void_p, ct.c_longlong], ct.c_int)
+_sig('ma_serverLatency', [ct.c_void_p, ct.c_longlong], ct.c_double)
+_sig('ma_serverStats', [ct.c_void_p, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_serverLoad', [ct.c_void_p, ct.c_double, ct.c_double, ct.POINTER(ct.c_double), ct.c_uint, ct.c_double,
+                       ct.c_double, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_serverDestroy', [ct.c_void_p], None)
