@@ -153,7 +153,7 @@ PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &
       << "    switch (w.kind) {\n";
   for (size_t k = 0; k < kinds.size(); k++)
     src << "      case " << k << ": ok = k" << k << "::run_tile(((const k" << k << "::Args *)b.args[" << k
-        << "])[w.inst], (int)w.tile, smem, bar, phase); break;\n";
+        << "])[w.inst], (int)w.tile, smem, bar, phase, true); break;\n";
   src << "      default: skel_fail((u32 *)b.err, ERR_BAD_LAUNCH); ok = false;\n"
       << "    }\n"
       << "    if (!ok) break;\n"

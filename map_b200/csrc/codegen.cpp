@@ -401,7 +401,8 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   body << "}\n";
   body << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
   body << G.center_loads(true) << G.body(false) << G.stores() << "}\n";
-  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase) {\n"
+  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
+       << "                                         bool gdesc) {\n"
        << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
        << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
        << "  const int x = t.x0 + lx;\n"
@@ -420,7 +421,7 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
        << "}\n";
   wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  u32 phase = 0;\n"
-       << "  run_tile(a, blockIdx.x, nullptr, nullptr, phase);\n"
+       << "  run_tile(a, blockIdx.x, nullptr, nullptr, phase, false);\n"
        << "}\n";
 }
 
@@ -483,7 +484,9 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
        << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
        << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n"
        << "    }\n";
-  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase) {\n"
+  // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
+  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
+       << "                                         bool gdesc) {\n"
        << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n";
   if (use_tma) {
     size_t total = 0;
@@ -491,8 +494,9 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << "  if (tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ")) {\n"
          << "    __syncthreads();   // earlier readers of the staging buffer are done\n"
          << "    if (threadIdx.x == 0) {\n"
-         << "      fence_proxy_async();\n"
-         << "      mbar_arrive_expect_tx(bar, " << total << "u);\n";
+         << "      fence_proxy_async();\n";
+    for (int k = 0; k < nst; k++) body << "      if (gdesc) tensormap_acquire(&a.tm[" << k << "]);\n";
+    body << "      mbar_arrive_expect_tx(bar, " << total << "u);\n";
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
       body << "      tma_load_2d(smem + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
@@ -526,9 +530,9 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     wrap << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
          << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
          << "  __syncthreads();\n"
-         << "  run_tile(a, blockIdx.x, smem, bar, phase);\n";
+         << "  run_tile(a, blockIdx.x, smem, bar, phase, false);\n";
   else
-    wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase);\n";
+    wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
   wrap << "}\n";
   if (!use_tma) P.tma.clear();
 }

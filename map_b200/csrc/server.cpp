@@ -94,6 +94,33 @@ struct Server::Impl {
   // pinned staging for argument / work-list uploads, one per stream
   void *stage[2] = {nullptr, nullptr};
   size_t stage_cap[2] = {0, 0};
+  // Local / Focal kinds seen so far, in registration order; the persistent
+  // module holds all of them, so it is rebuilt (compiled) only when a new kind appears
+  std::vector<KernelPlan> reg_plans;
+  std::map<std::string, int> reg_index;
+  int module_kinds = -1;
+  PersistentModule pm;
+  KernelHandle pk;
+  int pk_grid = 0;
+  int register_kind(const KernelPlan &P) {
+    auto it = reg_index.find(P.body);
+    if (it != reg_index.end()) return it->second;
+    int k = (int)reg_plans.size();
+    reg_index[P.body] = k;
+    reg_plans.push_back(P);
+    return k;
+  }
+  void ensure_module() {
+    if (module_kinds == (int)reg_plans.size() || reg_plans.empty()) return;
+    CudaEnv &env = CudaEnv::get();
+    std::vector<const KernelPlan *> kp;
+    for (auto &p : reg_plans) kp.push_back(&p);
+    pm = build_persistent_module(kp);
+    pk = env.kernel(pm.source, pm.kname, pm.smem);
+    pk_grid = env.sm_count() * std::max(1, env.occupancy(pk, 256, pm.smem));
+    module_kinds = (int)reg_plans.size();
+  }
+  void warm_up();
   // statistics
   long long batches = 0, completed = 0, failed = 0, max_batch_seen = 0, batched_requests = 0;
   size_t peak_used = 0;
@@ -123,12 +150,8 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
 
   Runtime &rt = Runtime::get();
   std::lock_guard<std::recursive_mutex> lk(rt.mtx);
-  struct KindSet {
-    std::map<std::string, int> index;
-    std::vector<KernelPlan> plans;
-    std::vector<std::vector<unsigned char>> args;
-    std::vector<int> members;
-  } kinds;
+  std::vector<std::vector<unsigned char>> kind_args;   // per registered kind, this batch's members
+  std::vector<int> kind_members;
   struct Item { uint32_t kind, inst, tile, pad; };
   std::vector<std::vector<Item>> levels(2);
   struct Many { KernelPlan plan; std::vector<unsigned char> args; int n = 0; };
@@ -203,21 +226,15 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
         }
         if (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL) {
           if (lv > 1) throw MapError("serving: program too deep");
-          auto it = kinds.index.find(P.body);
-          int k;
-          if (it == kinds.index.end()) {
-            k = (int)kinds.plans.size();
-            kinds.index[P.body] = k;
-            kinds.plans.push_back(P);
-            kinds.args.emplace_back();
-            kinds.members.push_back(0);
-          } else {
-            k = it->second;
+          const int k = register_kind(P);
+          if ((int)kind_args.size() <= k) {
+            kind_args.resize(k + 1);
+            kind_members.resize(k + 1, 0);
           }
           uint64_t aux[4] = {0, 0, 0, 0};
           auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
-          kinds.args[k].insert(kinds.args[k].end(), a.begin(), a.end());
-          const uint32_t idx = (uint32_t)kinds.members[k]++;
+          kind_args[k].insert(kind_args[k].end(), a.begin(), a.end());
+          const uint32_t idx = (uint32_t)kind_members[k]++;
           const int tiles = ((g.W + P.tile_w - 1) / P.tile_w) * ((g.H + P.tile_h - 1) / P.tile_h);
           for (int t = 0; t < tiles; t++) levels[lv].push_back(Item{(uint32_t)k, idx, (uint32_t)t, 0});
         } else if (g.skeleton == SK_RADIAL) {
@@ -260,8 +277,10 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   }
   batch = ok;
   // stage every upload into this stream's pinned buffer
+  kind_args.resize(reg_plans.size());
+  kind_members.resize(reg_plans.size(), 0);
   std::vector<std::pair<const void *, size_t>> blobs;
-  for (auto &a : kinds.args) blobs.push_back({a.data(), a.size()});
+  for (auto &a : kind_args) blobs.push_back({a.data(), std::max<size_t>(a.size(), 1)});
   for (auto &lv : levels) blobs.push_back({lv.data(), lv.size() * sizeof(Item)});
   for (auto &kv : radial) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
   for (auto &kv : spread) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
@@ -285,22 +304,14 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   cuda_check(cudaMemcpyAsync(dbuf, stage[si], off, cudaMemcpyHostToDevice, st), "upload batch arrays");
   size_t bi = 0;
   std::vector<void *> d_kind_args;
-  for (size_t k = 0; k < kinds.args.size(); k++) d_kind_args.push_back(dptr[bi++]);
+  for (size_t k = 0; k < kind_args.size(); k++) d_kind_args.push_back(dptr[bi++]);
   std::vector<void *> d_levels;
   for (size_t l = 0; l < levels.size(); l++) d_levels.push_back(dptr[bi++]);
 
   // persistent launch per level over the Local / Focal kinds; radial after level 0; spread after level 1
-  KernelHandle pk;
-  int grid = 0;
-  size_t smem = 0;
-  if (!kinds.plans.empty()) {
-    std::vector<const KernelPlan *> kp;
-    for (auto &p : kinds.plans) kp.push_back(&p);
-    PersistentModule pm = build_persistent_module(kp);
-    pk = env.kernel(pm.source, pm.kname, pm.smem);
-    smem = pm.smem;
-    grid = env.sm_count() * std::max(1, env.occupancy(pk, 256, smem));
-  }
+  ensure_module();
+  const size_t smem = pm.smem;
+  const int grid = pk_grid;
   auto launch_level = [&](int l) {
     if (levels[l].empty()) return;
     struct {
@@ -310,13 +321,13 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
       uint64_t err;
       uint64_t args[64];
     } ba;
-    if (kinds.plans.size() > 64) throw MapError("serving: too many kinds");
+    if (reg_plans.size() > 64) throw MapError("serving: too many kinds");
     ba.items = (uint64_t)(uintptr_t)d_levels[l];
     ba.n = (int64_t)levels[l].size();
     ba.counter = (uint64_t)(uintptr_t)((char *)dbuf + 16 * l);
     ba.err = (uint64_t)(uintptr_t)env.err_word();
-    for (size_t k = 0; k < kinds.plans.size(); k++) ba.args[k] = (uint64_t)(uintptr_t)d_kind_args[k];
-    env.launch(pk, std::min<int>(grid, (int)levels[l].size()), 256, smem, (CUstream_st *)st, &ba, 32 + 8 * kinds.plans.size());
+    for (size_t k = 0; k < reg_plans.size(); k++) ba.args[k] = (uint64_t)(uintptr_t)d_kind_args[k];
+    env.launch(pk, std::min<int>(grid, (int)levels[l].size()), 256, smem, (CUstream_st *)st, &ba, 32 + 8 * reg_plans.size());
   };
   launch_level(0);
   for (auto &kv : radial) {
@@ -439,6 +450,27 @@ void Server::Impl::complete_loop() {
   }
 }
 
+// Registers and compiles every program kind up front (templates over a 64x64
+// window of the DEM), so no request waits for a compilation.
+void Server::Impl::warm_up() {
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  CudaEnv &env = CudaEnv::get();
+  const int w = std::min(64, W), h = std::min(64, H);
+  Node *win = rt.dev_input(dem, pitch, Arr2{{w, h}, 2}, F32, Arr2{{w, h}, 2});
+  std::vector<Node *> outs = {prog_hillshade(rt, win), prog_slope(rt, win),
+                              prog_viewshed(rt, win, w / 2, h / 2, 10.0f, 16.0), prog_flow(rt, win)};
+  for (Node *o : outs) {
+    FusionResult fr = fuse(collect_nodes({o}), {o});
+    for (auto &gp : fr.groups) {
+      KernelPlan P = generate_kernel(*gp);
+      if (gp->skeleton == SK_LOCAL || gp->skeleton == SK_FOCAL) register_kind(P);
+      else if (gp->skeleton == SK_RADIAL || gp->skeleton == SK_SPREAD) env.kernel(P.source, P.kname + "_many", 0);
+    }
+  }
+  ensure_module();
+}
+
 Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch) : impl_(new Impl) {
   if (!dem || W <= 0 || H <= 0 || pitch < (long long)W * 4) throw MapError("server: invalid DEM");
   CudaEnv &env = CudaEnv::get();
@@ -451,6 +483,7 @@ Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, in
   I.budget = budget_bytes;
   I.max_batch = std::max(1, max_batch);
   for (int i = 0; i < 2; i++) cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+  I.warm_up();
   I.dispatcher = std::thread([&I] { I.dispatch_loop(); });
   I.completer = std::thread([&I] { I.complete_loop(); });
 }

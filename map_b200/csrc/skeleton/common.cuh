@@ -147,6 +147,13 @@ __device__ __forceinline__ bool mbar_wait_bounded(u64 *bar, u32 parity, u32 limi
   return false;
 }
 
+// A tensor map that lives in global memory and was written through the generic
+// proxy (e.g. an argument array copied from the host into reused memory) must be
+// acquired by the tensor-map proxy before a TMA load uses it.
+__device__ __forceinline__ void tensormap_acquire(const TmaDesc *tmap) {
+  asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"((u64)tmap) : "memory");
+}
+
 // 2-D tiled TMA load of box (x, y) of `tmap` into shared memory; completion is
 // signalled on `bar` (complete_tx). x must be a multiple of 16 bytes of elements.
 __device__ __forceinline__ void tma_load_2d(void *dst, const TmaDesc *tmap, u64 *bar, int x, int y) {
