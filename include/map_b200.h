@@ -185,6 +185,23 @@ size_t ma_serverLoad(ma_Server *s, double rate, double seconds, const double *mi
                      double radius, char *buf, size_t len);
 void ma_serverDestroy(ma_Server *s);
 
+/* Per-zone statistics (no counterpart in the reference, whose zonal skeleton
+ * runtime/skeleton/ZonalSkeleton.cpp:33-292 reduces a whole raster to one
+ * value): for every zone id 0 .. nzones-1 of the int32 `zone` raster, the
+ * count, min, max, float32 sum and mean of the float32 `value` cells in it.
+ * Cells with a zone id outside [0, nzones) or a NaN value are skipped; an empty
+ * zone reports count 0, sum 0, min +inf, max -inf, mean NaN. All pointers are
+ * device memory; rasters are row-major with the given pitches in bytes
+ * (4-byte aligned; 16-byte aligned pointers and pitches take the vector path);
+ * the outputs are arrays of nzones elements and any of them may be NULL.
+ * Enqueued on `stream` (a cudaStream_t, NULL for the legacy default stream);
+ * returns before the work ends. Working bins of nzones x 24 bytes come from the
+ * stream's memory pool. count, min and max are exact; the sum's rounding depends
+ * on the order of the device's atomic additions. */
+int ma_zoneStats(const void *value, long long value_pitch, const void *zone, long long zone_pitch, int W, int H,
+                 int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum, float *mean,
+                 void *stream);
+
 /* Introspection for tests and tools. */
 int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
 int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */

@@ -4,6 +4,7 @@
 #include "../../include/map_b200.h"
 #include "batch.hpp"
 #include "server.hpp"
+#include "zonestats.hpp"
 #include "codegen.hpp"
 #include "cuda_env.hpp"
 #include "executor.hpp"
@@ -665,6 +666,29 @@ void ma_serverDestroy(ma_Server *h) {
   } catch (const std::exception &e) {
     fail(e.what());
   }
+}
+
+int ma_zoneStats(const void *value, long long value_pitch, const void *zone, long long zone_pitch, int W, int H,
+                 int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum, float *mean,
+                 void *stream) {
+  return int_call([&] {
+    CudaEnv::get().ensure_device();
+    ZoneStatsArgs a;
+    a.value = value;
+    a.value_pitch = value_pitch;
+    a.zone = zone;
+    a.zone_pitch = zone_pitch;
+    a.W = W;
+    a.H = H;
+    a.nzones = nzones;
+    a.count = count;
+    a.vmin = vmin;
+    a.vmax = vmax;
+    a.sum = sum;
+    a.mean = mean;
+    zone_stats(a, (CUstream_st *)stream);
+    return 0;
+  });
 }
 
 int ma_nodeCount(void) { return (int)Runtime::get().nodes.size(); }

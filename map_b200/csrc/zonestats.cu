@@ -1,0 +1,328 @@
+// Per-zone statistics of a float32 value raster over an int32 zone raster:
+// count, min, max, sum and mean of the values of every zone 0 .. nzones-1.
+//
+// The reference's zonal skeleton (runtime/skeleton/ZonalSkeleton.cpp:33-292)
+// reduces a whole raster to one scalar; a zone raster that splits the
+// reduction into bins is a new operation of this library. The per-cell rules
+// are those of the reference's reductions (runtime/skeleton/util.cpp:518-540,
+// util/ReductionType.cpp): SUM adds in float32, MIN / MAX compare.
+//
+// Rules of this operation:
+//   * a cell counts when its zone id is in [0, nzones) and its value is not NaN;
+//     other cells are skipped (zone ids outside the range are "no data");
+//   * min / max order floats as IEEE totalOrder does for non-NaN values
+//     (-0 before +0), so they are exact and independent of the visiting order;
+//   * count is exact (64-bit); sum accumulates in float32 (its rounding depends on
+//     the order in which the hardware serves the atomics, so it may differ in the
+//     last bits between runs); mean = sum / (float)count;
+//   * an empty zone reports count 0, sum 0, min +inf, max -inf, mean NaN.
+//
+// Kernels (one pass over the rasters, HBM-bound: 8 bytes per cell):
+//   1. zs_accumulate: a persistent grid; each CTA owns a contiguous range of
+//      128-cell row chunks and keeps the zones' bins in shared memory. A warp loads
+//      a chunk with 16-byte loads (4 cells per lane), folds each lane's cells of its
+//      leading zone, merges equal-zone runs of lanes with a segmented shuffle scan,
+//      and the last lane of each run updates the shared bins with atomics. At the
+//      end the CTA adds its non-empty bins into the global bins with atomics.
+//      Zone counts whose bins do not fit in shared memory use the global bins
+//      directly.
+//   2. zs_finalize: converts the global bins into the caller's output arrays.
+// Global bins must start at zero before step 1 (a zero bin is the empty bin:
+// min / max are kept as order-preserving integer keys whose empty value is 0).
+#include "zonestats.hpp"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <mutex>
+#include <string>
+
+namespace mapb {
+namespace {
+
+struct Bin {
+  unsigned long long count;
+  float sum;
+  unsigned nmin;   // ~key(min): atomicMax of ~key is atomicMin of key
+  unsigned max;    // key(max)
+  unsigned pad;
+};
+static_assert(sizeof(Bin) == 24, "bin layout");
+
+constexpr int kThreads = 256;
+constexpr int kUnroll = 4;           // chunks in flight per warp
+constexpr int kChunk = 128;          // cells per warp chunk (32 lanes x 4)
+constexpr int kMaxSmemZones = 8192;  // 128 KiB of shared bins
+
+// Order-preserving map of a non-NaN float to an unsigned key in [1, 2^32-1).
+__device__ __forceinline__ unsigned fkey(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+__device__ __forceinline__ float fkey_inv(unsigned k) {
+  return __uint_as_float((k & 0x80000000u) ? (k & 0x7fffffffu) : ~k);
+}
+
+struct SmemBins {
+  unsigned *cnt;
+  float *sum;
+  unsigned *nmin;
+  unsigned *max;
+};
+
+template <bool SMEM>
+__device__ __forceinline__ void bin_add(const SmemBins &s, Bin *g, int z, unsigned c, float sm, unsigned nmn,
+                                        unsigned mx) {
+  if (SMEM) {
+    atomicAdd(&s.cnt[z], c);
+    atomicAdd(&s.sum[z], sm);
+    atomicMax(&s.nmin[z], nmn);
+    atomicMax(&s.max[z], mx);
+  } else {
+    atomicAdd(&g[z].count, (unsigned long long)c);
+    atomicAdd(&g[z].sum, sm);
+    atomicMax(&g[z].nmin, nmn);
+    atomicMax(&g[z].max, mx);
+  }
+}
+
+struct Geometry {
+  const char *val;
+  long long vpitch;
+  const char *zone;
+  long long zpitch;
+  int W, H, nzones;
+  long long nchunk_x;      // chunks per row
+  long long chunks;        // total chunks
+  long long per_cta;       // chunks per CTA (contiguous range)
+  int vec;                 // 16-byte loads allowed for full chunks
+};
+
+template <bool SMEM>
+__global__ void __launch_bounds__(kThreads) zs_accumulate(const Geometry geo, Bin *gbins) {
+  extern __shared__ __align__(16) unsigned char zs_smem[];
+  SmemBins sb = {nullptr, nullptr, nullptr, nullptr};
+  const int nz = geo.nzones;
+  if (SMEM) {
+    sb.cnt = (unsigned *)zs_smem;
+    sb.sum = (float *)(sb.cnt + nz);
+    sb.nmin = (unsigned *)(sb.sum + nz);
+    sb.max = sb.nmin + nz;
+    for (int i = threadIdx.x; i < 4 * nz; i += blockDim.x) ((unsigned *)zs_smem)[i] = 0u;
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const long long c0 = (long long)blockIdx.x * geo.per_cta;
+  const long long c1 = min(geo.chunks, c0 + geo.per_cta);
+  const unsigned below = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);   // lanes <= this one
+
+  for (long long cb = c0 + (long long)warp * kUnroll; cb < c1; cb += (long long)nwarps * kUnroll) {
+    float v[kUnroll][4];
+    int z[kUnroll][4];
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) {
+      const long long c = cb + u;
+#pragma unroll
+      for (int j = 0; j < 4; j++) z[u][j] = -1;
+      if (c < c1) {
+        const long long y = c / geo.nchunk_x;
+        const int x = (int)(c - y * geo.nchunk_x) * kChunk + lane * 4;
+        const float *vr = (const float *)(geo.val + y * geo.vpitch);
+        const int *zr = (const int *)(geo.zone + y * geo.zpitch);
+        if (geo.vec && x + 3 < geo.W) {
+          const float4 a = __ldcs((const float4 *)(vr + x));
+          const int4 b = __ldcs((const int4 *)(zr + x));
+          v[u][0] = a.x; v[u][1] = a.y; v[u][2] = a.z; v[u][3] = a.w;
+          z[u][0] = b.x; z[u][1] = b.y; z[u][2] = b.z; z[u][3] = b.w;
+        } else {
+#pragma unroll
+          for (int j = 0; j < 4; j++)
+            if (x + j < geo.W) {
+              v[u][j] = __ldcs(vr + x + j);
+              z[u][j] = __ldcs(zr + x + j);
+            }
+        }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) {
+      // lane aggregate over the cells of the lane's first counted zone
+      int key = -1;
+      unsigned cnt = 0, nmn = 0, mx = 0;
+      float sm = 0.0f;
+#pragma unroll
+      for (int j = 0; j < 4; j++) {
+        const int zz = z[u][j];
+        const float vv = v[u][j];
+        if ((unsigned)zz >= (unsigned)nz || vv != vv) continue;
+        const unsigned k = fkey(vv);
+        if (key < 0) key = zz;
+        if (zz == key) {
+          cnt++;
+          sm = (cnt == 1) ? vv : sm + vv;
+          nmn = max(nmn, ~k);
+          mx = max(mx, k);
+        } else {
+          bin_add<SMEM>(sb, gbins, zz, 1u, vv, ~k, k);   // a lane straddling a zone edge
+        }
+      }
+      // segmented inclusive scan over runs of lanes with equal keys
+      const int up = __shfl_up_sync(0xffffffffu, key, 1);
+      const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || up != key);
+      const int seg_start = 31 - __clz(heads & below);
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const unsigned c2 = __shfl_up_sync(0xffffffffu, cnt, off);
+        const float s2 = __shfl_up_sync(0xffffffffu, sm, off);
+        const unsigned n2 = __shfl_up_sync(0xffffffffu, nmn, off);
+        const unsigned m2 = __shfl_up_sync(0xffffffffu, mx, off);
+        if (lane - off >= seg_start) {
+          sm = s2 + sm;
+          cnt += c2;
+          nmn = max(nmn, n2);
+          mx = max(mx, m2);
+        }
+      }
+      const int dn = __shfl_down_sync(0xffffffffu, key, 1);
+      const bool tail = lane == 31 || dn != key;
+      if (tail && key >= 0 && cnt > 0) bin_add<SMEM>(sb, gbins, key, cnt, sm, nmn, mx);
+    }
+  }
+  if (SMEM) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nz; i += blockDim.x) {
+      const unsigned c = sb.cnt[i];
+      if (c == 0) continue;
+      atomicAdd(&gbins[i].count, (unsigned long long)c);
+      atomicAdd(&gbins[i].sum, sb.sum[i]);
+      atomicMax(&gbins[i].nmin, sb.nmin[i]);
+      atomicMax(&gbins[i].max, sb.max[i]);
+    }
+  }
+}
+
+__global__ void zs_finalize(const Bin *gbins, int nz, unsigned long long *count, float *vmin, float *vmax, float *sum,
+                            float *mean) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nz) return;
+  const Bin b = gbins[i];
+  if (count) count[i] = b.count;
+  if (sum) sum[i] = b.sum;
+  if (vmin) vmin[i] = b.count ? fkey_inv(~b.nmin) : INFINITY;
+  if (vmax) vmax[i] = b.count ? fkey_inv(b.max) : -INFINITY;
+  if (mean) mean[i] = b.count ? b.sum / (float)b.count : NAN;
+}
+
+void check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) throw MapError(std::string("zone statistics: ") + what + ": " + cudaGetErrorString(e));
+}
+
+struct DevInfo {
+  int sms = 0;
+  bool ready = false;
+};
+
+DevInfo &dev_info() {
+  static std::mutex m;
+  static DevInfo info[64];
+  int d = 0;
+  check(cudaGetDevice(&d), "cudaGetDevice");
+  if (d < 0 || d >= 64) throw MapError("zone statistics: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(m);
+  DevInfo &I = info[d];
+  if (!I.ready) {
+    check(cudaDeviceGetAttribute(&I.sms, cudaDevAttrMultiProcessorCount, d), "cudaDeviceGetAttribute");
+    check(cudaFuncSetAttribute(zs_accumulate<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               kMaxSmemZones * 16),
+          "cudaFuncSetAttribute");
+    I.ready = true;
+  }
+  return I;
+}
+
+}  // namespace
+
+static void zone_stats_validate(const ZoneStatsArgs &a) {
+  if (a.W < 0 || a.H < 0) throw MapError("zone statistics: negative raster size");
+  if (a.nzones < 1) throw MapError("zone statistics: nzones must be at least 1");
+  if (a.W > 0 && a.H > 0) {
+    if (!a.value || !a.zone) throw MapError("zone statistics: null raster pointer");
+    if (a.value_pitch < (long long)a.W * 4 || a.zone_pitch < (long long)a.W * 4)
+      throw MapError("zone statistics: pitch smaller than a row");
+    if (((uintptr_t)a.value | (uintptr_t)a.zone) % 4 != 0 || a.value_pitch % 4 != 0 || a.zone_pitch % 4 != 0)
+      throw MapError("zone statistics: rasters and pitches must be 4-byte aligned");
+  }
+}
+
+// Enqueues the accumulation and finalisation on `st`; `bins` holds
+// zone_stats_bin_bytes(nzones) bytes of zeros.
+static void zone_stats_run(const ZoneStatsArgs &a, void *bins, cudaStream_t st) {
+  DevInfo &I = dev_info();
+  const long long cells = (long long)a.W * a.H;
+  if (cells > 0) {
+    Geometry g;
+    g.val = (const char *)a.value;
+    g.vpitch = a.value_pitch;
+    g.zone = (const char *)a.zone;
+    g.zpitch = a.zone_pitch;
+    g.W = a.W;
+    g.H = a.H;
+    g.nzones = a.nzones;
+    g.nchunk_x = (a.W + kChunk - 1) / kChunk;
+    g.chunks = g.nchunk_x * a.H;
+    g.vec = (((uintptr_t)a.value | (uintptr_t)a.zone) % 16 == 0 && a.value_pitch % 16 == 0 &&
+             a.zone_pitch % 16 == 0)
+                ? 1
+                : 0;
+    const bool smem = a.nzones <= kMaxSmemZones;
+    const size_t smem_bytes = smem ? (size_t)a.nzones * 16 : 0;
+    int occ = 0;
+    if (smem)
+      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, zs_accumulate<true>, kThreads, smem_bytes),
+            "occupancy");
+    else
+      check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, zs_accumulate<false>, kThreads, 0), "occupancy");
+    occ = std::max(1, occ);
+    // enough chunks per CTA that every warp has work; per-CTA counts stay below 2^32
+    const long long max_ctas = (long long)I.sms * occ;
+    long long ctas = std::min<long long>(max_ctas, (g.chunks + (kThreads / 32) * kUnroll - 1) /
+                                                       ((kThreads / 32) * kUnroll));
+    // per-CTA shared counts are 32-bit: at most 2^31 cells per CTA
+    ctas = std::max<long long>(ctas, (g.chunks + (1LL << 24) - 1) >> 24);
+    ctas = std::max<long long>(1, ctas);
+    g.per_cta = (g.chunks + ctas - 1) / ctas;
+    ctas = (g.chunks + g.per_cta - 1) / g.per_cta;
+    if (smem)
+      zs_accumulate<true><<<(unsigned)ctas, kThreads, smem_bytes, st>>>(g, (Bin *)bins);
+    else
+      zs_accumulate<false><<<(unsigned)ctas, kThreads, 0, st>>>(g, (Bin *)bins);
+    check(cudaGetLastError(), "accumulate launch");
+  }
+  zs_finalize<<<(a.nzones + 255) / 256, 256, 0, st>>>((const Bin *)bins, a.nzones, a.count, a.vmin, a.vmax, a.sum,
+                                                       a.mean);
+  check(cudaGetLastError(), "finalize launch");
+}
+
+static size_t zone_stats_bin_bytes(int nzones) { return (size_t)nzones * sizeof(Bin); }
+
+void zone_stats(const ZoneStatsArgs &a, cudaStream_t st) {
+  zone_stats_validate(a);
+  const size_t bytes = zone_stats_bin_bytes(a.nzones);
+  void *bins = nullptr;
+  check(cudaMallocAsync(&bins, bytes, st), "cudaMallocAsync(bins)");
+  cudaError_t e = cudaMemsetAsync(bins, 0, bytes, st);
+  if (e == cudaSuccess) {
+    try {
+      zone_stats_run(a, bins, st);
+    } catch (...) {
+      cudaFreeAsync(bins, st);
+      throw;
+    }
+  }
+  cudaFreeAsync(bins, st);
+  check(e, "cudaMemsetAsync(bins)");
+}
+
+}  // namespace mapb

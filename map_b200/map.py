@@ -737,6 +737,64 @@ def viewshed(dem, obs, h):
     return (maxr * dist + h) - dem
 
 
+def zonal_stats_device(value_ptr, value_pitch, zone_ptr, zone_pitch, W, H, nzones, count=0, vmin=0, vmax=0, sum=0,
+                       mean=0, stream=None):
+    """Per-zone statistics over device memory (pointers as ints, pitches in
+    bytes); enqueued on `stream` (default: the library's stream), returns at
+    once. Outputs are device arrays of `nzones` elements (0 to skip one)."""
+    _lib.ma_zoneStats(ct.c_void_p(value_ptr), value_pitch, ct.c_void_p(zone_ptr), zone_pitch, W, H, nzones,
+                      ct.c_void_p(count), ct.c_void_p(vmin), ct.c_void_p(vmax), ct.c_void_p(sum),
+                      ct.c_void_p(mean), ct.c_void_p(_lib.ma_stream() if stream is None else stream))
+
+
+def zonal_stats(value, zones, nzones):
+    """Per-zone count / min / max / sum / mean of a float32 raster over an int32
+    zone raster (a Raster or a 2-D NumPy array each). Cells with a zone id
+    outside [0, nzones) or a NaN value are skipped. Returns a dict of NumPy
+    arrays of `nzones` elements: count (uint64), min, max, sum, mean (float32)."""
+    import numpy as np
+    bufs = []
+
+    def stage(x, dt, npdt):
+        if isinstance(x, Raster):
+            if x.datatype() != dt:
+                raise MapError("zonal_stats: raster has datatype %s, %s expected" % (DataTypeId[x.datatype()],
+                                                                                     DataTypeId[dt]))
+            w, h = x.datasize()
+            ptr = _lib.ma_devAlloc(max(1, w * h * 4))
+            bufs.append(ptr)
+            to_device(x, ptr, w * 4)
+            return ptr, w, h
+        a = np.ascontiguousarray(x, dtype=npdt)
+        if a.ndim != 2:
+            raise MapError("zonal_stats: arrays must be 2-D")
+        ptr = _lib.ma_devAlloc(max(1, a.nbytes))
+        bufs.append(ptr)
+        if a.nbytes:
+            _lib.ma_memcpy(ptr, a.ctypes.data_as(ct.c_void_p), a.nbytes, 1)
+        return ptr, a.shape[1], a.shape[0]
+
+    try:
+        vp, w, h = stage(value, F32, np.float32)
+        zp, zw, zh = stage(zones, S32, np.int32)
+        if (w, h) != (zw, zh):
+            raise MapError("zonal_stats: value and zone rasters differ in size")
+        nz = int(nzones)
+        out = _lib.ma_devAlloc(max(1, nz) * 24)
+        bufs.append(out)
+        zonal_stats_device(vp, w * 4, zp, w * 4, w, h, nz, out, out + 8 * nz, out + 12 * nz, out + 16 * nz,
+                           out + 20 * nz)
+        _lib.ma_sync()
+        raw = np.empty(nz * 24, np.uint8)
+        _lib.ma_memcpy(raw.ctypes.data_as(ct.c_void_p), out, raw.nbytes, 2)
+        f = raw[8 * nz:].view(np.float32)
+        return {"count": raw[:8 * nz].view(np.uint64).copy(), "min": f[:nz].copy(), "max": f[nz:2 * nz].copy(),
+                "sum": f[2 * nz:3 * nz].copy(), "mean": f[3 * nz:].copy()}
+    finally:
+        for b in bufs:
+            _lib.ma_devFree(b)
+
+
 def sync():
     _lib.ma_sync()
 
@@ -862,6 +920,8 @@ _sig('ma_plainSchedule', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t],
 if hasattr(_lib, 'ma_focalFlow'):
     _sig('ma_focalFlow', [Raster], Node)
 _sig('ma_devAlloc', [ct.c_size_t], ct.c_void_p)
+_sig('ma_zoneStats', [ct.c_void_p, ct.c_longlong, ct.c_void_p, ct.c_longlong, ct.c_int, ct.c_int, ct.c_int,
+                      ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p], ct.c_int)
 _sig('ma_devFree', [ct.c_void_p], None, check=False)
 _sig('ma_hostAlloc', [ct.c_size_t], ct.c_void_p)
 _sig('ma_hostFree', [ct.c_void_p], None, check=False)

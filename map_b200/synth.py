@@ -78,35 +78,45 @@ def uniform_f32(h, w, seed):
     return rng.random((h, w), dtype=np.float32)
 
 
-def voronoi_s32(h, w, n, seed, xp=np, device=None, chunk_rows=256):
-    """int32 (h, w) zone ids: index of the nearest of n uniform seed points."""
+def voronoi_s32(h, w, n, seed, xp=np, device=None):
+    """int32 (h, w) zone ids: index of the nearest of n uniform seed points
+    (distance from cell centres; ties go to the lowest index).
+
+    Cells are processed in square tiles; a seed can own a cell of a tile only if
+    its distance to the tile is at most the smallest, over all seeds, of the
+    distance to the tile's farthest corner, so each tile compares its cells
+    with those candidate seeds only."""
     rng = np.random.default_rng(seed)
     pts = rng.random((n, 2)) * np.array([w, h])
+    T = max(16, int(2 * np.sqrt(h * w / max(n, 1))))
     if xp is np:
         out = np.empty((h, w), np.int32)
-        xs = np.arange(w) + 0.5
-        for y0 in range(0, h, chunk_rows):
-            ys = np.arange(y0, min(h, y0 + chunk_rows)) + 0.5
-            best = np.full((len(ys), w), np.inf)
-            arg = np.zeros((len(ys), w), np.int32)
-            for k in range(n):
-                d = (ys[:, None] - pts[k, 1]) ** 2 + (xs[None, :] - pts[k, 0]) ** 2
-                m = d < best
-                best[m] = d[m]
-                arg[m] = k
-            out[y0:y0 + len(ys)] = arg
-        return out
-    P = xp.as_tensor(pts, dtype=xp.float32, device=device)
-    out = xp.empty((h, w), dtype=xp.int32, device=device)
-    xs = xp.arange(w, device=device, dtype=xp.float32) + 0.5
-    for y0 in range(0, h, chunk_rows):
-        ys = xp.arange(y0, min(h, y0 + chunk_rows), device=device, dtype=xp.float32) + 0.5
-        best = xp.full((len(ys), w), float("inf"), device=device)
-        arg = xp.zeros((len(ys), w), dtype=xp.int32, device=device)
-        for k in range(n):
-            d = (ys[:, None] - P[k, 1]) ** 2 + (xs[None, :] - P[k, 0]) ** 2
-            m = d < best
-            best = xp.where(m, d, best)
-            arg = xp.where(m, xp.full_like(arg, k), arg)
-        out[y0:y0 + len(ys)] = arg
+    else:
+        out = xp.empty((h, w), dtype=xp.int32, device=device)
+        P = xp.as_tensor(pts, dtype=xp.float64, device=device)
+    for y0 in range(0, h, T):
+        y1 = min(h, y0 + T)
+        for x0 in range(0, w, T):
+            x1 = min(w, x0 + T)
+            # distances from every seed to the tile's cell-centre rectangle
+            dx_near = np.maximum(np.maximum(x0 + 0.5 - pts[:, 0], pts[:, 0] - (x1 - 0.5)), 0.0)
+            dy_near = np.maximum(np.maximum(y0 + 0.5 - pts[:, 1], pts[:, 1] - (y1 - 0.5)), 0.0)
+            dx_far = np.maximum(np.abs(x0 + 0.5 - pts[:, 0]), np.abs(x1 - 0.5 - pts[:, 0]))
+            dy_far = np.maximum(np.abs(y0 + 0.5 - pts[:, 1]), np.abs(y1 - 0.5 - pts[:, 1]))
+            r2 = np.min(dx_far ** 2 + dy_far ** 2)
+            cand = np.nonzero(dx_near ** 2 + dy_near ** 2 <= r2)[0]
+            if xp is np:
+                ys = np.arange(y0, y1) + 0.5
+                xs = np.arange(x0, x1) + 0.5
+                c = pts[cand]
+                d = (ys[None, :, None] - c[:, 1, None, None]) ** 2 + (xs[None, None, :] - c[:, 0, None, None]) ** 2
+                out[y0:y1, x0:x1] = cand[np.argmin(d, axis=0)]
+            else:
+                ys = xp.arange(y0, y1, device=device, dtype=xp.float64) + 0.5
+                xs = xp.arange(x0, x1, device=device, dtype=xp.float64) + 0.5
+                ci = xp.as_tensor(cand, device=device)
+                c = P[ci]
+                d = (ys[None, :, None] - c[:, 1, None, None]) ** 2 + (xs[None, None, :] - c[:, 0, None, None]) ** 2
+                out[y0:y1, x0:x1] = ci[xp.argmin(d, dim=0)].to(xp.int32)
     return out
+

@@ -348,3 +348,40 @@ void orc_radial_f32(const float *in, int W, int H, int sx, int sy, int op, float
     }
   }
 }
+
+/* ---------------------------------------------------- per-zone statistics */
+
+/* Per-zone count / min / max / sum of a float32 value raster over an int32
+ * zone raster: a new operation with no counterpart in the reference (its zonal
+ * skeleton, runtime/skeleton/ZonalSkeleton.cpp:33-292, reduces the whole raster
+ * to one value); the per-cell rules are the reference's SUM / MIN / MAX
+ * reductions (runtime/skeleton/util.cpp:518-540). A cell counts when
+ * 0 <= zone < nzones and the value is not NaN. min / max compare floats in
+ * totalOrder (-0 before +0). sum32 adds in float32 in row-major order, sum64 in
+ * double; either may be NULL. Empty zones: count 0, min +inf, max -inf, sums 0. */
+static uint32_t fkey32(float f) {
+  uint32_t b;
+  memcpy(&b, &f, 4);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+
+void orc_zone_stats(const float *val, const int32_t *zone, long long n, int nzones, uint64_t *count, float *vmin,
+                    float *vmax, float *sum32, double *sum64) {
+  for (int z = 0; z < nzones; z++) {
+    count[z] = 0;
+    vmin[z] = INFINITY;
+    vmax[z] = -INFINITY;
+    if (sum32) sum32[z] = 0.0f;
+    if (sum64) sum64[z] = 0.0;
+  }
+  for (long long i = 0; i < n; i++) {
+    const int32_t z = zone[i];
+    const float v = val[i];
+    if (z < 0 || z >= nzones || v != v) continue;
+    if (count[z] == 0 || fkey32(v) < fkey32(vmin[z])) vmin[z] = v;
+    if (count[z] == 0 || fkey32(v) > fkey32(vmax[z])) vmax[z] = v;
+    count[z]++;
+    if (sum32) sum32[z] += v;
+    if (sum64) sum64[z] += (double)v;
+  }
+}

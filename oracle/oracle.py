@@ -47,6 +47,8 @@ def lib():
         L.orc_flowacc_s32.restype = ct.c_int
         L.orc_radial_f32.argtypes = [f32p, I, I, I, I, I, f32p]
         L.orc_wsum_f32.argtypes = [ct.POINTER(ct.c_void_p), f32p, I, ct.c_size_t, f32p]
+        u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+        L.orc_zone_stats.argtypes = [f32p, i32p, ct.c_longlong, I, u64p, f32p, f32p, f32p, f64p]
         L.orc_focal_src.argtypes = [I, I, I, I, I, I, I, I, I, ct.POINTER(I), ct.POINTER(I)]
         L.orc_focal_src.restype = I
         _lib = L
@@ -139,6 +141,22 @@ def wsum_f32(layers, weights):
     out = np.empty_like(ls[0])
     lib().orc_wsum_f32(ptrs, w, len(ls), ls[0].size, out)
     return out
+
+
+def zone_stats(value, zone, nzones):
+    """Per-zone count (uint64), min, max, float32 sum (row-major order) and
+    float64 sum of `value` (float32) over `zone` (int32); cells with a zone id
+    outside [0, nzones) or a NaN value are skipped."""
+    v = _c(value, np.float32)
+    z = _c(zone, np.int32)
+    assert v.shape == z.shape
+    cnt = np.zeros(nzones, np.uint64)
+    mn = np.zeros(nzones, np.float32)
+    mx = np.zeros(nzones, np.float32)
+    s32 = np.zeros(nzones, np.float32)
+    s64 = np.zeros(nzones, np.float64)
+    lib().orc_zone_stats(v, z, v.size, nzones, cnt, mn, mx, s32, s64)
+    return {"count": cnt, "min": mn, "max": mx, "sum32": s32, "sum64": s64}
 
 
 def focal_src(W, H, bs, border, x, y, dx, dy):

@@ -170,3 +170,29 @@ def test_reduction_neutrals_match_reference():
     assert np.frombuffer(out[:4].tobytes(), np.float32)[0] == -np.inf
     ref.ref_neutral(7, 10, out.ctypes.data, ct.byref(odt))  # MIN on S32
     assert np.frombuffer(out[:4].tobytes(), np.int32)[0] == np.iinfo(np.int32).max
+
+
+def test_zone_stats_known_answer():
+    nan = float("nan")
+    value = np.array([[1.0, 2.0, -0.0, nan, 4.0],
+                      [0.0, 5.0, -3.0, 7.0, -1.5]], np.float32)
+    zone = np.array([[0, 0, 1, 1, 3],
+                     [1, -1, 2, 9, 3]], np.int32)
+    r = O.zone_stats(value, zone, 4)
+    assert list(r["count"]) == [2, 2, 1, 2]
+    assert list(r["min"]) == [1.0, 0.0, -3.0, -1.5] and np.signbit(r["min"][1])
+    assert list(r["max"]) == [2.0, 0.0, -3.0, 4.0] and not np.signbit(r["max"][1])
+    assert list(r["sum32"]) == [3.0, 0.0, -3.0, 2.5]
+    assert list(r["sum64"]) == [3.0, 0.0, -3.0, 2.5]
+    empty = O.zone_stats(np.zeros((0, 3), np.float32), np.zeros((0, 3), np.int32), 2)
+    assert list(empty["count"]) == [0, 0] and np.all(np.isposinf(empty["min"])) and np.all(np.isneginf(empty["max"]))
+
+
+def test_voronoi_generator_is_nearest_seed():
+    h, w, n = 61, 83, 29
+    z = synth.voronoi_s32(h, w, n, seed=2)
+    rng = np.random.default_rng(2)
+    pts = rng.random((n, 2)) * np.array([w, h])
+    ys, xs = np.mgrid[0:h, 0:w] + 0.5
+    d = (ys[None] - pts[:, 1, None, None]) ** 2 + (xs[None] - pts[:, 0, None, None]) ** 2
+    assert (np.argmin(d, axis=0) == z).all()
