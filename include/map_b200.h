@@ -202,6 +202,23 @@ int ma_zoneStats(const void *value, long long value_pitch, const void *zone, lon
                  int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum, float *mean,
                  void *stream);
 
+/* ma_zoneStats without any device-memory allocation. No counterpart in the
+ * reference (see ma_zoneStats). For callers that must not allocate while they
+ * run: a server that reserved its whole HBM budget up front, where a pool
+ * allocation could fail or exceed the budget, or a latency-critical loop,
+ * where an allocation may synchronise the device or grow the memory pool.
+ * The working bins are one fixed array per device in the library's own device
+ * memory, so nzones may be at most 16384; larger counts return an error. Runs
+ * on the calling thread's current device. The first call on a device does the
+ * set-up (looks up the array, loads the kernels): make it before any stream
+ * capture begins. All calls on a device share the array: calls whose work can
+ * overlap on the device (several streams or host threads) race and corrupt each
+ * other's results, so order them on one stream. Same arguments, rules and
+ * results as ma_zoneStats. */
+int ma_zoneStatsNoAlloc(const void *value, long long value_pitch, const void *zone, long long zone_pitch, int W,
+                        int H, int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum,
+                        float *mean, void *stream);
+
 /* Introspection for tests and tools. */
 int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
 int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */

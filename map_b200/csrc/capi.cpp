@@ -691,6 +691,28 @@ int ma_zoneStats(const void *value, long long value_pitch, const void *zone, lon
   });
 }
 
+int ma_zoneStatsNoAlloc(const void *value, long long value_pitch, const void *zone, long long zone_pitch, int W,
+                        int H, int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum,
+                        float *mean, void *stream) {
+  return int_call([&] {
+    ZoneStatsArgs a;
+    a.value = value;
+    a.value_pitch = value_pitch;
+    a.zone = zone;
+    a.zone_pitch = zone_pitch;
+    a.W = W;
+    a.H = H;
+    a.nzones = nzones;
+    a.count = count;
+    a.vmin = vmin;
+    a.vmax = vmax;
+    a.sum = sum;
+    a.mean = mean;
+    zone_stats_no_alloc(a, (CUstream_st *)stream);
+    return 0;
+  });
+}
+
 int ma_nodeCount(void) { return (int)Runtime::get().nodes.size(); }
 void ma_collectGarbage(void) {
   void_call([&] { Runtime::get().collect_garbage(); });

@@ -325,4 +325,59 @@ void zone_stats(const ZoneStatsArgs &a, cudaStream_t st) {
   check(e, "cudaMemsetAsync(bins)");
 }
 
+// ------------------------------------------------- allocation-free variant
+//
+// For callers that must not allocate device memory while they run: a server
+// that reserved its whole HBM budget up front (an allocation from the stream's
+// pool could fail or push it past the budget), or a latency-critical loop in
+// which an allocation may stall (cudaMalloc / cudaFree synchronise the device,
+// and a pool allocation may have to grow the pool).
+//
+// Its working bins live in one fixed file-scope array per device instead of the
+// stream's memory pool, so it serves at most kStaticZones zones (larger zone
+// counts are rejected with an error). The first call on a device does the
+// set-up for that device: it looks up the array's address and loads the
+// kernels; make it before any stream capture begins. Every call on a device
+// shares the one array: calls whose work may overlap on the device (different
+// streams, or several host threads) race and corrupt each other's results, so
+// issue them in order on one stream. Each call clears the bins it uses
+// (cudaMemsetAsync on the caller's stream) before it accumulates into them.
+
+constexpr int kStaticZones = 16384;   // 16384 x 24 B = 384 KiB per device
+static __device__ __align__(256) Bin zs_static_bins[kStaticZones];
+
+// Address of the array on the current device (set-up on the first call there).
+static void *static_bins() {
+  static std::mutex m;
+  static void *addr[64] = {};
+  int d = 0;
+  check(cudaGetDevice(&d), "cudaGetDevice");
+  if (d < 0 || d >= 64) throw MapError("zone statistics: device ordinal out of range");
+  std::lock_guard<std::mutex> lk(m);
+  if (!addr[d]) {
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, zs_static_bins);
+    if (e != cudaSuccess || !p)
+      throw MapError(std::string("zone statistics: cudaGetSymbolAddress of the static bins failed: ") +
+                     cudaGetErrorString(e));
+    dev_info();   // loads the shared-bin accumulation kernel
+    cudaFuncAttributes fa;
+    check(cudaFuncGetAttributes(&fa, zs_accumulate<false>), "cudaFuncGetAttributes");
+    check(cudaFuncGetAttributes(&fa, zs_finalize), "cudaFuncGetAttributes");
+    addr[d] = p;
+  }
+  return addr[d];
+}
+
+void zone_stats_no_alloc(const ZoneStatsArgs &a, cudaStream_t st) {
+  zone_stats_validate(a);
+  if (a.nzones > kStaticZones)
+    throw MapError("zone statistics without allocation: nzones " + std::to_string(a.nzones) +
+                   " exceeds the fixed scratch of " + std::to_string(kStaticZones) +
+                   " zones (the allocating entry point has no such limit)");
+  void *bins = static_bins();
+  check(cudaMemsetAsync(bins, 0, zone_stats_bin_bytes(a.nzones), st), "cudaMemsetAsync(static bins)");
+  zone_stats_run(a, bins, st);
+}
+
 }  // namespace mapb

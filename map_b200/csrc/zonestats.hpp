@@ -26,4 +26,10 @@ struct ZoneStatsArgs {
 // stream's memory pool and frees them after use.
 void zone_stats(const ZoneStatsArgs &a, CUstream_st *stream);
 
+// Same computation without allocating device memory: the working bins are a
+// fixed per-device array of 16384 zones, shared by every call on the device
+// (overlapping calls race). Runs on the calling thread's current device; the
+// first call there does the set-up. See zonestats.cu for who needs it.
+void zone_stats_no_alloc(const ZoneStatsArgs &a, CUstream_st *stream);
+
 }  // namespace mapb
