@@ -280,7 +280,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   kind_args.resize(reg_plans.size());
   kind_members.resize(reg_plans.size(), 0);
   std::vector<std::pair<const void *, size_t>> blobs;
-  for (auto &a : kind_args) blobs.push_back({a.data(), std::max<size_t>(a.size(), 1)});
+  for (auto &a : kind_args) blobs.push_back({a.data(), a.size()});   // empty for kinds absent from this batch
   for (auto &lv : levels) blobs.push_back({lv.data(), lv.size() * sizeof(Item)});
   for (auto &kv : radial) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
   for (auto &kv : spread) blobs.push_back({kv.second.args.data(), kv.second.args.size()});
@@ -297,7 +297,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   size_t off = 256;   // first 256 bytes: work-list counters
   std::memset(stage[si], 0, 256);
   for (auto &b : blobs) {
-    std::memcpy((char *)stage[si] + off, b.first, b.second);
+    if (b.second) std::memcpy((char *)stage[si] + off, b.first, b.second);
     dptr.push_back((char *)dbuf + off);
     off += (b.second + 255) / 256 * 256;
   }

@@ -27,7 +27,7 @@ def _axis_weights(n, cells, xp, device=None):
 
 
 def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cells=4, xp=np, device=None):
-    """float32 (h, w) fractal Brownian value-noise DEM rescaled to [lo, hi]."""
+    """float32 (h, w) fractal Brownian value-noise DEM rescaled to [lo, hi], row-major."""
     rng = np.random.default_rng(seed)
     side = max(h, w)
     total = None
@@ -60,7 +60,8 @@ def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cell
         amp *= persistence
     mn, mx = total.min(), total.max()
     out = (total - mn) / (mx - mn) * (hi - lo) + lo
-    return out.astype(np.float32) if xp is np else out.float()
+    # row-major (C-contiguous) like every raster the engine reads through raw pointers
+    return np.ascontiguousarray(out, dtype=np.float32) if xp is np else out.float().contiguous()
 
 
 def bernoulli_u8(h, w, p, seed):

@@ -196,3 +196,10 @@ def test_voronoi_generator_is_nearest_seed():
     ys, xs = np.mgrid[0:h, 0:w] + 0.5
     d = (ys[None] - pts[:, 1, None, None]) ** 2 + (xs[None] - pts[:, 0, None, None]) ** 2
     assert (np.argmin(d, axis=0) == z).all()
+
+
+def test_synthetic_rasters_are_row_major():
+    # rasters are handed to the engine through raw pointers: they must be C-contiguous
+    for a in (synth.fbm_dem(130, 150, seed=1), synth.lognormal_f32(13, 15, seed=1), synth.uniform_f32(13, 15, seed=1),
+              synth.bernoulli_u8(13, 15, 0.3, seed=1), synth.voronoi_s32(13, 15, 5, seed=1)):
+        assert a.flags["C_CONTIGUOUS"]
