@@ -308,7 +308,7 @@ def bench_zonal_stats(M, synth, torch, dev, size=16384, nzones=1024, steps=10, w
                  and (oh[nzones:2 * nzones].view(np.uint32) == ref["max"].view(np.uint32)).all())
     rel_sum = float(np.max(np.abs(oh[2 * nzones:3 * nzones] - ref["sum64"]) / ref["sum64"]))
     mean64 = ref["sum64"] / ref["count"].astype(np.float64)
-    rel_mean = float(np.max(np.abs(oh[3 * nzones:] - mean64) / mean64))
+    rel_mean = float(np.max(np.abs(oh[3 * nzones:4 * nzones] - mean64) / mean64))
     del val, zone
     return {"workload": "per-zone count/min/max/sum/mean, %dx%d F32 lognormal(0,1) over %dx%d S32 Voronoi(%d)"
                         % (size, size, size, size, nzones),

@@ -105,6 +105,16 @@ int ma_getBorder(void);
  * 1 one launch per group per block in the scheduler's order (reference granularity). */
 void ma_setExecMode(int mode);
 int ma_getExecMode(void);
+/* Streamed evaluation: a program whose outputs go to host memory and whose
+ * groups are Local / Focal runs in row bands, each band's upload, kernels and
+ * download on their own streams so the host<->device copies of successive
+ * bands overlap each other and the kernels; rasters larger than device memory
+ * work this way too. rows = 0 chooses bands automatically (about 32 MiB of
+ * host traffic per band, used when a raster has at least four bands), rows > 0
+ * forces bands of that many rows, rows < 0 turns streaming off. Results are
+ * identical to whole-raster evaluation. */
+void ma_setStreamRows(int rows);
+int ma_getStreamRows(void);
 /* Block size given to rasters created without one (default 256 x 256). */
 void ma_setDefaultBlockSize(ma_Array bs);
 void ma_setDevice(int device);
@@ -222,6 +232,7 @@ int ma_zoneStatsNoAlloc(const void *value, long long value_pitch, const void *zo
 /* Introspection for tests and tools. */
 int ma_lastLaunchCount(void);      /* kernels launched by the last evaluation */
 int ma_lastGroupCount(void);       /* fusion groups of the last evaluation */
+int ma_lastBandCount(void);        /* row bands of the last evaluation (0: not streamed) */
 int ma_totalLaunchCount(void);
 /* Fusion + code generation (+ NVRTC compilation when compile != 0) of the
  * program that evaluates `vec`, without a device. Returns the number of

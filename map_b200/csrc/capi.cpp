@@ -348,6 +348,10 @@ void ma_setExecMode(int mode) {
   });
 }
 int ma_getExecMode(void) { return Runtime::get().exec_mode; }
+void ma_setStreamRows(int rows) {
+  void_call([&] { Runtime::get().stream_rows = rows; });
+}
+int ma_getStreamRows(void) { return Runtime::get().stream_rows; }
 void ma_setDefaultBlockSize(ma_Array bs) {
   void_call([&] {
     if (bs.n != 2 || bs.arr[0] <= 0 || bs.arr[1] <= 0) throw MapError("setDefaultBlockSize: invalid size");
@@ -460,6 +464,7 @@ int ma_memcpy(void *dst, const void *src, size_t bytes, int kind) {
 
 int ma_lastLaunchCount(void) { return Executor::get().last.launches; }
 int ma_lastGroupCount(void) { return Executor::get().last.groups; }
+int ma_lastBandCount(void) { return Executor::get().last.bands; }
 int ma_totalLaunchCount(void) { return CudaEnv::get().launches(); }
 
 int ma_compileOnly(ma_Node **vec, int num, int compile) {

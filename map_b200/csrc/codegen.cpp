@@ -500,7 +500,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
       body << "      tma_load_2d(smem + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
-           << ");\n";
+           << " - a.g.oy);\n";
     }
     body << "    }\n"
          << "    if (!mbar_wait_bounded(bar, phase, 1u << 26)) {\n"

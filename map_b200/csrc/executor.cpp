@@ -190,15 +190,20 @@ std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &
 
 std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
                                      std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
-                                     const uint64_t aux[4]) {
+                                     const uint64_t aux[4], const std::unordered_map<const Node *, Variant> *scalars) {
   CudaEnv &env = CudaEnv::get();
   std::vector<unsigned char> a(K.args_size, 0);
+  int32_t oy = 0;
   for (size_t k = 0; k < K.tma.size(); k++) {
     const TmaSpec &t = K.tma[k];
     DevRaster &r = get(K.in_rasters[t.in_index]);
     alignas(64) unsigned char desc[128];
-    env.encode_tma_2d(desc, r.dtype, r.ptr, (uint64_t)r.W, (uint64_t)r.H, (uint64_t)r.pitch, (uint32_t)t.box_w,
-                      (uint32_t)t.box_h);
+    // a row band is mapped from its buffer's first row; the kernel subtracts Geom::oy from row coordinates
+    void *base = r.rows ? (void *)((uintptr_t)r.ptr + (uintptr_t)(r.org * r.pitch)) : r.ptr;
+    const uint64_t rows = r.rows ? (uint64_t)r.rows : (uint64_t)r.H;
+    if (k == 0) oy = (int32_t)(r.rows ? r.org : 0);
+    else if (oy != (int32_t)(r.rows ? r.org : 0)) throw MapError("staged inputs of one group must share their row origin");
+    env.encode_tma_2d(desc, r.dtype, base, (uint64_t)r.W, rows, (uint64_t)r.pitch, (uint32_t)t.box_w, (uint32_t)t.box_h);
     std::memcpy(a.data() + K.off_tm + 128 * k, desc, 128);
   }
   for (size_t k = 0; k < K.in_rasters.size(); k++) {
@@ -217,11 +222,18 @@ std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const 
   }
   for (size_t k = 0; k < K.scalars.size(); k++) {
     Node *s = K.scalars[k];
-    if (!s->has_value) throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
-    Variant v = var_convert(s->value, s->meta.dtype);
+    const Variant *sv = &s->value;
+    if (scalars) {
+      auto it = scalars->find(s);
+      if (it != scalars->end()) sv = &it->second;
+      else if (!s->has_value) throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
+    } else if (!s->has_value) {
+      throw MapError(std::string("scalar input ") + kind_name(s->kind) + " has no value");
+    }
+    Variant v = var_convert(*sv, s->meta.dtype);
     std::memcpy(a.data() + K.off_s + 8 * k, &v.u, dt_size(v.dtype));
   }
-  int32_t geom[12] = {g.W, g.H, g.BS0, g.BS1, rx0, ry0, rx1, ry1, 0, 0, Runtime::get().border, 0};
+  int32_t geom[12] = {g.W, g.H, g.BS0, g.BS1, rx0, ry0, rx1, ry1, 0, 0, Runtime::get().border, oy};
   const int tx = (rx1 - rx0 + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
   geom[8] = tx;
   geom[9] = tx * ty;
@@ -336,6 +348,11 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
   }
   env.ensure_device();
   cudaStream_t st = (cudaStream_t)env.stream();
+  if (evaluate_streamed(P, targets, sinks)) {
+    last.launches = env.launches() - launches0;
+    last.host_ms = now_ms() - t0;
+    return;
+  }
   static bool pool_cfg = false;
   if (!pool_cfg) {
     cudaMemPool_t pool;
@@ -583,6 +600,236 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
   }
   last.launches = env.launches() - launches0;
   last.host_ms = now_ms() - t0;
+}
+
+// ------------------------------------------------------------ streamed bands
+//
+// A program from host rasters to host rasters made of Local / Focal groups runs
+// band by band: band b covers raster rows [y0, y1); group g computes rows
+// [y0 - need(g), y1 + need(g)) where need(g) is the halo its consumers still
+// require, so the output rows of the band only ever see values computed from
+// true neighbours, and border decisions use the whole raster's geometry
+// (kernels address rasters in raster rows through a virtual base), making the
+// result identical to whole-raster evaluation. Each of kSlots buffer sets holds
+// every raster's rows [y0 - M, y1 + M) plus a tile of padding (M = the largest
+// margin); uploads run on one stream, kernels on the engine's stream and
+// downloads on a third, chained by events, so band b+1 uploads while band b
+// computes and band b-1 downloads.
+
+namespace {
+
+constexpr int kSlots = 3;
+
+struct BandStreams {
+  cudaStream_t up = nullptr, down = nullptr;
+  cudaEvent_t ev_up[kSlots] = {}, ev_comp[kSlots] = {}, ev_down[kSlots] = {}, ev_alloc = nullptr;
+  bool ready = false;
+  void init() {
+    if (ready) return;
+    cuda_check(cudaStreamCreateWithFlags(&up, cudaStreamNonBlocking), "cudaStreamCreate");
+    cuda_check(cudaStreamCreateWithFlags(&down, cudaStreamNonBlocking), "cudaStreamCreate");
+    for (int i = 0; i < kSlots; i++) {
+      cuda_check(cudaEventCreateWithFlags(&ev_up[i], cudaEventDisableTiming), "cudaEventCreate");
+      cuda_check(cudaEventCreateWithFlags(&ev_comp[i], cudaEventDisableTiming), "cudaEventCreate");
+      cuda_check(cudaEventCreateWithFlags(&ev_down[i], cudaEventDisableTiming), "cudaEventCreate");
+    }
+    cuda_check(cudaEventCreateWithFlags(&ev_alloc, cudaEventDisableTiming), "cudaEventCreate");
+    ready = true;
+  }
+};
+
+BandStreams &band_streams() {
+  static BandStreams b;
+  return b;
+}
+
+}  // namespace
+
+bool Executor::evaluate_streamed(const Prepared &P, const std::vector<Node *> &targets, const std::vector<Sink> &sinks) {
+  Runtime &rt = Runtime::get();
+  if (rt.exec_mode != EXEC_FUSED || rt.stream_rows < 0 || sinks.empty()) return false;
+  std::set<Node *> sink_nodes;
+  for (const Sink &s : sinks) {
+    if (!s.host || s.dev || s.node->meta.numdim != D2) return false;
+    sink_nodes.insert(s.node);
+  }
+  for (Node *t : targets)
+    if (!sink_nodes.count(t)) return false;
+  for (Node *n : P.order)
+    if (n->kind == K_WRITE) return false;
+  int W = -1, H = -1, th_max = 1, hy_max = 0;
+  std::set<Node *> produced;
+  std::map<Node *, const Group *> producer;
+  for (auto &gp : P.fr.groups) {
+    const Group &g = *gp;
+    if (g.skeleton != SK_LOCAL && g.skeleton != SK_FOCAL) return false;
+    if (W < 0) {
+      W = g.W;
+      H = g.H;
+    } else if (g.W != W || g.H != H) {
+      return false;
+    }
+    const KernelPlan &K = P.plans[g.id];
+    th_max = std::max(th_max, K.tile_h);
+    hy_max = std::max(hy_max, K.halo_y);
+    for (Node *o : K.out_rasters) {
+      produced.insert(o);
+      producer[o] = &g;
+    }
+  }
+  if (W <= 0 || H <= 0) return false;
+  for (Node *s : sink_nodes)
+    if (!produced.count(s)) return false;
+  std::set<Node *> inputs;
+  for (auto &gp : P.fr.groups)
+    for (Node *n : P.plans[gp->id].in_rasters)
+      if (!produced.count(n)) inputs.insert(n);
+  std::vector<Node *> host_in, dev_in;
+  for (Node *n : inputs) {
+    if (n->meta.W() != W || n->meta.H() != H) return false;
+    if (n->kind == K_HOSTIN) {
+      host_in.push_back(n);
+    } else if (n->kind == K_DEVIN) {
+      if (((uintptr_t)n->dev->ptr & 127) != 0 || (n->dev->pitch & 15) != 0) return false;
+      dev_in.push_back(n);
+    } else {
+      return false;
+    }
+  }
+  size_t row_bytes = 0;
+  for (Node *n : host_in) row_bytes += (size_t)W * dt_size(n->meta.dtype);
+  for (Node *n : sink_nodes) row_bytes += (size_t)W * dt_size(n->meta.dtype);
+  int B;
+  if (rt.stream_rows > 0) {
+    B = rt.stream_rows;
+    if (B >= H) return false;
+  } else {
+    B = (int)std::min<size_t>((size_t)H, std::max<size_t>(64, ((size_t)32 << 20) / std::max<size_t>(row_bytes, 1)));
+    B = std::max(32, B / 32 * 32);
+    if ((long long)H < 4LL * B) return false;
+  }
+  // margins: rows beyond the band that each group must still produce
+  std::map<const Group *, int> need;
+  for (auto it = P.fr.groups.rbegin(); it != P.fr.groups.rend(); ++it) {
+    const Group *c = it->get();
+    const KernelPlan &K = P.plans[c->id];
+    const int nc = need[c];
+    for (Node *n : K.in_rasters) {
+      auto p = producer.find(n);
+      if (p != producer.end()) need[p->second] = std::max(need[p->second], nc + K.halo_y);
+    }
+  }
+  int M = 0;
+  for (auto &gp : P.fr.groups) M = std::max(M, need[gp.get()] + P.plans[gp->id].halo_y);
+
+  CudaEnv &env = CudaEnv::get();
+  cudaStream_t st = (cudaStream_t)env.stream();
+  BandStreams &bs = band_streams();
+  bs.init();
+  const int nb = (H + B - 1) / B;
+  const int slots = std::min(kSlots, nb);
+  const int rows_alloc = std::min(H, B + 2 * M) + th_max + hy_max + 1;
+  std::vector<Node *> banded(host_in.begin(), host_in.end());
+  banded.insert(banded.end(), produced.begin(), produced.end());
+  std::vector<std::unordered_map<Node *, DevRaster>> slot_buf(slots);
+  std::vector<void *> allocs;
+  auto release = [&]() {
+    for (void *p : allocs) cudaFreeAsync(p, st);
+    allocs.clear();
+  };
+  try {
+    for (int sidx = 0; sidx < slots; sidx++)
+      for (Node *n : banded) {
+        DevRaster r;
+        r.dtype = n->meta.dtype;
+        r.W = W;
+        r.H = H;
+        r.pitch = pitch_for(W, r.dtype);
+        void *p = nullptr;
+        cuda_check(cudaMallocAsync(&p, (size_t)r.pitch * rows_alloc, st), "cudaMallocAsync(band)");
+        allocs.push_back(p);
+        r.ptr = p;   // real address until a band is bound
+        r.rows = rows_alloc;
+        slot_buf[sidx][n] = r;
+      }
+    cuda_check(cudaEventRecord(bs.ev_alloc, st), "cudaEventRecord");
+    cuda_check(cudaStreamWaitEvent(bs.up, bs.ev_alloc, 0), "cudaStreamWaitEvent");
+    std::vector<void *> real(allocs);
+    std::unordered_map<Node *, DevRaster> bufs;
+    std::function<DevRaster &(Node *)> get = [&](Node *n) -> DevRaster & {
+      auto it = bufs.find(n);
+      if (it == bufs.end()) throw MapError("streamed evaluation: raster not bound");
+      return it->second;
+    };
+    for (int b = 0; b < nb; b++) {
+      const int sidx = b % slots;
+      const int y0 = b * B, y1 = std::min(H, y0 + B);
+      const int ya = std::max(0, y0 - M), yb = std::min(H, y1 + M);
+      if (b >= slots) cuda_check(cudaStreamWaitEvent(bs.up, bs.ev_down[sidx], 0), "cudaStreamWaitEvent");
+      bufs.clear();
+      size_t ai = (size_t)sidx * banded.size();
+      for (Node *n : banded) {
+        DevRaster r = slot_buf[sidx][n];
+        void *base = real[ai++];
+        r.org = ya;
+        r.ptr = (void *)((uintptr_t)base - (uintptr_t)((long long)ya * r.pitch));
+        bufs[n] = r;
+      }
+      for (Node *n : dev_in) {
+        DevRaster r;
+        r.ptr = n->dev->ptr;
+        r.pitch = n->dev->pitch;
+        r.dtype = n->meta.dtype;
+        r.W = W;
+        r.H = H;
+        r.org = ya;
+        r.rows = H - ya;
+        bufs[n] = r;
+      }
+      for (Node *n : host_in) {
+        const DevRaster &r = bufs[n];
+        const size_t row = (size_t)W * dt_size(n->meta.dtype);
+        cuda_check(cudaMemcpy2DAsync((char *)r.ptr + (long long)ya * r.pitch, r.pitch,
+                                     (const char *)n->host->ptr + (size_t)ya * row, row, row, yb - ya,
+                                     cudaMemcpyHostToDevice, bs.up),
+                   "band upload");
+      }
+      cuda_check(cudaEventRecord(bs.ev_up[sidx], bs.up), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(st, bs.ev_up[sidx], 0), "cudaStreamWaitEvent");
+      for (auto &gp : P.fr.groups) {
+        const Group &g = *gp;
+        const KernelPlan &K = P.plans[g.id];
+        const int ry0 = std::max(0, y0 - need[&g]), ry1 = std::min(H, y1 + need[&g]);
+        const int tx = (W + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+        KernelHandle kh = env.kernel(K.source, K.kname, K.smem_bytes);
+        uint64_t aux[4] = {0, 0, 0, 0};
+        auto a = pack_args(g, K, get, bufs, 0, ry0, W, ry1, aux);
+        env.launch(kh, tx * ty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+      }
+      cuda_check(cudaEventRecord(bs.ev_comp[sidx], st), "cudaEventRecord");
+      cuda_check(cudaStreamWaitEvent(bs.down, bs.ev_comp[sidx], 0), "cudaStreamWaitEvent");
+      for (const Sink &s : sinks) {
+        const DevRaster &r = bufs.at(s.node);
+        const size_t row = (size_t)W * dt_size(s.node->meta.dtype);
+        cuda_check(cudaMemcpy2DAsync((char *)s.host + (size_t)y0 * row, row, (const char *)r.ptr + (long long)y0 * r.pitch,
+                                     r.pitch, row, y1 - y0, cudaMemcpyDeviceToHost, bs.down),
+                   "band download");
+      }
+      cuda_check(cudaEventRecord(bs.ev_down[sidx], bs.down), "cudaEventRecord");
+    }
+    cuda_check(cudaStreamSynchronize(bs.down), "stream synchronize");
+    cuda_check(cudaStreamSynchronize(bs.up), "stream synchronize");
+    release();
+    sync();
+  } catch (...) {
+    cudaStreamSynchronize(bs.up);
+    cudaStreamSynchronize(bs.down);
+    cudaStreamSynchronize(st);
+    release();
+    throw;
+  }
+  last.bands = nb;
+  return true;
 }
 
 }  // namespace mapb

@@ -10,6 +10,9 @@
 //  * plain: one launch per group per block, issued in the order of a ready-queue
 //    of (group, block) jobs keyed by a Morton interleave of (x, y, group), with the
 //    focal 3x3 block dependencies of runtime/task/FocalTask.cpp:36-115.
+// Programs from host rasters to host rasters can instead stream through row
+// bands (evaluate_streamed), which replaces the reference Cache's spilling of
+// blocks between host and device (runtime/Cache.cpp:505-571).
 #pragma once
 
 #include "codegen.hpp"
@@ -31,6 +34,11 @@ struct DevRaster {
   bool owned = false;
   int dtype = 0;
   int W = 0, H = 0;
+  // Row band of a raster (streamed evaluation): the buffer holds raster rows
+  // org .. org + rows - 1 and `ptr` is the virtual address of raster row 0
+  // (buffer - org * pitch, modulo 2^64), so kernels index it with raster rows.
+  long long org = 0;
+  int rows = 0;          // 0: the whole raster is held
 };
 
 // Where a requested raster goes after evaluation.
@@ -54,9 +62,11 @@ std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &
 
 // Packs the kernel argument struct of plan K for a launch over region
 // [rx0,rx1) x [ry0,ry1); rasters are looked up with `get` (inputs) and in `bufs` (outputs).
+// `scalars`, when given, overrides the values of scalar argument nodes.
 std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
                                      std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
-                                     const uint64_t aux[4]);
+                                     const uint64_t aux[4],
+                                     const std::unordered_map<const Node *, Variant> *scalars = nullptr);
 
 // Every node `targets` depend on (themselves included), in id (= topological) order.
 std::vector<Node *> collect_nodes(const std::vector<Node *> &targets);
@@ -65,6 +75,7 @@ struct EvalStats {
   int launches = 0;
   int groups = 0;
   int compiled = 0;
+  int bands = 0;     // row bands of a streamed evaluation (0: whole rasters)
   double host_ms = 0;
 };
 
@@ -89,6 +100,9 @@ class Executor {
     std::vector<Node *> order;
   };
   Prepared prepare(const std::vector<Node *> &targets, const std::set<Node *> &tset, bool compile);
+  // Row-band streaming of host-to-host Local / Focal programs; false (and no
+  // work done) when the program does not qualify.
+  bool evaluate_streamed(const Prepared &P, const std::vector<Node *> &targets, const std::vector<Sink> &sinks);
 };
 
 }  // namespace mapb

@@ -92,6 +92,9 @@ struct Runtime {
   // configuration
   int border = BORDER_BLOCK_MIRROR;
   int exec_mode = EXEC_FUSED;
+  // Row bands of streamed evaluations (host rasters in, host rasters out):
+  // 0 automatic, < 0 never stream, > 0 stream whenever a raster has more rows.
+  int stream_rows = 0;
   Arr2 default_bs{{256, 256}, 2};
 
   // factories (each returns a node owned by the runtime, possibly pre-existing)

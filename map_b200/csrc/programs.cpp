@@ -75,11 +75,14 @@ Node *prog_hillshade(Runtime &rt, Node *dem, double zenith, double azimuth) {
   return rt.binary(t1, rt.binary(t2, t3, MUL), ADD);
 }
 
-Node *prog_viewshed(Runtime &rt, Node *dem, int obs_x, int obs_y, float obs_h, double radius) {
+Node *prog_viewshed(Runtime &rt, Node *dem, int obs_x, int obs_y, float obs_h, double radius, Node **ox_out,
+                    Node **oy_out) {
   Node *h = cflt(rt, obs_h);
   Node *shift = rt.binary(dem, h, SUB);
   Node *ox = rt.scalar_param(vs32(obs_x));
   Node *oy = rt.scalar_param(vs32(obs_y));
+  if (ox_out) *ox_out = ox;
+  if (oy_out) *oy_out = oy;
   Node *x = rt.binary(ox, rt.index(dem, D1), SUB);
   Node *y = rt.binary(oy, rt.index(dem, D2), SUB);
   Node *dist = rt.unary(rt.binary(rt.binary(rt.binary(x, x, MUL), rt.binary(y, y, MUL), ADD), cflt(rt, 0.0), ADD), SQRT);

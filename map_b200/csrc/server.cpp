@@ -37,6 +37,10 @@ long long pitch_for(int W, int dt) {
   return (b + 127) / 128 * 128;
 }
 
+// Launch phases of a batch, in stream order. A request is complete once the
+// last phase its program uses has finished.
+enum Phase { PH_LEVEL0 = 0, PH_RADIAL = 1, PH_LEVEL1 = 2, PH_SPREAD = 3, N_PHASES = 4 };
+
 struct Req {
   long long id = 0;
   int type = 0, x0 = 0, y0 = 0, w = 0, h = 0, ox = 0, oy = 0;
@@ -54,7 +58,6 @@ struct Req {
   long long out_pitch = 0;
   int out_dt = F32;
   std::vector<void *> scratch;
-  Node *out_node = nullptr;
 };
 
 size_t request_bytes(int type, int w, int h) {
@@ -63,11 +66,24 @@ size_t request_bytes(int type, int w, int h) {
   return b;
 }
 
-struct InFlight {
-  std::vector<Req *> reqs;
+// A program kind over a window size, fused and code-generated once. Its nodes
+// stand for any request of that shape: a request binds its own buffers to the
+// template's rasters and its own observer to the template's scalar arguments.
+struct Template {
+  FusionResult fr;
+  std::vector<KernelPlan> plans;   // per group, in group order
+  std::vector<int> level;          // dependency level per group
+  std::vector<int> kind;           // persistent-module kind per Local / Focal group (-1 otherwise)
+  Node *win = nullptr, *out = nullptr;
+  Node *ox = nullptr, *oy = nullptr;   // viewshed observer arguments
+  int last_phase = PH_LEVEL0;
+};
+
+// One phase of one batch: the requests that complete with it.
+struct PhaseDone {
   cudaEvent_t ev = nullptr;
-  int stream = 0;
-  std::vector<void *> dev_free;
+  std::vector<Req *> reqs;
+  void *batch_mem = nullptr;   // freed with the batch's last phase
 };
 
 }  // namespace
@@ -83,17 +99,18 @@ struct Server::Impl {
   std::condition_variable cv_pending, cv_done, cv_inflight;
   std::deque<Req *> pending;
   std::map<long long, std::unique_ptr<Req>> reqs;
-  std::deque<InFlight> inflight;
+  std::deque<PhaseDone> inflight[3];   // per completion queue: stream 0, stream 1, spreading stream
   size_t used = 0;
   long long next_id = 1;
   bool stop = false;
   std::thread dispatcher, completer;
-  cudaStream_t streams[2] = {nullptr, nullptr};
-  cudaEvent_t last_ev[2] = {nullptr, nullptr};
+  cudaStream_t streams[3] = {nullptr, nullptr, nullptr};   // two batch streams + the spreading stream
+  cudaEvent_t staged[2] = {nullptr, nullptr};               // upload of the stream's last batch done
   int next_stream = 0;
-  // pinned staging for argument / work-list uploads, one per stream
+  // pinned staging for argument / work-list uploads, one per batch stream
   void *stage[2] = {nullptr, nullptr};
   size_t stage_cap[2] = {0, 0};
+
   // Local / Focal kinds seen so far, in registration order; the persistent
   // module holds all of them, so it is rebuilt (compiled) only when a new kind appears
   std::vector<KernelPlan> reg_plans;
@@ -102,6 +119,12 @@ struct Server::Impl {
   PersistentModule pm;
   KernelHandle pk;
   int pk_grid = 0;
+  std::map<std::string, std::unique_ptr<Template>> templates;
+
+  // statistics
+  long long batches = 0, completed = 0, failed = 0, max_batch_seen = 0, batched_requests = 0;
+  size_t peak_used = 0;
+
   int register_kind(const KernelPlan &P) {
     auto it = reg_index.find(P.body);
     if (it != reg_index.end()) return it->second;
@@ -120,12 +143,9 @@ struct Server::Impl {
     pk_grid = env.sm_count() * std::max(1, env.occupancy(pk, 256, pm.smem));
     module_kinds = (int)reg_plans.size();
   }
+  // compile = false defers the persistent module's (re)compilation to the caller
+  Template &template_for(int type, int w, int h, float obs_h, bool compile = true);
   void warm_up();
-  // statistics
-  long long batches = 0, completed = 0, failed = 0, max_batch_seen = 0, batched_requests = 0;
-  size_t peak_used = 0;
-  int gc_counter = 0;
-
   void dispatch_loop();
   void complete_loop();
   void run_batch(std::vector<Req *> &batch);
@@ -140,45 +160,89 @@ void Server::Impl::free_request(Req *r, cudaStream_t st) {
   r->scratch.clear();
 }
 
+Template &Server::Impl::template_for(int type, int w, int h, float obs_h, bool compile) {
+  uint32_t hb;
+  std::memcpy(&hb, &obs_h, 4);
+  const std::string key = std::to_string(type) + "|" + std::to_string(w) + "x" + std::to_string(h) + "|" +
+                          (type == REQ_VIEWSHED ? std::to_string(hb) : std::string("-"));
+  auto it = templates.find(key);
+  if (it != templates.end()) return *it->second;
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  CudaEnv &env = CudaEnv::get();
+  auto T = std::make_unique<Template>();
+  // the pointer only identifies the input: requests bind their own window buffers
+  T->win = rt.dev_input(dem, pitch_for(w, F32), Arr2{{w, h}, 2}, F32, Arr2{{w, h}, 2});
+  switch (type) {
+    case REQ_HILLSHADE: T->out = prog_hillshade(rt, T->win); break;
+    case REQ_SLOPE: T->out = prog_slope(rt, T->win); break;
+    // distinct placeholder coordinates keep the two argument nodes distinct
+    case REQ_VIEWSHED: T->out = prog_viewshed(rt, T->win, 1, 2, obs_h, 0.0, &T->ox, &T->oy); break;
+    case REQ_FLOW: T->out = prog_flow(rt, T->win); break;
+    default: throw MapError("unknown request type");
+  }
+  T->out->ref++;
+  T->fr = fuse(collect_nodes({T->out}), {T->out});
+  std::map<const Group *, int> level;
+  for (auto &gp : T->fr.groups) {
+    const Group &g = *gp;
+    int lv = 0;
+    for (Group *p : g.prev) lv = std::max(lv, level[p] + 1);
+    level[&g] = lv;
+    if (g.skeleton == SK_HOST) throw MapError(std::string("serving: unexpected host step ") + kind_name(g.nodes[0]->kind));
+    KernelPlan P = generate_kernel(g);
+    int k = -1;
+    if (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL) {
+      if (lv > 1) throw MapError("serving: program too deep");
+      k = register_kind(P);
+      T->last_phase = std::max(T->last_phase, lv == 0 ? (int)PH_LEVEL0 : (int)PH_LEVEL1);
+    } else if (g.skeleton == SK_RADIAL) {
+      env.kernel(P.source, P.kname + "_many", 0);
+      T->last_phase = std::max(T->last_phase, (int)PH_RADIAL);
+    } else if (g.skeleton == SK_SPREAD) {
+      env.kernel(P.source, P.kname + "_many", 0);
+      T->last_phase = std::max(T->last_phase, (int)PH_SPREAD);
+    } else {
+      throw MapError("serving: zonal groups are not served");
+    }
+    T->plans.push_back(std::move(P));
+    T->level.push_back(lv);
+    T->kind.push_back(k);
+  }
+  if (compile) ensure_module();
+  Template &ref = *T;
+  templates[key] = std::move(T);
+  return ref;
+}
+
 void Server::Impl::run_batch(std::vector<Req *> &batch) {
   CudaEnv &env = CudaEnv::get();
   const int si = next_stream;
   next_stream ^= 1;
   cudaStream_t st = streams[si];
-  // the staging buffer of this stream was last used by the batch recorded in last_ev
-  if (last_ev[si]) cuda_check(cudaEventSynchronize(last_ev[si]), "cudaEventSynchronize");
+  cudaStream_t sp = streams[2];
+  // the pinned staging buffer of this stream is free once its last upload is done
+  if (staged[si]) cuda_check(cudaEventSynchronize(staged[si]), "cudaEventSynchronize");
 
-  Runtime &rt = Runtime::get();
-  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
   std::vector<std::vector<unsigned char>> kind_args;   // per registered kind, this batch's members
   std::vector<int> kind_members;
   struct Item { uint32_t kind, inst, tile, pad; };
   std::vector<std::vector<Item>> levels(2);
-  struct Many { KernelPlan plan; std::vector<unsigned char> args; int n = 0; };
+  struct Many { const KernelPlan *plan = nullptr; std::vector<unsigned char> args; int n = 0; };
   std::map<std::string, Many> radial, spread;
-  std::vector<FusionResult> keep;
   std::vector<Req *> ok;
+  std::vector<int> phase_of;
 
   for (Req *r : batch) {
     try {
+      Template &T = template_for(r->type, r->w, r->h, r->oh, false);
       r->stream = si;
       r->win_pitch = pitch_for(r->w, F32);
       cuda_check(cudaMallocAsync(&r->win, (size_t)r->win_pitch * r->h, st), "cudaMallocAsync(window)");
       cuda_check(cudaMemcpy2DAsync(r->win, r->win_pitch, (char *)dem + (size_t)r->y0 * pitch + (size_t)r->x0 * 4, pitch,
                                    (size_t)r->w * 4, r->h, cudaMemcpyDeviceToDevice, st),
                  "window copy");
-      Node *win = rt.dev_input(r->win, r->win_pitch, Arr2{{r->w, r->h}, 2}, F32, Arr2{{r->w, r->h}, 2});
-      Node *out = nullptr;
-      switch (r->type) {
-        case REQ_HILLSHADE: out = prog_hillshade(rt, win); break;
-        case REQ_SLOPE: out = prog_slope(rt, win); break;
-        case REQ_VIEWSHED: out = prog_viewshed(rt, win, r->ox, r->oy, r->oh, r->radius); break;
-        case REQ_FLOW: out = prog_flow(rt, win); break;
-        default: throw MapError("unknown request type");
-      }
-      out->ref++;
-      r->out_node = out;
-      r->out_dt = out->meta.dtype;
+      r->out_dt = T.out->meta.dtype;
       r->out_pitch = pitch_for(r->w, r->out_dt);
       cuda_check(cudaMallocAsync(&r->out, (size_t)r->out_pitch * r->h, st), "cudaMallocAsync(output)");
       std::unordered_map<Node *, DevRaster> bufs;
@@ -188,31 +252,31 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
       wr.dtype = F32;
       wr.W = r->w;
       wr.H = r->h;
-      bufs[win] = wr;
+      bufs[T.win] = wr;
       DevRaster orr;
       orr.ptr = r->out;
       orr.pitch = r->out_pitch;
       orr.dtype = r->out_dt;
       orr.W = r->w;
       orr.H = r->h;
-      bufs[out] = orr;
+      bufs[T.out] = orr;
       std::function<DevRaster &(Node *)> get = [&](Node *n) -> DevRaster & {
         auto it = bufs.find(n);
         if (it == bufs.end()) throw MapError("serving: raster not bound");
         return it->second;
       };
-      keep.push_back(fuse(collect_nodes({out}), {out}));
-      std::map<const Group *, int> level;
-      for (auto &gp : keep.back().groups) {
-        const Group &g = *gp;
-        int lv = 0;
-        for (Group *p : g.prev) lv = std::max(lv, level[p] + 1);
-        level[&g] = lv;
-        if (g.skeleton == SK_HOST) {
-          Node *n = g.nodes[0];
-          throw MapError(std::string("serving: unexpected host step ") + kind_name(n->kind));
-        }
-        KernelPlan P = generate_kernel(g);
+      std::unordered_map<const Node *, Variant> scal;
+      if (T.ox) {
+        Variant vx{}, vy{};
+        vx.dtype = vy.dtype = S32;
+        vx.u.s32 = r->ox;
+        vy.u.s32 = r->oy;
+        scal[T.ox] = vx;
+        scal[T.oy] = vy;
+      }
+      for (size_t gi = 0; gi < T.fr.groups.size(); gi++) {
+        const Group &g = *T.fr.groups[gi];
+        const KernelPlan &P = T.plans[gi];
         for (Node *o : P.out_rasters) {
           if (bufs.count(o)) continue;
           DevRaster t;
@@ -225,22 +289,21 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           bufs[o] = t;
         }
         if (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL) {
-          if (lv > 1) throw MapError("serving: program too deep");
-          const int k = register_kind(P);
+          const int k = T.kind[gi];
           if ((int)kind_args.size() <= k) {
             kind_args.resize(k + 1);
             kind_members.resize(k + 1, 0);
           }
           uint64_t aux[4] = {0, 0, 0, 0};
-          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           kind_args[k].insert(kind_args[k].end(), a.begin(), a.end());
           const uint32_t idx = (uint32_t)kind_members[k]++;
           const int tiles = ((g.W + P.tile_w - 1) / P.tile_w) * ((g.H + P.tile_h - 1) / P.tile_h);
-          for (int t = 0; t < tiles; t++) levels[lv].push_back(Item{(uint32_t)k, idx, (uint32_t)t, 0});
+          for (int t = 0; t < tiles; t++) levels[T.level[gi]].push_back(Item{(uint32_t)k, idx, (uint32_t)t, 0});
         } else if (g.skeleton == SK_RADIAL) {
           Many &mn = radial[P.source];
-          if (mn.n == 0) mn.plan = P;
-          long long lim = P.core->radius > 0 ? (long long)P.core->radius : -1;
+          mn.plan = &P;
+          const long long lim = r->radius > 0 ? (long long)r->radius : -1;
           int ri = 0;
           for (size_t k = 0; k < P.out_rasters.size(); k++)
             if (P.out_rasters[k] == P.core) ri = (int)k;
@@ -249,33 +312,38 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
               DevRaster &d = bufs.at(o);
               cuda_check(cudaMemset2DAsync(d.ptr, d.pitch, 0xFF, (size_t)d.W * dt_size(d.dtype), d.H, st), "memset");
             }
-          uint64_t aux[4] = {(uint64_t)P.core->coord.arr[0], (uint64_t)P.core->coord.arr[1], (uint64_t)lim, (uint64_t)ri};
-          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          uint64_t aux[4] = {(uint64_t)r->ox, (uint64_t)r->oy, (uint64_t)lim, (uint64_t)ri};
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
-        } else if (g.skeleton == SK_SPREAD) {
+        } else {   // SK_SPREAD
           Many &mn = spread[P.source];
-          if (mn.n == 0) mn.plan = P;
+          mn.plan = &P;
           const size_t N = (size_t)g.W * g.H;
           void *work = nullptr;
           cuda_check(cudaMallocAsync(&work, 3 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
           r->scratch.push_back(work);
           uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
                              (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
-          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+          auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
-        } else {
-          throw MapError("serving: zonal groups are not served");
         }
       }
       ok.push_back(r);
+      phase_of.push_back(T.last_phase);
     } catch (const std::exception &e) {
+      std::lock_guard<std::mutex> lk(m);
       r->state = 3;
       r->err = e.what();
+      failed++;
+      cv_done.notify_all();
     }
   }
   batch = ok;
+  if (batch.empty()) return;
+  ensure_module();
+
   // stage every upload into this stream's pinned buffer
   kind_args.resize(reg_plans.size());
   kind_members.resize(reg_plans.size(), 0);
@@ -288,6 +356,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   for (auto &b : blobs) total += (b.second + 255) / 256 * 256;
   if (total > stage_cap[si]) {
     if (stage[si]) cudaFreeHost(stage[si]);
+    stage[si] = nullptr;
     stage_cap[si] = std::max(total, (size_t)1 << 20);
     cuda_check(cudaMallocHost(&stage[si], stage_cap[si]), "cudaMallocHost(staging)");
   }
@@ -302,14 +371,19 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     off += (b.second + 255) / 256 * 256;
   }
   cuda_check(cudaMemcpyAsync(dbuf, stage[si], off, cudaMemcpyHostToDevice, st), "upload batch arrays");
+  if (!staged[si]) cuda_check(cudaEventCreateWithFlags(&staged[si], cudaEventDisableTiming), "cudaEventCreate");
+  cuda_check(cudaEventRecord(staged[si], st), "cudaEventRecord");
   size_t bi = 0;
   std::vector<void *> d_kind_args;
   for (size_t k = 0; k < kind_args.size(); k++) d_kind_args.push_back(dptr[bi++]);
   std::vector<void *> d_levels;
   for (size_t l = 0; l < levels.size(); l++) d_levels.push_back(dptr[bi++]);
 
-  // persistent launch per level over the Local / Focal kinds; radial after level 0; spread after level 1
-  ensure_module();
+  // phases: persistent launch over level-0 Local / Focal groups; radial scans;
+  // level-1 groups; flow accumulations on the spreading stream (so their long
+  // sweeps hold up neither stream's next batch nor this batch's other requests)
+  cudaEvent_t ev[N_PHASES];
+  for (int p = 0; p < N_PHASES; p++) cuda_check(cudaEventCreateWithFlags(&ev[p], cudaEventDisableTiming), "cudaEventCreate");
   const size_t smem = pm.smem;
   const int grid = pk_grid;
   auto launch_level = [&](int l) {
@@ -327,37 +401,49 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     ba.counter = (uint64_t)(uintptr_t)((char *)dbuf + 16 * l);
     ba.err = (uint64_t)(uintptr_t)env.err_word();
     for (size_t k = 0; k < reg_plans.size(); k++) ba.args[k] = (uint64_t)(uintptr_t)d_kind_args[k];
-    env.launch(pk, std::min<int>(grid, (int)levels[l].size()), 256, smem, (CUstream_st *)st, &ba, 32 + 8 * reg_plans.size());
+    env.launch(pk, std::min<int>(grid, (int)levels[l].size()), 256, smem, (CUstream_st *)st, &ba,
+               32 + 8 * reg_plans.size());
   };
   launch_level(0);
+  cuda_check(cudaEventRecord(ev[PH_LEVEL0], st), "cudaEventRecord");
   for (auto &kv : radial) {
     Many &mn = kv.second;
-    KernelHandle kh = env.kernel(mn.plan.source, mn.plan.kname + "_many", 0);
+    KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_many", 0);
     struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
     env.launch(kh, 8 * mn.n, 512, 0, (CUstream_st *)st, &ma, sizeof ma);
   }
+  cuda_check(cudaEventRecord(ev[PH_RADIAL], st), "cudaEventRecord");
   launch_level(1);
-  for (auto &kv : spread) {
-    Many &mn = kv.second;
-    KernelHandle kh = env.kernel(mn.plan.source, mn.plan.kname + "_many", 0);
-    struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
-    env.launch(kh, mn.n, 1024, 0, (CUstream_st *)st, &ma, sizeof ma);
+  cuda_check(cudaEventRecord(ev[PH_LEVEL1], st), "cudaEventRecord");
+  if (!spread.empty()) {
+    cuda_check(cudaStreamWaitEvent(sp, ev[PH_LEVEL1], 0), "cudaStreamWaitEvent");
+    for (auto &kv : spread) {
+      Many &mn = kv.second;
+      KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_many", 0);
+      struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
+      env.launch(kh, mn.n, 1024, 0, (CUstream_st *)sp, &ma, sizeof ma);
+    }
+    cuda_check(cudaEventRecord(ev[PH_SPREAD], sp), "cudaEventRecord");
   }
-  InFlight f;
-  f.reqs = batch;
-  f.stream = si;
-  f.dev_free.push_back(dbuf);
-  cuda_check(cudaEventCreateWithFlags(&f.ev, cudaEventDisableTiming), "cudaEventCreate");
-  cuda_check(cudaEventRecord(f.ev, st), "cudaEventRecord");
-  if (last_ev[si]) cudaEventDestroy(last_ev[si]);
-  cuda_check(cudaEventCreateWithFlags(&last_ev[si], cudaEventDisableTiming), "cudaEventCreate");
-  cuda_check(cudaEventRecord(last_ev[si], st), "cudaEventRecord");
   {
     std::lock_guard<std::mutex> lk2(m);
     batches++;
     batched_requests += (long long)batch.size();
     max_batch_seen = std::max<long long>(max_batch_seen, (long long)batch.size());
-    inflight.push_back(std::move(f));
+    // completion records, one per phase; the batch arrays go with the batch's last one
+    const int last = spread.empty() ? (int)PH_LEVEL1 : (int)PH_SPREAD;
+    for (int p = 0; p < N_PHASES; p++) {
+      if (p == PH_SPREAD && spread.empty()) {
+        cudaEventDestroy(ev[p]);
+        continue;
+      }
+      PhaseDone d;
+      d.ev = ev[p];
+      for (size_t i = 0; i < batch.size(); i++)
+        if (phase_of[i] == p) d.reqs.push_back(batch[i]);
+      if (p == last) d.batch_mem = dbuf;
+      inflight[p == PH_SPREAD ? 2 : si].push_back(std::move(d));
+    }
   }
   cv_inflight.notify_all();
 }
@@ -373,7 +459,8 @@ void Server::Impl::dispatch_loop() {
       if (stop) return;
       while (!pending.empty() && (int)batch.size() < max_batch) {
         Req *r = pending.front();
-        if (used + r->bytes > budget && !(batch.empty() && inflight.empty() && used == 0)) break;
+        const bool idle = inflight[0].empty() && inflight[1].empty() && inflight[2].empty();
+        if (used + r->bytes > budget && !(batch.empty() && idle && used == 0)) break;
         used += r->bytes;
         peak_used = std::max(peak_used, used);
         r->state = 1;
@@ -391,35 +478,51 @@ void Server::Impl::dispatch_loop() {
     } catch (const std::exception &e) {
       std::lock_guard<std::mutex> lk(m);
       for (Req *r : batch) {
+        if (r->state >= 2) continue;
         r->state = 3;
         r->err = e.what();
+        failed++;
       }
       cv_done.notify_all();
     }
   }
 }
 
+// Retires phases as their events fire. Each of the three queues (two batch
+// streams and the spreading stream) completes in order, but independently of
+// the others, so the completion thread polls the head of every queue.
 void Server::Impl::complete_loop() {
   CudaEnv &env = CudaEnv::get();
   cudaSetDevice(env.device());
   while (true) {
-    InFlight f;
+    PhaseDone d;
+    int q = -1;
+    cudaError_t e = cudaSuccess;
     {
       std::unique_lock<std::mutex> lk(m);
-      cv_inflight.wait(lk, [&] { return stop || !inflight.empty(); });
-      if (inflight.empty() && stop) return;
-      f = std::move(inflight.front());
-      inflight.pop_front();
+      cv_inflight.wait(lk, [&] { return stop || !inflight[0].empty() || !inflight[1].empty() || !inflight[2].empty(); });
+      if (stop && inflight[0].empty() && inflight[1].empty() && inflight[2].empty()) return;
+      for (int i = 0; i < 3 && q < 0; i++) {
+        if (inflight[i].empty()) continue;
+        e = cudaEventQuery(inflight[i].front().ev);
+        if (e != cudaErrorNotReady) q = i;
+      }
+      if (q >= 0) {
+        d = std::move(inflight[q].front());
+        inflight[q].pop_front();
+      }
     }
-    cudaError_t e = cudaEventSynchronize(f.ev);
+    if (q < 0) {
+      std::this_thread::sleep_for(std::chrono::microseconds(20));
+      continue;
+    }
     const double t = now_s();
-    cudaEventDestroy(f.ev);
-    cudaStream_t st = streams[f.stream];
-    for (void *p : f.dev_free) cudaFreeAsync(p, st);
-    std::vector<Node *> unref;
+    cudaEventDestroy(d.ev);
+    cudaStream_t st = streams[q];
+    if (d.batch_mem) cudaFreeAsync(d.batch_mem, st);
     {
       std::lock_guard<std::mutex> lk(m);
-      for (Req *r : f.reqs) {
+      for (Req *r : d.reqs) {
         r->t_done = t;
         if (e != cudaSuccess) {
           r->state = 3;
@@ -429,8 +532,6 @@ void Server::Impl::complete_loop() {
           r->state = 2;
           completed++;
         }
-        unref.push_back(r->out_node);
-        r->out_node = nullptr;
         if (r->auto_release) {
           free_request(r, st);
           used -= r->bytes;
@@ -438,36 +539,20 @@ void Server::Impl::complete_loop() {
         }
       }
     }
-    {
-      Runtime &rt = Runtime::get();
-      std::lock_guard<std::recursive_mutex> lk(rt.mtx);
-      for (Node *n : unref)
-        if (n && rt.owns(n) && n->ref > 0) n->ref--;
-      if (++gc_counter % 64 == 0) rt.collect_garbage();
-    }
     cv_done.notify_all();
     cv_pending.notify_all();
   }
 }
 
-// Registers and compiles every program kind up front (templates over a 64x64
-// window of the DEM), so no request waits for a compilation.
+// Builds the templates of every program kind at the load generator's window
+// sizes, which registers and compiles every kernel up front, so no request
+// waits for a compilation.
 void Server::Impl::warm_up() {
-  Runtime &rt = Runtime::get();
-  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
-  CudaEnv &env = CudaEnv::get();
+  for (int s : {256, 512, 1024})
+    if (s <= W && s <= H)
+      for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, s, s, 10.0f, false);
   const int w = std::min(64, W), h = std::min(64, H);
-  Node *win = rt.dev_input(dem, pitch, Arr2{{w, h}, 2}, F32, Arr2{{w, h}, 2});
-  std::vector<Node *> outs = {prog_hillshade(rt, win), prog_slope(rt, win),
-                              prog_viewshed(rt, win, w / 2, h / 2, 10.0f, 16.0), prog_flow(rt, win)};
-  for (Node *o : outs) {
-    FusionResult fr = fuse(collect_nodes({o}), {o});
-    for (auto &gp : fr.groups) {
-      KernelPlan P = generate_kernel(*gp);
-      if (gp->skeleton == SK_LOCAL || gp->skeleton == SK_FOCAL) register_kind(P);
-      else if (gp->skeleton == SK_RADIAL || gp->skeleton == SK_SPREAD) env.kernel(P.source, P.kname + "_many", 0);
-    }
-  }
+  for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, w, h, 10.0f, false);
   ensure_module();
 }
 
@@ -482,7 +567,13 @@ Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, in
   I.H = H;
   I.budget = budget_bytes;
   I.max_batch = std::max(1, max_batch);
-  for (int i = 0; i < 2; i++) cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+  // keep freed pool memory mapped: requests allocate and free continuously
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, env.device()) == cudaSuccess) {
+    uint64_t thr = UINT64_MAX;
+    cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+  }
+  for (int i = 0; i < 3; i++) cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
   I.warm_up();
   I.dispatcher = std::thread([&I] { I.dispatch_loop(); });
   I.completer = std::thread([&I] { I.complete_loop(); });
@@ -505,7 +596,7 @@ Server::~Server() {
   I.cv_inflight.notify_all();
   for (;;) {
     std::unique_lock<std::mutex> lk(I.m);
-    if (I.inflight.empty()) break;
+    if (I.inflight[0].empty() && I.inflight[1].empty() && I.inflight[2].empty()) break;
     I.cv_done.wait_for(lk, std::chrono::milliseconds(5));
   }
   {
@@ -514,18 +605,18 @@ Server::~Server() {
   }
   I.cv_inflight.notify_all();
   I.completer.join();
+  for (int i = 0; i < 3; i++) cudaStreamSynchronize(I.streams[i]);
+  for (auto &kv : I.reqs) I.free_request(kv.second.get(), I.streams[0]);
+  cudaStreamSynchronize(I.streams[0]);
   for (int i = 0; i < 2; i++) {
-    cudaStreamSynchronize(I.streams[i]);
-    for (auto &kv : I.reqs) if (kv.second->stream == i) I.free_request(kv.second.get(), I.streams[i]);
-    cudaStreamSynchronize(I.streams[i]);
-    if (I.last_ev[i]) cudaEventDestroy(I.last_ev[i]);
-    cudaStreamDestroy(I.streams[i]);
+    if (I.staged[i]) cudaEventDestroy(I.staged[i]);
     if (I.stage[i]) cudaFreeHost(I.stage[i]);
   }
+  for (int i = 0; i < 3; i++) cudaStreamDestroy(I.streams[i]);
   Runtime &rt = Runtime::get();
   std::lock_guard<std::recursive_mutex> lk(rt.mtx);
-  for (auto &kv : I.reqs)
-    if (kv.second->out_node && rt.owns(kv.second->out_node) && kv.second->out_node->ref > 0) kv.second->out_node->ref--;
+  for (auto &kv : I.templates)
+    if (kv.second->out && rt.owns(kv.second->out) && kv.second->out->ref > 0) kv.second->out->ref--;
 }
 
 long long Server::submit(int type, int x0, int y0, int w, int h, int obs_x, int obs_y, float obs_h, double radius,
@@ -616,7 +707,7 @@ std::string Server::stats_json() {
   s << "{\"batches\": " << I.batches << ", \"completed\": " << I.completed << ", \"failed\": " << I.failed
     << ", \"mean_batch\": " << (I.batches ? (double)I.batched_requests / I.batches : 0.0)
     << ", \"max_batch\": " << I.max_batch_seen << ", \"peak_bytes\": " << I.peak_used << ", \"budget_bytes\": " << I.budget
-    << "}";
+    << ", \"templates\": " << I.templates.size() << ", \"kinds\": " << I.reg_plans.size() << "}";
   return s.str();
 }
 

@@ -38,7 +38,7 @@ struct Geom {
   s32 tiles_x;       // tiles per region row
   s32 tiles;         // tiles in the region
   s32 border;        // 0 block mirror, 1 raster mirror, 2 dead
-  s32 pad;
+  s32 oy;            // raster row held by row 0 of the staged inputs' tensor maps (row bands; else 0)
 };
 
 enum { ERR_TMA_TIMEOUT = 1, ERR_BAD_LAUNCH = 2, ERR_ITER_LIMIT = 4, ERR_SPIN_LIMIT = 8 };

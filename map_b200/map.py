@@ -714,6 +714,19 @@ def get_exec_mode():
     return _lib.ma_getExecMode()
 
 
+def set_stream_rows(rows):
+    """Row bands of streamed host-to-host evaluation: 0 automatic, < 0 off, > 0 forced."""
+    _lib.ma_setStreamRows(rows)
+
+
+def get_stream_rows():
+    return _lib.ma_getStreamRows()
+
+
+def last_band_count():
+    return _lib.ma_lastBandCount()
+
+
 def set_default_blocksize(bs):
     _lib.ma_setDefaultBlockSize(Array(bs))
 
@@ -913,6 +926,9 @@ _sig('ma_sync', [], ct.c_int)
 _sig('ma_stream', [], ct.c_void_p)
 _sig('ma_lastLaunchCount', [], ct.c_int, check=False)
 _sig('ma_lastGroupCount', [], ct.c_int, check=False)
+_sig('ma_lastBandCount', [], ct.c_int, check=False)
+_sig('ma_setStreamRows', [ct.c_int], None)
+_sig('ma_getStreamRows', [], ct.c_int, check=False)
 _sig('ma_compileOnly', [ct.POINTER(Node), ct.c_int, ct.c_int], ct.c_int)
 _sig('ma_describeGroups', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_generatedSource', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
