@@ -43,7 +43,10 @@ def parse():
     p.add_argument("--block", type=int, default=256)
     p.add_argument("--e2e-steps", type=int, default=3)
     p.add_argument("--no-clocks", action="store_true")
-    p.add_argument("--no-mix", action="store_true", help="skip the batched-mix and serving sections")
+    p.add_argument("--no-mix", action="store_true", help="skip the batched-mix, zonal and serving sections")
+    p.add_argument("--sections", default="batched,zonal_stats,serving",
+                   help="comma-separated extra sections after the headline (batched, zonal_stats, serving)")
+    p.add_argument("--zonal-size", type=int, default=16384)
     return p.parse_args()
 
 
@@ -89,14 +92,58 @@ def cpu_baseline(dem_window, seconds_budget=12.0, threads=None):
 # ---------------------------------------------------------------- clocks
 
 class Clocks:
-    def __init__(self, index, enabled=True):
-        self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_rank%d.csv" % index) if enabled else None
+    """Samples the GPU's SM clock and clock-event (throttle) reasons during a
+    timed region: NVML read in-process every 2 ms on a thread (so that regions of
+    a few tens of ms get samples), else `nvidia-smi -lms 100` into a CSV file.
+    Only reads; changes no setting."""
+
+    def __init__(self, index, enabled=True, device=None):
+        self.enabled = enabled
         self.index = index
+        self.device = device
+        self.rows = []
+        self.proc = None
+        self.thread = None
+        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_rank%d.csv" % index) if enabled else None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.device if self.device is not None else self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(("GPU-" + uuid) if not uuid.startswith("GPU-") else uuid)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
-        if self.path is None:
+        if not self.enabled:
             return self
+        import threading
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap,
+                    "hw_power_brake_slowdown": nv.nvmlClocksEventReasonHwPowerBrakeSlowdown}
+            self.stop = threading.Event()
+
+            def run():
+                while not self.stop.is_set():
+                    try:
+                        sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                        rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                        self.rows.append((sm, [k for k, b in bits.items() if rs & b]))
+                    except Exception:
+                        pass
+                    self.stop.wait(0.002)
+            self.thread = threading.Thread(target=run, daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             os.makedirs(os.path.dirname(self.path), exist_ok=True)
             self.f = open(self.path, "w")
@@ -111,6 +158,9 @@ class Clocks:
         return self
 
     def __exit__(self, *a):
+        if self.thread is not None:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -120,6 +170,13 @@ class Clocks:
             self.f.close()
 
     def summary(self):
+        if self.thread is not None:
+            if not self.rows:
+                return None
+            sm = [r[0] for r in self.rows]
+            reasons = sorted({k for r in self.rows for k in r[1]})
+            return {"sm_mhz": statistics.median(sm), "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                    "samples": len(self.rows), "source": "nvml, 2 ms"}
         if self.proc is None or self.path is None:
             return None
         rows = []
@@ -134,7 +191,7 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower().startswith("active")})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 100 ms"}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -375,7 +432,7 @@ def main():
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     barrier()
     torch.cuda.synchronize()
-    with Clocks(local, enabled=not args.no_clocks) as clk:
+    with Clocks(local, enabled=not args.no_clocks, device=local) as clk:
         ev0.record(stream)
         for _ in range(args.steps):
             M.to_device(hs, out_t.data_ptr(), pitch, sync=False)
@@ -462,19 +519,15 @@ def main():
         ck = clk.summary()
         if ck:
             line["clocks"] = ck
-        if world == 1 and not args.no_mix:
+        sections = [x for x in args.sections.split(",") if x] if (world == 1 and not args.no_mix) else []
+        runners = {"batched": lambda: bench_batched(M, W, synth, torch, dev),
+                   "zonal_stats": lambda: bench_zonal_stats(M, synth, torch, dev, size=args.zonal_size),
+                   "serving": lambda: bench_serving(M, synth, torch, dev)}
+        for name in sections:
             try:
-                line["batched"] = bench_batched(M, W, synth, torch, dev)
+                line[name] = runners[name]()
             except Exception as e:   # reported, not fatal: the headline line still prints
-                line["batched"] = {"error": str(e)[:300]}
-            try:
-                line["zonal_stats"] = bench_zonal_stats(M, synth, torch, dev)
-            except Exception as e:
-                line["zonal_stats"] = {"error": str(e)[:300]}
-            try:
-                line["serving"] = bench_serving(M, synth, torch, dev)
-            except Exception as e:
-                line["serving"] = {"error": str(e)[:300]}
+                line[name] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()

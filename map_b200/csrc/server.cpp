@@ -79,6 +79,11 @@ struct Template {
   int last_phase = PH_LEVEL0;
 };
 
+// Flow accumulations run one CTA per request; batches take turns over several
+// streams so that consecutive batches' accumulations run side by side.
+constexpr int kSpreadStreams = 8;
+constexpr int kQueues = 2 + kSpreadStreams;   // two batch streams, then the spreading streams
+
 // One phase of one batch: the requests that complete with it.
 struct PhaseDone {
   cudaEvent_t ev = nullptr;
@@ -99,14 +104,14 @@ struct Server::Impl {
   std::condition_variable cv_pending, cv_done, cv_inflight;
   std::deque<Req *> pending;
   std::map<long long, std::unique_ptr<Req>> reqs;
-  std::deque<PhaseDone> inflight[3];   // per completion queue: stream 0, stream 1, spreading stream
+  std::deque<PhaseDone> inflight[kQueues];   // per stream, in stream order
   size_t used = 0;
   long long next_id = 1;
   bool stop = false;
   std::thread dispatcher, completer;
-  cudaStream_t streams[3] = {nullptr, nullptr, nullptr};   // two batch streams + the spreading stream
+  cudaStream_t streams[kQueues] = {};   // two batch streams, then the spreading streams
   cudaEvent_t staged[2] = {nullptr, nullptr};               // upload of the stream's last batch done
-  int next_stream = 0;
+  int next_stream = 0, next_spread = 0;
   // pinned staging for argument / work-list uploads, one per batch stream
   void *stage[2] = {nullptr, nullptr};
   size_t stage_cap[2] = {0, 0};
@@ -148,6 +153,11 @@ struct Server::Impl {
   void warm_up();
   void dispatch_loop();
   void complete_loop();
+  bool idle() const {
+    for (int i = 0; i < kQueues; i++)
+      if (!inflight[i].empty()) return false;
+    return true;
+  }
   void run_batch(std::vector<Req *> &batch);
   void free_request(Req *r, cudaStream_t st);
 };
@@ -220,7 +230,9 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   const int si = next_stream;
   next_stream ^= 1;
   cudaStream_t st = streams[si];
-  cudaStream_t sp = streams[2];
+  const int spi = 2 + next_spread;
+  next_spread = (next_spread + 1) % kSpreadStreams;
+  cudaStream_t sp = streams[spi];
   // the pinned staging buffer of this stream is free once its last upload is done
   if (staged[si]) cuda_check(cudaEventSynchronize(staged[si]), "cudaEventSynchronize");
 
@@ -442,7 +454,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
       for (size_t i = 0; i < batch.size(); i++)
         if (phase_of[i] == p) d.reqs.push_back(batch[i]);
       if (p == last) d.batch_mem = dbuf;
-      inflight[p == PH_SPREAD ? 2 : si].push_back(std::move(d));
+      inflight[p == PH_SPREAD ? spi : si].push_back(std::move(d));
     }
   }
   cv_inflight.notify_all();
@@ -459,8 +471,7 @@ void Server::Impl::dispatch_loop() {
       if (stop) return;
       while (!pending.empty() && (int)batch.size() < max_batch) {
         Req *r = pending.front();
-        const bool idle = inflight[0].empty() && inflight[1].empty() && inflight[2].empty();
-        if (used + r->bytes > budget && !(batch.empty() && idle && used == 0)) break;
+        if (used + r->bytes > budget && !(batch.empty() && idle() && used == 0)) break;
         used += r->bytes;
         peak_used = std::max(peak_used, used);
         r->state = 1;
@@ -488,9 +499,9 @@ void Server::Impl::dispatch_loop() {
   }
 }
 
-// Retires phases as their events fire. Each of the three queues (two batch
-// streams and the spreading stream) completes in order, but independently of
-// the others, so the completion thread polls the head of every queue.
+// Retires phases as their events fire. Each stream's queue completes in order,
+// but independently of the others, so the completion thread polls the head of
+// every queue.
 void Server::Impl::complete_loop() {
   CudaEnv &env = CudaEnv::get();
   cudaSetDevice(env.device());
@@ -500,9 +511,9 @@ void Server::Impl::complete_loop() {
     cudaError_t e = cudaSuccess;
     {
       std::unique_lock<std::mutex> lk(m);
-      cv_inflight.wait(lk, [&] { return stop || !inflight[0].empty() || !inflight[1].empty() || !inflight[2].empty(); });
-      if (stop && inflight[0].empty() && inflight[1].empty() && inflight[2].empty()) return;
-      for (int i = 0; i < 3 && q < 0; i++) {
+      cv_inflight.wait(lk, [&] { return stop || !idle(); });
+      if (stop && idle()) return;
+      for (int i = 0; i < kQueues && q < 0; i++) {
         if (inflight[i].empty()) continue;
         e = cudaEventQuery(inflight[i].front().ev);
         if (e != cudaErrorNotReady) q = i;
@@ -573,7 +584,8 @@ Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, in
     uint64_t thr = UINT64_MAX;
     cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
   }
-  for (int i = 0; i < 3; i++) cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
+  for (int i = 0; i < kQueues; i++)
+    cuda_check(cudaStreamCreateWithFlags(&I.streams[i], cudaStreamNonBlocking), "cudaStreamCreate");
   I.warm_up();
   I.dispatcher = std::thread([&I] { I.dispatch_loop(); });
   I.completer = std::thread([&I] { I.complete_loop(); });
@@ -596,7 +608,7 @@ Server::~Server() {
   I.cv_inflight.notify_all();
   for (;;) {
     std::unique_lock<std::mutex> lk(I.m);
-    if (I.inflight[0].empty() && I.inflight[1].empty() && I.inflight[2].empty()) break;
+    if (I.idle()) break;
     I.cv_done.wait_for(lk, std::chrono::milliseconds(5));
   }
   {
@@ -605,14 +617,14 @@ Server::~Server() {
   }
   I.cv_inflight.notify_all();
   I.completer.join();
-  for (int i = 0; i < 3; i++) cudaStreamSynchronize(I.streams[i]);
+  for (int i = 0; i < kQueues; i++) cudaStreamSynchronize(I.streams[i]);
   for (auto &kv : I.reqs) I.free_request(kv.second.get(), I.streams[0]);
   cudaStreamSynchronize(I.streams[0]);
   for (int i = 0; i < 2; i++) {
     if (I.staged[i]) cudaEventDestroy(I.staged[i]);
     if (I.stage[i]) cudaFreeHost(I.stage[i]);
   }
-  for (int i = 0; i < 3; i++) cudaStreamDestroy(I.streams[i]);
+  for (int i = 0; i < kQueues; i++) cudaStreamDestroy(I.streams[i]);
   Runtime &rt = Runtime::get();
   std::lock_guard<std::recursive_mutex> lk(rt.mtx);
   for (auto &kv : I.templates)
