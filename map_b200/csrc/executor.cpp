@@ -268,6 +268,39 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
   return P;
 }
 
+std::shared_ptr<Executor::Prepared> Executor::prepare_cached(const std::vector<Node *> &targets,
+                                                             const std::set<Node *> &tset) {
+  Runtime &rt = Runtime::get();
+  std::string key = std::to_string(rt.exec_mode) + ";";
+  for (Node *t : targets) key += std::to_string(t->id) + ",";
+  key += ";";
+  for (Node *t : tset) key += std::to_string(t->id) + ",";
+  auto sig = [](const Prepared &P) {
+    std::vector<char> v;
+    for (Node *n : P.order)
+      if (n->meta.numdim == D0) v.push_back(n->has_value ? 1 : 0);
+    return v;
+  };
+  auto it = cache_.find(key);
+  if (it != cache_.end() && it->second.epoch == rt.epoch && it->second.d0sig == sig(*it->second.P)) {
+    it->second.used = ++cache_tick_;
+    return it->second.P;
+  }
+  auto P = std::make_shared<Prepared>(prepare(targets, tset, true));
+  if (cache_.size() >= 64) {   // evict the least recently used entry
+    auto lru = cache_.begin();
+    for (auto c = cache_.begin(); c != cache_.end(); ++c)
+      if (c->second.used < lru->second.used) lru = c;
+    cache_.erase(lru);
+  }
+  CacheEntry &e = cache_[key];
+  e.P = P;
+  e.d0sig = sig(*P);
+  e.epoch = rt.epoch;
+  e.used = ++cache_tick_;
+  return P;
+}
+
 std::vector<std::string> Executor::compile_only(const std::vector<Node *> &targets, bool compile) {
   std::lock_guard<std::recursive_mutex> lk(Runtime::get().mtx);
   std::set<Node *> tset(targets.begin(), targets.end());
@@ -329,7 +362,8 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
   for (Node *t : targets)
     if (!rt.owns(t)) throw MapError("evaluate: unknown node");
   std::set<Node *> tset(targets.begin(), targets.end());
-  Prepared P = prepare(targets, tset, true);
+  std::shared_ptr<Prepared> PP = prepare_cached(targets, tset);
+  const Prepared &P = *PP;
   last = EvalStats();
   last.groups = (int)P.fr.groups.size();
   const int launches0 = env.launches();

@@ -100,6 +100,17 @@ class Executor {
     std::vector<Node *> order;
   };
   Prepared prepare(const std::vector<Node *> &targets, const std::set<Node *> &tset, bool compile);
+  // Programs evaluated again (same target nodes, same launch mode, same known
+  // scalar values, no node destroyed since) reuse their fusion and kernel plans.
+  struct CacheEntry {
+    std::shared_ptr<Prepared> P;
+    std::vector<char> d0sig;   // has_value of every D0 node of P.order
+    uint64_t epoch = 0;
+    uint64_t used = 0;
+  };
+  std::map<std::string, CacheEntry> cache_;
+  uint64_t cache_tick_ = 0;
+  std::shared_ptr<Prepared> prepare_cached(const std::vector<Node *> &targets, const std::set<Node *> &tset);
   // Row-band streaming of host-to-host Local / Focal programs; false (and no
   // work done) when the program does not qualify.
   bool evaluate_streamed(const Prepared &P, const std::vector<Node *> &targets, const std::vector<Sink> &sinks);

@@ -450,10 +450,12 @@ void Runtime::collect_garbage() {
     if (!live.count(u.get())) live_set.erase(u.get());
   nodes.erase(std::remove_if(nodes.begin(), nodes.end(), [&](const std::unique_ptr<Node> &u) { return !live.count(u.get()); }),
               nodes.end());
+  epoch++;
 }
 
 void Runtime::reset() {
   std::lock_guard<std::recursive_mutex> lk(mtx);
+  epoch++;
   cse.clear();
   live_set.clear();
   nodes.clear();

@@ -95,6 +95,8 @@ struct Runtime {
   // Row bands of streamed evaluations (host rasters in, host rasters out):
   // 0 automatic, < 0 never stream, > 0 stream whenever a raster has more rows.
   int stream_rows = 0;
+  // incremented whenever nodes are destroyed (caches keyed by node ids check it)
+  uint64_t epoch = 0;
   Arr2 default_bs{{256, 256}, 2};
 
   // factories (each returns a node owned by the runtime, possibly pre-existing)
