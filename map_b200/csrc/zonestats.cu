@@ -19,13 +19,16 @@
 //
 // Kernels (one pass over the rasters, HBM-bound: 8 bytes per cell):
 //   1. zs_accumulate: a persistent grid; each CTA owns a contiguous range of
-//      128-cell row chunks and keeps the zones' bins in shared memory. A warp loads
-//      a chunk with 16-byte loads (4 cells per lane), folds each lane's cells of its
-//      leading zone, merges equal-zone runs of lanes with a segmented shuffle scan,
-//      and the last lane of each run updates the shared bins with atomics. At the
-//      end the CTA adds its non-empty bins into the global bins with atomics.
-//      Zone counts whose bins do not fit in shared memory use the global bins
-//      directly.
+//      128-cell row chunks and keeps the zones' bins in shared memory, and each
+//      warp walks a contiguous part of that range, 4 chunks in flight, loading a
+//      chunk with 16-byte loads (4 cells per lane). The warp stages its 4 chunks
+//      (512 cells) in shared memory in cell order and each lane folds 16
+//      consecutive cells into a running aggregate (count, sum, min / max keys);
+//      zones come in long runs along rows, so lanes of equal zones are adjacent:
+//      a segmented shuffle scan merges them and the last lane of each run adds the
+//      aggregate to the shared bins with atomics. At the end the CTA adds its
+//      non-empty bins into the global bins with atomics. Zone counts whose bins do
+//      not fit in shared memory use the global bins directly.
 //   2. zs_finalize: converts the global bins into the caller's output arrays.
 // Global bins must start at zero before step 1 (a zero bin is the empty bin:
 // min / max are kept as order-preserving integer keys whose empty value is 0).
@@ -100,9 +103,52 @@ struct Geometry {
   int vec;                 // 16-byte loads allowed for full chunks
 };
 
+// Running aggregate of one lane over consecutive cells of one zone.
+struct LaneAcc {
+  int key;
+  unsigned cnt, nmn, mx;
+  float sm;
+};
+
+// Adds every lane's aggregate to the bins, lanes of equal zones merged first by a
+// segmented shuffle scan (runs of equal keys, in lane order) so only the last
+// lane of each run issues atomics. Called by all 32 lanes; key < 0 lanes skip.
 template <bool SMEM>
-__global__ void __launch_bounds__(kThreads) zs_accumulate(const Geometry geo, Bin *gbins) {
+__device__ __forceinline__ void warp_flush(const SmemBins &sb, Bin *gbins, const LaneAcc &a, int lane, unsigned below) {
+  int key = a.cnt ? a.key : -1;
+  unsigned cnt = a.cnt, nmn = a.nmn, mx = a.mx;
+  float sm = a.sm;
+  const int up = __shfl_up_sync(0xffffffffu, key, 1);
+  const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || up != key);
+  const int seg_start = 31 - __clz(heads & below);
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const unsigned c2 = __shfl_up_sync(0xffffffffu, cnt, off);
+    const float s2 = __shfl_up_sync(0xffffffffu, sm, off);
+    const unsigned n2 = __shfl_up_sync(0xffffffffu, nmn, off);
+    const unsigned m2 = __shfl_up_sync(0xffffffffu, mx, off);
+    if (lane - off >= seg_start) {
+      sm = s2 + sm;
+      cnt += c2;
+      nmn = max(nmn, n2);
+      mx = max(mx, m2);
+    }
+  }
+  const int dn = __shfl_down_sync(0xffffffffu, key, 1);
+  if ((lane == 31 || dn != key) && key >= 0 && cnt > 0) bin_add<SMEM>(sb, gbins, key, cnt, sm, nmn, mx);
+}
+
+constexpr int kStep = kChunk * kUnroll;          // cells a warp stages per step (512)
+constexpr int kRun = kStep / 32;                   // consecutive cells a lane folds per step (16)
+constexpr int kStage = kStep + kStep / 32;         // staging words per warp and array (one pad word per 32)
+
+__device__ __forceinline__ int stage_idx(int i) { return i + (i >> 5); }   // conflict-free both ways
+
+template <bool SMEM>
+__global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo, Bin *gbins) {
   extern __shared__ __align__(16) unsigned char zs_smem[];
+  __shared__ float st_v[kThreads / 32][kStage];
+  __shared__ int st_z[kThreads / 32][kStage];
   SmemBins sb = {nullptr, nullptr, nullptr, nullptr};
   const int nz = geo.nzones;
   if (SMEM) {
@@ -114,23 +160,49 @@ __global__ void __launch_bounds__(kThreads) zs_accumulate(const Geometry geo, Bi
     __syncthreads();
   }
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  // the CTA's contiguous chunk range, split into one contiguous sub-range per warp
   const long long c0 = (long long)blockIdx.x * geo.per_cta;
   const long long c1 = min(geo.chunks, c0 + geo.per_cta);
+  const long long per_warp = (c1 - c0 + nwarps - 1) / nwarps;
+  const long long w0 = min(c1, c0 + (long long)warp * per_warp);
+  const long long w1 = min(c1, w0 + per_warp);
   const unsigned below = (lane == 31) ? 0xffffffffu : ((2u << lane) - 1u);   // lanes <= this one
+  float *sv = st_v[warp];
+  int *sz = st_z[warp];
+  const int st_base = lane * 4 + (lane >> 3);       // stage_idx(4 * lane), the lane's 4 cells of a chunk
+  const int run_base = lane * kRun + (lane >> 1);   // stage_idx(16 * lane), the lane's run
+  // row and chunk column of chunk cb, advanced incrementally (one division per warp)
+  long long yb = w0 / geo.nchunk_x;
+  long long xb = w0 - yb * geo.nchunk_x;
 
-  for (long long cb = c0 + (long long)warp * kUnroll; cb < c1; cb += (long long)nwarps * kUnroll) {
+  for (long long cb = w0; cb < w1; cb += kUnroll) {
     float v[kUnroll][4];
     int z[kUnroll][4];
 #pragma unroll
+    // the step's 4 chunks usually lie in one row: one row pointer for all of them
+    const bool one_row = xb + kUnroll <= geo.nchunk_x && cb + kUnroll <= w1;
+    const float *vrow = (const float *)(geo.val + yb * geo.vpitch);
+    const int *zrow = (const int *)(geo.zone + yb * geo.zpitch);
     for (int u = 0; u < kUnroll; u++) {
       const long long c = cb + u;
 #pragma unroll
       for (int j = 0; j < 4; j++) z[u][j] = -1;
-      if (c < c1) {
-        const long long y = c / geo.nchunk_x;
-        const int x = (int)(c - y * geo.nchunk_x) * kChunk + lane * 4;
-        const float *vr = (const float *)(geo.val + y * geo.vpitch);
-        const int *zr = (const int *)(geo.zone + y * geo.zpitch);
+      if (c < w1) {
+        const float *vr = vrow;
+        const int *zr = zrow;
+        int x;
+        if (one_row) {
+          x = ((int)xb + u) * kChunk + lane * 4;
+        } else {
+          long long y = yb, cx = xb + u;
+          while (cx >= geo.nchunk_x) {
+            cx -= geo.nchunk_x;
+            y++;
+          }
+          x = (int)cx * kChunk + lane * 4;
+          vr = (const float *)(geo.val + y * geo.vpitch);
+          zr = (const int *)(geo.zone + y * geo.zpitch);
+        }
         if (geo.vec && x + 3 < geo.W) {
           const float4 a = __ldcs((const float4 *)(vr + x));
           const int4 b = __ldcs((const int4 *)(zr + x));
@@ -146,48 +218,47 @@ __global__ void __launch_bounds__(kThreads) zs_accumulate(const Geometry geo, Bi
         }
       }
     }
+    // stage the step's cells in order, then let each lane fold a run of consecutive cells
+    // cell u*128 + 4*lane + j sits at stage_idx() = u*132 + st_base + j
 #pragma unroll
-    for (int u = 0; u < kUnroll; u++) {
-      // lane aggregate over the cells of the lane's first counted zone
-      int key = -1;
-      unsigned cnt = 0, nmn = 0, mx = 0;
-      float sm = 0.0f;
+    for (int u = 0; u < kUnroll; u++)
 #pragma unroll
       for (int j = 0; j < 4; j++) {
-        const int zz = z[u][j];
-        const float vv = v[u][j];
-        if ((unsigned)zz >= (unsigned)nz || vv != vv) continue;
-        const unsigned k = fkey(vv);
-        if (key < 0) key = zz;
-        if (zz == key) {
-          cnt++;
-          sm = (cnt == 1) ? vv : sm + vv;
-          nmn = max(nmn, ~k);
-          mx = max(mx, k);
-        } else {
-          bin_add<SMEM>(sb, gbins, zz, 1u, vv, ~k, k);   // a lane straddling a zone edge
-        }
+        sv[st_base + u * (kChunk + kChunk / 32) + j] = v[u][j];
+        sz[st_base + u * (kChunk + kChunk / 32) + j] = z[u][j];
       }
-      // segmented inclusive scan over runs of lanes with equal keys
-      const int up = __shfl_up_sync(0xffffffffu, key, 1);
-      const unsigned heads = __ballot_sync(0xffffffffu, lane == 0 || up != key);
-      const int seg_start = 31 - __clz(heads & below);
+    __syncwarp();
+    // the lane's run: cells 16*lane + k at stage_idx() = run_base + k
+    int key = -1;
+    unsigned cnt = 0u, kmin = 0xffffffffu, kmax = 0u;
+    float sm = 0.0f;
 #pragma unroll
-      for (int off = 1; off < 32; off <<= 1) {
-        const unsigned c2 = __shfl_up_sync(0xffffffffu, cnt, off);
-        const float s2 = __shfl_up_sync(0xffffffffu, sm, off);
-        const unsigned n2 = __shfl_up_sync(0xffffffffu, nmn, off);
-        const unsigned m2 = __shfl_up_sync(0xffffffffu, mx, off);
-        if (lane - off >= seg_start) {
-          sm = s2 + sm;
-          cnt += c2;
-          nmn = max(nmn, n2);
-          mx = max(mx, m2);
-        }
+    for (int k = 0; k < kRun; k++) {
+      const int zz = sz[run_base + k];
+      const float vv = sv[run_base + k];
+      if ((unsigned)zz >= (unsigned)nz || vv != vv) continue;
+      if (zz != key) {
+        // a zone edge inside the lane's run (rare): the finished part goes straight to the bins
+        if (cnt) bin_add<SMEM>(sb, gbins, key, cnt, sm, ~kmin, kmax);
+        key = zz;
+        cnt = 0u;
+        kmin = 0xffffffffu;
+        kmax = 0u;
+        sm = 0.0f;
       }
-      const int dn = __shfl_down_sync(0xffffffffu, key, 1);
-      const bool tail = lane == 31 || dn != key;
-      if (tail && key >= 0 && cnt > 0) bin_add<SMEM>(sb, gbins, key, cnt, sm, nmn, mx);
+      const unsigned kk = fkey(vv);
+      cnt++;
+      sm += vv;
+      kmin = min(kmin, kk);
+      kmax = max(kmax, kk);
+    }
+    // lanes are in cell order, so equal zones form runs of lanes: merge and add
+    warp_flush<SMEM>(sb, gbins, LaneAcc{key, cnt, ~kmin, kmax, sm}, lane, below);
+    __syncwarp();   // the staging area is rewritten by the next step
+    xb += kUnroll;
+    while (xb >= geo.nchunk_x) {
+      xb -= geo.nchunk_x;
+      yb++;
     }
   }
   if (SMEM) {
