@@ -436,22 +436,16 @@ def bench_zonal_stats(M, synth, torch, dev, size=16384, nzones=1024, steps=10, w
 def main():
     faulthandler.enable()
     args = parse()
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    from map_b200 import multigpu as MG
+    rank, local, world = MG.rank_info()
     if args.impl == "reference":
         run_reference(args, rank, world)
         return
 
     import numpy as np
     import torch
-    dist = None
-    if world > 1:
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    else:
-        torch.cuda.set_device(local)
+    torch.cuda.set_device(local)
+    dist = MG.init("nccl", world)
 
     from map_b200 import map as M
     from map_b200 import synth
@@ -470,8 +464,7 @@ def main():
     stream = torch.cuda.ExternalStream(M.stream(), device=dev)
 
     def barrier():
-        if dist is not None:
-            dist.barrier()
+        MG.barrier(dist)
 
     # warm-up (compiles and loads the kernel)
     for _ in range(args.warmup):
@@ -489,17 +482,14 @@ def main():
         for _ in range(args.steps):
             M.to_device(hs, out_t.data_ptr(), pitch, sync=False)
         ev1.record(stream)
-        ev1.synchronize()
+        while not ev1.query():   # poll (not a blocking wait) so the clock sampler keeps running
+            time.sleep(0.0005)
     M.sync()
     torch.cuda.synchronize()
     barrier()
     launches = M._lib.ma_totalLaunchCount() - launches0
-    ms = ev0.elapsed_time(ev1) / args.steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = cells * world / (ms * 1e-3) / 1e9
+    ms = MG.max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
+    value = MG.job_throughput(cells, world, ms) / 1e9
 
     # parity spot check on a window against the oracle (cells away from the window edge)
     parity = None
@@ -528,12 +518,8 @@ def main():
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
         M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e_value = cells * world / (e2e_ms * 1e-3) / 1e9
+    e2e_ms = MG.max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps, dist, dev)
+    e2e_value = MG.job_throughput(cells, world, e2e_ms) / 1e9
     M._lib.ma_hostFree(ct.c_void_p(h_in))
     M._lib.ma_hostFree(ct.c_void_p(h_out))
 
@@ -582,9 +568,7 @@ def main():
             except Exception as e:   # reported, not fatal: the headline line still prints
                 line[name] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
-    if dist is not None:
-        dist.barrier()
-        dist.destroy_process_group()
+    MG.finish(dist)
 
 
 if __name__ == "__main__":

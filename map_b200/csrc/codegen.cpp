@@ -105,6 +105,12 @@ struct Gen {
 
   std::string T(Node *n) const { return dt_ctype(n->meta.dtype); }
 
+  // Nodes whose value is always 0 or 1: relational and logical results.
+  static bool zero_one(const Node *p) {
+    if (p->kind == K_BINARY) return p->op >= EQ && p->op <= OR;
+    if (p->kind == K_UNARY) return p->op == NOT;
+    return false;
+  }
   std::string val(Node *p) const {
     auto m = member.find(p);
     if (m != member.end()) return "v" + std::to_string(m->second);
@@ -248,6 +254,12 @@ struct Gen {
         if (const char *sym = binary_sym(n->op)) {
           if (dt_is_float(pt) && (n->op == MOD || binary_is_bitwise(n->op)))
             throw MapError(std::string("binary op ") + binary_name(n->op) + " is not defined on floating types");
+          // a 0 / 1 mask entering float arithmetic: a select gives the value the
+          // integer-to-float conversion would, without the conversion
+          if (dt_is_float(pt)) {
+            if (!dt_is_float(n->prev[0]->meta.dtype) && zero_one(n->prev[0])) l = "(" + l + " ? (" + pts + ")1 : (" + pts + ")0)";
+            if (!dt_is_float(n->prev[1]->meta.dtype) && zero_one(n->prev[1])) r = "(" + r + " ? (" + pts + ")1 : (" + pts + ")0)";
+          }
           s << "const " << t << " " << v << " = (" << t << ")(" << l << " " << sym << " " << r << ");";
         } else {
           std::string L = "(" + pts + ")(" + l + ")", R = "(" + pts + ")(" + r + ")";
@@ -476,7 +488,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   for (int k = 0; k < nst; k++) call << ", f" << k;
   call << ", x, y, lx, ly)";
   const int rows = TH * TW / NT, rstep = NT / TW;
-  std::ostringstream loop;
+  std::ostringstream loop, loop_full;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
        << "    const int x = t.x0 + lx;\n"
        << "#pragma unroll 2\n"
@@ -484,6 +496,14 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
        << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
        << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n"
        << "    }\n";
+  // interior tiles are full: every cell of the tile is inside the raster
+  loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+            << "    const int x = t.x0 + lx;\n"
+            << "#pragma unroll 2\n"
+            << "    for (int k = 0; k < " << rows << "; ++k) {\n"
+            << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
+            << "      " << call.str() << ";\n"
+            << "    }\n";
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
        << "                                         bool gdesc) {\n"
@@ -515,7 +535,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       body << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
            << " *)(smem + " << t.smem_off << ")};\n";
     }
-    body << loop.str() << "    return true;\n  }\n";
+    body << loop_full.str() << "    return true;\n  }\n";
   }
   body << "  {\n";
   for (int k = 0; k < nst; k++) {
