@@ -487,21 +487,30 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   call << "focal_cell(a";
   for (int k = 0; k < nst; k++) call << ", f" << k;
   call << ", x, y, lx, ly)";
-  const int rows = TH * TW / NT, rstep = NT / TW;
+  // Each thread computes `rows` consecutive rows of one column, so the taps of
+  // neighbouring cells in the column are the same shared-memory words (loaded
+  // once when the loop is unrolled); a warp still covers 32 consecutive columns.
+  const int rows = TH * TW / NT;
+  bool heavy = false;   // bodies with library math functions unroll by 2 only (code size)
+  for (Node *n : G.g.nodes)
+    if ((n->kind == K_UNARY && n->op >= SIN && n->op <= CBRT) ||
+        (n->kind == K_BINARY && (n->op == ATAN2 || n->op == POW || n->op == HYPOT || n->op == FMOD)))
+      heavy = true;
+  const std::string unroll = heavy ? "#pragma unroll 2\n" : "#pragma unroll\n";
   std::ostringstream loop, loop_full;
-  loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+  loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
        << "    const int x = t.x0 + lx;\n"
-       << "#pragma unroll 2\n"
+       << unroll
        << "    for (int k = 0; k < " << rows << "; ++k) {\n"
-       << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
+       << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
        << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n"
        << "    }\n";
   // interior tiles are full: every cell of the tile is inside the raster
-  loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+  loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
             << "    const int x = t.x0 + lx;\n"
-            << "#pragma unroll 2\n"
+            << unroll
             << "    for (int k = 0; k < " << rows << "; ++k) {\n"
-            << "      const int ly = ly0 + k * " << rstep << ", y = t.y0 + ly;\n"
+            << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
             << "      " << call.str() << ";\n"
             << "    }\n";
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
