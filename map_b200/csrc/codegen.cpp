@@ -724,8 +724,62 @@ static std::string gen_spread(Gen &G) {
   s << "    return (" << T << ")(" << G.val(scan->prev[0]) << ");\n}\n";
   const int kd = G.rin.at(scan->prev[1]);
   const int ko = G.outk.at(scan);
-  // aux[0] in-degree (s32[N]), aux[1] frontier A (s32[N]), aux[2] frontier B, aux[3] round limit
-  s << "__device__ __forceinline__ void spread_run(const Args &a) {\n"
+  // aux[0] in-degree (s32[N]); aux[3] step limit of one downstream walk.
+  // Large rasters: two grid-wide passes (kernels KNAME_init then KNAME), each CTA
+  // striding over the cells from `first` by `step`:
+  //  * init: zero the accumulation and count each cell's upstream neighbours
+  //    (cells nothing flows into are marked as sources);
+  //  * walk: from every source, a thread carries (accumulation + water) down the
+  //    flow path, adding it to the next cell; it goes on into that cell only if
+  //    its push was the cell's last pending one (the cell is then complete),
+  //    else it stops. Every cell is completed once, by exactly one thread, after
+  //    all of its upstream pushes (fences order each push before its count).
+  s << "#define SPREAD_SOURCE 0x40000000\n"
+    << "__device__ __forceinline__ void spread_init(const Args &a, s64 first, s64 step) {\n"
+    << "  const int W = a.g.W, H = a.g.H;\n"
+    << "  const s64 N = (s64)W * H;\n"
+    << "  s32 *indeg = (s32 *)a.aux[0];\n"
+    << "  const RasterArg D = a.in[" << kd << "];\n"
+    << "  const RasterArg O = a.out[" << ko << "];\n"
+    << "  for (s64 c = first; c < N; c += step) {\n"
+    << "    const int x = (int)(c % W), y = (int)(c / W);\n"
+    << "    *cell_ptr<" << T << ">(O, x, y) = (" << T << ")0;\n"
+    << "    int cnt = 0;\n"
+    << "    for (int d = 0; d < 8; ++d) {\n"
+    << "      const int nx = x - d8_dx(d), ny = y - d8_dy(d);\n"
+    << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+    << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) cnt++;\n"
+    << "    }\n"
+    << "    indeg[c] = cnt ? cnt : SPREAD_SOURCE;\n"
+    << "  }\n"
+    << "}\n"
+    << "__device__ __forceinline__ void spread_walk(const Args &a, s64 first, s64 step) {\n"
+    << "  const int W = a.g.W, H = a.g.H;\n"
+    << "  const s64 N = (s64)W * H;\n"
+    << "  s32 *indeg = (s32 *)a.aux[0];\n"
+    << "  const long long limit = (long long)a.aux[3];\n"
+    << "  const RasterArg D = a.in[" << kd << "];\n"
+    << "  const RasterArg O = a.out[" << ko << "];\n"
+    << "  for (s64 c = first; c < N; c += step) {\n"
+    << "    if (indeg[c] != SPREAD_SOURCE) continue;\n"
+    << "    int x = (int)(c % W), y = (int)(c / W);\n"
+    << "    " << T << " carry = water_at(a, x, y);\n"
+    << "    for (long long it = 0;; ++it) {\n"
+    << "      if (it > limit) { skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
+    << "      const s64 dn = d8_down(D, W, H, x, y);\n"
+    << "      if (dn < 0) break;\n"
+    << "      const int dx = (int)(dn % W), dy = (int)(dn / W);\n"
+    << "      atomic_add_any(cell_ptr<" << T << ">(O, dx, dy), carry);\n"
+    << "      if (atomic_dec_acq_rel(&indeg[dn]) != 1) break;   // orders the push before the count\n"
+    << "      x = dx;\n"
+    << "      y = dy;\n"
+    << "      carry = (" << T << ")(ld_coherent<" << T << ">(O, x, y) + water_at(a, x, y));\n"
+    << "    }\n"
+    << "  }\n"
+    << "}\n";
+  // Small rasters: one CTA runs a topological (Kahn) sweep, frontier by frontier
+  // with block barriers (aux[1], aux[2]: frontier lists of N cells).
+  s << "__device__ __forceinline__ void spread_kahn(const Args &a) {\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  const s64 N = (s64)W * H;\n"
     << "  s32 *indeg = (s32 *)a.aux[0];\n"
@@ -767,14 +821,32 @@ static std::string gen_spread(Gen &G) {
     << "    s32 *t = fa; fa = fb; fb = t;\n"
     << "    __syncthreads();\n"
     << "  }\n"
-    << "}\n";
-  s << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME(const __grid_constant__ Args a) {\n"
-    << "  spread_run(a);\n"
     << "}\n"
-    << "struct ManyArgs { u64 args; s64 n; };\n"
-    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_many(const __grid_constant__ ManyArgs m) {\n"
+    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn(const __grid_constant__ Args a) {\n"
+    << "  spread_kahn(a);\n"
+    << "}\n"
+    << "struct KahnManyArgs { u64 args; s64 n; };\n"
+    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn_many(const __grid_constant__ KahnManyArgs m) {\n"
     << "  if ((s64)blockIdx.x >= m.n) return;\n"
-    << "  spread_run(((const Args *)m.args)[blockIdx.x]);\n"
+    << "  spread_kahn(((const Args *)m.args)[blockIdx.x]);\n"
+    << "}\n";
+  s << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init(const __grid_constant__ Args a) {\n"
+    << "  spread_init(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
+    << "}\n"
+    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ Args a) {\n"
+    << "  spread_walk(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
+    << "}\n"
+    // many rasters in one launch: blockIdx.y selects the raster, blockIdx.x strides over its cells
+    << "struct ManyArgs { u64 args; s64 n; };\n"
+    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  if ((s64)blockIdx.y >= m.n) return;\n"
+    << "  spread_init(((const Args *)m.args)[blockIdx.y], (s64)blockIdx.x * blockDim.x + threadIdx.x,\n"
+    << "              (s64)gridDim.x * blockDim.x);\n"
+    << "}\n"
+    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  if ((s64)blockIdx.y >= m.n) return;\n"
+    << "  spread_walk(((const Args *)m.args)[blockIdx.y], (s64)blockIdx.x * blockDim.x + threadIdx.x,\n"
+    << "              (s64)gridDim.x * blockDim.x);\n"
     << "}\n";
   return s.str();
 }

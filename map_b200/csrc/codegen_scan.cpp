@@ -14,12 +14,14 @@
 // Spreading (runtime/skeleton/SpreadingSkeleton.cpp:288-393): the reference
 // relaxes "pending spread" one neighbour per iteration, block by block, until
 // stable; the fixed point is, for every cell, the sum of the water of all
-// strictly-upstream cells. Here the same fixed point is reached by a
-// topological (Kahn) sweep on the device: in-degrees are counted by pulling
-// from the 8 neighbours, cells with no pending upstream form the frontier, and
-// each frontier cell pushes (its accumulation + its water) to its downstream
-// cell with an atomic add; a cell joins the next frontier when its last
-// upstream neighbour has pushed. Integer sums are exact and order-independent.
+// strictly-upstream cells. Here the same fixed point is reached without
+// iterating to convergence. In-degrees are counted by pulling from the 8
+// neighbours; then either one CTA sweeps frontier by frontier (topological
+// order; rasters up to 64 K cells) or, for larger rasters, a thread per source
+// walks down its flow path pushing (accumulation + water) with atomic adds and
+// continues into a cell only when its push was the cell's last pending one, so
+// each cell is completed exactly once after all its upstream cells. Integer
+// sums are exact and order-independent.
 #include "codegen.hpp"
 #include "cuda_env.hpp"
 #include "executor.hpp"
@@ -27,11 +29,18 @@
 #include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <functional>
 #include <unordered_map>
 
 namespace mapb {
+
+// Flow accumulations of at most this many cells run as one CTA's frontier sweep;
+// larger ones as the two grid-wide passes (in-degrees, then downstream walks),
+// which spread over every SM (measured at 1024²: 1.7 ms against 5.6 ms for one
+// CTA). Serving runs one CTA per window instead, many windows side by side.
+constexpr size_t kSpreadKahnCells = (size_t)1 << 16;
 
 void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node *, DevRaster> &bufs,
                     const std::function<DevRaster &(Node *)> &get, const std::function<DevRaster(Node *)> &alloc_out) {
@@ -66,7 +75,15 @@ void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node
   uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
                      (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
   auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
-  env.launch(kh, 1, 1024, 0, (CUstream_st *)st, a.data(), a.size());
+  if (N <= kSpreadKahnCells) {
+    // one CTA, frontier by frontier: the lowest latency for rasters of a few million cells
+    env.launch(env.kernel(P.source, P.kname + "_kahn", 0), 1, 1024, 0, (CUstream_st *)st, a.data(), a.size());
+  } else {
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((N + 255) / 256, (size_t)env.sm_count() * 8));
+    KernelHandle ki = env.kernel(P.source, P.kname + "_init", 0);
+    env.launch(ki, grid, 256, 0, (CUstream_st *)st, a.data(), a.size());
+    env.launch(kh, grid, 256, 0, (CUstream_st *)st, a.data(), a.size());
+  }
   cuda_check(cudaFreeAsync(work, st), "cudaFreeAsync");
 }
 

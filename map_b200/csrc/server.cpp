@@ -210,7 +210,7 @@ Template &Server::Impl::template_for(int type, int w, int h, float obs_h, bool c
       env.kernel(P.source, P.kname + "_many", 0);
       T->last_phase = std::max(T->last_phase, (int)PH_RADIAL);
     } else if (g.skeleton == SK_SPREAD) {
-      env.kernel(P.source, P.kname + "_many", 0);
+      env.kernel(P.source, P.kname + "_kahn_many", 0);
       T->last_phase = std::max(T->last_phase, (int)PH_SPREAD);
     } else {
       throw MapError("serving: zonal groups are not served");
@@ -240,7 +240,12 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   std::vector<int> kind_members;
   struct Item { uint32_t kind, inst, tile, pad; };
   std::vector<std::vector<Item>> levels(2);
-  struct Many { const KernelPlan *plan = nullptr; std::vector<unsigned char> args; int n = 0; };
+  struct Many {
+    const KernelPlan *plan = nullptr;
+    std::vector<unsigned char> args;
+    int n = 0;
+    long long max_cells = 0;
+  };
   std::map<std::string, Many> radial, spread;
   std::vector<Req *> ok;
   std::vector<int> phase_of;
@@ -340,6 +345,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
+          mn.max_cells = std::max<long long>(mn.max_cells, (long long)N);
         }
       }
       ok.push_back(r);
@@ -431,7 +437,8 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     cuda_check(cudaStreamWaitEvent(sp, ev[PH_LEVEL1], 0), "cudaStreamWaitEvent");
     for (auto &kv : spread) {
       Many &mn = kv.second;
-      KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_many", 0);
+      // one CTA per window: the frontier sweep has the lowest latency at window sizes
+      KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_kahn_many", 0);
       struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
       env.launch(kh, mn.n, 1024, 0, (CUstream_st *)sp, &ma, sizeof ma);
     }

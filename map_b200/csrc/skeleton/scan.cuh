@@ -45,6 +45,14 @@ template <class T> __device__ __forceinline__ T ld_coherent(const RasterArg &r, 
 template <class T> __device__ __forceinline__ T *cell_ptr(const RasterArg &r, int x, int y) {
   return (T *)(r.p + (u64)(s64)y * (u64)r.pitch) + x;
 }
+// Decrements *p with acquire-release ordering at device scope (the caller's earlier
+// writes are visible to whoever sees the result, and later reads see theirs);
+// returns the previous value.
+__device__ __forceinline__ s32 atomic_dec_acq_rel(s32 *p) {
+  s32 old;
+  asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], -1;" : "=r"(old) : "l"(p) : "memory");
+  return old;
+}
 __device__ __forceinline__ void atomic_add_any(s32 *p, s32 v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_any(u32 *p, u32 v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add_any(float *p, float v) { atomicAdd(p, v); }

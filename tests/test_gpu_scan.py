@@ -90,3 +90,27 @@ def test_flow_accumulation_known_answer(M):
     assert (dirs[:, :-1] == 1).all() and (dirs[:, -1] == 0).all()
     acc = M.to_numpy(M.flow_accumulation(M.ones_like(dem, M.S32), M.from_numpy(dirs)))
     assert np.array_equal(acc, np.tile(np.arange(40, dtype=np.int32), (10, 1)))
+
+
+def test_flow_accumulation_large_raster_walks_bit_exact(M):
+    # a large raster: the grid-wide in-degree pass and downstream walks
+    shape = (2100, 2100)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=21)
+    dem = M.from_numpy(dem_np, bs=[512, 512])
+    dirs = M.flow_direction(dem)
+    got = M.to_numpy(M.flow_accumulation(M.ones_like(dem, M.S32), dirs))
+    ref, cyclic = O.flowacc_s32(np.ones(shape, np.int32), M.to_numpy(dirs))
+    assert not cyclic
+    assert np.array_equal(got, ref)
+
+
+def test_flow_accumulation_large_raster_float_water(M):
+    # float water on the walk path: sums of exactly representable values stay exact
+    shape = (2100, 2050)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=22)
+    dem = M.from_numpy(dem_np, bs=[512, 512])
+    dirs = M.flow_direction(dem)
+    water = np.full(shape, 0.5, np.float32)
+    got = M.to_numpy(M.flow_accumulation(M.from_numpy(water, bs=[512, 512]), dirs))
+    ref, _ = O.flowacc_s32(np.ones(shape, np.int32), M.to_numpy(dirs))
+    assert np.array_equal(got, ref.astype(np.float32) * np.float32(0.5))
