@@ -825,8 +825,9 @@ static std::string gen_spread(Gen &G) {
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn(const __grid_constant__ Args a) {\n"
     << "  spread_kahn(a);\n"
     << "}\n"
-    << "struct KahnManyArgs { u64 args; s64 n; };\n"
-    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn_many(const __grid_constant__ KahnManyArgs m) {\n"
+    // many rasters in one launch (serving windows): one CTA each
+    << "struct ManyArgs { u64 args; s64 n; };\n"
+    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn_many(const __grid_constant__ ManyArgs m) {\n"
     << "  if ((s64)blockIdx.x >= m.n) return;\n"
     << "  spread_kahn(((const Args *)m.args)[blockIdx.x]);\n"
     << "}\n";
@@ -835,18 +836,6 @@ static std::string gen_spread(Gen &G) {
     << "}\n"
     << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ Args a) {\n"
     << "  spread_walk(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
-    << "}\n"
-    // many rasters in one launch: blockIdx.y selects the raster, blockIdx.x strides over its cells
-    << "struct ManyArgs { u64 args; s64 n; };\n"
-    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init_many(const __grid_constant__ ManyArgs m) {\n"
-    << "  if ((s64)blockIdx.y >= m.n) return;\n"
-    << "  spread_init(((const Args *)m.args)[blockIdx.y], (s64)blockIdx.x * blockDim.x + threadIdx.x,\n"
-    << "              (s64)gridDim.x * blockDim.x);\n"
-    << "}\n"
-    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_many(const __grid_constant__ ManyArgs m) {\n"
-    << "  if ((s64)blockIdx.y >= m.n) return;\n"
-    << "  spread_walk(((const Args *)m.args)[blockIdx.y], (s64)blockIdx.x * blockDim.x + threadIdx.x,\n"
-    << "              (s64)gridDim.x * blockDim.x);\n"
     << "}\n";
   return s.str();
 }

@@ -238,16 +238,6 @@ void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CU
   launches_++;
 }
 
-void CudaEnv::launch_grid(const KernelHandle &k, int grid_x, int grid_y, int block, size_t smem, CUstream_st *stream,
-                          void *args, size_t) {
-  if (grid_x <= 0 || grid_y <= 0) return;
-  void *params[] = {args};
-  drv_check(g_drv.launchKernel(reinterpret_cast<CUfunction>(k.fn), (unsigned)grid_x, (unsigned)grid_y, 1, (unsigned)block, 1,
-                               1, (unsigned)smem, reinterpret_cast<CUstream>(stream), params, nullptr),
-            "cuLaunchKernel");
-  launches_++;
-}
-
 int CudaEnv::occupancy(const KernelHandle &k, int block, size_t smem) {
   int n = 0;
   drv_check(g_drv.occupancy(&n, reinterpret_cast<CUfunction>(k.fn), block, smem), "cuOccupancyMaxActiveBlocksPerMultiprocessor");

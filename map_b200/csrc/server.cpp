@@ -244,7 +244,6 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     const KernelPlan *plan = nullptr;
     std::vector<unsigned char> args;
     int n = 0;
-    long long max_cells = 0;
   };
   std::map<std::string, Many> radial, spread;
   std::vector<Req *> ok;
@@ -345,7 +344,6 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
-          mn.max_cells = std::max<long long>(mn.max_cells, (long long)N);
         }
       }
       ok.push_back(r);
