@@ -641,7 +641,7 @@ static std::string gen_radial(Gen &G) {
   const std::string nt = var_literal(reduction_neutral(scan->op, scan->meta.dtype));
   std::ostringstream s;
   s << "#include \"map_scan.cuh\"\n" << G.args_struct(0, false);
-  s << "__device__ __forceinline__ void radial_cell(const Args &a, int x, int y, " << T << " lit, bool observer) {\n"
+  s << "__device__ __forceinline__ " << T << " radial_cell(const Args &a, int x, int y, " << T << " lit, bool observer) {\n"
     << G.center_loads(false);
   for (Node *n : G.g.nodes) {
     if (n == scan) {
@@ -653,32 +653,51 @@ static std::string gen_radial(Gen &G) {
       s << "    " << G.stmt(n, false) << "\n";
     }
   }
-  s << G.stores() << "}\n";
+  s << G.stores() << "    return " << v << ";\n}\n";
   int ri = G.outk.at(scan);
-  // aux[0] start x, aux[1] start y, aux[2] last front (or -1 for all)
+  // aux[0] start x, aux[1] start y, aux[2] last front (or -1 for all).
+  // The previous front lives in shared memory (two buffers of the launch's
+  // dynamic size / 2) when it fits, else it is re-read from the scan's output.
   s << "__device__ __forceinline__ void radial_run(const Args &a, int octant) {\n"
+    << "  extern __shared__ __align__(16) unsigned char radial_smem[];\n"
     << "  const int sx = (int)a.aux[0], sy = (int)a.aux[1];\n"
     << "  const long long lim = (long long)a.aux[2];\n"
     << "  const RasterArg R = a.out[" << ri << "];\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  int p0, p1, q0, q1;\n"
     << "  octant_units(octant, p0, p1, q0, q1);\n"
-    << "  if (threadIdx.x == 0) radial_cell(a, sx, sy, (" << T << ")0, true);\n"
     << "  const int ep = p0 > 0 ? W - 1 - sx : p0 < 0 ? sx : p1 > 0 ? H - 1 - sy : sy;\n"
     << "  const int eq = q0 > 0 ? W - 1 - sx : q0 < 0 ? sx : q1 > 0 ? H - 1 - sy : sy;\n"
     << "  const int dmax = (lim >= 0 && lim < ep) ? (int)lim : ep;\n"
+    << "  u32 dyn;\n"
+    << "  asm(\"mov.u32 %0, %%dynamic_smem_size;\" : \"=r\"(dyn));\n"
+    << "  const int cap = (int)(dyn / (2 * sizeof(" << T << ")));\n"
+    << "  " << T << " *prev = cap > eq ? (" << T << " *)radial_smem : nullptr;\n"
+    << "  " << T << " *cur = prev ? prev + cap : nullptr;\n"
+    << "  if (threadIdx.x == 0) {\n"
+    << "    const " << T << " v0 = radial_cell(a, sx, sy, (" << T << ")0, true);\n"
+    << "    if (prev) prev[0] = v0;\n"
+    << "  }\n"
     << "  __syncthreads();\n"
     << "  for (int d0 = 1; d0 <= dmax; ++d0) {\n"
     << "    const int d1max = d0 < eq ? d0 : eq;\n"
     << "    for (int d1 = threadIdx.x; d1 <= d1max; d1 += blockDim.x) {\n"
     << "      const int x = sx + p0 * d0 + q0 * d1, y = sy + p1 * d0 + q1 * d1;\n"
-    << "      const " << T << " va = (d1 <= d0 - 1) ? ld_coherent<" << T
-    << ">(R, sx + p0 * (d0 - 1) + q0 * d1, sy + p1 * (d0 - 1) + q1 * d1) : (" << T << ")0;\n"
-    << "      const " << T << " vb = (d1 >= 1) ? ld_coherent<" << T
-    << ">(R, sx + p0 * (d0 - 1) + q0 * (d1 - 1), sy + p1 * (d0 - 1) + q1 * (d1 - 1)) : (" << T << ")0;\n"
-    << "      radial_cell(a, x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
+    << "      " << T << " va = (" << T << ")0, vb = (" << T << ")0;\n"
+    << "      if (prev) {\n"
+    << "        if (d1 <= d0 - 1) va = prev[d1];\n"
+    << "        if (d1 >= 1) vb = prev[d1 - 1];\n"
+    << "      } else {\n"
+    << "        if (d1 <= d0 - 1) va = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * d1, sy + p1 * (d0 - 1) + q1 * d1);\n"
+    << "        if (d1 >= 1) vb = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * (d1 - 1), sy + p1 * (d0 - 1) + q1 * (d1 - 1));\n"
+    << "      }\n"
+    << "      const " << T << " vv = radial_cell(a, x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
+    << "      if (cur) cur[d1] = vv;\n"
     << "    }\n"
     << "    __syncthreads();\n"
+    << "    " << T << " *t = prev;\n"
+    << "    prev = cur;\n"
+    << "    cur = t;\n"
     << "  }\n"
     << "}\n";
   // one scan: 8 CTAs (one per octant); many scans: 8 CTAs per Args of a device array
@@ -696,13 +715,8 @@ static std::string gen_radial(Gen &G) {
 // Spreading skeleton (runtime/skeleton/SpreadingSkeleton.cpp:288-393). The
 // reference relaxes pending spread one neighbour per iteration, block by block,
 // until stable; the fixed point is, for every cell, the sum of the water of all
-// strictly-upstream cells. The same fixed point is reached here by a topological
-// (Kahn) sweep inside one CTA: in-degrees are counted by pulling from the 8
-// neighbours, cells with no pending upstream form the frontier, and each
-// frontier cell pushes (its accumulation + its water) to its downstream cell
-// with an atomic add; a cell joins the next frontier when its last upstream
-// neighbour has pushed. The sweep ends when the frontier is empty or after N+1
-// rounds (error flag). Integer sums are exact and independent of order.
+// strictly-upstream cells. It is reached here without iterating to convergence
+// (see the passes below; codegen_scan.cpp picks the form by raster size).
 static std::string gen_spread(Gen &G) {
   KernelPlan &P = G.plan;
   Node *scan = P.core;

@@ -58,6 +58,10 @@ struct KernelPlan {
 
 KernelPlan generate_kernel(const Group &g, TileCfg cfg = TileCfg());
 
+// Dynamic shared memory of a radial scan launch over a W x H raster: two front
+// buffers when they fit (0 otherwise: the kernel then re-reads fronts from its output).
+size_t radial_front_smem(int W, int H, int dtype);
+
 // Reference float-constant rounding: constants written into kernel text by the
 // reference go through std::to_string ("%f", six decimals) before the device
 // compiler parses them (util/VariantType.cpp:89-104, runtime/skeleton/util.cpp mask_decl).

@@ -42,6 +42,11 @@ namespace mapb {
 // CTA). Serving runs one CTA per window instead, many windows side by side.
 constexpr size_t kSpreadKahnCells = (size_t)1 << 16;
 
+size_t radial_front_smem(int W, int H, int dtype) {
+  const size_t b = 2 * (size_t)std::max(W, H) * dt_size(dtype);   // previous and current front
+  return b <= (size_t)200 * 1024 ? b : 0;                          // larger: fronts re-read from the output
+}
+
 void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node *, DevRaster> &bufs,
                     const std::function<DevRaster &(Node *)> &get, const std::function<DevRaster(Node *)> &alloc_out) {
   CudaEnv &env = CudaEnv::get();
@@ -65,7 +70,8 @@ void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node
     }
     uint64_t aux[4] = {(uint64_t)scan->coord.arr[0], (uint64_t)scan->coord.arr[1], (uint64_t)lim, (uint64_t)ri};
     auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
-    env.launch(kh, 8, 512, 0, (CUstream_st *)st, a.data(), a.size());
+    const size_t smem = radial_front_smem(g.W, g.H, scan->meta.dtype);
+    env.launch(env.kernel(P.source, P.kname, smem), 8, 512, smem, (CUstream_st *)st, a.data(), a.size());
     return;
   }
   const size_t N = (size_t)g.W * g.H;

@@ -244,6 +244,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     const KernelPlan *plan = nullptr;
     std::vector<unsigned char> args;
     int n = 0;
+    int max_dim = 0;   // largest window side (radial front buffers)
   };
   std::map<std::string, Many> radial, spread;
   std::vector<Req *> ok;
@@ -332,6 +333,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
+          mn.max_dim = std::max(mn.max_dim, std::max(g.W, g.H));
         } else {   // SK_SPREAD
           Many &mn = spread[P.source];
           mn.plan = &P;
@@ -424,9 +426,10 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   cuda_check(cudaEventRecord(ev[PH_LEVEL0], st), "cudaEventRecord");
   for (auto &kv : radial) {
     Many &mn = kv.second;
-    KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_many", 0);
+    const size_t smem = radial_front_smem(mn.max_dim, mn.max_dim, mn.plan->core->meta.dtype);
+    KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_many", smem);
     struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
-    env.launch(kh, 8 * mn.n, 512, 0, (CUstream_st *)st, &ma, sizeof ma);
+    env.launch(kh, 8 * mn.n, 512, smem, (CUstream_st *)st, &ma, sizeof ma);
   }
   cuda_check(cudaEventRecord(ev[PH_RADIAL], st), "cudaEventRecord");
   launch_level(1);
