@@ -298,7 +298,7 @@ def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
     return {"rasters": n_rasters, "cells": cells, "value": round(cells / (batch_ms * 1e-3) / 1e9, 3),
             "plain_value": round(cells / (plain_ms * 1e-3) / 1e9, 3), "unit": "Gcells/s",
             "speedup_vs_plain": round(plain_ms / batch_ms, 2), "ms_per_step": round(batch_ms, 3),
-            "plain_ms": round(plain_ms, 3), "plain_launches": plain_launches, "batched_launches_per_step": info["phases"],
+            "plain_ms": round(plain_ms, 3), "plain_launches": plain_launches, "batched_launches_per_step": info["launches"],
             "prepare_s": round(prep_s, 2), "kinds": info["kinds"], "plain_equals_batched": same,
             "programs": "fused hillshade + 6-layer weighted overlay per raster"}
 

@@ -73,11 +73,18 @@ std::string tune_key(const Group &g, const KernelPlan &p) {
   return k.str();
 }
 
-TileCfg autotune_group(const Group &g, const std::function<DevRaster &(Node *)> &get,
-                       std::unordered_map<Node *, DevRaster> &bufs) {
-  KernelPlan base = generate_kernel(g);
-  if (g.skeleton != SK_LOCAL && g.skeleton != SK_FOCAL) return TileCfg();
-  const std::string key = tune_key(g, base);
+// Tile shape of a kind chosen in the form it runs: for each candidate shape, one
+// persistent launch over the tiles of all the kind's members, timed with events;
+// the winner is cached per (skeleton, halo, dtypes, largest member's shape bucket,
+// body). Candidates that do not fit the persistent module's 256 threads are skipped.
+TileCfg autotune_kind(const std::vector<const Group *> &members, const std::function<DevRaster &(Node *)> &get,
+                      std::unordered_map<Node *, DevRaster> &bufs) {
+  const Group *big = members[0];
+  for (const Group *g : members)
+    if ((long long)g->W * g->H > (long long)big->W * big->H) big = g;
+  if (big->skeleton != SK_LOCAL && big->skeleton != SK_FOCAL) return TileCfg();
+  KernelPlan base = generate_kernel(*big);
+  const std::string key = tune_key(*big, base) + "/m" + std::to_string(members.size());
   {
     std::lock_guard<std::mutex> lk(g_tune_mtx);
     tune_load();
@@ -98,19 +105,58 @@ TileCfg autotune_group(const Group &g, const std::function<DevRaster &(Node *)> 
     cfg.th = c[1];
     cfg.nt = 256;
     if (!tile_cfg_valid(cfg)) continue;
-    KernelPlan P = generate_kernel(g, cfg);
-    KernelHandle kh = env.kernel(P.source, P.kname, P.smem_bytes);
-    uint64_t aux[4] = {0, 0, 0, 0};
-    auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
-    const int tiles = ((g.W + cfg.tw - 1) / cfg.tw) * ((g.H + cfg.th - 1) / cfg.th);
-    env.launch(kh, tiles, cfg.nt, P.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+    KernelPlan P0 = generate_kernel(*big, cfg);
+    std::vector<unsigned char> args;
+    std::vector<uint32_t> items;   // (kind 0, member, tile, pad)
+    uint32_t mi = 0;
+    for (const Group *g : members) {
+      KernelPlan P = generate_kernel(*g, cfg);
+      uint64_t aux[4] = {0, 0, 0, 0};
+      auto a = pack_args(*g, P, get, bufs, 0, 0, g->W, g->H, aux);
+      args.insert(args.end(), a.begin(), a.end());
+      const int tiles = ((g->W + cfg.tw - 1) / cfg.tw) * ((g->H + cfg.th - 1) / cfg.th);
+      for (int t = 0; t < tiles; t++) {
+        items.push_back(0u);
+        items.push_back(mi);
+        items.push_back((uint32_t)t);
+        items.push_back(0u);
+      }
+      mi++;
+    }
+    PersistentModule pm = build_persistent_module({&P0});
+    KernelHandle kh = env.kernel(pm.source, pm.kname, pm.smem);
+    const int grid = env.sm_count() * std::max(1, env.occupancy(kh, 256, pm.smem));
+    void *d = nullptr;
+    const size_t nitem = items.size() / 4;
+    const size_t bytes = 256 + args.size() + items.size() * 4;
+    cuda_check(cudaMallocAsync(&d, bytes, st), "cudaMallocAsync(tuning)");
+    char *dargs = (char *)d + 256, *ditems = dargs + args.size();
+    cuda_check(cudaMemcpyAsync(dargs, args.data(), args.size(), cudaMemcpyHostToDevice, st), "upload");
+    cuda_check(cudaMemcpyAsync(ditems, items.data(), items.size() * 4, cudaMemcpyHostToDevice, st), "upload");
+    struct {
+      uint64_t items;
+      int64_t n;
+      uint64_t counter;
+      uint64_t err;
+      uint64_t args[1];
+    } ba{(uint64_t)(uintptr_t)ditems, (int64_t)nitem, (uint64_t)(uintptr_t)d, (uint64_t)(uintptr_t)env.err_word(),
+         {(uint64_t)(uintptr_t)dargs}};
+    auto run = [&]() {
+      cuda_check(cudaMemsetAsync(d, 0, 4, st), "cudaMemsetAsync");
+      env.launch(kh, std::min<int>(grid, (int)nitem), 256, pm.smem, (CUstream_st *)st, &ba, sizeof ba);
+    };
+    run();
     cuda_check(cudaEventRecord(e0, st), "cudaEventRecord");
-    for (int r = 0; r < 3; r++) env.launch(kh, tiles, cfg.nt, P.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+    for (int r = 0; r < 3; r++) run();
     cuda_check(cudaEventRecord(e1, st), "cudaEventRecord");
     cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize");
     float ms = 0;
     cuda_check(cudaEventElapsedTime(&ms, e0, e1), "cudaEventElapsedTime");
-    if (ms < best_ms) { best_ms = ms; best = cfg; }
+    cuda_check(cudaFreeAsync(d, st), "cudaFreeAsync");
+    if (ms < best_ms) {
+      best_ms = ms;
+      best = cfg;
+    }
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -136,18 +182,17 @@ PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &
       << "struct BatchArgs { u64 items; s64 n; u64 counter; u64 err; u64 args[" << kinds.size() << "]; };\n"
       << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ BatchArgs b) {\n"
       << "  extern __shared__ __align__(128) unsigned char smem[];\n"
-      << "  __shared__ int item_s;\n"
+      << "  __shared__ int item_s[2];\n"
       << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
-      << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
+      << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); item_s[0] = atomicAdd((int *)b.counter, 1); }\n"
       << "  __syncthreads();\n"
       << "  u32 phase = 0;\n"
       << "  const BItem *items = (const BItem *)b.items;\n"
-      << "  for (;;) {\n"
-      << "    if (threadIdx.x == 0) item_s = atomicAdd((int *)b.counter, 1);\n"
-      << "    __syncthreads();\n"
-      << "    const int i = item_s;\n"
-      << "    __syncthreads();\n"
+      // the next item's index is claimed while the current tile runs (its atomic's latency is hidden)
+      << "  for (int slot = 0;; slot ^= 1) {\n"
+      << "    const int i = item_s[slot];\n"
       << "    if (i >= b.n) break;\n"
+      << "    if (threadIdx.x == 0) item_s[slot ^ 1] = atomicAdd((int *)b.counter, 1);\n"
       << "    const BItem w = items[i];\n"
       << "    bool ok = true;\n"
       << "    switch (w.kind) {\n";
@@ -156,7 +201,9 @@ PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &
         << "])[w.inst], (int)w.tile, smem, bar, phase, true); break;\n";
   src << "      default: skel_fail((u32 *)b.err, ERR_BAD_LAUNCH); ok = false;\n"
       << "    }\n"
-      << "    if (!ok) break;\n"
+      // a barrier that also makes the stop decision uniform: the claimed index is
+      // visible afterwards, and this slot may be rewritten
+      << "    if (__syncthreads_or(!ok)) break;\n"
       << "  }\n"
       << "}\n";
   pm.source = src.str();
@@ -176,6 +223,11 @@ struct Batch::Kind {
   std::vector<unsigned char> args;   // one Args struct per member, back to back
   int members = 0;
   void *d_args = nullptr;
+  // the kind's own persistent module: its register and shared-memory needs alone
+  // set its occupancy
+  PersistentModule pm;
+  KernelHandle kh;
+  int grid = 0;
 };
 
 struct Batch::Impl {
@@ -187,10 +239,12 @@ struct Batch::Impl {
   std::vector<std::vector<Item>> phases;
   void *d_items = nullptr;
   void *d_counter = nullptr;
-  std::string source, kname;
-  KernelHandle kh;
-  size_t smem = 0;
-  int grid = 0;
+  // per dependency level, the contiguous item ranges of one kind (one launch each)
+  struct Segment { int kind; size_t off, n; };
+  std::vector<std::vector<Segment>> segments;
+  std::vector<cudaStream_t> branch;   // streams the kinds of one level fork onto while capturing
+  std::vector<cudaEvent_t> fork_ev;
+  int launches = 0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   long long cells = 0;
@@ -207,6 +261,8 @@ Batch::~Batch() {
   for (auto &k : impl_->kinds)
     if (k.d_args) cudaFree(k.d_args);
   if (impl_->d_items) cudaFree(impl_->d_items);
+  for (cudaStream_t b : impl_->branch) cudaStreamDestroy(b);
+  for (cudaEvent_t e : impl_->fork_ev) cudaEventDestroy(e);
   if (impl_->d_counter) cudaFree(impl_->d_counter);
   for (void *p : impl_->owned) cudaFree(p);
 }
@@ -322,9 +378,12 @@ void Batch::prepare(bool autotune) {
   }
   cuda_check(cudaStreamSynchronize(st), "stream synchronize");
 
-  // tile shapes: tuned on each kind's largest member
-  for (auto &kd : I.kinds) {
-    kd.cfg = autotune ? autotune_group(*kd.proto, get, bufs) : TileCfg();
+  // tile shapes: tuned per kind over all its members, in the persistent form
+  std::vector<std::vector<const Group *>> kind_members(I.kinds.size());
+  for (auto &m : members) kind_members[m.kind].push_back(m.g);
+  for (size_t k = 0; k < I.kinds.size(); k++) {
+    Kind &kd = I.kinds[k];
+    kd.cfg = autotune ? autotune_kind(kind_members[k], get, bufs) : TileCfg();
     kd.plan = generate_kernel(*kd.proto, kd.cfg);
     if (kd.cfg.nt != 256) throw MapError("batch: tile configurations must use 256 threads");
   }
@@ -348,56 +407,89 @@ void Batch::prepare(bool autotune) {
     I.tiles += tiles;
   }
 
-  // batch module: every kind's tile function in its own namespace + a persistent dispatcher
-  std::vector<const KernelPlan *> kp;
-  for (auto &kd : I.kinds) kp.push_back(&kd.plan);
-  PersistentModule pm = build_persistent_module(kp);
-  I.source = pm.source;
-  I.kname = pm.kname;
-  I.smem = pm.smem;
-  I.kh = env.kernel(I.source, I.kname, I.smem);
-  int occ = std::max(1, env.occupancy(I.kh, 256, I.smem));
-  I.grid = env.sm_count() * occ;
+  // items of one level are independent: run them kind by kind, so the CTAs of an
+  // SM mostly execute one tile function at a time (instruction-cache locality)
+  for (auto &p : I.phases)
+    std::stable_sort(p.begin(), p.end(), [](const Impl::Item &x, const Impl::Item &y) { return x.kind < y.kind; });
+
+  // one persistent module per kind; a level's items are contiguous per kind
+  for (auto &kd : I.kinds) {
+    kd.pm = build_persistent_module({&kd.plan});
+    kd.kh = env.kernel(kd.pm.source, kd.pm.kname, kd.pm.smem);
+    kd.grid = env.sm_count() * std::max(1, env.occupancy(kd.kh, 256, kd.pm.smem));
+  }
+  std::vector<Impl::Item> all;
+  I.segments.assign(nphase, {});
+  size_t nseg = 0;
+  for (int ph = 0; ph < nphase; ph++) {
+    const auto &p = I.phases[ph];
+    for (size_t a = 0; a < p.size();) {
+      size_t b = a;
+      while (b < p.size() && p[b].kind == p[a].kind) b++;
+      I.segments[ph].push_back(Impl::Segment{(int)p[a].kind, all.size(), b - a});
+      for (size_t q = a; q < b; q++) all.push_back(Impl::Item{0u, p[q].inst, p[q].tile, 0u});   // kind 0 of its module
+      nseg++;
+      a = b;
+    }
+  }
+  I.launches = (int)nseg;
 
   // device arrays
   for (auto &kd : I.kinds) {
     cuda_check(cudaMalloc(&kd.d_args, kd.args.size()), "cudaMalloc(batch args)");
     cuda_check(cudaMemcpy(kd.d_args, kd.args.data(), kd.args.size(), cudaMemcpyHostToDevice), "upload args");
   }
-  size_t nitems = 0;
-  for (auto &p : I.phases) nitems += p.size();
-  cuda_check(cudaMalloc(&I.d_items, std::max<size_t>(1, nitems) * sizeof(Impl::Item)), "cudaMalloc(items)");
-  cuda_check(cudaMalloc(&I.d_counter, (size_t)std::max(1, nphase) * 256), "cudaMalloc(counter)");
-  size_t off = 0;
-  for (auto &p : I.phases) {
-    cuda_check(cudaMemcpy((char *)I.d_items + off * sizeof(Impl::Item), p.data(), p.size() * sizeof(Impl::Item),
-                          cudaMemcpyHostToDevice),
-               "upload items");
-    off += p.size();
+  cuda_check(cudaMalloc(&I.d_items, std::max<size_t>(1, all.size()) * sizeof(Impl::Item)), "cudaMalloc(items)");
+  cuda_check(cudaMalloc(&I.d_counter, std::max<size_t>(1, nseg) * 256), "cudaMalloc(counter)");
+  if (!all.empty())
+    cuda_check(cudaMemcpy(I.d_items, all.data(), all.size() * sizeof(Impl::Item), cudaMemcpyHostToDevice), "upload items");
+  size_t maxk = 1;
+  for (auto &segs : I.segments) maxk = std::max(maxk, segs.size());
+  for (size_t b = 1; b < maxk; b++) {
+    cudaStream_t bs;
+    cuda_check(cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking), "cudaStreamCreate");
+    I.branch.push_back(bs);
+  }
+  for (size_t e = 0; e < 2 * maxk; e++) {
+    cudaEvent_t ev;
+    cuda_check(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "cudaEventCreate");
+    I.fork_ev.push_back(ev);
   }
 
-  // capture: per dependency level, reset its counter then one persistent launch
+  // capture: per dependency level, the level's kinds run side by side (one branch
+  // each: reset the segment's counter, then its persistent launch), joined before
+  // the next level
   cuda_check(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
   try {
-    off = 0;
+    size_t si = 0;
     for (int ph = 0; ph < nphase; ph++) {
-      void *ctr = (char *)I.d_counter + 256 * ph;
-      cuda_check(cudaMemsetAsync(ctr, 0, 4, st), "cudaMemsetAsync");
-      struct {
-        uint64_t items;
-        int64_t n;
-        uint64_t counter;
-        uint64_t err;
-        uint64_t args[64];
-      } ba;
-      if (I.kinds.size() > 64) throw MapError("batch: too many kernel kinds");
-      ba.items = (uint64_t)(uintptr_t)((Impl::Item *)I.d_items + off);
-      ba.n = (int64_t)I.phases[ph].size();
-      ba.counter = (uint64_t)(uintptr_t)ctr;
-      ba.err = (uint64_t)(uintptr_t)env.err_word();
-      for (size_t k = 0; k < I.kinds.size(); k++) ba.args[k] = (uint64_t)(uintptr_t)I.kinds[k].d_args;
-      env.launch(I.kh, I.grid, 256, I.smem, (CUstream_st *)st, &ba, 32 + 8 * I.kinds.size());
-      off += I.phases[ph].size();
+      const auto &segs = I.segments[ph];
+      cuda_check(cudaEventRecord(I.fork_ev[0], st), "cudaEventRecord");
+      for (size_t b = 1; b < segs.size(); b++) cuda_check(cudaStreamWaitEvent(I.branch[b - 1], I.fork_ev[0], 0), "fork");
+      for (size_t b = 0; b < segs.size(); b++) {
+        const Impl::Segment &sg = segs[b];
+        const Kind &kd = I.kinds[sg.kind];
+        cudaStream_t bst = b == 0 ? st : I.branch[b - 1];
+        void *ctr = (char *)I.d_counter + 256 * (si++);
+        cuda_check(cudaMemsetAsync(ctr, 0, 4, bst), "cudaMemsetAsync");
+        struct {
+          uint64_t items;
+          int64_t n;
+          uint64_t counter;
+          uint64_t err;
+          uint64_t args[1];
+        } ba;
+        ba.items = (uint64_t)(uintptr_t)((Impl::Item *)I.d_items + sg.off);
+        ba.n = (int64_t)sg.n;
+        ba.counter = (uint64_t)(uintptr_t)ctr;
+        ba.err = (uint64_t)(uintptr_t)env.err_word();
+        ba.args[0] = (uint64_t)(uintptr_t)kd.d_args;
+        env.launch(kd.kh, std::min<int>(kd.grid, (int)sg.n), 256, kd.pm.smem, (CUstream_st *)bst, &ba, sizeof ba);
+      }
+      for (size_t b = 1; b < segs.size(); b++) {
+        cuda_check(cudaEventRecord(I.fork_ev[b], I.branch[b - 1]), "cudaEventRecord");
+        cuda_check(cudaStreamWaitEvent(st, I.fork_ev[b], 0), "join");
+      }
     }
   } catch (...) {
     cudaGraph_t g;
@@ -421,13 +513,14 @@ std::string Batch::info() const {
   std::ostringstream s;
   s << "{\"instances\": " << inst_.size();
   if (impl_) {
-    s << ", \"cells\": " << impl_->cells << ", \"tiles\": " << impl_->tiles << ", \"grid\": " << impl_->grid
-      << ", \"phases\": " << impl_->phases.size() << ", \"kernel\": \"" << impl_->kname << "\", \"kinds\": [";
+    s << ", \"cells\": " << impl_->cells << ", \"tiles\": " << impl_->tiles << ", \"phases\": " << impl_->phases.size()
+      << ", \"launches\": " << impl_->launches << ", \"kinds\": [";
     for (size_t k = 0; k < impl_->kinds.size(); k++) {
       auto &kd = impl_->kinds[k];
       s << (k ? ", " : "") << "{\"skeleton\": \"" << skeleton_name(kd.proto->skeleton) << "\", \"members\": " << kd.members
         << ", \"tile\": [" << kd.cfg.tw << ", " << kd.cfg.th << "], \"threads\": " << kd.cfg.nt
-        << ", \"tma\": " << (kd.plan.tma.empty() ? "false" : "true") << "}";
+        << ", \"tma\": " << (kd.plan.tma.empty() ? "false" : "true") << ", \"kernel\": \"" << kd.pm.kname
+        << "\", \"grid\": " << kd.grid << "}";
     }
     s << "], \"autotuned\": " << (impl_->tuned ? "true" : "false");
   }

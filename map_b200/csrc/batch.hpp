@@ -58,10 +58,11 @@ struct PersistentModule {
 };
 PersistentModule build_persistent_module(const std::vector<const KernelPlan *> &kinds);
 
-// Autotuned tile shape for group `g`, whose inputs/outputs are bound through
-// `get` / `bufs` (launches candidate kernels on the library stream).
-TileCfg autotune_group(const Group &g, const std::function<DevRaster &(Node *)> &get,
-                       std::unordered_map<Node *, DevRaster> &bufs);
+// Autotuned tile shape for a kind (groups of identical code, inputs / outputs bound
+// through `get` / `bufs`): times one persistent launch over all members' tiles per
+// candidate shape on the library stream.
+TileCfg autotune_kind(const std::vector<const Group *> &members, const std::function<DevRaster &(Node *)> &get,
+                      std::unordered_map<Node *, DevRaster> &bufs);
 std::string tune_key(const Group &g, const KernelPlan &p);
 
 }  // namespace mapb

@@ -520,7 +520,15 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   if (use_tma) {
     size_t total = 0;
     for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
-    body << "  if (tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ")) {\n"
+    // interior tiles, and edge tiles whose out-of-raster halo has one value per
+    // cell, are staged by TMA (zero fill outside the map, then the border rule)
+    // a tiled TMA copy must start on a 16-byte boundary in x: tiles whose origin is
+    // not a multiple of the staged types' alignment (plain-mode blocks of odd
+    // widths) take the gather path
+    int align_e = 1;
+    for (auto &t : P.tma) align_e = std::max(align_e, 16 / (int)dt_size(t.dtype));
+    body << "  const bool inner = tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ");\n"
+         << "  if (t.x0 % " << align_e << " == 0 && (inner || edge_staging(a.g))) {\n"
          << "    __syncthreads();   // earlier readers of the staging buffer are done\n"
          << "    if (threadIdx.x == 0) {\n"
          << "      fence_proxy_async();\n";
@@ -537,14 +545,24 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
          << "      mbar_wait_bounded(bar, phase, 1u << 26);\n"
          << "      return false;\n"
          << "    }\n"
-         << "    phase ^= 1u;\n";
+         << "    phase ^= 1u;\n"
+         << "    if (!inner) {\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      std::string ty = dt_ctype(t.dtype);
+      body << "      stage_fix_border<" << ty << ", " << t.box_w << ", " << t.box_h << ">((" << ty << " *)(smem + " << t.smem_off
+           << "), a.g, t.x0 - " << t.pad_x << ", t.y0 - " << hy << ", " << hx << ", " << hy << ");\n";
+    }
+    body << "      __syncthreads();\n"
+         << "    }\n";
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
       std::string ty = dt_ctype(t.dtype);
       body << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
            << " *)(smem + " << t.smem_off << ")};\n";
     }
-    body << loop_full.str() << "    return true;\n  }\n";
+    body << "    if (inner) {\n" << loop_full.str() << "    } else {\n" << loop.str() << "    }\n"
+         << "    return true;\n  }\n";
   }
   body << "  {\n";
   for (int k = 0; k < nst; k++) {

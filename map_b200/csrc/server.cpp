@@ -361,6 +361,9 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
   batch = ok;
   if (batch.empty()) return;
   ensure_module();
+  // items of one level are independent: run them kind by kind (instruction-cache locality)
+  for (auto &lv : levels)
+    std::stable_sort(lv.begin(), lv.end(), [](const Item &x, const Item &y) { return x.kind < y.kind; });
 
   // stage every upload into this stream's pinned buffer
   kind_args.resize(reg_plans.size());

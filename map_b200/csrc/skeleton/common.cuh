@@ -92,6 +92,31 @@ __device__ __forceinline__ bool focal_src(const Geom &g, int x, int y, int dx, i
   return true;
 }
 
+// Whether a tile at the raster edge can be staged like an interior one: its halo
+// cells outside the raster then hold the same value for every centre cell that
+// reads them (dead border: zero; raster mirror: the mirrored cell; block mirror:
+// only when the raster is one block, where it is the raster mirror).
+__device__ __forceinline__ bool edge_staging(const Geom &g) {
+  return g.border == 2 || g.border == 1 || (g.BS0 >= g.W && g.BS1 >= g.H);
+}
+
+// After a staged box of an edge tile has landed (raster cell (ox + bx, oy + by) at
+// s[by * SW + bx]), overwrites its cells outside the raster that a centre cell can
+// reach (within hx / hy of the edge) with the border rule's value. The sources
+// are inside the raster, so no cell is both read and written.
+template <class T, int SW, int SH>
+__device__ __forceinline__ void stage_fix_border(T *s, const Geom &g, int ox, int oy, int hx, int hy) {
+  for (int i = threadIdx.x; i < SW * SH; i += blockDim.x) {
+    const int bx = i % SW, by = i / SW;
+    const int rx = ox + bx, ry = oy + by;
+    if ((unsigned)rx < (unsigned)g.W && (unsigned)ry < (unsigned)g.H) continue;
+    if (rx < -hx || rx >= g.W + hx || ry < -hy || ry >= g.H + hy) continue;
+    T v = (T)0;
+    if (g.border != 2) v = s[(reflect_idx(ry, g.H) - oy) * SW + (reflect_idx(rx, g.W) - ox)];
+    s[i] = v;
+  }
+}
+
 // Focal tap served straight from global memory with the border rule (edge tiles).
 template <class T> struct GatherTap {
   RasterArg r;

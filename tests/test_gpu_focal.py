@@ -33,6 +33,9 @@ def hill_tolerance_ok(gpu, ref32, ref64):
     ((190, 333), (64, 64), 2, 0),
     ((64, 64), (64, 64), 0, 0),
     ((1, 40), (16, 16), 1, 0),
+    ((300, 500), (500, 300), 0, 0),   # one block: edge tiles staged like interior ones
+    ((200, 270), (90, 70), 0, 1),     # plain launches from block origins not on a 16-byte boundary
+    ((190, 333), (100, 60), 1, 1),
 ])
 def test_hillshade_matches_oracle(fresh, shape, bs, border, mode):
     M = fresh
@@ -85,6 +88,19 @@ def test_life_bit_exact(fresh, border):
     st = M.from_numpy(st_np, bs=[64, 64])
     out = M.to_numpy(W.life(st, 12))
     ref = O.life(st_np, (64, 64), 12, border)
+    assert np.array_equal(out, ref)
+
+
+@pytest.mark.parametrize("border,bs,mode", [(0, (100, 60), 1), (2, (100, 60), 1), (1, (384, 256), 0)])
+def test_life_odd_blocks_and_staged_edges_bit_exact(fresh, border, bs, mode):
+    # U8 rasters stage in 16-byte units: plain launches from block origins at x = 100,
+    # 200, ... take the gather path; one-block rasters stage their edge tiles too
+    M = fresh
+    M.set_border(border)
+    M.set_exec_mode(mode)
+    st_np = synth.bernoulli_u8(256, 384, 0.3, seed=12)
+    out = M.to_numpy(W.life(M.from_numpy(st_np, bs=list(bs)), 6))
+    ref = O.life(st_np, bs, 6, border)
     assert np.array_equal(out, ref)
 
 
