@@ -76,8 +76,9 @@ Node *prog_hillshade(Runtime &rt, Node *dem, double zenith, double azimuth) {
 }
 
 Node *prog_viewshed(Runtime &rt, Node *dem, int obs_x, int obs_y, float obs_h, double radius, Node **ox_out,
-                    Node **oy_out) {
-  Node *h = cflt(rt, obs_h);
+                    Node **oy_out, Node **oh_out) {
+  Node *h = rt.scalar_param(vf32(obs_h));
+  if (oh_out) *oh_out = h;
   Node *shift = rt.binary(dem, h, SUB);
   Node *ox = rt.scalar_param(vs32(obs_x));
   Node *oy = rt.scalar_param(vs32(obs_y));

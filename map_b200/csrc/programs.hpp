@@ -14,10 +14,10 @@ namespace mapb {
 Node *prog_slope(Runtime &rt, Node *dem);
 Node *prog_aspect(Runtime &rt, Node *dem);
 Node *prog_hillshade(Runtime &rt, Node *dem, double zenith = 45.0, double azimuth = 315.0);
-// Observer coordinates are kernel arguments, so every observer shares one kernel.
-// ox_out / oy_out receive the observer coordinate argument nodes.
+// The observer's coordinates and height are kernel arguments (ox_out, oy_out,
+// oh_out receive their nodes), so every observer shares one kernel.
 Node *prog_viewshed(Runtime &rt, Node *dem, int obs_x, int obs_y, float obs_h, double radius, Node **ox_out = nullptr,
-                    Node **oy_out = nullptr);
+                    Node **oy_out = nullptr, Node **oh_out = nullptr);
 Node *prog_flow(Runtime &rt, Node *dem, Node **dirs_out = nullptr);
 
 }  // namespace mapb

@@ -75,7 +75,7 @@ struct Template {
   std::vector<int> level;          // dependency level per group
   std::vector<int> kind;           // persistent-module kind per Local / Focal group (-1 otherwise)
   Node *win = nullptr, *out = nullptr;
-  Node *ox = nullptr, *oy = nullptr;   // viewshed observer arguments
+  Node *ox = nullptr, *oy = nullptr, *oh = nullptr;   // viewshed observer arguments
   int last_phase = PH_LEVEL0;
 };
 
@@ -125,6 +125,13 @@ struct Server::Impl {
   KernelHandle pk;
   int pk_grid = 0;
   std::map<std::string, std::unique_ptr<Template>> templates;
+  static constexpr size_t kMaxTemplates = 512;
+  std::vector<std::unique_ptr<Template>> transient;   // templates built past the cache limit (one batch)
+  void drop(Template &T) {
+    Runtime &rt = Runtime::get();
+    std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+    if (T.out && rt.owns(T.out) && T.out->ref > 0) T.out->ref--;
+  }
 
   // statistics
   long long batches = 0, completed = 0, failed = 0, max_batch_seen = 0, batched_requests = 0;
@@ -149,7 +156,7 @@ struct Server::Impl {
     module_kinds = (int)reg_plans.size();
   }
   // compile = false defers the persistent module's (re)compilation to the caller
-  Template &template_for(int type, int w, int h, float obs_h, bool compile = true);
+  Template &template_for(int type, int w, int h, bool compile = true);
   void warm_up();
   void dispatch_loop();
   void complete_loop();
@@ -170,11 +177,8 @@ void Server::Impl::free_request(Req *r, cudaStream_t st) {
   r->scratch.clear();
 }
 
-Template &Server::Impl::template_for(int type, int w, int h, float obs_h, bool compile) {
-  uint32_t hb;
-  std::memcpy(&hb, &obs_h, 4);
-  const std::string key = std::to_string(type) + "|" + std::to_string(w) + "x" + std::to_string(h) + "|" +
-                          (type == REQ_VIEWSHED ? std::to_string(hb) : std::string("-"));
+Template &Server::Impl::template_for(int type, int w, int h, bool compile) {
+  const std::string key = std::to_string(type) + "|" + std::to_string(w) + "x" + std::to_string(h);
   auto it = templates.find(key);
   if (it != templates.end()) return *it->second;
   Runtime &rt = Runtime::get();
@@ -187,7 +191,7 @@ Template &Server::Impl::template_for(int type, int w, int h, float obs_h, bool c
     case REQ_HILLSHADE: T->out = prog_hillshade(rt, T->win); break;
     case REQ_SLOPE: T->out = prog_slope(rt, T->win); break;
     // distinct placeholder coordinates keep the two argument nodes distinct
-    case REQ_VIEWSHED: T->out = prog_viewshed(rt, T->win, 1, 2, obs_h, 0.0, &T->ox, &T->oy); break;
+    case REQ_VIEWSHED: T->out = prog_viewshed(rt, T->win, 1, 2, 3.0f, 0.0, &T->ox, &T->oy, &T->oh); break;
     case REQ_FLOW: T->out = prog_flow(rt, T->win); break;
     default: throw MapError("unknown request type");
   }
@@ -221,11 +225,20 @@ Template &Server::Impl::template_for(int type, int w, int h, float obs_h, bool c
   }
   if (compile) ensure_module();
   Template &ref = *T;
-  templates[key] = std::move(T);
+  if (templates.size() < kMaxTemplates) templates[key] = std::move(T);
+  else transient.push_back(std::move(T));   // a window size beyond the cache: used for this batch only
   return ref;
 }
 
 void Server::Impl::run_batch(std::vector<Req *> &batch) {
+  // templates built past the cache limit serve this batch only (every exit path)
+  struct TransientRelease {
+    Impl &I;
+    ~TransientRelease() {
+      for (auto &T : I.transient) I.drop(*T);
+      I.transient.clear();
+    }
+  } release_transient{*this};
   CudaEnv &env = CudaEnv::get();
   const int si = next_stream;
   next_stream ^= 1;
@@ -252,7 +265,7 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
 
   for (Req *r : batch) {
     try {
-      Template &T = template_for(r->type, r->w, r->h, r->oh, false);
+      Template &T = template_for(r->type, r->w, r->h, false);
       r->stream = si;
       r->win_pitch = pitch_for(r->w, F32);
       cuda_check(cudaMallocAsync(&r->win, (size_t)r->win_pitch * r->h, st), "cudaMallocAsync(window)");
@@ -284,12 +297,15 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
       };
       std::unordered_map<const Node *, Variant> scal;
       if (T.ox) {
-        Variant vx{}, vy{};
+        Variant vx{}, vy{}, vh{};
         vx.dtype = vy.dtype = S32;
         vx.u.s32 = r->ox;
         vy.u.s32 = r->oy;
+        vh.dtype = F32;
+        vh.u.f32 = r->oh;
         scal[T.ox] = vx;
         scal[T.oy] = vy;
+        scal[T.oh] = vh;
       }
       for (size_t gi = 0; gi < T.fr.groups.size(); gi++) {
         const Group &g = *T.fr.groups[gi];
@@ -572,9 +588,9 @@ void Server::Impl::complete_loop() {
 void Server::Impl::warm_up() {
   for (int s : {256, 512, 1024})
     if (s <= W && s <= H)
-      for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, s, s, 10.0f, false);
+      for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, s, s, false);
   const int w = std::min(64, W), h = std::min(64, H);
-  for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, w, h, 10.0f, false);
+  for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, w, h, false);
   ensure_module();
 }
 
@@ -636,10 +652,7 @@ Server::~Server() {
     if (I.stage[i]) cudaFreeHost(I.stage[i]);
   }
   for (int i = 0; i < kQueues; i++) cudaStreamDestroy(I.streams[i]);
-  Runtime &rt = Runtime::get();
-  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
-  for (auto &kv : I.templates)
-    if (kv.second->out && rt.owns(kv.second->out) && kv.second->out->ref > 0) kv.second->out->ref--;
+  for (auto &kv : I.templates) I.drop(*kv.second);
 }
 
 long long Server::submit(int type, int x0, int y0, int w, int h, int obs_x, int obs_y, float obs_h, double radius,

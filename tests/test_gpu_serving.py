@@ -100,3 +100,29 @@ def test_open_loop_load_reports_percentiles(served):
     r = srv.load(rate=300, seconds=1.0, seed=1, radius=167)
     assert r["completed"] == r["requests"] > 100
     assert 0 < r["p50_ms"] <= r["p99_ms"]
+
+
+def test_observer_height_is_an_argument(served):
+    # any observer height reuses the compiled viewshed kernel and matches the engine
+    M, srv, dem_np = served
+    kinds0 = srv.stats()["kinds"]
+    x0, y0, w, h, obs = 40, 60, 200, 180, (70, 90)
+    for oh in (25.0, 3.5):
+        rid = srv.submit(M.Server.VIEWSHED, x0, y0, w, h, obs=obs, obs_h=oh, radius=60)
+        got = srv.result(rid, (h, w), np.float32)
+        want = window_expected(M, dem_np, M.Server.VIEWSHED, x0, y0, w, h, obs, oh, 60)
+        nan = np.isnan(want)
+        assert np.array_equal(np.isnan(got), nan)
+        assert np.array_equal(got[~nan], want[~nan])
+    assert srv.stats()["kinds"] == kinds0
+
+
+def test_window_sizes_beyond_the_template_cache_still_work(served):
+    # odd window sizes each build a template; results stay exact whether cached or not
+    M, srv, dem_np = served
+    for k in range(5):
+        w, h = 97 + 13 * k, 61 + 7 * k
+        rid = srv.submit(M.Server.SLOPE, 11 * k, 5 * k, w, h)
+        got = srv.result(rid, (h, w), np.float32)
+        want = window_expected(M, dem_np, M.Server.SLOPE, 11 * k, 5 * k, w, h)
+        assert np.array_equal(got, want)
