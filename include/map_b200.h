@@ -115,6 +115,13 @@ int ma_getExecMode(void);
  * identical to whole-raster evaluation. */
 void ma_setStreamRows(int rows);
 int ma_getStreamRows(void);
+/* Paired cells: focal groups with float math compute the cells of two rows per
+ * thread step, their float additions, subtractions, multiplications and the
+ * polynomial parts of sin, cos and atan2 as packed f32x2 instructions. Results
+ * are bit-identical either way; on = 0 computes one cell at a time. Engine
+ * option with no counterpart in the reference. */
+void ma_setPairedCells(int on);
+int ma_getPairedCells(void);
 /* Block size given to rasters created without one (default 256 x 256). */
 void ma_setDefaultBlockSize(ma_Array bs);
 void ma_setDevice(int device);

@@ -352,6 +352,10 @@ void ma_setStreamRows(int rows) {
   void_call([&] { Runtime::get().stream_rows = rows; });
 }
 int ma_getStreamRows(void) { return Runtime::get().stream_rows; }
+void ma_setPairedCells(int on) {
+  void_call([&] { Runtime::get().paired_cells = on ? 1 : 0; });
+}
+int ma_getPairedCells(void) { return Runtime::get().paired_cells; }
 void ma_setDefaultBlockSize(ma_Array bs) {
   void_call([&] {
     if (bs.n != 2 || bs.arr[0] <= 0 || bs.arr[1] <= 0) throw MapError("setDefaultBlockSize: invalid size");

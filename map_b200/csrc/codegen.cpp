@@ -2,6 +2,8 @@
 // skeletons (see codegen.hpp); the scan skeletons run through codegen_scan.cpp.
 #include "codegen.hpp"
 
+#include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <map>
 #include <set>
@@ -54,6 +56,14 @@ const char *unary_fn(int op) {
     case ROUND: return "round";
     default: return nullptr;
   }
+}
+
+// Device function computing unary op on a float type: the engine's own sine
+// and cosine for float32 (skeleton/common.cuh), the CUDA library otherwise.
+std::string float_fn_own(int dt, int op) {
+  if (dt == F32 && op == SIN) return "map_sinf";
+  if (dt == F32 && op == COS) return "map_cosf";
+  return float_fn(dt, unary_fn(op));
 }
 
 const char *binary_sym(int op) {
@@ -127,6 +137,249 @@ struct Gen {
     auto s = staged.find(in);
     if (s == staged.end()) throw MapError("codegen: focal read of a raster that is not staged");
     return "f" + std::to_string(s->second) + ".tap(x, y, lx, ly, " + std::to_string(dx) + ", " + std::to_string(dy) + ")";
+  }
+  // the same tap of the cell pair (x, y), (x, y + 1)
+  std::string tap2(Node *in, int dx, int dy) const {
+    auto s = staged.find(in);
+    if (s == staged.end()) throw MapError("codegen: focal read of a raster that is not staged");
+    return "f" + std::to_string(s->second) + ".tap2(x, y, lx, ly, " + std::to_string(dx) + ", " + std::to_string(dy) + ")";
+  }
+
+  // One term acc = acc + tap * w of a float convolution. A zero weight gives an
+  // exact signed-zero product, so fma(tap, w, acc) equals the multiply and add;
+  // weights 1 and -1 give exact products tap and -tap. Other weights and types
+  // keep the multiply and add.
+  static std::string conv_term(const std::string &acc, const std::string &ct, const std::string &tp, int tap_dt,
+                               int acc_dt, const Variant &w, bool pair) {
+    const std::string lit = var_literal(reference_literal_value(w));
+    if (acc_dt == F32 && tap_dt == F32 && (dt_is_float(w.dtype) ? w.dtype == F32 : dt_size(w.dtype) <= 4)) {
+      const double wv = var_as_f64(w);
+      if (wv == 0.0)
+        return acc + " = " + (pair ? "pr_fmaf(" : "fmaf(") + tp + ", " + (dt_is_float(w.dtype) ? lit : std::string("0.0f")) +
+               ", " + acc + ");";
+      if (wv == 1.0) return acc + " = " + ct + "(" + acc + " + " + tp + ");";
+      if (wv == -1.0) return acc + " = " + ct + "(" + acc + " - " + tp + ");";
+      // a packed product is added lane by lane (see pr_add_lanes)
+      if (pair) return acc + " = pr_add_lanes(" + acc + ", " + tp + " * " + lit + ");";
+    }
+    return acc + " = " + ct + "(" + acc + " + " + tp + " * " + lit + ");";
+  }
+
+  // ---- paired cells (two rows per thread step, skeleton/common.cuh PR<T>)
+
+  // Whether every node of the group has a pair form (float functions on F32 only).
+  bool pairable() const {
+    for (Node *n : g.nodes) {
+      switch (n->kind) {
+        case K_CONSTANT: case K_INDEX: case K_CAST: case K_BARRIER: case K_CONDITIONAL: case K_NEIGHBOR:
+        case K_CONVOLUTION: case K_FOCALFUNC:
+          break;
+        case K_UNARY: {
+          if (n->op == POS || n->op == NEG || n->op == NOT || n->op == bNOT) break;
+          const int pdt = n->prev[0]->meta.dtype;
+          if (!unary_fn(n->op)) return false;
+          if (dt_is_float(pdt)) {
+            if (pdt != F32) return false;
+            break;
+          }
+          if (n->op == ABS || n->op == CEIL || n->op == FLOOR || n->op == TRUNC || n->op == ROUND) break;
+          return false;
+        }
+        case K_BINARY: {
+          if (binary_sym(n->op)) break;
+          const int pt = dt_promote(n->prev[0]->meta.dtype, n->prev[1]->meta.dtype);
+          if (n->op == MAX2 || n->op == MIN2) break;
+          if ((n->op == ATAN2 || n->op == POW || n->op == HYPOT || n->op == FMOD) && pt == F32) break;
+          return false;
+        }
+        default:
+          return false;
+      }
+    }
+    return true;
+  }
+
+  bool is_literal_one(Node *c) const { return literal.count(c) && var_as_f64(c->cnst) == 1.0; }
+
+  // Whether the pair form of n is a packed float multiply whose product may be
+  // inexact (a sum with it is then added lane by lane, see pr_add_lanes):
+  // products with a 0/1 mask or with +-1 are exact.
+  bool inexact_product(Node *n) const {
+    if (!member.count(n) || n->kind != K_BINARY || n->meta.dtype != F32) return false;
+    double rc = 0;
+    if (n->op == DIV) return pow2_reciprocal(n->prev[1], rc);
+    if (n->op != MUL) return false;
+    for (Node *p : n->prev) {
+      if (!dt_is_float(p->meta.dtype) && zero_one(p)) return false;
+      if (literal.count(p) && std::fabs(var_as_f64(p->cnst)) == 1.0) return false;
+    }
+    return true;
+  }
+
+  // 1/c for a scalar literal c = +-2^k whose reciprocal is a normal float
+  bool pow2_reciprocal(Node *c, double &rc) const {
+    if (!literal.count(c)) return false;
+    const double v = var_as_f64(c->cnst);
+    if (!(v != 0) || !std::isfinite(v)) return false;
+    int e = 0;
+    const double m = std::frexp(std::fabs(v), &e);
+    if (m != 0.5) return false;
+    rc = 1.0 / v;
+    return std::fabs(rc) >= 0x1p-126 && std::fabs(rc) <= 0x1p+127;
+  }
+
+  // Statement of node n in the pair form: the value of the cells (x, y) and
+  // (x, y + 1) as PR<T>, every conversion written as PR<T>(...).
+  std::string stmt2(Node *n) const {
+    std::ostringstream s;
+    const std::string t = T(n);
+    const std::string pt_ = "PR<" + t + ">";
+    const std::string v = "v" + std::to_string(member.at(n));
+    const std::string decl = "const " + pt_ + " " + v + " = ";
+    switch (n->kind) {
+      case K_CONSTANT:
+        s << decl << pt_ << "(" << var_literal(reference_literal_value(n->cnst)) << ");";
+        break;
+      case K_INDEX:
+        if (n->op == D1) s << decl << pt_ << "((" << t << ")(x), (" << t << ")(x));";
+        else s << decl << pt_ << "((" << t << ")(y), (" << t << ")(y + 1));";
+        break;
+      case K_CAST: case K_BARRIER:
+        s << decl << pt_ << "(" << val(n->prev[0]) << ");";
+        break;
+      case K_UNARY: {
+        std::string p = val(n->prev[0]);
+        int pdt = n->prev[0]->meta.dtype;
+        switch (n->op) {
+          case POS: s << decl << pt_ << "(+" << p << ");"; break;
+          case NEG: s << decl << pt_ << "(-" << p << ");"; break;
+          case NOT: s << decl << pt_ << "(!" << p << ");"; break;
+          case bNOT: s << decl << pt_ << "(~" << p << ");"; break;
+          default: {
+            auto mate = sincos_mate.find(n);
+            if (mate != sincos_mate.end()) {
+              if (sincos_first.count(n)) {
+                Node *sn = n->op == SIN ? n : mate->second, *cn = n->op == COS ? n : mate->second;
+                s << "PR<float> v" << member.at(sn) << ", v" << member.at(cn) << "; map_sincosf(PR<float>(" << p
+                  << "), &v" << member.at(sn) << ", &v" << member.at(cn) << ");";
+              }
+              break;
+            }
+            if (dt_is_float(pdt)) {
+              const std::string f = float_fn_own(pdt, n->op);   // own functions overload PR; library ones are pr_*
+              s << decl << pt_ << "(" << (f.compare(0, 4, "map_") == 0 ? f : "pr_" + f) << "(PR<float>(" << p << ")));";
+            } else if (n->op == ABS) {
+              s << decl << pt_ << "(psel(" << p << " < 0, -" << p << ", " << p << "));";
+            } else {
+              s << decl << pt_ << "(" << p << ");";   // CEIL / FLOOR / TRUNC / ROUND of an integer
+            }
+          }
+        }
+        break;
+      }
+      case K_BINARY: {
+        std::string l = val(n->prev[0]), r = val(n->prev[1]);
+        int pt = dt_promote(n->prev[0]->meta.dtype, n->prev[1]->meta.dtype);
+        std::string pts = dt_ctype(pt);
+        if (const char *sym = binary_sym(n->op)) {
+          if (dt_is_float(pt) && (n->op == MOD || binary_is_bitwise(n->op)))
+            throw MapError(std::string("binary op ") + binary_name(n->op) + " is not defined on floating types");
+          if (dt_is_float(pt)) {
+            if (!dt_is_float(n->prev[0]->meta.dtype) && zero_one(n->prev[0])) l = "psel(" + l + ", (" + pts + ")1, (" + pts + ")0)";
+            if (!dt_is_float(n->prev[1]->meta.dtype) && zero_one(n->prev[1])) r = "psel(" + r + ", (" + pts + ")1, (" + pts + ")0)";
+          }
+          double rc = 0;
+          Node *one = nullptr;   // 1 * x and x * 1 of a float x are x (exactly, signs and NaN included)
+          if (n->op == MUL && pt == F32) {
+            if (is_literal_one(n->prev[0]) && n->prev[1]->meta.dtype == F32) one = n->prev[1];
+            else if (is_literal_one(n->prev[1]) && n->prev[0]->meta.dtype == F32) one = n->prev[0];
+          }
+          if (one) {
+            s << decl << pt_ << "(" << val(one) << ");";
+          } else if (n->op == ADD && pt == F32 && (inexact_product(n->prev[0]) || inexact_product(n->prev[1]))) {
+            s << decl << "pr_add_lanes(" << l << ", " << r << ");";
+          } else if (n->op == DIV && pt == F32 && pow2_reciprocal(n->prev[1], rc)) {
+            // division by a literal power of two: the multiply by its (exact)
+            // reciprocal rounds the same real value, and packs
+            char b[48];
+            std::snprintf(b, sizeof b, "%af", rc);
+            s << decl << pt_ << "(" << l << " * " << b << ");";
+          } else {
+            s << decl << pt_ << "(" << l << " " << sym << " " << r << ");";
+          }
+        } else {
+          std::string L = "PR<" + pts + ">(" + l + ")", R = "PR<" + pts + ">(" + r + ")";
+          switch (n->op) {
+            case MAX2: s << decl << pt_ << "(red_max(" << L << ", " << R << "));"; break;
+            case MIN2: s << decl << pt_ << "(red_min(" << L << ", " << R << "));"; break;
+            case ATAN2: s << decl << pt_ << "(map_atan2f(" << L << ", " << R << "));"; break;
+            case POW: s << decl << pt_ << "(pr_powf(" << L << ", " << R << "));"; break;
+            case HYPOT: s << decl << pt_ << "(pr_hypotf(" << L << ", " << R << "));"; break;
+            case FMOD: s << decl << pt_ << "(pr_fmodf(" << L << ", " << R << "));"; break;
+            default: throw MapError("codegen: invalid binary op");
+          }
+        }
+        break;
+      }
+      case K_CONDITIONAL:
+        s << decl << "psel(" << val(n->prev[0]) << ", " << pt_ << "(" << val(n->prev[1]) << "), " << pt_ << "("
+          << val(n->prev[2]) << "));";
+        break;
+      case K_NEIGHBOR:
+        s << decl << pt_ << "(" << tap2(n->prev[0], n->coord.arr[0], n->coord.arr[1]) << ");";
+        break;
+      case K_CONVOLUTION: {
+        int hx = n->halo_x(), hy = n->halo_y(), mw = n->mask_ds.arr[0];
+        s << pt_ << " " << v << " = " << pt_ << "((" << t << ")0);";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++)
+            s << "\n    " << conv_term(v, pt_, tap2(n->prev[0], i0, i1), n->prev[0]->meta.dtype, n->meta.dtype,
+                                       n->mask[(i1 + hy) * mw + (i0 + hx)], true);
+        break;
+      }
+      case K_FOCALFUNC: {
+        int hx = n->halo_x(), hy = n->halo_y();
+        s << pt_ << " " << v << " = " << pt_ << "(" << var_literal(reduction_neutral(n->op, n->meta.dtype)) << ");";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++)
+            s << "\n    " << v << " = RedOp<" << n->op << ", " << pt_ << ">::f(" << v << ", " << pt_ << "("
+              << tap2(n->prev[0], i0, i1) << "));";
+        break;
+      }
+      default:
+        throw MapError(std::string("codegen: node kind ") + kind_name(n->kind) + " has no pair form");
+    }
+    return s.str();
+  }
+
+  std::string stores2() const {
+    std::ostringstream s;
+    for (auto &kv : outk) {
+      Node *o = kv.first;
+      s << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "));\n"
+        << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y + 1, lane1(" << val(o) << "));\n";
+    }
+    return s.str();
+  }
+
+  std::string center_loads2() const {
+    std::ostringstream s;
+    for (Node *p : plan.in_rasters) {
+      if (!center_read.count(p)) continue;
+      int k = rin.at(p);
+      std::string t = T(p);
+      if (staged.count(p)) s << "    const PR<" << t << "> i" << k << " = " << tap2(p, 0, 0) << ";\n";
+      else
+        s << "    const PR<" << t << "> i" << k << "(ldr<" << t << ">(a.in[" << k << "], x, y), ldr<" << t << ">(a.in[" << k
+          << "], x, y + 1));\n";
+    }
+    return s.str();
+  }
+
+  std::string body2() const {
+    std::ostringstream s;
+    for (Node *n : g.nodes) s << "    " << stmt2(n) << "\n";
+    return s.str();
   }
 
   void classify() {
@@ -229,13 +482,13 @@ struct Gen {
             if (mate != sincos_mate.end()) {
               if (sincos_first.count(n)) {
                 Node *sn = n->op == SIN ? n : mate->second, *cn = n->op == COS ? n : mate->second;
-                s << "float v" << member.at(sn) << ", v" << member.at(cn) << "; sincosf(" << p << ", &v" << member.at(sn)
+                s << "float v" << member.at(sn) << ", v" << member.at(cn) << "; map_sincosf(" << p << ", &v" << member.at(sn)
                   << ", &v" << member.at(cn) << ");";
               }
               break;
             }
             if (dt_is_float(pdt)) {
-              s << "const " << t << " " << v << " = " << float_fn(pdt, fn) << "(" << p << ");";
+              s << "const " << t << " " << v << " = " << float_fn_own(pdt, n->op) << "(" << p << ");";
             } else if (n->op == ABS) {
               s << "const " << t << " " << v << " = (" << t << ")(" << p << " < 0 ? -" << p << " : " << p << ");";
             } else if (n->op == CEIL || n->op == FLOOR || n->op == TRUNC || n->op == ROUND) {
@@ -292,11 +545,9 @@ struct Gen {
         int hx = n->halo_x(), hy = n->halo_y(), mw = n->mask_ds.arr[0];
         s << t << " " << v << " = (" << t << ")0;";
         for (int i1 = -hy; i1 <= hy; i1++)
-          for (int i0 = -hx; i0 <= hx; i0++) {
-            const Variant &m = n->mask[(i1 + hy) * mw + (i0 + hx)];
-            s << "\n    " << v << " = (" << t << ")(" << v << " + " << tap(n->prev[0], i0, i1) << " * "
-              << var_literal(reference_literal_value(m)) << ");";
-          }
+          for (int i0 = -hx; i0 <= hx; i0++)
+            s << "\n    " << conv_term(v, "(" + t + ")", tap(n->prev[0], i0, i1), n->prev[0]->meta.dtype, n->meta.dtype,
+                                       n->mask[(i1 + hy) * mw + (i0 + hx)], false);
         break;
       }
       case K_FOCALFUNC: {
@@ -485,10 +736,13 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
   body << ", int x, int y, int lx, int ly) {\n";
   body << G.center_loads(false) << G.body(false) << G.stores() << "}\n";
-  std::ostringstream call;
+  std::ostringstream call, call2;
   call << "focal_cell(a";
+  call2 << "focal_cell2(a";
   for (int k = 0; k < nst; k++) call << ", f" << k;
+  for (int k = 0; k < nst; k++) call2 << ", f" << k;
   call << ", x, y, lx, ly)";
+  call2 << ", x, y, lx, ly)";
   // Each thread computes `rows` consecutive rows of one column, so the taps of
   // neighbouring cells in the column are the same shared-memory words (loaded
   // once when the loop is unrolled); a warp still covers 32 consecutive columns.
@@ -498,22 +752,40 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     if ((n->kind == K_UNARY && n->op >= SIN && n->op <= CBRT) ||
         (n->kind == K_BINARY && (n->op == ATAN2 || n->op == POW || n->op == HYPOT || n->op == FMOD)))
       heavy = true;
-  const std::string unroll = heavy ? "#pragma unroll 2\n" : "#pragma unroll\n";
+  // Float-heavy bodies compute the cells of two consecutive rows together
+  // (PR<T> pairs: packed f32x2 arithmetic, one issue slot for both cells).
+  const bool pair = heavy && rows % 2 == 0 && Runtime::get().paired_cells && G.pairable();
+  if (pair) {
+    body << "template <";
+    for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
+    body << ">\n__device__ __forceinline__ void focal_cell2(const Args &a";
+    for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
+    body << ", int x, int y, int lx, int ly) {\n";
+    body << G.center_loads2() << G.body2() << G.stores2() << "}\n";
+  }
+  const std::string unroll = pair ? "#pragma unroll 1\n" : heavy ? "#pragma unroll 2\n" : "#pragma unroll\n";
+  const int step = pair ? 2 : 1;
   std::ostringstream loop, loop_full;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
        << "    const int x = t.x0 + lx;\n"
        << unroll
-       << "    for (int k = 0; k < " << rows << "; ++k) {\n"
-       << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
-       << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n"
-       << "    }\n";
+       << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+       << "      const int ly = ly0 + k, y = t.y0 + ly;\n";
+  if (pair)
+    loop << "      if (x < t.xe) {\n"
+         << "        if (y + 1 < t.ye) " << call2.str() << ";\n"
+         << "        else if (y < t.ye) " << call.str() << ";\n"
+         << "      }\n";
+  else
+    loop << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n";
+  loop << "    }\n";
   // interior tiles are full: every cell of the tile is inside the raster
   loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
             << "    const int x = t.x0 + lx;\n"
             << unroll
-            << "    for (int k = 0; k < " << rows << "; ++k) {\n"
+            << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
             << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
-            << "      " << call.str() << ";\n"
+            << "      " << (pair ? call2.str() : call.str()) << ";\n"
             << "    }\n";
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"

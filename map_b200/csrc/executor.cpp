@@ -271,7 +271,7 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
 std::shared_ptr<Executor::Prepared> Executor::prepare_cached(const std::vector<Node *> &targets,
                                                              const std::set<Node *> &tset) {
   Runtime &rt = Runtime::get();
-  std::string key = std::to_string(rt.exec_mode) + ";";
+  std::string key = std::to_string(rt.exec_mode) + "," + std::to_string(rt.paired_cells) + ";";
   for (Node *t : targets) key += std::to_string(t->id) + ",";
   key += ";";
   for (Node *t : tset) key += std::to_string(t->id) + ",";

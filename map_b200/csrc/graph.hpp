@@ -95,6 +95,9 @@ struct Runtime {
   // Row bands of streamed evaluations (host rasters in, host rasters out):
   // 0 automatic, < 0 never stream, > 0 stream whenever a raster has more rows.
   int stream_rows = 0;
+  // Focal groups of float math compute two cells per thread step on packed
+  // f32x2 instructions (bit-identical to one cell at a time); 0 turns it off.
+  int paired_cells = 1;
   // incremented whenever nodes are destroyed (caches keyed by node ids check it)
   uint64_t epoch = 0;
   Arr2 default_bs{{256, 256}, 2};

@@ -74,29 +74,343 @@ template <class T> __device__ __forceinline__ void str(const RasterArg &r, int x
 // (atan(t)/t - 1)/s on [0, 1] by iteratively reweighted least squares (Lawson)
 // for minimum relative error, then undo the reduction with pi/2 and pi split
 // into two floats (one step per octant), and give the result the sign of y.
-__device__ __forceinline__ float map_atan2f(float y, float x) {
+// The three steps are separate so that the polynomial can also run on packed
+// pairs (map_atan2f on PR<float> below) with the same operations.
+#define MAP_ATAN_Q0 -0x1.d62fecp-10f
+#define MAP_ATAN_Q1 0x1.65a65ap-7f
+#define MAP_ATAN_Q2 -0x1.fed15ep-6f
+#define MAP_ATAN_Q3 0x1.dac9e2p-5f
+#define MAP_ATAN_Q4 -0x1.583490p-4f
+#define MAP_ATAN_Q5 0x1.c099fep-4f
+#define MAP_ATAN_Q6 -0x1.2421b6p-3f
+#define MAP_ATAN_Q7 0x1.9991fep-3f
+#define MAP_ATAN_Q8 -0x1.55553ep-2f
+__device__ __forceinline__ float map_atan2_arg(float y, float x) {
   const float ax = fabsf(x), ay = fabsf(y);
   const float mx = ax > ay ? ax : ay, mn = ax > ay ? ay : ax;   // a NaN operand makes t NaN below
   float t = mn / mx;
   if (ax == 0.0f && ay == 0.0f) t = 0.0f;
   if (isinf(ax) && isinf(ay)) t = 1.0f;
+  return t;
+}
+__device__ __forceinline__ float map_atan_poly(float t) {
   const float s = t * t;
-  float q = -0x1.d62fecp-10f;
-  q = fmaf(q, s, 0x1.65a65ap-7f);
-  q = fmaf(q, s, -0x1.fed15ep-6f);
-  q = fmaf(q, s, 0x1.dac9e2p-5f);
-  q = fmaf(q, s, -0x1.583490p-4f);
-  q = fmaf(q, s, 0x1.c099fep-4f);
-  q = fmaf(q, s, -0x1.2421b6p-3f);
-  q = fmaf(q, s, 0x1.9991fep-3f);
-  q = fmaf(q, s, -0x1.55553ep-2f);
-  float r = fmaf(t * s, q, t);
+  float q = MAP_ATAN_Q0;
+  q = fmaf(q, s, MAP_ATAN_Q1);
+  q = fmaf(q, s, MAP_ATAN_Q2);
+  q = fmaf(q, s, MAP_ATAN_Q3);
+  q = fmaf(q, s, MAP_ATAN_Q4);
+  q = fmaf(q, s, MAP_ATAN_Q5);
+  q = fmaf(q, s, MAP_ATAN_Q6);
+  q = fmaf(q, s, MAP_ATAN_Q7);
+  q = fmaf(q, s, MAP_ATAN_Q8);
+  return fmaf(t * s, q, t);
+}
+__device__ __forceinline__ float map_atan2_finish(float r, float y, float x) {
   // one reconstruction per octant, the constant's low part added first
   const bool neg = signbit(x);
-  if (ay > ax) r = neg ? (-0x1.777a5cp-25f + r) + 0x1.921fb6p+0f    // pi/2 + r
-                       : (-0x1.777a5cp-25f - r) + 0x1.921fb6p+0f;   // pi/2 - r
-  else if (neg) r = (-0x1.777a5cp-24f - r) + 0x1.921fb6p+1f;       // pi - r
+  if (fabsf(y) > fabsf(x)) r = neg ? (-0x1.777a5cp-25f + r) + 0x1.921fb6p+0f    // pi/2 + r
+                                   : (-0x1.777a5cp-25f - r) + 0x1.921fb6p+0f;   // pi/2 - r
+  else if (neg) r = (-0x1.777a5cp-24f - r) + 0x1.921fb6p+1f;                   // pi - r
   return copysignf(r, y);
+}
+__device__ __forceinline__ float map_atan2f(float y, float x) {
+  return map_atan2_finish(map_atan_poly(map_atan2_arg(y, x)), y, x);
+}
+
+// ------------------------------------------------------------------ sine / cosine (float)
+
+// Sine and cosine of float32 arguments, at most 1.6 ulp from the correctly
+// rounded value (checked against double-precision sin/cos on 100 M samples,
+// including the floats nearest to multiples of pi/2). Method (Cody and Waite):
+// x = j*pi/2 + r with j = rint(x*2/pi) (added to 1.5*2^23 so that the rounding
+// gives the integer and its low bits the quadrant) and r = x - j*(P1 + P2 + P3),
+// pi/2 split into three floats, each truncated so all three are positive (the
+// first product is exact for |x| <= 65536); then sin(r) = r + r*s*S(s) and
+// cos(r) = 1 + s*C(s), s = r*r, with S (degree 2) and C (degree 3) fitted on
+// [0, pi/4] by iteratively reweighted least squares (Lawson) for minimum
+// relative error; the quadrant swaps and negates. Larger |x| (and infinities)
+// go to the CUDA library's functions, which reduce with more bits of 2/pi.
+#define MAP_2OPI 0x1.45f306p-1f
+#define MAP_PIO2_1 0x1.921fb4p+0f
+#define MAP_PIO2_2 0x1.4442d0p-24f
+#define MAP_PIO2_3 0x1.84698ap-48f
+#define MAP_RINT 0x1.8p23f
+#define MAP_TRIG_BOUND 65536.0f
+#define MAP_SIN_1 -0x1.555546p-3f
+#define MAP_SIN_2 0x1.11073ap-7f
+#define MAP_SIN_3 -0x1.9943e2p-13f
+#define MAP_COS_1 -0x1.0p-1f
+#define MAP_COS_2 0x1.55553cp-5f
+#define MAP_COS_3 -0x1.6c07f2p-10f
+#define MAP_COS_4 0x1.99169cp-16f
+
+// v = r + r*s*S(s) for |r| <= pi/4 is sin r; a zero keeps the sign of r (sin(-0) = -0)
+__device__ __forceinline__ float map_sin_sign(float v, float r) {
+  return __uint_as_float(__float_as_uint(v) | (__float_as_uint(r) & 0x80000000u));
+}
+// quadrant q: sin x = (q odd ? cos r : sin r), negated when bit 1 of q is set;
+// cos x = (q odd ? sin r : cos r), negated when bit 1 of q + 1 is set
+__device__ __forceinline__ float map_quadrant_sin(u32 q, float sr, float cr) {
+  const float v = (q & 1u) ? cr : sr;
+  return __uint_as_float(__float_as_uint(v) ^ ((q << 30) & 0x80000000u));
+}
+__device__ __forceinline__ float map_quadrant_cos(u32 q, float sr, float cr) {
+  const float v = (q & 1u) ? sr : cr;
+  return __uint_as_float(__float_as_uint(v) ^ (((q + 1u) << 30) & 0x80000000u));
+}
+// reduced argument and quadrant of |x| <= MAP_TRIG_BOUND; sin r and cos r
+__device__ __forceinline__ void map_sincos_reduced(float x, u32 &q, float &sr, float &cr) {
+  const float t = fmaf(x, MAP_2OPI, MAP_RINT);
+  const float j = t - MAP_RINT;
+  q = __float_as_uint(t);
+  float r = fmaf(j, -MAP_PIO2_1, x);
+  r = fmaf(j, -MAP_PIO2_2, r);
+  r = fmaf(j, -MAP_PIO2_3, r);
+  const float s = r * r;
+  float p = fmaf(s, MAP_SIN_3, MAP_SIN_2);
+  p = fmaf(s, p, MAP_SIN_1);
+  sr = map_sin_sign(fmaf(r * s, p, r), r);
+  float c = fmaf(s, MAP_COS_4, MAP_COS_3);
+  c = fmaf(s, c, MAP_COS_2);
+  c = fmaf(s, c, MAP_COS_1);
+  cr = fmaf(s, c, 1.0f);
+}
+__device__ __forceinline__ void map_sincosf(float x, float *sp, float *cp) {
+  if (fabsf(x) > MAP_TRIG_BOUND) { sincosf(x, sp, cp); return; }
+  u32 q;
+  float sr, cr;
+  map_sincos_reduced(x, q, sr, cr);
+  *sp = map_quadrant_sin(q, sr, cr);
+  *cp = map_quadrant_cos(q, sr, cr);
+}
+__device__ __forceinline__ float map_sinf(float x) {
+  if (fabsf(x) > MAP_TRIG_BOUND) return sinf(x);
+  u32 q;
+  float sr, cr;
+  map_sincos_reduced(x, q, sr, cr);
+  return map_quadrant_sin(q, sr, cr);
+}
+__device__ __forceinline__ float map_cosf(float x) {
+  if (fabsf(x) > MAP_TRIG_BOUND) return cosf(x);
+  u32 q;
+  float sr, cr;
+  map_sincos_reduced(x, q, sr, cr);
+  return map_quadrant_cos(q, sr, cr);
+}
+
+// ------------------------------------------------------------------ paired cells
+
+// PR<T>: the values of two cells of one column (rows y and y + 1) carried
+// together, so that float work of both cells issues as Blackwell's packed
+// f32x2 instructions (one issue slot for two IEEE operations). Every operation
+// applies to each lane with exactly the scalar semantics: the C++ usual
+// arithmetic conversions, then per-lane IEEE round-to-nearest (addition,
+// subtraction and multiplication of floats are packed; division and the other
+// operations run per lane). Generated code spells every conversion as PR<T>(...).
+template <class T> struct map_scalar {};
+#define MAP_SCALAR(T) template <> struct map_scalar<T> { typedef T type; };
+MAP_SCALAR(bool) MAP_SCALAR(char) MAP_SCALAR(signed char) MAP_SCALAR(unsigned char) MAP_SCALAR(short)
+MAP_SCALAR(unsigned short) MAP_SCALAR(int) MAP_SCALAR(unsigned) MAP_SCALAR(long) MAP_SCALAR(unsigned long)
+MAP_SCALAR(long long) MAP_SCALAR(unsigned long long) MAP_SCALAR(float) MAP_SCALAR(double)
+#undef MAP_SCALAR
+
+template <class T> struct PR {
+  T a, b;
+  __device__ __forceinline__ PR() {}
+  __device__ __forceinline__ PR(T a_, T b_) : a(a_), b(b_) {}
+  template <class U> __device__ __forceinline__ explicit PR(const PR<U> &o) : a((T)o.a), b((T)o.b) {}
+  template <class U, class = typename map_scalar<U>::type> __device__ __forceinline__ explicit PR(U s) : a((T)s), b((T)s) {}
+};
+
+template <class T> __device__ __forceinline__ T lane0(const PR<T> &p) { return p.a; }
+template <class T> __device__ __forceinline__ T lane1(const PR<T> &p) { return p.b; }
+template <class T, class = typename map_scalar<T>::type> __device__ __forceinline__ T lane0(const T &s) { return s; }
+template <class T, class = typename map_scalar<T>::type> __device__ __forceinline__ T lane1(const T &s) { return s; }
+
+__device__ __forceinline__ float2 pr_f2(const PR<float> &x) { return make_float2(x.a, x.b); }
+__device__ __forceinline__ PR<float> pr_of(float2 v) { return PR<float>(v.x, v.y); }
+__device__ __forceinline__ float2 f2_of(float c) { return make_float2(c, c); }
+
+// lane-wise arithmetic on operands already converted to their common type
+template <class T> __device__ __forceinline__ PR<T> pr_add(const PR<T> &x, const PR<T> &y) { return PR<T>(x.a + y.a, x.b + y.b); }
+template <class T> __device__ __forceinline__ PR<T> pr_sub(const PR<T> &x, const PR<T> &y) { return PR<T>(x.a - y.a, x.b - y.b); }
+template <class T> __device__ __forceinline__ PR<T> pr_mul(const PR<T> &x, const PR<T> &y) { return PR<T>(x.a * y.a, x.b * y.b); }
+template <class T> __device__ __forceinline__ PR<T> pr_div(const PR<T> &x, const PR<T> &y) { return PR<T>(x.a / y.a, x.b / y.b); }
+template <class T> __device__ __forceinline__ PR<T> pr_mod(const PR<T> &x, const PR<T> &y) { return PR<T>(x.a % y.a, x.b % y.b); }
+// The device compiler fuses a packed multiply into a packed add that consumes
+// it (also when the add is written as fma(x, 1, y)), whatever the fmad setting:
+// such a sum would be rounded once instead of twice. Generated code therefore
+// adds an inexact packed product with pr_add_lanes (scalar adds, which are not
+// fused); x - y = fma(y, -1, x) keeps both roundings for products on either side
+// (both checked on B200).
+__device__ __forceinline__ PR<float> pr_add(const PR<float> &x, const PR<float> &y) {
+  return pr_of(__fadd2_rn(pr_f2(x), pr_f2(y)));
+}
+template <class A, class B> __device__ __forceinline__ PR<float> pr_add_lanes(const A &x, const B &y) {
+  return PR<float>((float)lane0(x) + (float)lane0(y), (float)lane1(x) + (float)lane1(y));
+}
+__device__ __forceinline__ PR<float> pr_sub(const PR<float> &x, const PR<float> &y) {
+  return pr_of(__ffma2_rn(pr_f2(y), f2_of(-1.0f), pr_f2(x)));
+}
+__device__ __forceinline__ PR<float> pr_mul(const PR<float> &x, const PR<float> &y) {
+  return pr_of(__fmul2_rn(pr_f2(x), pr_f2(y)));
+}
+
+#define MAP_PR_ARITH(OP, FN)                                                                                   \
+  template <class A, class B>                                                                                  \
+  __device__ __forceinline__ auto operator OP(const PR<A> &x, const PR<B> &y)->PR<decltype(x.a OP y.a)> {     \
+    typedef decltype(x.a OP y.a) C;                                                                            \
+    return FN(PR<C>(x), PR<C>(y));                                                                             \
+  }                                                                                                            \
+  template <class A, class B, class = typename map_scalar<B>::type>                                            \
+  __device__ __forceinline__ auto operator OP(const PR<A> &x, const B &y)->PR<decltype(x.a OP y)> {           \
+    typedef decltype(x.a OP y) C;                                                                              \
+    return FN(PR<C>(x), PR<C>(y));                                                                             \
+  }                                                                                                            \
+  template <class A, class B, class = typename map_scalar<A>::type>                                            \
+  __device__ __forceinline__ auto operator OP(const A &x, const PR<B> &y)->PR<decltype(x OP y.a)> {           \
+    typedef decltype(x OP y.a) C;                                                                              \
+    return FN(PR<C>(x), PR<C>(y));                                                                             \
+  }
+MAP_PR_ARITH(+, pr_add) MAP_PR_ARITH(-, pr_sub) MAP_PR_ARITH(*, pr_mul) MAP_PR_ARITH(/, pr_div) MAP_PR_ARITH(%, pr_mod)
+#undef MAP_PR_ARITH
+
+// comparisons, logical, bitwise and shift operators: per lane, C++ result types
+#define MAP_PR_LANE(OP)                                                                                        \
+  template <class A, class B>                                                                                  \
+  __device__ __forceinline__ auto operator OP(const PR<A> &x, const PR<B> &y)->PR<decltype(x.a OP y.a)> {     \
+    return PR<decltype(x.a OP y.a)>(x.a OP y.a, x.b OP y.b);                                                   \
+  }                                                                                                            \
+  template <class A, class B, class = typename map_scalar<B>::type>                                            \
+  __device__ __forceinline__ auto operator OP(const PR<A> &x, const B &y)->PR<decltype(x.a OP y)> {           \
+    return PR<decltype(x.a OP y)>(x.a OP y, x.b OP y);                                                         \
+  }                                                                                                            \
+  template <class A, class B, class = typename map_scalar<A>::type>                                            \
+  __device__ __forceinline__ auto operator OP(const A &x, const PR<B> &y)->PR<decltype(x OP y.a)> {           \
+    return PR<decltype(x OP y.a)>(x OP y.a, x OP y.b);                                                         \
+  }
+MAP_PR_LANE(==) MAP_PR_LANE(!=) MAP_PR_LANE(<) MAP_PR_LANE(>) MAP_PR_LANE(<=) MAP_PR_LANE(>=)
+MAP_PR_LANE(&&) MAP_PR_LANE(||) MAP_PR_LANE(&) MAP_PR_LANE(|) MAP_PR_LANE(^) MAP_PR_LANE(<<) MAP_PR_LANE(>>)
+#undef MAP_PR_LANE
+
+template <class A> __device__ __forceinline__ auto operator+(const PR<A> &x)->PR<decltype(+x.a)> {
+  return PR<decltype(+x.a)>(+x.a, +x.b);
+}
+template <class A> __device__ __forceinline__ auto operator-(const PR<A> &x)->PR<decltype(-x.a)> {
+  return PR<decltype(-x.a)>(-x.a, -x.b);
+}
+// -x = x * -1 exactly (the sign flips, zeros included)
+__device__ __forceinline__ PR<float> operator-(const PR<float> &x) { return pr_of(__fmul2_rn(pr_f2(x), f2_of(-1.0f))); }
+template <class A> __device__ __forceinline__ PR<bool> operator!(const PR<A> &x) { return PR<bool>(!x.a, !x.b); }
+template <class A> __device__ __forceinline__ auto operator~(const PR<A> &x)->PR<decltype(~x.a)> {
+  return PR<decltype(~x.a)>(~x.a, ~x.b);
+}
+
+// c ? x : y per lane (the condition a pair or one scalar for both lanes)
+template <class C, class A, class B>
+__device__ __forceinline__ auto psel(const PR<C> &c, const A &x, const B &y)->PR<decltype(true ? lane0(x) : lane0(y))> {
+  typedef decltype(true ? lane0(x) : lane0(y)) R;
+  return PR<R>(c.a ? (R)lane0(x) : (R)lane0(y), c.b ? (R)lane1(x) : (R)lane1(y));
+}
+template <class C, class A, class B, class = typename map_scalar<C>::type>
+__device__ __forceinline__ auto psel(const C &c, const A &x, const B &y)->PR<decltype(true ? lane0(x) : lane0(y))> {
+  typedef decltype(true ? lane0(x) : lane0(y)) R;
+  return PR<R>(c ? (R)lane0(x) : (R)lane0(y), c ? (R)lane1(x) : (R)lane1(y));
+}
+
+// a + t*w with w == 0 (the product is an exact signed zero, so this equals the
+// separate multiply and add)
+__device__ __forceinline__ PR<float> pr_fmaf(const PR<float> &t, float w, const PR<float> &a) {
+  return pr_of(__ffma2_rn(pr_f2(t), f2_of(w), pr_f2(a)));
+}
+
+// library functions of the device math API, per lane. They take new names
+// (pr_sqrtf, ...): overloading the library's own names changes which
+// implementation the device compiler picks for them (sqrtf stops being the
+// correctly rounded square root).
+#define MAP_PR_F1(fn) \
+  __device__ __forceinline__ PR<float> pr_##fn(const PR<float> &x) { return PR<float>(fn(x.a), fn(x.b)); }
+MAP_PR_F1(sinf) MAP_PR_F1(cosf) MAP_PR_F1(tanf) MAP_PR_F1(asinf) MAP_PR_F1(acosf) MAP_PR_F1(atanf)
+MAP_PR_F1(sinhf) MAP_PR_F1(coshf) MAP_PR_F1(tanhf) MAP_PR_F1(asinhf) MAP_PR_F1(acoshf) MAP_PR_F1(atanhf)
+MAP_PR_F1(expf) MAP_PR_F1(exp2f) MAP_PR_F1(exp10f) MAP_PR_F1(logf) MAP_PR_F1(log2f) MAP_PR_F1(log10f)
+MAP_PR_F1(sqrtf) MAP_PR_F1(cbrtf) MAP_PR_F1(fabsf) MAP_PR_F1(ceilf) MAP_PR_F1(floorf) MAP_PR_F1(truncf)
+MAP_PR_F1(roundf)
+#undef MAP_PR_F1
+#define MAP_PR_F2(fn)                                                                   \
+  __device__ __forceinline__ PR<float> pr_##fn(const PR<float> &x, const PR<float> &y) { \
+    return PR<float>(fn(x.a, y.a), fn(x.b, y.b));                                       \
+  }
+MAP_PR_F2(powf) MAP_PR_F2(hypotf) MAP_PR_F2(fmodf) MAP_PR_F2(atan2f)
+#undef MAP_PR_F2
+
+// the engine's own atan2, sin and cos on pairs: the same operations as the
+// scalar forms above (bit-identical lanes), the polynomials packed
+__device__ __forceinline__ PR<float> map_atan_poly(const PR<float> &t) {
+  const float2 T = pr_f2(t);
+  const float2 s = __fmul2_rn(T, T);
+  float2 q = f2_of(MAP_ATAN_Q0);
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q1));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q2));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q3));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q4));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q5));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q6));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q7));
+  q = __ffma2_rn(q, s, f2_of(MAP_ATAN_Q8));
+  return pr_of(__ffma2_rn(__fmul2_rn(T, s), q, T));
+}
+__device__ __forceinline__ PR<float> map_atan2f(const PR<float> &y, const PR<float> &x) {
+  const PR<float> r = map_atan_poly(PR<float>(map_atan2_arg(y.a, x.a), map_atan2_arg(y.b, x.b)));
+  return PR<float>(map_atan2_finish(r.a, y.a, x.a), map_atan2_finish(r.b, y.b, x.b));
+}
+__device__ __forceinline__ void map_sincos_reduced(const PR<float> &x, u32 &qa, u32 &qb, PR<float> &sr, PR<float> &cr) {
+  const float2 X = pr_f2(x);
+  const float2 t = __ffma2_rn(X, f2_of(MAP_2OPI), f2_of(MAP_RINT));
+  const float2 j = __ffma2_rn(t, f2_of(1.0f), f2_of(-MAP_RINT));
+  qa = __float_as_uint(t.x);
+  qb = __float_as_uint(t.y);
+  float2 r = __ffma2_rn(j, f2_of(-MAP_PIO2_1), X);
+  r = __ffma2_rn(j, f2_of(-MAP_PIO2_2), r);
+  r = __ffma2_rn(j, f2_of(-MAP_PIO2_3), r);
+  const float2 s = __fmul2_rn(r, r);
+  float2 p = __ffma2_rn(s, f2_of(MAP_SIN_3), f2_of(MAP_SIN_2));
+  p = __ffma2_rn(s, p, f2_of(MAP_SIN_1));
+  const float2 v = __ffma2_rn(__fmul2_rn(r, s), p, r);
+  sr = PR<float>(map_sin_sign(v.x, r.x), map_sin_sign(v.y, r.y));
+  float2 c = __ffma2_rn(s, f2_of(MAP_COS_4), f2_of(MAP_COS_3));
+  c = __ffma2_rn(s, c, f2_of(MAP_COS_2));
+  c = __ffma2_rn(s, c, f2_of(MAP_COS_1));
+  cr = pr_of(__ffma2_rn(s, c, f2_of(1.0f)));
+}
+__device__ __forceinline__ bool map_trig_far(const PR<float> &x) {
+  return fabsf(x.a) > MAP_TRIG_BOUND || fabsf(x.b) > MAP_TRIG_BOUND;
+}
+__device__ __forceinline__ void map_sincosf(const PR<float> &x, PR<float> *sp, PR<float> *cp) {
+  if (map_trig_far(x)) {
+    map_sincosf(x.a, &sp->a, &cp->a);
+    map_sincosf(x.b, &sp->b, &cp->b);
+    return;
+  }
+  u32 qa, qb;
+  PR<float> sr, cr;
+  map_sincos_reduced(x, qa, qb, sr, cr);
+  *sp = PR<float>(map_quadrant_sin(qa, sr.a, cr.a), map_quadrant_sin(qb, sr.b, cr.b));
+  *cp = PR<float>(map_quadrant_cos(qa, sr.a, cr.a), map_quadrant_cos(qb, sr.b, cr.b));
+}
+__device__ __forceinline__ PR<float> map_sinf(const PR<float> &x) {
+  if (map_trig_far(x)) return PR<float>(map_sinf(x.a), map_sinf(x.b));
+  u32 qa, qb;
+  PR<float> sr, cr;
+  map_sincos_reduced(x, qa, qb, sr, cr);
+  return PR<float>(map_quadrant_sin(qa, sr.a, cr.a), map_quadrant_sin(qb, sr.b, cr.b));
+}
+__device__ __forceinline__ PR<float> map_cosf(const PR<float> &x) {
+  if (map_trig_far(x)) return PR<float>(map_cosf(x.a), map_cosf(x.b));
+  u32 qa, qb;
+  PR<float> sr, cr;
+  map_sincos_reduced(x, qa, qb, sr, cr);
+  return PR<float>(map_quadrant_cos(qa, sr.a, cr.a), map_quadrant_cos(qb, sr.b, cr.b));
 }
 
 // ------------------------------------------------------------------ border rule
@@ -161,6 +475,10 @@ template <class T> struct GatherTap {
     if (!focal_src(*g, x, y, dx, dy, sx, sy)) return (T)0;
     return ldr<T>(r, sx, sy);
   }
+  // the same tap of the cells (x, y) and (x, y + 1)
+  __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
+    return PR<T>(tap(x, y, lx, ly, dx, dy), tap(x, y + 1, lx, ly + 1, dx, dy));
+  }
 };
 
 // Focal tap served from a tile staged in shared memory (interior tiles).
@@ -169,6 +487,9 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   const T *s;
   __device__ __forceinline__ T tap(int x, int y, int lx, int ly, int dx, int dy) const {
     return s[(ly + HY + dy) * SW + (lx + PX + dx)];
+  }
+  __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
+    return PR<T>(s[(ly + HY + dy) * SW + (lx + PX + dx)], s[(ly + 1 + HY + dy) * SW + (lx + PX + dx)]);
   }
 };
 
@@ -262,6 +583,15 @@ template <class T> struct RedOp<3, T> { __device__ static T f(T a, T b) { return
 template <class T> struct RedOp<4, T> { __device__ static T f(T a, T b) { return (T)(a | b); } };
 template <class T> struct RedOp<6, T> { __device__ static T f(T a, T b) { return red_max<T>(a, b); } };
 template <class T> struct RedOp<7, T> { __device__ static T f(T a, T b) { return red_min<T>(a, b); } };
+// pairs: per lane (sums and products go through the pair operators)
+template <class T> __device__ __forceinline__ PR<T> red_max(const PR<T> &a, const PR<T> &b) {
+  return PR<T>(red_max<T>(a.a, b.a), red_max<T>(a.b, b.b));
+}
+template <class T> __device__ __forceinline__ PR<T> red_min(const PR<T> &a, const PR<T> &b) {
+  return PR<T>(red_min<T>(a.a, b.a), red_min<T>(a.b, b.b));
+}
+template <class T> struct RedOp<6, PR<T>> { __device__ static PR<T> f(PR<T> a, PR<T> b) { return red_max(a, b); } };
+template <class T> struct RedOp<7, PR<T>> { __device__ static PR<T> f(PR<T> a, PR<T> b) { return red_min(a, b); } };
 
 // Reinterprets the bytes of a value as another type of at most 8 bytes.
 template <class To, class From> __device__ __forceinline__ To bit_cast8(From v) {

@@ -723,6 +723,16 @@ def get_stream_rows():
     return _lib.ma_getStreamRows()
 
 
+def set_paired_cells(on):
+    """Two cells per thread step on packed f32x2 instructions in float focal groups
+    (bit-identical results); False computes one cell at a time."""
+    _lib.ma_setPairedCells(1 if on else 0)
+
+
+def get_paired_cells():
+    return bool(_lib.ma_getPairedCells())
+
+
 def last_band_count():
     return _lib.ma_lastBandCount()
 
@@ -929,6 +939,8 @@ _sig('ma_lastGroupCount', [], ct.c_int, check=False)
 _sig('ma_lastBandCount', [], ct.c_int, check=False)
 _sig('ma_setStreamRows', [ct.c_int], None)
 _sig('ma_getStreamRows', [], ct.c_int, check=False)
+_sig('ma_setPairedCells', [ct.c_int], None)
+_sig('ma_getPairedCells', [], ct.c_int, check=False)
 _sig('ma_compileOnly', [ct.POINTER(Node), ct.c_int, ct.c_int], ct.c_int)
 _sig('ma_describeGroups', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_generatedSource', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)

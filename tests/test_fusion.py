@@ -140,3 +140,24 @@ def test_sin_cos_pairs_share_sincosf(M):
     src = M.generated_source(M.sin(x) * 2.0 + M.cos(x))
     import re
     assert "sincosf(" in src and not re.search(r"\bsinf\(", src) and not re.search(r"\bcosf\(", src)
+
+
+def test_paired_cells_codegen(M):
+    """Float focal groups get the two-rows-per-step form (focal_cell2) unless it is
+    switched off; integer focal groups (life) keep one cell per step. Both forms
+    compile."""
+    from map_b200 import workloads as W
+    dem = M.from_numpy(np.zeros((64, 64), np.float32), bs=[32, 32])
+    try:
+        hs = W.hillshade(dem)
+        assert "focal_cell2" in M.generated_source(hs)
+        assert M.compile_only(hs) == 1
+        M.set_paired_cells(False)
+        assert not M.get_paired_cells()
+        hs = W.hillshade(dem)
+        assert "focal_cell2" not in M.generated_source(hs)
+        assert M.compile_only(hs) == 1
+    finally:
+        M.set_paired_cells(True)
+    grid = M.from_numpy(np.zeros((64, 64), np.uint8), bs=[32, 32])
+    assert "focal_cell2" not in M.generated_source(W.life(grid, 1))
