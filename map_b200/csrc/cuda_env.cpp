@@ -16,6 +16,7 @@
 #include <map>
 #include <mutex>
 #include <sstream>
+#include <unordered_map>
 
 namespace mapb {
 
@@ -49,6 +50,10 @@ std::mutex g_mtx;
 std::map<std::string, std::vector<unsigned char>> g_cubins;   // key: source hash
 std::map<std::string, CUmodule> g_modules;                   // key: source hash
 std::map<std::string, KernelHandle> g_kernels;               // key: source hash + name
+// Launch-path lookup by kernel name (names carry a hash of their group's
+// source) and source length, so a launch does not hash the source again.
+struct FastEntry { size_t source_size; KernelHandle h; };
+std::unordered_map<std::string, FastEntry> g_fast;
 
 std::string hash_hex(const std::string &s) {
   uint64_t h = 1469598103934665603ull;
@@ -60,14 +65,18 @@ std::string hash_hex(const std::string &s) {
 
 const char *kNvrtcOpts[] = {"--gpu-architecture=sm_100a", "-std=c++17", "--fmad=false", "-lineinfo", "-DMAPB_NVRTC=1"};
 
-std::string options_key() {
-  std::string k;
-  for (const char *o : kNvrtcOpts) k += std::string(o) + " ";
-  int maj = 0, min = 0;
-  nvrtcVersion(&maj, &min);
-  k += std::to_string(maj) + "." + std::to_string(min);
-  for (auto &h : kSkeletonHeaders) k += hash_hex(h.source);
-  return k;
+// compile options, NVRTC version and skeleton header hashes (fixed for the process)
+const std::string &options_key() {
+  static const std::string key = [] {
+    std::string k;
+    for (const char *o : kNvrtcOpts) k += std::string(o) + " ";
+    int maj = 0, min = 0;
+    nvrtcVersion(&maj, &min);
+    k += std::to_string(maj) + "." + std::to_string(min);
+    for (auto &h : kSkeletonHeaders) k += hash_hex(h.source);
+    return k;
+  }();
+  return key;
 }
 
 void drv_check(CUresult r, const char *what) {
@@ -203,11 +212,20 @@ void CudaEnv::ensure_device() {
 
 KernelHandle CudaEnv::kernel(const std::string &source, const std::string &name, size_t dyn_smem) {
   ensure_device();
+  {
+    std::lock_guard<std::mutex> lk(g_mtx);
+    auto f = g_fast.find(name);
+    if (f != g_fast.end() && f->second.source_size == source.size() && f->second.h.max_dyn_smem >= dyn_smem)
+      return f->second.h;
+  }
   const auto &cubin = compile(source);
   std::lock_guard<std::mutex> lk(g_mtx);
   const std::string key = hash_hex(source) + "/" + name;
   auto it = g_kernels.find(key);
-  if (it != g_kernels.end() && it->second.max_dyn_smem >= dyn_smem) return it->second;
+  if (it != g_kernels.end() && it->second.max_dyn_smem >= dyn_smem) {
+    g_fast[name] = FastEntry{source.size(), it->second};
+    return it->second;
+  }
   const std::string mkey = hash_hex(source);
   CUmodule mod;
   auto mit = g_modules.find(mkey);
@@ -226,6 +244,7 @@ KernelHandle CudaEnv::kernel(const std::string &source, const std::string &name,
               "cuFuncSetAttribute");
   h.max_dyn_smem = dyn_smem;
   g_kernels[key] = h;
+  g_fast[name] = FastEntry{source.size(), h};
   return h;
 }
 
