@@ -933,8 +933,21 @@ static std::string gen_radial(Gen &G) {
   const std::string nt = var_literal(reduction_neutral(scan->op, scan->meta.dtype));
   std::ostringstream s;
   s << "#include \"map_scan.cuh\"\n" << G.args_struct(0, false);
-  s << "__device__ __forceinline__ " << T << " radial_cell(const Args &a, int x, int y, " << T << " lit, bool observer) {\n"
-    << G.center_loads(false);
+  // the centre inputs of one cell, loaded ahead of its computation
+  s << "struct In {\n";
+  for (Node *p : P.in_rasters)
+    if (G.center_read.count(p)) s << "  " << G.T(p) << " i" << G.rin.at(p) << ";\n";
+  s << "  int dummy;\n};\n";
+  s << "__device__ __forceinline__ void radial_load(const Args &a, In &in, int x, int y) {\n";
+  for (Node *p : P.in_rasters)
+    if (G.center_read.count(p)) {
+      const int k = G.rin.at(p);
+      s << "  in.i" << k << " = ldr<" << G.T(p) << ">(a.in[" << k << "], x, y);\n";
+    }
+  s << "}\n";
+  s << "__device__ __forceinline__ " << T << " radial_cell(const Args &a, const In &in, int x, int y, " << T
+    << " lit, bool observer) {\n"
+    << G.center_loads(true);
   for (Node *n : G.g.nodes) {
     if (n == scan) {
       s << "    " << T << " " << v << " = lit;\n"
@@ -950,7 +963,11 @@ static std::string gen_radial(Gen &G) {
   // aux[0] start x, aux[1] start y, aux[2] last front (or -1 for all).
   // The previous front lives in shared memory (two buffers of the launch's
   // dynamic size / 2) when it fits, else it is re-read from the scan's output.
-  s << "__device__ __forceinline__ void radial_run(const Args &a, int octant) {\n"
+  // A thread takes the cells d1 = base + threadIdx.x + k * blockDim.x of a front,
+  // RADIAL_K at a time: it issues the input loads of all of them first, so one
+  // memory latency is paid per chunk of a front rather than per cell.
+  s << "#define RADIAL_K 8\n"
+    << "__device__ __forceinline__ void radial_run(const Args &a, int octant) {\n"
     << "  extern __shared__ __align__(16) unsigned char radial_smem[];\n"
     << "  const int sx = (int)a.aux[0], sy = (int)a.aux[1];\n"
     << "  const long long lim = (long long)a.aux[2];\n"
@@ -967,24 +984,37 @@ static std::string gen_radial(Gen &G) {
     << "  " << T << " *prev = cap > eq ? (" << T << " *)radial_smem : nullptr;\n"
     << "  " << T << " *cur = prev ? prev + cap : nullptr;\n"
     << "  if (threadIdx.x == 0) {\n"
-    << "    const " << T << " v0 = radial_cell(a, sx, sy, (" << T << ")0, true);\n"
+    << "    In in0;\n"
+    << "    radial_load(a, in0, sx, sy);\n"
+    << "    const " << T << " v0 = radial_cell(a, in0, sx, sy, (" << T << ")0, true);\n"
     << "    if (prev) prev[0] = v0;\n"
     << "  }\n"
     << "  __syncthreads();\n"
     << "  for (int d0 = 1; d0 <= dmax; ++d0) {\n"
     << "    const int d1max = d0 < eq ? d0 : eq;\n"
-    << "    for (int d1 = threadIdx.x; d1 <= d1max; d1 += blockDim.x) {\n"
-    << "      const int x = sx + p0 * d0 + q0 * d1, y = sy + p1 * d0 + q1 * d1;\n"
-    << "      " << T << " va = (" << T << ")0, vb = (" << T << ")0;\n"
-    << "      if (prev) {\n"
-    << "        if (d1 <= d0 - 1) va = prev[d1];\n"
-    << "        if (d1 >= 1) vb = prev[d1 - 1];\n"
-    << "      } else {\n"
-    << "        if (d1 <= d0 - 1) va = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * d1, sy + p1 * (d0 - 1) + q1 * d1);\n"
-    << "        if (d1 >= 1) vb = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * (d1 - 1), sy + p1 * (d0 - 1) + q1 * (d1 - 1));\n"
+    << "    for (int base = 0; base <= d1max; base += RADIAL_K * (int)blockDim.x) {\n"
+    << "      In in[RADIAL_K];\n"
+    << "#pragma unroll\n"
+    << "      for (int k = 0; k < RADIAL_K; ++k) {\n"
+    << "        const int d1 = base + (int)threadIdx.x + k * (int)blockDim.x;\n"
+    << "        if (d1 <= d1max) radial_load(a, in[k], sx + p0 * d0 + q0 * d1, sy + p1 * d0 + q1 * d1);\n"
     << "      }\n"
-    << "      const " << T << " vv = radial_cell(a, x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
-    << "      if (cur) cur[d1] = vv;\n"
+    << "#pragma unroll\n"
+    << "      for (int k = 0; k < RADIAL_K; ++k) {\n"
+    << "        const int d1 = base + (int)threadIdx.x + k * (int)blockDim.x;\n"
+    << "        if (d1 > d1max) break;\n"
+    << "        const int x = sx + p0 * d0 + q0 * d1, y = sy + p1 * d0 + q1 * d1;\n"
+    << "        " << T << " va = (" << T << ")0, vb = (" << T << ")0;\n"
+    << "        if (prev) {\n"
+    << "          if (d1 <= d0 - 1) va = prev[d1];\n"
+    << "          if (d1 >= 1) vb = prev[d1 - 1];\n"
+    << "        } else {\n"
+    << "          if (d1 <= d0 - 1) va = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * d1, sy + p1 * (d0 - 1) + q1 * d1);\n"
+    << "          if (d1 >= 1) vb = ld_coherent<" << T << ">(R, sx + p0 * (d0 - 1) + q0 * (d1 - 1), sy + p1 * (d0 - 1) + q1 * (d1 - 1));\n"
+    << "        }\n"
+    << "        const " << T << " vv = radial_cell(a, in[k], x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
+    << "        if (cur) cur[d1] = vv;\n"
+    << "      }\n"
     << "    }\n"
     << "    __syncthreads();\n"
     << "    " << T << " *t = prev;\n"
