@@ -1115,15 +1115,26 @@ static std::string gen_spread(Gen &G) {
     << "}\n";
   // Small rasters: one CTA runs a topological (Kahn) sweep, frontier by frontier
   // with block barriers (aux[1], aux[2]: frontier lists of N cells).
-  s << "__device__ __forceinline__ void spread_kahn(const Args &a) {\n"
+  // Frontier entries pack a cell index (below 2^24) with its D8 code, fetched
+  // by the thread that completes the cell while its in-degree atomic is in
+  // flight, so a round reads no direction; the first KAHN_SMEM entries of a
+  // frontier live in shared memory, the rest in the global lists.
+  s << "#define KAHN_SMEM 4096\n"
+    << "__device__ __forceinline__ void kahn_put(u32 *sf, u32 *gf, int i, u32 e) {\n"
+    << "  if (i < KAHN_SMEM) sf[i] = e; else gf[i] = e;\n"
+    << "}\n"
+    << "__device__ __forceinline__ void spread_kahn(const Args &a) {\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  const s64 N = (s64)W * H;\n"
     << "  s32 *indeg = (s32 *)a.aux[0];\n"
-    << "  s32 *fa = (s32 *)a.aux[1], *fb = (s32 *)a.aux[2];\n"
+    << "  u32 *fa = (u32 *)a.aux[1], *fb = (u32 *)a.aux[2];\n"
     << "  const long long limit = (long long)a.aux[3];\n"
     << "  const RasterArg D = a.in[" << kd << "];\n"
     << "  const RasterArg O = a.out[" << ko << "];\n"
     << "  __shared__ int n_cur, n_next;\n"
+    << "  __shared__ u32 kf[2][KAHN_SMEM];\n"
+    << "  if (N >= ((s64)1 << 24)) { if (threadIdx.x == 0) skel_fail(a.err, ERR_BAD_LAUNCH); return; }\n"
+    << "  u32 *sa = kf[0], *sb = kf[1];\n"
     << "  if (threadIdx.x == 0) { n_cur = 0; n_next = 0; }\n"
     << "  __syncthreads();\n"
     << "  for (s64 c = threadIdx.x; c < N; c += blockDim.x) {\n"
@@ -1136,7 +1147,7 @@ static std::string gen_spread(Gen &G) {
     << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) cnt++;\n"
     << "    }\n"
     << "    indeg[c] = cnt;\n"
-    << "    if (cnt == 0) fa[atomicAdd(&n_cur, 1)] = (s32)c;\n"
+    << "    if (cnt == 0) kahn_put(sa, fa, atomicAdd(&n_cur, 1), (u32)(((u64)c << 8) | ldr<u8>(D, x, y)));\n"
     << "  }\n"
     << "  __syncthreads();\n"
     << "  for (long long it = 0;; ++it) {\n"
@@ -1144,17 +1155,23 @@ static std::string gen_spread(Gen &G) {
     << "    if (n == 0) break;\n"
     << "    if (it > limit) { if (threadIdx.x == 0) skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
     << "    for (int i = threadIdx.x; i < n; i += blockDim.x) {\n"
-    << "      const s32 c = fa[i];\n"
+    << "      const u32 e = i < KAHN_SMEM ? sa[i] : fa[i];\n"
+    << "      const int c = (int)(e >> 8);\n"
+    << "      const int d = d8_index((u8)(e & 255));\n"
+    << "      if (d < 0) continue;\n"
     << "      const int x = c % W, y = c / W;\n"
-    << "      const s64 dn = d8_down(D, W, H, x, y);\n"
-    << "      if (dn < 0) continue;\n"
+    << "      const int nx = x + d8_dx(d), ny = y + d8_dy(d);\n"
+    << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+    << "      const int dn = ny * W + nx;\n"
     << "      const " << T << " v = (" << T << ")(ld_coherent<" << T << ">(O, x, y) + water_at(a, x, y));\n"
-    << "      atomic_add_any(cell_ptr<" << T << ">(O, (int)(dn % W), (int)(dn / W)), v);\n"
-    << "      if (atomicSub(&indeg[dn], 1) == 1) fb[atomicAdd(&n_next, 1)] = (s32)dn;\n"
+    << "      atomic_add_any(cell_ptr<" << T << ">(O, nx, ny), v);\n"
+    << "      const u8 code = ldr<u8>(D, nx, ny);\n"
+    << "      if (atomicSub(&indeg[dn], 1) == 1) kahn_put(sb, fb, atomicAdd(&n_next, 1), ((u32)dn << 8) | code);\n"
     << "    }\n"
     << "    __syncthreads();\n"
     << "    if (threadIdx.x == 0) { n_cur = n_next; n_next = 0; }\n"
-    << "    s32 *t = fa; fa = fb; fb = t;\n"
+    << "    u32 *t = fa; fa = fb; fb = t;\n"
+    << "    t = sa; sa = sb; sb = t;\n"
     << "    __syncthreads();\n"
     << "  }\n"
     << "}\n"
