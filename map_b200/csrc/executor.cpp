@@ -258,7 +258,11 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
   std::set<std::string> seen;
   for (auto &g : P.fr.groups) {
     if (g->skeleton == SK_HOST) { P.plans[g->id].skeleton = SK_HOST; continue; }
-    P.plans[g->id] = generate_kernel(*g);
+    // standalone focal kernels: 128 threads on a 64 x 32 tile (16 rows per thread),
+    // measured 1.5% faster than 256 threads on the hillshade and 2% on life
+    TileCfg cfg;
+    if (g->skeleton == SK_FOCAL) cfg.nt = 128;
+    P.plans[g->id] = generate_kernel(*g, cfg);
     if (compile && seen.insert(P.plans[g->id].source).second) {
       const std::string *src = &P.plans[g->id].source;
       jobs.push_back(std::async(std::launch::async, [src]() { CudaEnv::get().compile(*src); }));
