@@ -1123,7 +1123,12 @@ static std::string gen_spread(Gen &G) {
     << "__device__ __forceinline__ void kahn_put(u32 *sf, u32 *gf, int i, u32 e) {\n"
     << "  if (i < KAHN_SMEM) sf[i] = e; else gf[i] = e;\n"
     << "}\n"
-    << "__device__ __forceinline__ void spread_kahn(const Args &a) {\n"
+    // pre: the in-degrees were counted by spread_init (sources marked), by a
+    // many-CTA launch before this one; the sweep then only collects the sources.
+    // Round r takes its frontier size from cnt[r % 3], appends to cnt[(r + 1) % 3]
+    // and clears cnt[(r + 2) % 3] (read by everyone before the previous barrier):
+    // one block barrier per round.
+    << "__device__ __forceinline__ void spread_kahn(const Args &a, bool pre) {\n"
     << "  const int W = a.g.W, H = a.g.H;\n"
     << "  const s64 N = (s64)W * H;\n"
     << "  s32 *indeg = (s32 *)a.aux[0];\n"
@@ -1131,29 +1136,38 @@ static std::string gen_spread(Gen &G) {
     << "  const long long limit = (long long)a.aux[3];\n"
     << "  const RasterArg D = a.in[" << kd << "];\n"
     << "  const RasterArg O = a.out[" << ko << "];\n"
-    << "  __shared__ int n_cur, n_next;\n"
+    << "  __shared__ int cnt[3];\n"
     << "  __shared__ u32 kf[2][KAHN_SMEM];\n"
     << "  if (N >= ((s64)1 << 24)) { if (threadIdx.x == 0) skel_fail(a.err, ERR_BAD_LAUNCH); return; }\n"
     << "  u32 *sa = kf[0], *sb = kf[1];\n"
-    << "  if (threadIdx.x == 0) { n_cur = 0; n_next = 0; }\n"
+    << "  if (threadIdx.x == 0) { cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }\n"
     << "  __syncthreads();\n"
-    << "  for (s64 c = threadIdx.x; c < N; c += blockDim.x) {\n"
-    << "    const int x = (int)(c % W), y = (int)(c / W);\n"
-    << "    *cell_ptr<" << T << ">(O, x, y) = (" << T << ")0;\n"
-    << "    int cnt = 0;\n"
-    << "    for (int d = 0; d < 8; ++d) {\n"
-    << "      const int nx = x - d8_dx(d), ny = y - d8_dy(d);\n"
-    << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
-    << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) cnt++;\n"
+    << "  if (pre) {\n"
+    << "#pragma unroll 4\n"
+    << "    for (s64 c = threadIdx.x; c < N; c += blockDim.x)\n"
+    << "      if (indeg[c] == SPREAD_SOURCE)\n"
+    << "        kahn_put(sa, fa, atomicAdd(&cnt[0], 1), (u32)(((u64)c << 8) | ldr<u8>(D, (int)(c % W), (int)(c / W))));\n"
+    << "  } else {\n"
+    << "    for (s64 c = threadIdx.x; c < N; c += blockDim.x) {\n"
+    << "      const int x = (int)(c % W), y = (int)(c / W);\n"
+    << "      *cell_ptr<" << T << ">(O, x, y) = (" << T << ")0;\n"
+    << "      int k = 0;\n"
+    << "      for (int d = 0; d < 8; ++d) {\n"
+    << "        const int nx = x - d8_dx(d), ny = y - d8_dy(d);\n"
+    << "        if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+    << "        if (d8_index(ldr<u8>(D, nx, ny)) == d) k++;\n"
+    << "      }\n"
+    << "      indeg[c] = k;\n"
+    << "      if (k == 0) kahn_put(sa, fa, atomicAdd(&cnt[0], 1), (u32)(((u64)c << 8) | ldr<u8>(D, x, y)));\n"
     << "    }\n"
-    << "    indeg[c] = cnt;\n"
-    << "    if (cnt == 0) kahn_put(sa, fa, atomicAdd(&n_cur, 1), (u32)(((u64)c << 8) | ldr<u8>(D, x, y)));\n"
     << "  }\n"
     << "  __syncthreads();\n"
     << "  for (long long it = 0;; ++it) {\n"
-    << "    const int n = n_cur;\n"
+    << "    const int r = (int)(it % 3);\n"
+    << "    const int n = cnt[r];\n"
     << "    if (n == 0) break;\n"
     << "    if (it > limit) { if (threadIdx.x == 0) skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
+    << "    int *nn = &cnt[r == 2 ? 0 : r + 1];\n"
     << "    for (int i = threadIdx.x; i < n; i += blockDim.x) {\n"
     << "      const u32 e = i < KAHN_SMEM ? sa[i] : fa[i];\n"
     << "      const int c = (int)(e >> 8);\n"
@@ -1166,23 +1180,35 @@ static std::string gen_spread(Gen &G) {
     << "      const " << T << " v = (" << T << ")(ld_coherent<" << T << ">(O, x, y) + water_at(a, x, y));\n"
     << "      atomic_add_any(cell_ptr<" << T << ">(O, nx, ny), v);\n"
     << "      const u8 code = ldr<u8>(D, nx, ny);\n"
-    << "      if (atomicSub(&indeg[dn], 1) == 1) kahn_put(sb, fb, atomicAdd(&n_next, 1), ((u32)dn << 8) | code);\n"
+    << "      if (atomicSub(&indeg[dn], 1) == 1) kahn_put(sb, fb, atomicAdd(nn, 1), ((u32)dn << 8) | code);\n"
     << "    }\n"
+    << "    if (threadIdx.x == 0) cnt[r == 0 ? 2 : r - 1] = 0;\n"
     << "    __syncthreads();\n"
-    << "    if (threadIdx.x == 0) { n_cur = n_next; n_next = 0; }\n"
     << "    u32 *t = fa; fa = fb; fb = t;\n"
     << "    t = sa; sa = sb; sb = t;\n"
-    << "    __syncthreads();\n"
     << "  }\n"
     << "}\n"
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn(const __grid_constant__ Args a) {\n"
-    << "  spread_kahn(a);\n"
+    << "  spread_kahn(a, false);\n"
     << "}\n"
     // many rasters in one launch (serving windows): one CTA each
     << "struct ManyArgs { u64 args; s64 n; };\n"
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn_many(const __grid_constant__ ManyArgs m) {\n"
     << "  if ((s64)blockIdx.x >= m.n) return;\n"
-    << "  spread_kahn(((const Args *)m.args)[blockIdx.x]);\n"
+    << "  spread_kahn(((const Args *)m.args)[blockIdx.x], false);\n"
+    << "}\n"
+    // many rasters, in-degree pass spread over PREP_SLICES CTAs per raster (prep),
+    // then the one-CTA sweep of each raster from its marked sources (kahnp)
+    << "#define PREP_SLICES 32\n"
+    << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_prep_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  const s64 r = blockIdx.x / PREP_SLICES;\n"
+    << "  if (r >= m.n) return;\n"
+    << "  spread_init(((const Args *)m.args)[r], (s64)(blockIdx.x % PREP_SLICES) * blockDim.x + threadIdx.x,\n"
+    << "              (s64)PREP_SLICES * blockDim.x);\n"
+    << "}\n"
+    << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahnp_many(const __grid_constant__ ManyArgs m) {\n"
+    << "  if ((s64)blockIdx.x >= m.n) return;\n"
+    << "  spread_kahn(((const Args *)m.args)[blockIdx.x], true);\n"
     << "}\n";
   s << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init(const __grid_constant__ Args a) {\n"
     << "  spread_init(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"

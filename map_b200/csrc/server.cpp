@@ -214,7 +214,8 @@ Template &Server::Impl::template_for(int type, int w, int h, bool compile) {
       env.kernel(P.source, P.kname + "_many", 0);
       T->last_phase = std::max(T->last_phase, (int)PH_RADIAL);
     } else if (g.skeleton == SK_SPREAD) {
-      env.kernel(P.source, P.kname + "_kahn_many", 0);
+      env.kernel(P.source, P.kname + "_prep_many", 0);
+      env.kernel(P.source, P.kname + "_kahnp_many", 0);
       T->last_phase = std::max(T->last_phase, (int)PH_SPREAD);
     } else {
       throw MapError("serving: zonal groups are not served");
@@ -457,9 +458,12 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     cuda_check(cudaStreamWaitEvent(sp, ev[PH_LEVEL1], 0), "cudaStreamWaitEvent");
     for (auto &kv : spread) {
       Many &mn = kv.second;
-      // one CTA per window: the frontier sweep has the lowest latency at window sizes
-      KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_kahn_many", 0);
+      // in-degrees by 32 CTAs per window, then one CTA per window sweeps the
+      // frontiers (the lowest latency at window sizes)
+      KernelHandle kp = env.kernel(mn.plan->source, mn.plan->kname + "_prep_many", 0);
+      KernelHandle kh = env.kernel(mn.plan->source, mn.plan->kname + "_kahnp_many", 0);
       struct { uint64_t args; int64_t n; } ma{(uint64_t)(uintptr_t)dptr[bi++], mn.n};
+      env.launch(kp, (int)(mn.n * 32), 256, 0, (CUstream_st *)sp, &ma, sizeof ma);
       env.launch(kh, mn.n, 1024, 0, (CUstream_st *)sp, &ma, sizeof ma);
     }
     cuda_check(cudaEventRecord(ev[PH_SPREAD], sp), "cudaEventRecord");
