@@ -1060,7 +1060,8 @@ static std::string gen_spread(Gen &G) {
   s << "    return (" << T << ")(" << G.val(scan->prev[0]) << ");\n}\n";
   const int kd = G.rin.at(scan->prev[1]);
   const int ko = G.outk.at(scan);
-  // aux[0] in-degree (s32[N]); aux[3] step limit of one downstream walk.
+  const bool packed = dt == S32 || dt == U32;
+  // aux[0] in-degree (s32[N]; u64[N] in the packed sweep); aux[3] step limit of one downstream walk.
   // Large rasters: two grid-wide passes (kernels KNAME_init then KNAME), each CTA
   // striding over the cells from `first` by `step`:
   //  * init: zero the accumulation and count each cell's upstream neighbours
@@ -1188,14 +1189,105 @@ static std::string gen_spread(Gen &G) {
     << "    t = sa; sa = sb; sb = t;\n"
     << "  }\n"
     << "}\n"
+    ;
+  // 32-bit integer accumulations: one 64-bit word per cell holds the cell's
+  // accumulation (high half) and its pending upstream pushes (low half). A push
+  // adds (value << 32) - 1 in one atomic: the count never borrows (it is at
+  // least 1 before each push) and the sum wraps like the 32-bit type. The
+  // pusher that sees the count at 1 knows the final sum from the returned old
+  // word, writes the cell's output and queues the cell with the value it will
+  // push (sum + water): a round is one atomic round trip, the direction code of
+  // the next cell fetched beside it. Frontier entries: (value << 32) | (cell << 8) | code.
+  if (packed) {
+    s << "#define KAHN_SMEM_P 2048\n"
+      << "__device__ __forceinline__ void spread_init_packed(const Args &a, s64 first, s64 step) {\n"
+      << "  const int W = a.g.W, H = a.g.H;\n"
+      << "  const s64 N = (s64)W * H;\n"
+      << "  u64 *pk = (u64 *)a.aux[0];\n"
+      << "  const RasterArg D = a.in[" << kd << "];\n"
+      << "  const RasterArg O = a.out[" << ko << "];\n"
+      << "  for (s64 c = first; c < N; c += step) {\n"
+      << "    const int x = (int)(c % W), y = (int)(c / W);\n"
+      << "    *cell_ptr<" << T << ">(O, x, y) = (" << T << ")0;\n"
+      << "    u32 k = 0;\n"
+      << "    for (int d = 0; d < 8; ++d) {\n"
+      << "      const int nx = x - d8_dx(d), ny = y - d8_dy(d);\n"
+      << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+      << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) k++;\n"
+      << "    }\n"
+      << "    pk[c] = (u64)k;\n"
+      << "  }\n"
+      << "}\n"
+      << "__device__ __forceinline__ void kahn_put_p(u64 *sf, u64 *gf, int i, u64 e) {\n"
+      << "  if (i < KAHN_SMEM_P) sf[i] = e; else gf[i] = e;\n"
+      << "}\n"
+      << "__device__ __forceinline__ u64 kahn_entry(int c, u8 code, " << T << " push) {\n"
+      << "  return ((u64)(u32)push << 32) | ((u64)(u32)c << 8) | code;\n"
+      << "}\n"
+      << "__device__ __forceinline__ void spread_kahn_packed(const Args &a, bool pre) {\n"
+      << "  const int W = a.g.W, H = a.g.H;\n"
+      << "  const s64 N = (s64)W * H;\n"
+      << "  u64 *pk = (u64 *)a.aux[0];\n"
+      << "  u64 *fa = (u64 *)a.aux[1], *fb = (u64 *)a.aux[2];\n"
+      << "  const long long limit = (long long)a.aux[3];\n"
+      << "  const RasterArg D = a.in[" << kd << "];\n"
+      << "  const RasterArg O = a.out[" << ko << "];\n"
+      << "  __shared__ int cnt[3];\n"
+      << "  __shared__ u64 kf[2][KAHN_SMEM_P];\n"
+      << "  if (N >= ((s64)1 << 24)) { if (threadIdx.x == 0) skel_fail(a.err, ERR_BAD_LAUNCH); return; }\n"
+      << "  u64 *sa = kf[0], *sb = kf[1];\n"
+      << "  if (threadIdx.x == 0) { cnt[0] = 0; cnt[1] = 0; cnt[2] = 0; }\n"
+      << "  if (!pre) spread_init_packed(a, threadIdx.x, blockDim.x);\n"
+      << "  __syncthreads();\n"
+      << "#pragma unroll 4\n"
+      << "  for (s64 c = threadIdx.x; c < N; c += blockDim.x)\n"
+      << "    if (pk[c] == 0) {\n"
+      << "      const int x = (int)(c % W), y = (int)(c / W);\n"
+      << "      kahn_put_p(sa, fa, atomicAdd(&cnt[0], 1), kahn_entry((int)c, ldr<u8>(D, x, y), water_at(a, x, y)));\n"
+      << "    }\n"
+      << "  __syncthreads();\n"
+      << "  for (long long it = 0;; ++it) {\n"
+      << "    const int r = (int)(it % 3);\n"
+      << "    const int n = cnt[r];\n"
+      << "    if (n == 0) break;\n"
+      << "    if (it > limit) { if (threadIdx.x == 0) skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
+      << "    int *nn = &cnt[r == 2 ? 0 : r + 1];\n"
+      << "    for (int i = threadIdx.x; i < n; i += blockDim.x) {\n"
+      << "      const u64 e = i < KAHN_SMEM_P ? sa[i] : fa[i];\n"
+      << "      const int c = (int)((u32)e >> 8);\n"
+      << "      const int d = d8_index((u8)(e & 255));\n"
+      << "      if (d < 0) continue;\n"
+      << "      const int x = c % W, y = c / W;\n"
+      << "      const int nx = x + d8_dx(d), ny = y + d8_dy(d);\n"
+      << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+      << "      const int dn = ny * W + nx;\n"
+      << "      const u32 v = (u32)(e >> 32);\n"
+      << "      const u8 code = ldr<u8>(D, nx, ny);\n"
+      << "      const u64 old = atomicAdd((unsigned long long *)&pk[dn], ((u64)v << 32) - 1ull);\n"
+      << "      if ((u32)old == 1u) {\n"
+      << "        const " << T << " sum = (" << T << ")((u32)(old >> 32) + v);\n"
+      << "        *cell_ptr<" << T << ">(O, nx, ny) = sum;\n"
+      << "        kahn_put_p(sb, fb, atomicAdd(nn, 1), kahn_entry(dn, code, (" << T << ")(sum + water_at(a, nx, ny))));\n"
+      << "      }\n"
+      << "    }\n"
+      << "    if (threadIdx.x == 0) cnt[r == 0 ? 2 : r - 1] = 0;\n"
+      << "    __syncthreads();\n"
+      << "    u64 *t = fa; fa = fb; fb = t;\n"
+      << "    t = sa; sa = sb; sb = t;\n"
+      << "  }\n"
+      << "}\n";
+  }
+  const std::string kahn_fn = packed ? "spread_kahn_packed" : "spread_kahn";
+  const std::string init_fn = packed ? "spread_init_packed" : "spread_init";
+  s
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn(const __grid_constant__ Args a) {\n"
-    << "  spread_kahn(a, false);\n"
+    << "  " << kahn_fn << "(a, false);\n"
     << "}\n"
     // many rasters in one launch (serving windows): one CTA each
     << "struct ManyArgs { u64 args; s64 n; };\n"
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahn_many(const __grid_constant__ ManyArgs m) {\n"
     << "  if ((s64)blockIdx.x >= m.n) return;\n"
-    << "  spread_kahn(((const Args *)m.args)[blockIdx.x], false);\n"
+    << "  " << kahn_fn << "(((const Args *)m.args)[blockIdx.x], false);\n"
     << "}\n"
     // many rasters, in-degree pass spread over PREP_SLICES CTAs per raster (prep),
     // then the one-CTA sweep of each raster from its marked sources (kahnp)
@@ -1203,12 +1295,12 @@ static std::string gen_spread(Gen &G) {
     << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_prep_many(const __grid_constant__ ManyArgs m) {\n"
     << "  const s64 r = blockIdx.x / PREP_SLICES;\n"
     << "  if (r >= m.n) return;\n"
-    << "  spread_init(((const Args *)m.args)[r], (s64)(blockIdx.x % PREP_SLICES) * blockDim.x + threadIdx.x,\n"
+    << "  " << init_fn << "(((const Args *)m.args)[r], (s64)(blockIdx.x % PREP_SLICES) * blockDim.x + threadIdx.x,\n"
     << "              (s64)PREP_SLICES * blockDim.x);\n"
     << "}\n"
     << "extern \"C\" __global__ void __launch_bounds__(1024) KNAME_kahnp_many(const __grid_constant__ ManyArgs m) {\n"
     << "  if ((s64)blockIdx.x >= m.n) return;\n"
-    << "  spread_kahn(((const Args *)m.args)[blockIdx.x], true);\n"
+    << "  " << kahn_fn << "(((const Args *)m.args)[blockIdx.x], true);\n"
     << "}\n";
   s << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init(const __grid_constant__ Args a) {\n"
     << "  spread_init(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"

@@ -77,9 +77,9 @@ void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node
   const size_t N = (size_t)g.W * g.H;
   if (N >= (size_t)1 << 31) throw MapError("spreadScan: raster too large");
   void *work = nullptr;
-  cuda_check(cudaMallocAsync(&work, 3 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
-  uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
-                     (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
+  cuda_check(cudaMallocAsync(&work, 6 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
+  uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + 2 * N),
+                     (uint64_t)(uintptr_t)((int32_t *)work + 4 * N), (uint64_t)(N + 1)};
   auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
   if (N <= kSpreadKahnCells) {
     // one CTA, frontier by frontier: the lowest latency for rasters of a few million cells

@@ -62,7 +62,7 @@ struct Req {
 
 size_t request_bytes(int type, int w, int h) {
   size_t b = (size_t)pitch_for(w, F32) * h * 2;   // window copy + output
-  if (type == REQ_FLOW) b += (size_t)pitch_for(w, U8) * h + (size_t)w * h * 12;
+  if (type == REQ_FLOW) b += (size_t)pitch_for(w, U8) * h + (size_t)w * h * 24;   // directions + sweep scratch
   return b;
 }
 
@@ -356,10 +356,10 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           mn.plan = &P;
           const size_t N = (size_t)g.W * g.H;
           void *work = nullptr;
-          cuda_check(cudaMallocAsync(&work, 3 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
+          cuda_check(cudaMallocAsync(&work, 6 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
           r->scratch.push_back(work);
-          uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + N),
-                             (uint64_t)(uintptr_t)((int32_t *)work + 2 * N), (uint64_t)(N + 1)};
+          uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + 2 * N),
+                             (uint64_t)(uintptr_t)((int32_t *)work + 4 * N), (uint64_t)(N + 1)};
           auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux, &scal);
           mn.args.insert(mn.args.end(), a.begin(), a.end());
           mn.n++;
@@ -596,6 +596,24 @@ void Server::Impl::warm_up() {
   const int w = std::min(64, W), h = std::min(64, H);
   for (int type = REQ_HILLSHADE; type <= REQ_FLOW; type++) template_for(type, w, h, false);
   ensure_module();
+  // Grow the stream-ordered pool to the memory budget (at most 4 GiB) now: the
+  // pool keeps freed memory, so requests later allocate from it instead of
+  // stalling every stream while the pool maps new memory (measured: ~60 ms).
+  CudaEnv &env = CudaEnv::get();
+  cudaStream_t st = (cudaStream_t)env.stream();
+  const size_t chunk = (size_t)256 << 20;
+  const size_t want = std::min(budget, (size_t)4 << 30);
+  std::vector<void *> held;
+  for (size_t got = 0; got + chunk <= want; got += chunk) {
+    void *p = nullptr;
+    if (cudaMallocAsync(&p, chunk, st) != cudaSuccess) {
+      cudaGetLastError();
+      break;
+    }
+    held.push_back(p);
+  }
+  for (void *p : held) cudaFreeAsync(p, st);
+  cuda_check(cudaStreamSynchronize(st), "cudaStreamSynchronize(pool reserve)");
 }
 
 Server::Server(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch) : impl_(new Impl) {

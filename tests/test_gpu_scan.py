@@ -80,6 +80,24 @@ def test_flow_accumulation_bit_exact(M, shape):
     assert got.sum() > 0
 
 
+@pytest.mark.parametrize("dtype", [np.int32, np.uint32])
+def test_flow_accumulation_integer_water_one_cta_sweep(M, dtype):
+    # rasters up to 64 K cells take the one-CTA frontier sweep, whose 32-bit
+    # integer form carries the sum and the pending count in one 64-bit word
+    rng = np.random.default_rng(17)
+    shape = (250, 255)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=23)
+    dem = M.from_numpy(dem_np, bs=[128, 128])
+    dirs = M.flow_direction(dem)
+    lo = -1000 if dtype == np.int32 else 0
+    water = rng.integers(lo, 1000, shape).astype(dtype)
+    got = M.to_numpy(M.flow_accumulation(M.from_numpy(water, bs=[128, 128]), dirs))
+    ref, cyclic = O.flowacc_s32(water.astype(np.int32), M.to_numpy(dirs))
+    assert not cyclic
+    assert got.dtype == dtype
+    assert np.array_equal(got.astype(np.int32), ref)
+
+
 def test_flow_accumulation_known_answer(M):
     # a ramp falling to the east: every cell drains east (mirrored border reads
     # give no drop), the last column holds pits, and a cell's upstream count is
