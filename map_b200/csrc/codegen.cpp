@@ -1200,6 +1200,7 @@ static std::string gen_spread(Gen &G) {
   // the next cell fetched beside it. Frontier entries: (value << 32) | (cell << 8) | code.
   if (packed) {
     s << "#define KAHN_SMEM_P 2048\n"
+      << "#define KAHN_SOURCE 0x80000000u   // pending-count half of a source's word (nothing flows in)\n"
       << "__device__ __forceinline__ void spread_init_packed(const Args &a, s64 first, s64 step) {\n"
       << "  const int W = a.g.W, H = a.g.H;\n"
       << "  const s64 N = (s64)W * H;\n"
@@ -1215,7 +1216,7 @@ static std::string gen_spread(Gen &G) {
       << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
       << "      if (d8_index(ldr<u8>(D, nx, ny)) == d) k++;\n"
       << "    }\n"
-      << "    pk[c] = (u64)k;\n"
+      << "    pk[c] = k ? (u64)k : (u64)KAHN_SOURCE;\n"
       << "  }\n"
       << "}\n"
       << "__device__ __forceinline__ void kahn_put_p(u64 *sf, u64 *gf, int i, u64 e) {\n"
@@ -1241,7 +1242,7 @@ static std::string gen_spread(Gen &G) {
       << "  __syncthreads();\n"
       << "#pragma unroll 4\n"
       << "  for (s64 c = threadIdx.x; c < N; c += blockDim.x)\n"
-      << "    if (pk[c] == 0) {\n"
+      << "    if ((u32)pk[c] == KAHN_SOURCE) {\n"
       << "      const int x = (int)(c % W), y = (int)(c / W);\n"
       << "      kahn_put_p(sa, fa, atomicAdd(&cnt[0], 1), kahn_entry((int)c, ldr<u8>(D, x, y), water_at(a, x, y)));\n"
       << "    }\n"
@@ -1275,6 +1276,33 @@ static std::string gen_spread(Gen &G) {
       << "    u64 *t = fa; fa = fb; fb = t;\n"
       << "    t = sa; sa = sb; sb = t;\n"
       << "  }\n"
+      << "}\n"
+      // large rasters: the downstream walks with the packed word; the one atomic
+      // per step orders nothing else (the sum travels in the word), so it is relaxed
+      << "__device__ __forceinline__ void spread_walk_packed(const Args &a, s64 first, s64 step) {\n"
+      << "  const int W = a.g.W, H = a.g.H;\n"
+      << "  const s64 N = (s64)W * H;\n"
+      << "  u64 *pk = (u64 *)a.aux[0];\n"
+      << "  const long long limit = (long long)a.aux[3];\n"
+      << "  const RasterArg D = a.in[" << kd << "];\n"
+      << "  const RasterArg O = a.out[" << ko << "];\n"
+      << "  for (s64 c = first; c < N; c += step) {\n"
+      << "    if ((u32)pk[c] != KAHN_SOURCE) continue;\n"
+      << "    int x = (int)(c % W), y = (int)(c / W);\n"
+      << "    u32 carry = (u32)water_at(a, x, y);\n"
+      << "    for (long long it = 0;; ++it) {\n"
+      << "      if (it > limit) { skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
+      << "      const s64 dn = d8_down(D, W, H, x, y);\n"
+      << "      if (dn < 0) break;\n"
+      << "      const u64 old = atomicAdd((unsigned long long *)&pk[dn], ((u64)carry << 32) - 1ull);\n"
+      << "      if ((u32)old != 1u) break;\n"
+      << "      x = (int)(dn % W);\n"
+      << "      y = (int)(dn / W);\n"
+      << "      const " << T << " sum = (" << T << ")((u32)(old >> 32) + carry);\n"
+      << "      *cell_ptr<" << T << ">(O, x, y) = sum;\n"
+      << "      carry = (u32)(" << T << ")(sum + water_at(a, x, y));\n"
+      << "    }\n"
+      << "  }\n"
       << "}\n";
   }
   const std::string kahn_fn = packed ? "spread_kahn_packed" : "spread_kahn";
@@ -1303,10 +1331,10 @@ static std::string gen_spread(Gen &G) {
     << "  " << kahn_fn << "(((const Args *)m.args)[blockIdx.x], true);\n"
     << "}\n";
   s << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_init(const __grid_constant__ Args a) {\n"
-    << "  spread_init(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
+    << "  " << init_fn << "(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
     << "}\n"
     << "extern \"C\" __global__ void __launch_bounds__(256) KNAME(const __grid_constant__ Args a) {\n"
-    << "  spread_walk(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
+    << "  " << (packed ? "spread_walk_packed" : "spread_walk") << "(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
     << "}\n";
   return s.str();
 }

@@ -122,6 +122,21 @@ def test_flow_accumulation_large_raster_walks_bit_exact(M):
     assert np.array_equal(got, ref)
 
 
+def test_flow_accumulation_large_raster_integer_water(M):
+    # the walk path with the packed (sum, pending) word: signed water with
+    # negative values, compared with the oracle
+    rng = np.random.default_rng(29)
+    shape = (600, 640)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=24)
+    dem = M.from_numpy(dem_np, bs=[256, 256])
+    dirs = M.flow_direction(dem)
+    water = rng.integers(-500, 500, shape).astype(np.int32)
+    got = M.to_numpy(M.flow_accumulation(M.from_numpy(water, bs=[256, 256]), dirs))
+    ref, cyclic = O.flowacc_s32(water, M.to_numpy(dirs))
+    assert not cyclic
+    assert np.array_equal(got, ref)
+
+
 def test_flow_accumulation_large_raster_float_water(M):
     # float water on the walk path: sums of exactly representable values stay exact
     shape = (2100, 2050)
