@@ -1022,6 +1022,82 @@ static std::string gen_radial(Gen &G) {
     << "    cur = t;\n"
     << "  }\n"
     << "}\n";
+  // Large rasters: a cluster of CTAs per octant. CTA `rank` of a cluster of C
+  // owns the cells d1 in [rank*S, rank*S + S) of every front (S = ceil((eq+1)/C)),
+  // keeping its part of the previous and current fronts in its shared memory;
+  // the one previous-front value left of its segment is read from the
+  // neighbour's shared memory (DSMEM). One cluster barrier per front (every CTA
+  // of the cluster sweeps the same fronts, none leaves early) orders the fronts:
+  // reads of a front's buffer all come before the barrier, its reuse after.
+  s << "__device__ __forceinline__ u32 cl_rank() { u32 r; asm volatile(\"mov.u32 %0, %%cluster_ctarank;\" : \"=r\"(r)); return r; }\n"
+    << "__device__ __forceinline__ u32 cl_size() { u32 r; asm volatile(\"mov.u32 %0, %%cluster_nctarank;\" : \"=r\"(r)); return r; }\n"
+    << "__device__ __forceinline__ void cl_sync() {\n"
+    << "  asm volatile(\"barrier.cluster.arrive.release.aligned;\\n\\tbarrier.cluster.wait.acquire.aligned;\" ::: \"memory\");\n"
+    << "}\n"
+    << "template <class V> __device__ __forceinline__ V ld_peer(const V *p, u32 rank) {\n"
+    << "  u32 ra;\n"
+    << "  asm volatile(\"mapa.shared::cluster.u32 %0, %1, %2;\" : \"=r\"(ra) : \"r\"((u32)__cvta_generic_to_shared(p)), \"r\"(rank));\n"
+    << "  if constexpr (sizeof(V) == 8) {\n"
+    << "    u64 v; asm volatile(\"ld.shared::cluster.b64 %0, [%1];\" : \"=l\"(v) : \"r\"(ra) : \"memory\"); return bit_cast8<V>(v);\n"
+    << "  } else if constexpr (sizeof(V) == 4) {\n"
+    << "    u32 v; asm volatile(\"ld.shared::cluster.b32 %0, [%1];\" : \"=r\"(v) : \"r\"(ra) : \"memory\"); return bit_cast8<V>(v);\n"
+    << "  } else if constexpr (sizeof(V) == 2) {\n"
+    << "    u32 v; asm volatile(\"ld.shared::cluster.u16 %0, [%1];\" : \"=r\"(v) : \"r\"(ra) : \"memory\"); return bit_cast8<V>((u16)v);\n"
+    << "  } else {\n"
+    << "    u32 v; asm volatile(\"ld.shared::cluster.u8 %0, [%1];\" : \"=r\"(v) : \"r\"(ra) : \"memory\"); return bit_cast8<V>((u8)v);\n"
+    << "  }\n"
+    << "}\n"
+    << "__device__ __forceinline__ void radial_run_cluster(const Args &a, int octant) {\n"
+    << "  extern __shared__ __align__(16) unsigned char radial_smem[];\n"
+    << "  const int C = (int)cl_size(), rank = (int)cl_rank();\n"
+    << "  const int sx = (int)a.aux[0], sy = (int)a.aux[1];\n"
+    << "  const long long lim = (long long)a.aux[2];\n"
+    << "  const int W = a.g.W, H = a.g.H;\n"
+    << "  int p0, p1, q0, q1;\n"
+    << "  octant_units(octant, p0, p1, q0, q1);\n"
+    << "  const int ep = p0 > 0 ? W - 1 - sx : p0 < 0 ? sx : p1 > 0 ? H - 1 - sy : sy;\n"
+    << "  const int eq = q0 > 0 ? W - 1 - sx : q0 < 0 ? sx : q1 > 0 ? H - 1 - sy : sy;\n"
+    << "  const int dmax = (lim >= 0 && lim < ep) ? (int)lim : ep;\n"
+    << "  const int S = (eq + C) / C;\n"
+    << "  const int lo = rank * S;\n"
+    << "  " << T << " *prev = (" << T << " *)radial_smem;\n"
+    << "  " << T << " *cur = prev + S;\n"
+    << "  if (rank == 0 && threadIdx.x == 0) {\n"
+    << "    In in0;\n"
+    << "    radial_load(a, in0, sx, sy);\n"
+    << "    prev[0] = radial_cell(a, in0, sx, sy, (" << T << ")0, true);\n"
+    << "  }\n"
+    << "  cl_sync();\n"
+    << "  for (int d0 = 1; d0 <= dmax; ++d0) {\n"
+    << "    const int d1max = d0 < eq ? d0 : eq;\n"
+    << "    const int n = (lo + S - 1 < d1max ? lo + S - 1 : d1max) - lo + 1;   // cells of this front in the segment\n"
+    << "    for (int base = 0; base < n; base += RADIAL_K * (int)blockDim.x) {\n"
+    << "      In in[RADIAL_K];\n"
+    << "#pragma unroll\n"
+    << "      for (int k = 0; k < RADIAL_K; ++k) {\n"
+    << "        const int j = base + (int)threadIdx.x + k * (int)blockDim.x, d1 = lo + j;\n"
+    << "        if (j < n) radial_load(a, in[k], sx + p0 * d0 + q0 * d1, sy + p1 * d0 + q1 * d1);\n"
+    << "      }\n"
+    << "#pragma unroll\n"
+    << "      for (int k = 0; k < RADIAL_K; ++k) {\n"
+    << "        const int j = base + (int)threadIdx.x + k * (int)blockDim.x, d1 = lo + j;\n"
+    << "        if (j >= n) break;\n"
+    << "        const int x = sx + p0 * d0 + q0 * d1, y = sy + p1 * d0 + q1 * d1;\n"
+    << "        " << T << " va = (" << T << ")0, vb = (" << T << ")0;\n"
+    << "        if (d1 <= d0 - 1) va = prev[j];\n"
+    << "        if (d1 >= 1) vb = j >= 1 ? prev[j - 1] : ld_peer<" << T << ">(prev + (S - 1), (u32)(rank - 1));\n"
+    << "        cur[j] = radial_cell(a, in[k], x, y, radial_lit<" << T << ">(va, vb, d0, d1), false);\n"
+    << "      }\n"
+    << "    }\n"
+    << "    cl_sync();\n"
+    << "    " << T << " *t = prev;\n"
+    << "    prev = cur;\n"
+    << "    cur = t;\n"
+    << "  }\n"
+    << "}\n"
+    << "extern \"C\" __global__ void __launch_bounds__(512) KNAME_cl(const __grid_constant__ Args a) {\n"
+    << "  radial_run_cluster(a, (int)(blockIdx.x / cl_size()));\n"
+    << "}\n";
   // one scan: 8 CTAs (one per octant); many scans: 8 CTAs per Args of a device array
   s << "extern \"C\" __global__ void __launch_bounds__(512) KNAME(const __grid_constant__ Args a) {\n"
     << "  radial_run(a, blockIdx.x);\n"

@@ -29,6 +29,7 @@ typedef CUresult (*PFN_ModuleGetFunction)(CUfunction *, CUmodule, const char *);
 typedef CUresult (*PFN_LaunchKernel)(CUfunction, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, unsigned, CUstream,
                                      void **, void **);
 typedef CUresult (*PFN_FuncSetAttribute)(CUfunction, CUfunction_attribute, int);
+typedef CUresult (*PFN_LaunchKernelEx)(const CUlaunchConfig *, CUfunction, void **, void **);
 typedef CUresult (*PFN_TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
                                              const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
@@ -39,6 +40,7 @@ struct Driver {
   PFN_ModuleLoadData moduleLoadData = nullptr;
   PFN_ModuleGetFunction moduleGetFunction = nullptr;
   PFN_LaunchKernel launchKernel = nullptr;
+  PFN_LaunchKernelEx launchKernelEx = nullptr;
   PFN_FuncSetAttribute funcSetAttribute = nullptr;
   PFN_TensorMapEncodeTiled tensorMapEncodeTiled = nullptr;
   PFN_GetErrorString getErrorString = nullptr;
@@ -200,6 +202,7 @@ void CudaEnv::ensure_device() {
   load_entry(g_drv.moduleLoadData, "cuModuleLoadData");
   load_entry(g_drv.moduleGetFunction, "cuModuleGetFunction");
   load_entry(g_drv.launchKernel, "cuLaunchKernel");
+  load_entry(g_drv.launchKernelEx, "cuLaunchKernelEx");
   load_entry(g_drv.funcSetAttribute, "cuFuncSetAttribute");
   load_entry(g_drv.tensorMapEncodeTiled, "cuTensorMapEncodeTiled");
   load_entry(g_drv.getErrorString, "cuGetErrorString");
@@ -254,6 +257,34 @@ void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CU
   drv_check(g_drv.launchKernel(reinterpret_cast<CUfunction>(k.fn), (unsigned)grid, 1, 1, (unsigned)block, 1, 1, (unsigned)smem,
                                reinterpret_cast<CUstream>(stream), params, nullptr),
             "cuLaunchKernel");
+  launches_++;
+}
+
+// A launch whose CTAs form 1-D thread-block clusters of `cluster` CTAs (grid a
+// multiple of it): the CTAs of a cluster run at once on one GPC and share
+// their shared memory.
+void CudaEnv::launch_cluster(const KernelHandle &k, int grid, int block, int cluster, size_t smem, CUstream_st *stream,
+                             void *args) {
+  if (grid <= 0) return;
+  if (cluster <= 0 || grid % cluster != 0) throw MapError("cluster launch: grid is not a multiple of the cluster size");
+  void *params[] = {args};
+  CUlaunchAttribute attr;
+  attr.id = CU_LAUNCH_ATTRIBUTE_CLUSTER_DIMENSION;
+  attr.value.clusterDim.x = (unsigned)cluster;
+  attr.value.clusterDim.y = 1;
+  attr.value.clusterDim.z = 1;
+  CUlaunchConfig cfg = {};
+  cfg.gridDimX = (unsigned)grid;
+  cfg.gridDimY = 1;
+  cfg.gridDimZ = 1;
+  cfg.blockDimX = (unsigned)block;
+  cfg.blockDimY = 1;
+  cfg.blockDimZ = 1;
+  cfg.sharedMemBytes = (unsigned)smem;
+  cfg.hStream = reinterpret_cast<CUstream>(stream);
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  drv_check(g_drv.launchKernelEx(&cfg, reinterpret_cast<CUfunction>(k.fn), params, nullptr), "cuLaunchKernelEx");
   launches_++;
 }
 

@@ -41,6 +41,7 @@ class CudaEnv {
   bool device_ready() const { return device_ready_; }
   KernelHandle kernel(const std::string &source, const std::string &name, size_t dyn_smem);
   void launch(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args, size_t args_size);
+  void launch_cluster(const KernelHandle &k, int grid, int block, int cluster, size_t smem, CUstream_st *stream, void *args);
   int occupancy(const KernelHandle &k, int block, size_t smem);   // resident CTAs per SM
   void encode_tma_2d(void *desc128, int dtype, const void *base, uint64_t width, uint64_t height, uint64_t pitch_bytes,
                      uint32_t box_w, uint32_t box_h);

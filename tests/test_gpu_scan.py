@@ -37,6 +37,21 @@ def test_radial_max_bit_exact(M, shape, obs):
     assert np.array_equal(got[m], ref[m])
 
 
+@pytest.mark.parametrize("shape,obs", [((2100, 2300), (700, 1050)), ((2048, 2049), (2048, 2047)), ((3000, 2100), (2099, 13))])
+def test_radial_max_cluster_bit_exact(M, shape, obs):
+    # rasters of 2048 cells or more across: a cluster of CTAs per octant, each
+    # holding a segment of the fronts, the segment edges read from the
+    # neighbour's shared memory
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=33, hi=100.0)
+    dem = M.from_numpy(dem_np, bs=[512, 512])
+    slope_np, dist_np = slope_from_observer(dem_np, obs, 10.0)
+    got = M.to_numpy(M.rmax((dem - 10.0) / W.distance(dem, obs), obs))
+    ref = O.radial_f32(slope_np, obs, 6)
+    assert np.array_equal(np.isnan(got), np.isnan(ref))
+    m = ~np.isnan(ref)
+    assert np.array_equal(got[m], ref[m])
+
+
 def test_viewshed_program(M):
     dem_np = synth.fbm_dem(160, 200, seed=5, hi=50.0)
     obs = [77, 91]
