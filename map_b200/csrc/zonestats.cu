@@ -175,14 +175,16 @@ __global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo,
   long long yb = w0 / geo.nchunk_x;
   long long xb = w0 - yb * geo.nchunk_x;
 
-  for (long long cb = w0; cb < w1; cb += kUnroll) {
-    float v[kUnroll][4];
-    int z[kUnroll][4];
-#pragma unroll
+  // Loads of one step (kUnroll chunks of 128 cells) into registers; cells past
+  // the warp's range or the raster edge get zone -1.
+  float v[kUnroll][4];
+  int z[kUnroll][4];
+  auto load_step = [&](long long cb, long long xs, long long ys) {
     // the step's 4 chunks usually lie in one row: one row pointer for all of them
-    const bool one_row = xb + kUnroll <= geo.nchunk_x && cb + kUnroll <= w1;
-    const float *vrow = (const float *)(geo.val + yb * geo.vpitch);
-    const int *zrow = (const int *)(geo.zone + yb * geo.zpitch);
+    const bool one_row = xs + kUnroll <= geo.nchunk_x && cb + kUnroll <= w1;
+    const float *vrow = (const float *)(geo.val + ys * geo.vpitch);
+    const int *zrow = (const int *)(geo.zone + ys * geo.zpitch);
+#pragma unroll
     for (int u = 0; u < kUnroll; u++) {
       const long long c = cb + u;
 #pragma unroll
@@ -192,9 +194,9 @@ __global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo,
         const int *zr = zrow;
         int x;
         if (one_row) {
-          x = ((int)xb + u) * kChunk + lane * 4;
+          x = ((int)xs + u) * kChunk + lane * 4;
         } else {
-          long long y = yb, cx = xb + u;
+          long long y = ys, cx = xs + u;
           while (cx >= geo.nchunk_x) {
             cx -= geo.nchunk_x;
             y++;
@@ -218,6 +220,9 @@ __global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo,
         }
       }
     }
+  };
+  if (w0 < w1) load_step(w0, xb, yb);
+  for (long long cb = w0; cb < w1; cb += kUnroll) {
     // stage the step's cells in order, then let each lane fold a run of consecutive cells
     // cell u*128 + 4*lane + j sits at stage_idx() = u*132 + st_base + j
 #pragma unroll
@@ -227,6 +232,14 @@ __global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo,
         sv[st_base + u * (kChunk + kChunk / 32) + j] = v[u][j];
         sz[st_base + u * (kChunk + kChunk / 32) + j] = z[u][j];
       }
+    // the next step's loads go out now, into the registers just staged, and are
+    // in flight while this step is folded and flushed
+    xb += kUnroll;
+    while (xb >= geo.nchunk_x) {
+      xb -= geo.nchunk_x;
+      yb++;
+    }
+    if (cb + kUnroll < w1) load_step(cb + kUnroll, xb, yb);
     __syncwarp();
     // the lane's run: cells 16*lane + k at stage_idx() = run_base + k
     int key = -1;
@@ -255,11 +268,6 @@ __global__ void __launch_bounds__(kThreads, 3) zs_accumulate(const Geometry geo,
     // lanes are in cell order, so equal zones form runs of lanes: merge and add
     warp_flush<SMEM>(sb, gbins, LaneAcc{key, cnt, ~kmin, kmax, sm}, lane, below);
     __syncwarp();   // the staging area is rewritten by the next step
-    xb += kUnroll;
-    while (xb >= geo.nchunk_x) {
-      xb -= geo.nchunk_x;
-      yb++;
-    }
   }
   if (SMEM) {
     __syncthreads();
