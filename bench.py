@@ -104,7 +104,10 @@ class Clocks:
         self.rows = []
         self.proc = None
         self.thread = None
-        self.path = os.path.join(ROOT, "gpurun_out", "clocks_bench_rank%d.csv" % index) if enabled else None
+        # the nvidia-smi fallback's CSV: MAP_B200_CLOCKS_DIR, else the temporary directory
+        import tempfile
+        cdir = os.environ.get("MAP_B200_CLOCKS_DIR", tempfile.gettempdir())
+        self.path = os.path.join(cdir, "map_b200_clocks_rank%d.csv" % index) if enabled else None
 
     def _nvml_handle(self):
         import pynvml
