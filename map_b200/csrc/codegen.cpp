@@ -1276,6 +1276,7 @@ static std::string gen_spread(Gen &G) {
   // the next cell fetched beside it. Frontier entries: (value << 32) | (cell << 8) | code.
   if (packed) {
     s << "#define KAHN_SMEM_P 2048\n"
+      << "#ifndef KAHN_CHAIN\n#define KAHN_CHAIN 8\n#endif\n"
       << "#define KAHN_SOURCE 0x80000000u   // pending-count half of a source's word (nothing flows in)\n"
       << "__device__ __forceinline__ void spread_init_packed(const Args &a, s64 first, s64 step) {\n"
       << "  const int W = a.g.W, H = a.g.H;\n"
@@ -1329,22 +1330,31 @@ static std::string gen_spread(Gen &G) {
       << "    if (n == 0) break;\n"
       << "    if (it > limit) { if (threadIdx.x == 0) skel_fail(a.err, ERR_ITER_LIMIT); break; }\n"
       << "    int *nn = &cnt[r == 2 ? 0 : r + 1];\n"
+      // a thread that completes a cell goes on down its chain, up to KAHN_CHAIN
+      // cells per entry and round, before queueing the cell it reached
       << "    for (int i = threadIdx.x; i < n; i += blockDim.x) {\n"
       << "      const u64 e = i < KAHN_SMEM_P ? sa[i] : fa[i];\n"
-      << "      const int c = (int)((u32)e >> 8);\n"
-      << "      const int d = d8_index((u8)(e & 255));\n"
-      << "      if (d < 0) continue;\n"
-      << "      const int x = c % W, y = c / W;\n"
-      << "      const int nx = x + d8_dx(d), ny = y + d8_dy(d);\n"
-      << "      if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
-      << "      const int dn = ny * W + nx;\n"
-      << "      const u32 v = (u32)(e >> 32);\n"
-      << "      const u8 code = ldr<u8>(D, nx, ny);\n"
-      << "      const u64 old = atomicAdd((unsigned long long *)&pk[dn], ((u64)v << 32) - 1ull);\n"
-      << "      if ((u32)old == 1u) {\n"
+      << "      int c = (int)((u32)e >> 8);\n"
+      << "      u8 cc = (u8)(e & 255);\n"
+      << "      u32 v = (u32)(e >> 32);\n"
+      << "#pragma unroll 1\n"
+      << "      for (int step = 0; step < KAHN_CHAIN; ++step) {\n"
+      << "        const int d = d8_index(cc);\n"
+      << "        if (d < 0) break;\n"
+      << "        const int x = c % W, y = c / W;\n"
+      << "        const int nx = x + d8_dx(d), ny = y + d8_dy(d);\n"
+      << "        if (nx < 0 || ny < 0 || nx >= W || ny >= H) break;\n"
+      << "        const int dn = ny * W + nx;\n"
+      << "        const u8 code = ldr<u8>(D, nx, ny);\n"
+      << "        const u64 old = atomicAdd((unsigned long long *)&pk[dn], ((u64)v << 32) - 1ull);\n"
+      << "        if ((u32)old != 1u) break;\n"
       << "        const " << T << " sum = (" << T << ")((u32)(old >> 32) + v);\n"
       << "        *cell_ptr<" << T << ">(O, nx, ny) = sum;\n"
-      << "        kahn_put_p(sb, fb, atomicAdd(nn, 1), kahn_entry(dn, code, (" << T << ")(sum + water_at(a, nx, ny))));\n"
+      << "        const " << T << " push = (" << T << ")(sum + water_at(a, nx, ny));\n"
+      << "        if (step == KAHN_CHAIN - 1) { kahn_put_p(sb, fb, atomicAdd(nn, 1), kahn_entry(dn, code, push)); break; }\n"
+      << "        c = dn;\n"
+      << "        cc = code;\n"
+      << "        v = (u32)push;\n"
       << "      }\n"
       << "    }\n"
       << "    if (threadIdx.x == 0) cnt[r == 0 ? 2 : r - 1] = 0;\n"
