@@ -161,3 +161,26 @@ def test_paired_cells_codegen(M):
         M.set_paired_cells(True)
     grid = M.from_numpy(np.zeros((64, 64), np.uint8), bs=[32, 32])
     assert "focal_cell2" not in M.generated_source(W.life(grid, 1))
+
+
+def test_scan_kernel_forms_codegen(M):
+    """Radial groups carry the cluster form (KNAME_cl) beside the one-CTA forms;
+    flow accumulation of 32-bit integers uses the packed (sum, pending) word,
+    floats the separate in-degree array; every form compiles for sm_100a."""
+    import re
+    from map_b200 import workloads as W
+    dem = M.from_numpy(np.zeros((64, 64), np.float32), bs=[32, 32])
+    obs = [10, 20]
+    r = M.rmax((dem - 10.0) / W.distance(dem, obs), obs)
+    src = M.generated_source(r)
+    assert re.search(r"map_radial_[0-9a-f]+_cl\(", src) and "barrier.cluster.arrive" in src
+    assert M.compile_only(r) == 1
+    d8 = M.flow_direction(dem)
+    for dt, packed in ((M.S32, True), (M.U32, True), (M.F32, False)):
+        acc = M.flow_accumulation(M.ones_like(dem, dt), d8)
+        src = M.generated_source(acc)
+        for k in ("_kahn(", "_kahn_many(", "_prep_many(", "_kahnp_many(", "_init("):
+            assert re.search(r"map_spread_[0-9a-f]+" + re.escape(k), src), k
+        assert ("spread_kahn_packed" in src) == packed
+        assert ("spread_walk_packed" in src) == packed
+        assert M.compile_only(acc) >= 1
