@@ -1191,7 +1191,8 @@ static std::string gen_spread(Gen &G) {
     << "  }\n"
     << "}\n";
   // Small rasters: one CTA runs a topological (Kahn) sweep, frontier by frontier
-  // with block barriers (aux[1], aux[2]: frontier lists of N cells).
+  // with block barriers (aux[1], aux[2]: frontier lists of N entries, 4 bytes
+  // each, 8 in the packed sweep; the caller's scratch holds 24 bytes per cell).
   // Frontier entries pack a cell index (below 2^24) with its D8 code, fetched
   // by the thread that completes the cell while its in-degree atomic is in
   // flight, so a round reads no direction; the first KAHN_SMEM entries of a
