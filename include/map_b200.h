@@ -188,7 +188,10 @@ void ma_batchDestroy(ma_Batch *b);
  * device until ma_serverResult (copies to host and releases) or
  * ma_serverRelease. ma_serverLoad runs an open-loop Poisson load (rate req/s,
  * program mix weights mix[4], windows 256/512/1024 squared) and writes
- * latency percentiles and throughput as JSON. */
+ * latency percentiles and throughput as JSON. ma_serverCreate compiles every
+ * program at the three window sizes and grows the device's stream-ordered
+ * memory pool to min(budget_bytes, 4 GiB), which the pool keeps, so requests
+ * allocate without waiting for the pool to map new memory. */
 typedef struct ma_Server ma_Server;
 ma_Server *ma_serverCreate(void *dem, long long pitch, int W, int H, size_t budget_bytes, int max_batch);
 long long ma_serverSubmit(ma_Server *s, int type, int x0, int y0, int w, int h, int obs_x, int obs_y, float obs_h,
