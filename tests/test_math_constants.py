@@ -117,3 +117,27 @@ def test_atan2_within_2_ulp():
     x = (rng.uniform(-1, 1, n) * np.exp2(rng.uniform(-40, 40, n))).astype(f32)
     got = atan2(y, x)
     assert ulp_err(got, np.arctan2(y.astype(np.float64), x.astype(np.float64))).max() <= 2.0
+
+
+def test_packed_flow_word_arithmetic():
+    """The flow sweep's 64-bit cell word: sum in the high half, pending pushes in
+    the low half; a push adds (value << 32) - 1. Whatever the order of the
+    pushes, the count never borrows, the push that sees the count at 1 is the
+    last, and old sum + its value is the 32-bit wrap-around sum of all pushes."""
+    rng = np.random.default_rng(3)
+    M64 = (1 << 64) - 1
+    for trial in range(2000):
+        k = int(rng.integers(1, 9))
+        vals = [int(v) for v in rng.integers(-2 ** 31, 2 ** 31, k)]
+        word = k                                  # the in-degree count, sum 0
+        last = None
+        for i in rng.permutation(k):
+            v = vals[i] & 0xFFFFFFFF
+            old = word
+            word = (word + ((v << 32) - 1)) & M64
+            assert (old & 0xFFFFFFFF) >= 1        # no borrow out of the count
+            if (old & 0xFFFFFFFF) == 1:
+                assert last is None
+                last = (((old >> 32) + v) & 0xFFFFFFFF)
+        want = sum(vals) & 0xFFFFFFFF
+        assert last == want and (word & 0xFFFFFFFF) == 0 and (word >> 32) == want
