@@ -41,12 +41,16 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--size", type=int, default=16384)
     p.add_argument("--block", type=int, default=256)
-    p.add_argument("--e2e-steps", type=int, default=3)
+    p.add_argument("--e2e-steps", type=int, default=0, help="steps of the host-buffer e2e run (0: --steps)")
     p.add_argument("--no-clocks", action="store_true")
     p.add_argument("--no-mix", action="store_true", help="skip the batched-mix, zonal and serving sections")
-    p.add_argument("--sections", default="batched,life,zonal_stats,serving",
-                   help="comma-separated extra sections after the headline (batched, life, zonal_stats, serving)")
+    p.add_argument("--sections", default="plain,wsum,batched,life,zonal_stats,serving",
+                   help="comma-separated extra sections, each printed as its own JSON line before the headline "
+                        "(plain, wsum, batched, life, zonal_stats, serving; the parity section always runs)")
     p.add_argument("--zonal-size", type=int, default=16384)
+    p.add_argument("--literal-chain", action="store_true",
+                   help="generate hillshade as the literal operator chain (no algebraic rewrite)")
+    p.add_argument("--one-cell", action="store_true", help="one cell per thread step (no paired f32x2 cells)")
     return p.parse_args()
 
 
@@ -62,31 +66,51 @@ def peaks():
 
 # ---------------------------------------------------------------- CPU baseline
 
-def cpu_baseline(dem_window, seconds_budget=12.0, threads=None):
-    """Times the C oracle over horizontal strips of `dem_window` on all host
-    cores (ctypes releases the GIL), repeating whole passes up to the budget."""
+class CpuHillshade:
+    """The C oracle (restatement of the reference semantics), -O3 -march=native,
+    computing row bands of one raster on all host threads (ctypes releases the
+    GIL). The thread pool is created once, outside any timed region."""
+
+    def __init__(self, threads=None):
+        from oracle import oracle as O
+        self.O = O
+        self.L = O.lib_native()
+        self.threads = threads or os.cpu_count() or 1
+        self.pool = cf.ThreadPoolExecutor(max_workers=self.threads)
+        list(self.pool.map(lambda _: None, range(self.threads)))   # start the workers
+
+    def run(self, dem, out, rows, bs=(256, 256), border=0):
+        """Computes rows [0, rows) of the hillshade of the whole `dem` into `out`."""
+        n = self.threads * 4
+        cuts = [rows * i // n for i in range(n + 1)]
+        list(self.pool.map(lambda i: self.O.hillshade_rows(self.L, dem, out, bs, border, cuts[i], cuts[i + 1]),
+                           range(n)))
+
+    def close(self):
+        self.pool.shutdown()
+
+
+def cpu_baseline(dem_host, seconds_budget=10.0, rows=2048):
+    """Times whole passes over rows [0, rows) of the full DEM (borders decided by
+    the whole raster) on all host threads, repeating passes up to the budget."""
     import numpy as np
-    from oracle import oracle as O
-    threads = threads or os.cpu_count() or 1
-    h = dem_window.shape[0]
-    strips = [dem_window[max(0, i - 1):min(h, i + h // threads + 2)] for i in range(0, h, max(1, h // threads))]
-    strips = [np.ascontiguousarray(s) for s in strips]
-    cells = sum(s.size for s in strips)
-
-    def one(s):
-        O.hillshade_f32(s, (256, 256), 0)
-
+    cpu = CpuHillshade()
+    out = np.empty_like(dem_host)
+    rows = min(rows, dem_host.shape[0])
+    cpu.run(dem_host, out, rows)    # warm (page faults, library load)
     passes, t0 = 0, time.perf_counter()
-    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
-        while True:
-            list(ex.map(one, strips))
-            passes += 1
-            if time.perf_counter() - t0 > seconds_budget or passes >= 50:
-                break
+    while True:
+        cpu.run(dem_host, out, rows)
+        passes += 1
+        if time.perf_counter() - t0 > seconds_budget or passes >= 200:
+            break
     dt = time.perf_counter() - t0
-    return {"value": round(cells * passes / dt / 1e9, 6), "unit": "Gcells/s", "cores": threads, "kind": "port",
-            "sample": "%dx%d window of the DEM x %d passes, oracle/oracle.c hillshade on %d threads" % (
-                dem_window.shape[1], dem_window.shape[0], passes, threads)}
+    cpu.close()
+    cells = rows * dem_host.shape[1]
+    return {"value": round(cells * passes / dt / 1e9, 6), "unit": "Gcells/s", "cores": cpu.threads, "kind": "port",
+            "sample": "rows 0-%d of the %dx%d DEM (all columns) x %d passes, oracle/oracle.c hillshade "
+                      "(-O3 -march=native, -ffp-contract=off) in row bands on %d threads" % (
+                          rows, dem_host.shape[1], dem_host.shape[0], passes, cpu.threads)}
 
 
 # ---------------------------------------------------------------- clocks
@@ -201,30 +225,40 @@ class Clocks:
 
 def run_reference(args, rank, world):
     """The reference's CPU implementation of the path: its OpenCL pipeline cannot
-    be built here, so the oracle port (a C restatement of its semantics) runs on
-    the host cores, one bounded window of the workload per step."""
+    be built here, so the oracle port (a C restatement of its semantics,
+    -O3 -march=native) runs on all host cores. One step = the hillshade of the
+    whole size^2 DEM (rank 0's DEM of the GPU arm: same generator and seed),
+    computed in row bands by a thread pool created before the timed steps."""
     if rank != 0:
         return
     import numpy as np
     from map_b200 import synth
-    from oracle import build_oracle
-    build_oracle.build_oracle()
-    win = 2048
-    dem = synth.fbm_dem(win, win, seed=1234)
+    S = args.size
+    threads = os.cpu_count() or 1
+    dem = synth.fbm_dem(S, S, seed=1000, threads=threads)
+    out = np.empty_like(dem)
+    cpu = CpuHillshade(threads)
     times = []
     for i in range(args.warmup + args.steps):
-        r = cpu_baseline(dem, seconds_budget=0.0)
+        t0 = time.perf_counter()
+        cpu.run(dem, out, S)
+        dt = time.perf_counter() - t0
         if i >= args.warmup:
-            times.append(r)
-    v = statistics.median([t["value"] for t in times])
-    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "Gcells/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(win * win / (v * 1e9) * 1e3, 3),
+            times.append(dt)
+    cpu.close()
+    ms = statistics.median(times) * 1e3
+    v = S * S / (ms * 1e-3) / 1e9
+    sample = "the whole %dx%d DEM per step (%d warm-up + %d timed passes, median), oracle/oracle.c hillshade " \
+             "(-O3 -march=native) in row bands on %d threads" % (S, S, args.warmup, args.steps, threads)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": "Gcells/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "fused hillshade (hill.py), %dx%d F32 fBm DEM, 256x256 blocks" % (args.size, args.size),
-                       "sample": "%dx%d window per step" % (win, win)},
-            "cpu_baseline": {"value": v, "unit": "Gcells/s", "cores": times[0]["cores"], "kind": "port",
-                             "sample": times[0]["sample"]},
-            "e2e": {"value": v, "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "config": {"workload": "fused hillshade (hill.py), %dx%d F32 fBm DEM (8 octaves, persistence 0.5, "
+                                   "0-3000 m), %dx%d blocks, block-mirror border" % (S, S, args.block, args.block),
+                       "sample": "whole raster per step"},
+            "cpu_baseline": {"value": round(v, 6), "unit": "Gcells/s", "cores": threads, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(v, 6), "unit": "Gcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -232,9 +266,11 @@ def run_reference(args, rank, world):
 
 def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
     """512 rasters, sides log-uniform in [64, 2048], aspect uniform in [0.5, 2],
-    each running fused hillshade + a 6-layer weighted overlay: batched
-    persistent launch (graph replay) against the plain path (one launch per
-    group per 256x256 block, reference launch order). Raster-edge mirror border."""
+    each running fused hillshade + a 6-layer weighted overlay, three ways: the
+    plain path (one launch per group per 256x256 block, the reference's launch
+    order), the fused path (one launch per group per raster) and the batched
+    persistent launch (graph replay). Raster-edge mirror border. Every output of
+    every raster is compared between the three."""
     import numpy as np
     rng = np.random.default_rng(seed)
     gen = torch.Generator(device=dev)
@@ -252,38 +288,41 @@ def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
         dem = torch.zeros((h, pw), dtype=torch.float32, device=dev)
         dem[:, :w] = synth.fbm_dem(h, w, seed=seed * 1000 + i, xp=torch, device=dev)
         lay = [torch.rand((h, pw), generator=gen, device=dev) for _ in range(6)]
-        hs_o = torch.empty((h, pw), dtype=torch.float32, device=dev)
-        ov_o = torch.empty((h, pw), dtype=torch.float32, device=dev)
+        outs = [torch.zeros((h, pw), dtype=torch.float32, device=dev) for _ in range(6)]   # plain, fused, batched x 2
         bs = [256, 256]
         dn = M.from_device(dem.data_ptr(), pw * 4, [w, h], M.F32, bs)
         ln = [M.from_device(l.data_ptr(), pw * 4, [w, h], M.F32, bs) for l in lay]
-        progs.append((W.hillshade(dn), W.wsum(ln, weights), hs_o, ov_o, pw * 4))
+        progs.append((W.hillshade(dn), W.wsum(ln, weights), outs, pw * 4, w))
         keep.append((dem, lay, dn, ln))
         cells += w * h
     torch.cuda.synchronize()
     stream = torch.cuda.ExternalStream(M.stream(), device=dev)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # plain path
-    M.set_exec_mode(M.EXEC_PLAIN)
-    for hs, ov, ho, oo, pitch in progs[:8]:
-        M.to_device(hs, ho.data_ptr(), pitch, sync=False)
-        M.to_device(ov, oo.data_ptr(), pitch, sync=False)
-    M.sync()
-    n0 = M._lib.ma_totalLaunchCount()
-    e0.record(stream)
-    for hs, ov, ho, oo, pitch in progs:
-        M.to_device(hs, ho.data_ptr(), pitch, sync=False)
-        M.to_device(ov, oo.data_ptr(), pitch, sync=False)
-    e1.record(stream)
-    e1.synchronize()
-    plain_ms = e0.elapsed_time(e1)
-    plain_launches = M._lib.ma_totalLaunchCount() - n0
-    plain_ref = [ho[:64, :64].clone() for _, _, ho, _, _ in progs[:16]]
-    M.set_exec_mode(M.EXEC_FUSED)
+
+    def per_raster(mode, slot):
+        M.set_exec_mode(mode)
+        try:
+            for hs, ov, outs, pitch, _ in progs[:8]:      # warm (compiles)
+                M.to_device(hs, outs[slot].data_ptr(), pitch, sync=False)
+                M.to_device(ov, outs[slot + 1].data_ptr(), pitch, sync=False)
+            M.sync()
+            n0 = M._lib.ma_totalLaunchCount()
+            e0.record(stream)
+            for hs, ov, outs, pitch, _ in progs:
+                M.to_device(hs, outs[slot].data_ptr(), pitch, sync=False)
+                M.to_device(ov, outs[slot + 1].data_ptr(), pitch, sync=False)
+            e1.record(stream)
+            e1.synchronize()
+            return e0.elapsed_time(e1), M._lib.ma_totalLaunchCount() - n0
+        finally:
+            M.set_exec_mode(M.EXEC_FUSED)
+
+    plain_ms, plain_launches = per_raster(M.EXEC_PLAIN, 0)
+    fused_ms, fused_launches = per_raster(M.EXEC_FUSED, 2)
     # batched path
     b = M.Batch()
-    for hs, ov, ho, oo, pitch in progs:
-        b.add([hs, ov], [(ho.data_ptr(), pitch), (oo.data_ptr(), pitch)])
+    for hs, ov, outs, pitch, _ in progs:
+        b.add([hs, ov], [(outs[4].data_ptr(), pitch), (outs[5].data_ptr(), pitch)])
     t0 = time.perf_counter()
     b.prepare(autotune=True)
     prep_s = time.perf_counter() - t0
@@ -295,14 +334,22 @@ def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
     e1.synchronize()
     M.sync()
     batch_ms = e0.elapsed_time(e1) / steps
-    same = all(torch.equal(r, progs[i][2][:64, :64]) for i, r in enumerate(plain_ref))
+    plain_same = fused_same = True
+    for hs, ov, outs, pitch, w in progs:
+        for k in (0, 1):
+            bo = outs[4 + k][:, :w]
+            plain_same &= bool(torch.equal(outs[k][:, :w], bo))
+            fused_same &= bool(torch.equal(outs[2 + k][:, :w], bo))
     M.set_border(M.BORDER_BLOCK_MIRROR)
     info = b.info()
     return {"rasters": n_rasters, "cells": cells, "value": round(cells / (batch_ms * 1e-3) / 1e9, 3),
+            "fused_value": round(cells / (fused_ms * 1e-3) / 1e9, 3),
             "plain_value": round(cells / (plain_ms * 1e-3) / 1e9, 3), "unit": "Gcells/s",
-            "speedup_vs_plain": round(plain_ms / batch_ms, 2), "ms_per_step": round(batch_ms, 3),
-            "plain_ms": round(plain_ms, 3), "plain_launches": plain_launches, "batched_launches_per_step": info["launches"],
-            "prepare_s": round(prep_s, 2), "kinds": info["kinds"], "plain_equals_batched": same,
+            "speedup_vs_plain": round(plain_ms / batch_ms, 2), "speedup_vs_fused_per_raster": round(fused_ms / batch_ms, 2),
+            "ms_per_step": round(batch_ms, 3), "fused_ms": round(fused_ms, 3), "plain_ms": round(plain_ms, 3),
+            "plain_launches": plain_launches, "fused_launches": fused_launches,
+            "batched_launches_per_step": info["launches"], "prepare_s": round(prep_s, 2), "kinds": info["kinds"],
+            "all_outputs_plain_equal_batched": plain_same, "all_outputs_fused_equal_batched": fused_same,
             "programs": "fused hillshade + 6-layer weighted overlay per raster"}
 
 
@@ -434,6 +481,165 @@ def bench_zonal_stats(M, synth, torch, dev, size=16384, nzones=1024, steps=10, w
                              "sample": "the whole %dx%d raster, oracle restatement (1 thread)" % (size, size)}}
 
 
+# ---------------------------------------------------------------- hillshade sections
+
+def bench_parity(M, W, torch, dem_t, out_t, block, win=2048):
+    """Hillshade error statement on a win^2 window of the DEM (cells whose 3x3
+    neighbourhood lies inside the window, so the window's own borders do not
+    matter): the GPU result of the timed program against the FP32 oracle under the
+    test tolerance, and both against the FP64 oracle; then the literal operator
+    chain (rewrite off) on the same window."""
+    import numpy as np
+    from oracle import oracle as O
+    S = dem_t.shape[0]
+    y0, x0 = S // 2 - win // 2, S // 3
+    dem_win = dem_t[y0:y0 + win, x0:x0 + win].cpu().numpy()
+    bs = (block, block)
+    ref32 = O.hillshade_f32(dem_win, bs, 0)[1:-1, 1:-1]
+    ref64 = O.hillshade_f64(dem_win, bs, 0)[1:-1, 1:-1]
+    bound = O.hillshade_bound(dem_win, bs, 0)[1:-1, 1:-1]
+
+    def stats(got):
+        ok, d, only = O.hill_tolerance(got, ref32, bound)
+        e = np.abs(got.astype(np.float64) - ref64)
+        ulp = O.ulp_f32(ref64)
+        well = np.abs(ref64) >= 0.05
+        return {"within_tolerance": bool(ok.all()), "max_abs_diff_vs_fp32_oracle": float(d.max()),
+                "bit_identical_fraction": float((got == ref32).mean()),
+                "cells_only_via_cancellation_clause": int(only.sum()),
+                "max_abs_err_vs_fp64": float(e.max()), "max_ulp_err_vs_fp64_where_abs_ge_0.05": float((e / ulp)[well].max()),
+                "max_rel_err_vs_fp64_where_abs_ge_0.05": float((e / np.abs(ref64))[well].max())}
+
+    got = out_t[y0 + 1:y0 + win - 1, x0 + 1:x0 + win - 1].cpu().numpy()
+    e32 = np.abs(ref32.astype(np.float64) - ref64)
+    res = {"window": "%dx%d interior cells of a %dx%d window of the headline DEM" % (win - 2, win - 2, win, win),
+           "tolerance": "4 ulp or 1e-5 rel of the FP32 oracle, or 4x the FP32 chain's first-order rounding-error "
+                        "scale where its two terms cancel (oracle.hill_tolerance)",
+           "fp32_oracle": {"max_abs_err_vs_fp64": float(e32.max()),
+                           "max_ulp_err_vs_fp64_where_abs_ge_0.05": float((e32 / O.ulp_f32(ref64))[np.abs(ref64) >= 0.05].max())},
+           "gpu": stats(got), "gpu_rewrite": M.get_algebraic_rewrite()}
+    prev = M.get_algebraic_rewrite()
+    try:
+        M.set_algebraic_rewrite(not prev)
+        wt = torch.from_numpy(dem_win).to(dem_t.device)
+        d = M.from_device(wt.data_ptr(), win * 4, [win, win], M.F32, [block, block])
+        other = M.to_numpy(W.hillshade(d))[1:-1, 1:-1]
+        res["gpu_rewrite_off" if prev else "gpu_rewrite_on"] = stats(other)
+    finally:
+        M.set_algebraic_rewrite(prev)
+    return res
+
+
+def bench_plain(M, W, synth, torch, dev, block=256, steps=10, warmup=3):
+    """The plain path (one launch per fusion group per block, in the reference's
+    scheduler order) against the fused path (one launch per group): hillshade
+    on the 1024^2 DEM in 256^2 blocks (the reference's CPU-runnable
+    configuration) and on the 16384^2 DEM."""
+    out = {}
+    st = torch.cuda.ExternalStream(M.stream(), device=dev)
+    for S, k in ((1024, steps * 5), (16384, 3)):
+        dem_t = synth.fbm_dem(S, S, seed=77, xp=torch, device=dev).contiguous()
+        o_t = torch.empty_like(dem_t)
+        dem = M.from_device(dem_t.data_ptr(), S * 4, [S, S], M.F32, [block, block])
+        hs = W.hillshade(dem)
+        r = {}
+        for mode, name in ((M.EXEC_FUSED, "fused"), (M.EXEC_PLAIN, "plain")):
+            M.set_exec_mode(mode)
+            try:
+                for _ in range(warmup):
+                    M.to_device(hs, o_t.data_ptr(), S * 4, sync=False)
+                M.sync()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                l0 = M._lib.ma_totalLaunchCount()
+                t0 = time.perf_counter()
+                e0.record(st)
+                for _ in range(k):
+                    M.to_device(hs, o_t.data_ptr(), S * 4, sync=False)
+                e1.record(st)
+                e1.synchronize()
+                host_ms = (time.perf_counter() - t0) * 1e3 / k
+                ms = e0.elapsed_time(e1) / k
+                r[name] = {"ms_per_step": round(ms, 4), "value": round(S * S / (ms * 1e-3) / 1e9, 3),
+                           "launches_per_step": (M._lib.ma_totalLaunchCount() - l0) // k,
+                           "host_ms_per_step": round(host_ms, 4), "steps": k}
+                r[name + "_out"] = o_t.clone()
+            finally:
+                M.set_exec_mode(M.EXEC_FUSED)
+        same = bool(torch.equal(r.pop("fused_out"), r.pop("plain_out")))
+        out["%dx%d" % (S, S)] = dict(r, plain_equals_fused=same,
+                                     fused_vs_plain=round(r["plain"]["ms_per_step"] / r["fused"]["ms_per_step"], 2))
+        del dem_t, o_t, dem, hs
+    out["unit"] = "Gcells/s"
+    out["workload"] = "hillshade (hill.py), fBm DEM, %dx%d blocks, block-mirror border" % (block, block)
+    return out
+
+
+def bench_wsum(M, W, torch, dev, size=16384, steps=10, warmup=3):
+    """Weighted overlay (wsum.py generalised to 6 layers): 6 F32 uniform[0,1)
+    layers, weights summing to 1, one fused Local launch; 28 B/cell."""
+    import numpy as np
+    from oracle import oracle as O
+    weights = [0.1, 0.2, 0.3, 0.15, 0.15, 0.1]
+    g = torch.Generator(device=dev)
+    g.manual_seed(17)
+    lay = [torch.rand((size, size), generator=g, device=dev) for _ in range(6)]
+    o_t = torch.empty((size, size), dtype=torch.float32, device=dev)
+    ln = [M.from_device(l.data_ptr(), size * 4, [size, size], M.F32, [256, 256]) for l in lay]
+    prog = W.wsum(ln, weights)
+    st = torch.cuda.ExternalStream(M.stream(), device=dev)
+    for _ in range(warmup):
+        M.to_device(prog, o_t.data_ptr(), size * 4, sync=False)
+    M.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = M._lib.ma_totalLaunchCount()
+    e0.record(st)
+    for _ in range(steps):
+        M.to_device(prog, o_t.data_ptr(), size * 4, sync=False)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    launches = (M._lib.ma_totalLaunchCount() - l0) // steps
+    cells = size * size
+    peak, peak_kind = peaks()
+    gbs = cells * 28 / (ms * 1e-3) / 1e9
+    # bit-exact against the oracle on a 1024-row window (element-wise: any window is exact)
+    rows = 1024
+    ls_h = [np.ascontiguousarray(l[:rows].cpu().numpy()) for l in lay]
+    ref = O.wsum_f32(ls_h, np.array(weights, np.float32))
+    got = o_t[:rows].cpu().numpy()
+    exact = bool(np.array_equal(got.view(np.uint32), ref.view(np.uint32)))
+    # CPU baseline: the native oracle on the same window, passes up to ~5 s, all threads
+    L = O.lib_native()
+    n = rows * size
+    threads = os.cpu_count() or 1
+    outc = np.empty_like(ls_h[0])
+    cut = [n * i // threads for i in range(threads + 1)]
+    wv = np.array(weights, np.float32)
+
+    def part(i):
+        ptrs = (ct.c_void_p * 6)(*[l.ctypes.data + 4 * cut[i] for l in ls_h])
+        L.orc_wsum_f32(ptrs, wv, 6, cut[i + 1] - cut[i], outc.ctypes.data + 4 * cut[i])
+
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(part, range(threads)))
+        passes, t0 = 0, time.perf_counter()
+        while passes < 100 and time.perf_counter() - t0 < 5.0:
+            list(ex.map(part, range(threads)))
+            passes += 1
+        cdt = time.perf_counter() - t0
+    del lay, o_t
+    return {"workload": "weighted overlay (wsum.py) of 6 F32 uniform[0,1) layers, %dx%d, weights %s" % (size, size, weights),
+            "value": round(cells / (ms * 1e-3) / 1e9, 3), "unit": "Gcells/s", "ms_per_step": round(ms, 4),
+            "steps": steps, "warmup": warmup, "launches_per_step": launches,
+            "l2": "inputs larger than L2 (7 GiB per step)",
+            "roofline": {"bound": "hbm", "achieved": round(gbs, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(gbs / peak, 4), "bytes_per_cell": 28, "peak_kind": peak_kind},
+            "bit_exact_vs_oracle": exact,
+            "cpu_baseline": {"value": round(n * passes / cdt / 1e9, 4), "unit": "Gcells/s", "cores": threads,
+                             "kind": "port", "sample": "%d rows x %d columns x %d passes, oracle wsum (-O3 -march=native)"
+                                                       % (rows, size, passes)}}
+
+
 # ---------------------------------------------------------------- our arm
 
 def main():
@@ -454,6 +660,8 @@ def main():
     from map_b200 import synth
     from map_b200 import workloads as W
     M._lib.ma_setDevice(local)
+    M.set_algebraic_rewrite(not args.literal_chain)
+    M.set_paired_cells(not args.one_cell)
 
     S = args.size
     cells = S * S
@@ -494,52 +702,64 @@ def main():
     ms = MG.max_over_ranks(ev0.elapsed_time(ev1) / args.steps, dist, dev)
     value = MG.job_throughput(cells, world, ms) / 1e9
 
-    # parity spot check on a window against the oracle (cells away from the window edge)
-    parity = None
-    if rank == 0:
-        from oracle import oracle as O
-        win = 512
-        y0, x0 = S // 2 - win // 2, S // 3
-        dem_win = dem_t[y0:y0 + win, x0:x0 + win].cpu().numpy()
-        ref = O.hillshade_f32(dem_win, (args.block, args.block), 0)[1:-1, 1:-1]
-        got = out_t[y0 + 1:y0 + win - 1, x0 + 1:x0 + win - 1].cpu().numpy()
-        d = np.abs(got.astype(np.float64) - ref)
-        parity = {"cells_checked": int(d.size), "max_abs_diff_vs_oracle": float(d.max()),
-                  "bit_identical_fraction": float((got == ref).mean())}
-
-    # end to end through the public API with pinned host buffers
+    # end to end through the public API with pinned host buffers, every step
+    # uploading the DEM and downloading the result
+    e2e_steps = args.e2e_steps or args.steps
     nbytes = cells * 4
     h_in = M._lib.ma_hostAlloc(nbytes)
     h_out = M._lib.ma_hostAlloc(nbytes)
-    dem_host = dem_t.cpu().numpy()          # keep the array alive while it is copied
+    dem_host = dem_t.cpu().numpy()
     ct.memmove(h_in, dem_host.ctypes.data, nbytes)
-    del dem_host
     dem_h = M.Raster(M._lib.ma_fromHost(ct.c_void_p(h_in), M.Array([S, S]), M.F32, M.Array([args.block, args.block]), 0))
     hs_h = W.hillshade(dem_h)
     M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)  # warm
     barrier()
     t0 = time.perf_counter()
-    for _ in range(args.e2e_steps):
+    for _ in range(e2e_steps):
         M._lib.ma_toHost(hs_h, ct.c_void_p(h_out), nbytes)
-    e2e_ms = MG.max_over_ranks((time.perf_counter() - t0) * 1e3 / args.e2e_steps, dist, dev)
+    e2e_ms = MG.max_over_ranks((time.perf_counter() - t0) * 1e3 / e2e_steps, dist, dev)
     e2e_value = MG.job_throughput(cells, world, e2e_ms) / 1e9
+    e2e_same = bool(np.array_equal(np.ctypeslib.as_array(ct.cast(h_out, ct.POINTER(ct.c_float)), shape=(S, S)),
+                                   out_t.cpu().numpy()))
+    del hs_h, dem_h
     M._lib.ma_hostFree(ct.c_void_p(h_in))
     M._lib.ma_hostFree(ct.c_void_p(h_out))
 
     if rank == 0:
         peak, peak_kind = peaks()
         achieved = cells * BYTES_PER_CELL / (ms * 1e-3) / 1e9
-        traffic = None
+        traffic, traffic_src = None, None
         tpath = os.path.join(ROOT, "profiles", "hillshade_focal_traffic.json")
         if os.path.exists(tpath):
             try:
                 with open(tpath) as f:
                     tj = json.load(f)
-                traffic = tj.get("dram_bytes_per_launch_scaled_to_%d" % S)
+                key = "dram_bytes_per_launch_scaled_to_%d" % S
+                if tj.get("rewrite") == M.get_algebraic_rewrite() and key in tj:
+                    traffic = tj[key]
+                    traffic_src = tj.get("captured")
             except Exception:
                 traffic = None
-        cpu_win = dem_t[:2048, :2048].cpu().numpy()
-        cpu = cpu_baseline(cpu_win, seconds_budget=10.0)
+        sections = [x for x in args.sections.split(",") if x] if (world == 1 and not args.no_mix) else []
+        runners = {"parity": lambda: bench_parity(M, W, torch, dem_t, out_t, args.block),
+                   "plain": lambda: bench_plain(M, W, synth, torch, dev, args.block),
+                   "wsum": lambda: bench_wsum(M, W, torch, dev),
+                   "batched": lambda: bench_batched(M, W, synth, torch, dev),
+                   "life": lambda: bench_life(M, W, synth, torch, dev),
+                   "zonal_stats": lambda: bench_zonal_stats(M, synth, torch, dev, size=args.zonal_size),
+                   "serving": lambda: bench_serving(M, synth, torch, dev)}
+        summary = {}
+        for name in ["parity"] + sections:
+            try:
+                res = runners[name]()
+            except Exception as e:   # reported, not fatal: the headline line still prints
+                res = {"error": str(e)[:300]}
+            print(json.dumps({"section": name} | res), flush=True)
+            if name == "parity":
+                parity = res
+            elif isinstance(res, dict) and "value" in res:
+                summary[name] = {k: res[k] for k in ("value", "unit") if k in res}
+        cpu = cpu_baseline(dem_t.cpu().numpy(), seconds_budget=10.0)
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Gcells/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
@@ -547,29 +767,22 @@ def main():
             "config": {"workload": "fused hillshade (hill.py), %dx%d F32 fBm DEM (8 octaves, persistence 0.5, "
                                    "0-3000 m) per GPU, %dx%d blocks, block-mirror border" % (S, S, args.block, args.block),
                        "l2": "inputs larger than L2 (%.2f GiB in + %.2f GiB out per step)" % (nbytes / 2 ** 30, nbytes / 2 ** 30),
-                       "parallelism": "independent raster per GPU (weak scaling)"},
+                       "parallelism": "independent raster per GPU (weak scaling)",
+                       "algebraic_rewrite": M.get_algebraic_rewrite(), "paired_cells": M.get_paired_cells()},
             "e2e": {"value": round(e2e_value, 3), "unit": "Gcells/s", "h2d_bytes_per_step": nbytes,
-                    "d2h_bytes_per_step": nbytes},
+                    "d2h_bytes_per_step": nbytes, "steps": e2e_steps, "equals_device_result": e2e_same},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "frac": round(achieved / peak, 4), "traffic": traffic, "traffic_source": traffic_src,
                          "note": "achieved = 8 B/cell x cells / kernel time; peak %s (MEASURED_PEAKS.json hbm_gbs)" % peak_kind},
             "cpu_baseline": cpu,
-            "parity": parity,
+            "parity": {k: parity.get("gpu", {}).get(k) for k in ("within_tolerance", "max_abs_diff_vs_fp32_oracle",
+                                                                 "max_abs_err_vs_fp64")} if isinstance(parity, dict) else None,
+            "sections": summary,
         }
         ck = clk.summary()
         if ck:
             line["clocks"] = ck
-        sections = [x for x in args.sections.split(",") if x] if (world == 1 and not args.no_mix) else []
-        runners = {"batched": lambda: bench_batched(M, W, synth, torch, dev),
-                   "life": lambda: bench_life(M, W, synth, torch, dev),
-                   "zonal_stats": lambda: bench_zonal_stats(M, synth, torch, dev, size=args.zonal_size),
-                   "serving": lambda: bench_serving(M, synth, torch, dev)}
-        for name in sections:
-            try:
-                line[name] = runners[name]()
-            except Exception as e:   # reported, not fatal: the headline line still prints
-                line[name] = {"error": str(e)[:300]}
         print(json.dumps(line), flush=True)
     MG.finish(dist)
 

@@ -122,6 +122,16 @@ int ma_getStreamRows(void);
  * option with no counterpart in the reference. */
 void ma_setPairedCells(int on);
 int ma_getPairedCells(void);
+/* Algebraic rewrite of hillshade compositions (python/hill.py:41-49):
+ * cz cos(atan(k sqrt(x^2+y^2))) + sz sin(...) cos(ar - aspect(x, y)) is
+ * generated as (cz + sz k (y S - x C)) / sqrt(1 + k^2 (x^2 + y^2)), with the
+ * script's wrap constants (its PI = 3.141593) folded into S and C, so the
+ * kernel evaluates no transcendental function per cell. Results stay within
+ * the hillshade tolerance of the literal chain; cells where x^2 + y^2 is not
+ * finite take the literal chain. on = 0 generates the literal chain
+ * everywhere. Engine option with no counterpart in the reference. */
+void ma_setAlgebraicRewrite(int on);
+int ma_getAlgebraicRewrite(void);
 /* Block size given to rasters created without one (default 256 x 256). */
 void ma_setDefaultBlockSize(ma_Array bs);
 void ma_setDevice(int device);
@@ -143,6 +153,25 @@ ma_Node *ma_radialScanRadius(ma_Node *node, int type, ma_Array coord, double rad
 ma_Node *ma_fromHost(const void *data, ma_Array ds, int dt, ma_Array bs, int copy);
 /* Device-resident raster input (pitch in bytes); the memory is not copied. */
 ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs);
+
+/* Row bands (splitting one raster over several devices or processes; no
+ * counterpart in the reference, whose runtime forces one device,
+ * runtime/Runtime.cpp:110-111).
+ * ma_fromDeviceRows: a device input holding only rows [row0, row0 + rows) of a
+ *   ds raster, `dptr` the address of row row0 (16-byte aligned, pitch a
+ *   multiple of 16 bytes). Such an input is evaluated by ma_evalRows only.
+ * ma_evalRows: evaluates rows [y0, y1) of the n rasters into device memory
+ *   dst[i] (the address of row y0, pitch[i] bytes between rows). The program
+ *   must consist of Local and Focal groups over one raster shape, with device
+ *   inputs holding at least rows [y0 - m, y1 + m) (clipped to the raster),
+ *   m = ma_rowMargin(...). Border rules are applied in whole-raster
+ *   coordinates, so the rows equal those of a whole-raster evaluation.
+ *   Returns 0 on success and blocks until the rows are written.
+ * ma_rowMargin: m for the program computing the n rasters (no device needed),
+ *   or -1 with the reason in ma_lastError(). */
+ma_Node *ma_fromDeviceRows(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs, int row0, int rows);
+int ma_evalRows(ma_Node **nodes, int n, void **dst, const long long *pitch, int y0, int y1);
+int ma_rowMargin(ma_Node **nodes, int n);
 
 /* Evaluate `node` and copy the raster to dense row-major host memory of
  * `bytes` bytes. Returns 0 on success. */

@@ -299,6 +299,8 @@ void Batch::prepare(bool autotune) {
     r.dtype = dt;
     r.W = W;
     r.H = H;
+    if (n->kind == K_DEVIN && n->dev->rows)
+      throw MapError("batch: a device input holding a row band is evaluated by row ranges only (ma_evalRows)");
     if (n->kind == K_DEVIN && ((uintptr_t)n->dev->ptr & 15) == 0 && (n->dev->pitch & 15) == 0) {
       r.ptr = n->dev->ptr;
       r.pitch = n->dev->pitch;

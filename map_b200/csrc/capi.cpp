@@ -356,6 +356,11 @@ void ma_setPairedCells(int on) {
   void_call([&] { Runtime::get().paired_cells = on ? 1 : 0; });
 }
 int ma_getPairedCells(void) { return Runtime::get().paired_cells; }
+
+void ma_setAlgebraicRewrite(int on) {
+  void_call([&] { Runtime::get().algebraic_rewrite = on ? 1 : 0; });
+}
+int ma_getAlgebraicRewrite(void) { return Runtime::get().algebraic_rewrite; }
 void ma_setDefaultBlockSize(ma_Array bs) {
   void_call([&] {
     if (bs.n != 2 || bs.arr[0] <= 0 || bs.arr[1] <= 0) throw MapError("setDefaultBlockSize: invalid size");
@@ -371,6 +376,32 @@ ma_Node *ma_fromHost(const void *data, ma_Array ds, int dt, ma_Array bs, int cop
 }
 ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs) {
   return node_call([&] { return Runtime::get().dev_input(dptr, pitch, A(ds), dt, A(bs)); });
+}
+
+ma_Node *ma_fromDeviceRows(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs, int row0, int rows) {
+  return node_call([&] { return Runtime::get().dev_input_rows(dptr, pitch, A(ds), dt, A(bs), row0, rows); });
+}
+
+int ma_evalRows(ma_Node **nodes, int n, void **dst, const long long *pitch, int y0, int y1) {
+  return int_call([&] {
+    std::vector<Node *> v = node_vec(nodes, n);
+    if (!dst || !pitch) throw MapError("evalRows: null destination arrays");
+    std::vector<Sink> sinks;
+    for (int i = 0; i < n; i++) {
+      if (!dst[i]) throw MapError("evalRows: null destination");
+      Sink s;
+      s.node = v[i];
+      s.dev = dst[i];
+      s.dev_pitch = pitch[i];
+      sinks.push_back(s);
+    }
+    Executor::get().evaluate_rows({}, sinks, y0, y1);
+    return 0;
+  });
+}
+
+int ma_rowMargin(ma_Node **nodes, int n) {
+  return int_call([&] { return Executor::get().row_margin(node_vec(nodes, n)); });
 }
 
 int ma_toHost(ma_Node *node, void *dst, size_t bytes) {

@@ -1,6 +1,7 @@
 // Kernel generation for the Local, Focal, Zonal, Radiating and Spreading
 // skeletons (see codegen.hpp); the scan skeletons run through codegen_scan.cpp.
 #include "codegen.hpp"
+#include "rewrite.hpp"
 
 #include <cmath>
 #include <cstdio>
@@ -110,6 +111,10 @@ struct Gen {
   std::map<Node *, std::string> literal;   // scalar constants written into the source
   std::set<Node *> sincos_first;  // float sin/cos pairs on one argument: emitted once with sincosf
   std::map<Node *, Node *> sincos_mate;
+  // hillshade compositions computed through the shading identity (rewrite.hpp)
+  std::vector<ShadeMatch> shades;
+  std::map<Node *, int> shade_at;    // rewritten node -> index in `shades`
+  std::set<Node *> replaced;         // nodes only the rewritten values needed: not emitted
 
   Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
 
@@ -356,8 +361,8 @@ struct Gen {
     std::ostringstream s;
     for (auto &kv : outk) {
       Node *o = kv.first;
-      s << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "));\n"
-        << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y + 1, lane1(" << val(o) << "));\n";
+      s << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "));\n"
+        << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y + 1, lane1(" << val(o) << "));\n";
     }
     return s.str();
   }
@@ -378,7 +383,10 @@ struct Gen {
 
   std::string body2() const {
     std::ostringstream s;
-    for (Node *n : g.nodes) s << "    " << stmt2(n) << "\n";
+    for (Node *n : g.nodes) {
+      if (replaced.count(n)) continue;
+      s << "    " << (shade_at.count(n) ? shade_stmt(n, true) : stmt2(n)) << "\n";
+    }
     return s.str();
   }
 
@@ -434,6 +442,95 @@ struct Gen {
         }
       }
     }
+    if (Runtime::get().algebraic_rewrite && (g.skeleton == SK_LOCAL || g.skeleton == SK_FOCAL)) find_shades();
+  }
+
+  // Finds the hillshade compositions of the group and the nodes that only they need.
+  void find_shades() {
+    auto lit = [this](Node *n, double &v) {
+      if (literal.count(n)) { v = var_as_f64(n->cnst); return true; }
+      if (member.count(n) && n->kind == K_CONSTANT) { v = var_as_f64(reference_literal_value(n->cnst)); return true; }
+      return false;
+    };
+    auto mem = [this](Node *n) { return member.count(n) > 0 && n->kind != K_CONSTANT; };
+    std::set<Node *> in_pattern;
+    for (Node *n : g.nodes) {
+      if (in_pattern.count(n)) continue;
+      ShadeMatch m;
+      if (!match_shade(n, lit, mem, m)) continue;
+      shade_at[n] = (int)shades.size();
+      for (Node *p : m.pattern) in_pattern.insert(p);
+      shades.push_back(m);
+    }
+    if (shades.empty()) return;
+    std::set<Node *> outs(g.outputs.begin(), g.outputs.end());
+    // a pattern node is dropped when every consumer inside the group is a
+    // rewritten node or itself dropped (sin/cos mates only together)
+    for (bool changed = true; changed;) {
+      changed = false;
+      for (auto it = g.nodes.rbegin(); it != g.nodes.rend(); ++it) {
+        Node *p = *it;
+        if (!in_pattern.count(p) || shade_at.count(p) || replaced.count(p) || outs.count(p)) continue;
+        bool all = true;
+        for (Node *c : p->next)
+          if (member.count(c) && !shade_at.count(c) && !replaced.count(c)) all = false;
+        if (all) {
+          replaced.insert(p);
+          changed = true;
+        }
+      }
+      for (auto &kv : sincos_mate)
+        if (replaced.count(kv.first) != replaced.count(kv.second)) {
+          replaced.erase(kv.first);
+          replaced.erase(kv.second);
+        }
+    }
+  }
+
+  // Literal chain of shading composition i as a separate function: cells whose
+  // x^2 + y^2 is not finite take it.
+  std::string shade_slow_decl(int i) const {
+    const ShadeMatch &m = shades[i];
+    std::ostringstream s;
+    s << "__device__ __noinline__ float shade_slow" << i << "(const Args &a, const float " << val(m.x) << ", const float "
+      << val(m.y) << ") {\n";
+    for (Node *n : m.pattern) s << "  " << stmt(n, false) << "\n";
+    s << "  return " << val(m.hs) << ";\n}\n";
+    return s.str();
+  }
+  std::string shade_decls() const {
+    std::string s;
+    for (size_t i = 0; i < shades.size(); i++) s += shade_slow_decl((int)i);
+    return s;
+  }
+  static std::string fl(float f) {
+    char b[48];
+    std::snprintf(b, sizeof b, "%af", (double)f);
+    return b;
+  }
+  std::string shade_args(const ShadeMatch &m) const {
+    return fl(m.cz) + ", " + fl(m.szk) + ", " + fl(m.kk) + ", " + fl(m.S0) + ", " + fl(m.C0) + ", " + fl(m.S1) + ", " +
+           fl(m.C1) + ", " + fl(m.SH) + ", " + fl(m.S3);
+  }
+  // statement of a rewritten node (scalar or pair form)
+  std::string shade_stmt(Node *n, bool pair) const {
+    const int i = shade_at.at(n);
+    const ShadeMatch &m = shades[i];
+    const std::string v = "v" + std::to_string(member.at(n)), q = v + "_q", si = std::to_string(i);
+    const std::string tmpl = m.k_one ? "<true>" : "<false>";
+    std::ostringstream s;
+    if (!pair) {
+      s << "float " << q << "; float " << v << " = map_shade" << tmpl << "(" << val(m.x) << ", " << val(m.y) << ", "
+        << shade_args(m) << ", " << q << "); if (!(" << q << " < MAP_INF_F)) " << v << " = shade_slow" << si << "(a, "
+        << val(m.x) << ", " << val(m.y) << ");";
+    } else {
+      s << "PR<float> " << q << "; PR<float> " << v << " = map_shade" << tmpl << "(PR<float>(" << val(m.x)
+        << "), PR<float>(" << val(m.y) << "), " << shade_args(m) << ", " << q << "); if (!(" << q << ".a < MAP_INF_F)) "
+        << v << ".a = shade_slow" << si << "(a, lane0(" << val(m.x) << "), lane0(" << val(m.y) << ")); if (!(" << q
+        << ".b < MAP_INF_F)) " << v << ".b = shade_slow" << si << "(a, lane1(" << val(m.x) << "), lane1(" << val(m.y)
+        << "));";
+    }
+    return s.str();
   }
 
   // ---- per-node statements
@@ -592,11 +689,12 @@ struct Gen {
     return s.str();
   }
 
-  std::string stores() const {
+  // `unordered`: Local / Focal cells, whose kernels never read their outputs (str_out)
+  std::string stores(bool unordered = false) const {
     std::ostringstream s;
     for (auto &kv : outk) {
       Node *o = kv.first;
-      s << "    str<" << T(o) << ">(a.out[" << kv.second << "], x, y, " << val(o) << ");\n";
+      s << "    " << (unordered ? "str_out<" : "str<") << T(o) << ">(a.out[" << kv.second << "], x, y, " << val(o) << ");\n";
     }
     return s.str();
   }
@@ -616,7 +714,10 @@ struct Gen {
 
   std::string body(bool zonal_acc) const {
     std::ostringstream s;
-    for (Node *n : g.nodes) s << "    " << stmt(n, zonal_acc) << "\n";
+    for (Node *n : g.nodes) {
+      if (replaced.count(n)) continue;
+      s << "    " << (shade_at.count(n) ? shade_stmt(n, false) : stmt(n, zonal_acc)) << "\n";
+    }
     return s.str();
   }
 
@@ -654,7 +755,7 @@ std::string fnv_hex(const std::string &s) {
 static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap) {
   KernelPlan &P = G.plan;
   const int TW = P.tile_w, TH = P.tile_h, NT = P.threads, R = TH * TW / NT;
-  body << G.args_struct(0, false);
+  body << G.args_struct(0, false) << G.shade_decls();
   body << "struct In {\n";
   for (Node *p : P.in_rasters) body << "  " << G.T(p) << " i" << G.rin.at(p) << ";\n";
   body << "  int dummy;\n};\n";
@@ -665,7 +766,7 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   }
   body << "}\n";
   body << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
-  body << G.center_loads(true) << G.body(false) << G.stores() << "}\n";
+  body << G.center_loads(true) << G.body(false) << G.stores(true) << "}\n";
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
        << "                                         bool gdesc) {\n"
        << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
@@ -729,13 +830,13 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   if (use_tma && off + 16 > 200 * 1024) use_tma = false;
   P.smem_bytes = use_tma ? off + 16 : 0;
   P.bar_off = bar_off;
-  body << G.args_struct(use_tma ? nst : 0, false);
+  body << G.args_struct(use_tma ? nst : 0, false) << G.shade_decls();
   body << "template <";
   for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
   body << ">\n__device__ __forceinline__ void focal_cell(const Args &a";
   for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
   body << ", int x, int y, int lx, int ly) {\n";
-  body << G.center_loads(false) << G.body(false) << G.stores() << "}\n";
+  body << G.center_loads(false) << G.body(false) << G.stores(true) << "}\n";
   std::ostringstream call, call2;
   call << "focal_cell(a";
   call2 << "focal_cell2(a";
@@ -749,12 +850,13 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   const int rows = TH * TW / NT;
   bool heavy = false;   // bodies with library math functions unroll by 2 only (code size)
   for (Node *n : G.g.nodes)
-    if ((n->kind == K_UNARY && n->op >= SIN && n->op <= CBRT) ||
-        (n->kind == K_BINARY && (n->op == ATAN2 || n->op == POW || n->op == HYPOT || n->op == FMOD)))
+    if (!G.replaced.count(n) && ((n->kind == K_UNARY && n->op >= SIN && n->op <= CBRT) ||
+                                 (n->kind == K_BINARY && (n->op == ATAN2 || n->op == POW || n->op == HYPOT || n->op == FMOD))))
       heavy = true;
-  // Float-heavy bodies compute the cells of two consecutive rows together
-  // (PR<T> pairs: packed f32x2 arithmetic, one issue slot for both cells).
-  const bool pair = heavy && rows % 2 == 0 && Runtime::get().paired_cells && G.pairable();
+  // Float-heavy bodies, and bodies with a rewritten shading composition, compute
+  // the cells of two consecutive rows together (PR<T> pairs: packed f32x2
+  // arithmetic, one issue slot for both cells).
+  const bool pair = (heavy || !G.shades.empty()) && rows % 2 == 0 && Runtime::get().paired_cells && G.pairable();
   if (pair) {
     body << "template <";
     for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
@@ -763,7 +865,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << ", int x, int y, int lx, int ly) {\n";
     body << G.center_loads2() << G.body2() << G.stores2() << "}\n";
   }
-  const std::string unroll = pair ? "#pragma unroll 1\n" : heavy ? "#pragma unroll 2\n" : "#pragma unroll\n";
+  const std::string unroll = heavy ? (pair ? "#pragma unroll 1\n" : "#pragma unroll 2\n") : "#pragma unroll\n";
   const int step = pair ? 2 : 1;
   std::ostringstream loop, loop_full;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"

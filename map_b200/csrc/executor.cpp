@@ -275,7 +275,8 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
 std::shared_ptr<Executor::Prepared> Executor::prepare_cached(const std::vector<Node *> &targets,
                                                              const std::set<Node *> &tset) {
   Runtime &rt = Runtime::get();
-  std::string key = std::to_string(rt.exec_mode) + "," + std::to_string(rt.paired_cells) + ";";
+  std::string key = std::to_string(rt.exec_mode) + "," + std::to_string(rt.paired_cells) + "," +
+                    std::to_string(rt.algebraic_rewrite) + ";";
   for (Node *t : targets) key += std::to_string(t->id) + ",";
   key += ";";
   for (Node *t : tset) key += std::to_string(t->id) + ",";
@@ -424,6 +425,7 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
     const int W = n->meta.W(), H = n->meta.H(), dt = n->meta.dtype;
     const size_t row = (size_t)W * dt_size(dt);
     if (n->kind == K_DEVIN) {
+      if (n->dev->rows) throw MapError("a device input holding a row band is evaluated by row ranges only (ma_evalRows)");
       DevRaster r;
       r.ptr = n->dev->ptr;
       r.pitch = n->dev->pitch;
@@ -683,6 +685,200 @@ BandStreams &band_streams() {
 
 }  // namespace
 
+// Row structure of a program made only of Local / Focal groups over one raster
+// shape: need[g] = rows beyond a requested row range that group g must still
+// produce for the groups that read it; M = rows beyond the range that the
+// program reads from its inputs. False (with the reason) for other programs.
+struct RowPlan {
+  int W = -1, H = -1, th_max = 1, hy_max = 0, M = 0;
+  std::map<const Group *, int> need;
+  std::set<Node *> produced;
+  std::map<Node *, const Group *> producer;
+  std::set<Node *> inputs;
+};
+static bool row_plan(const FusionResult &fr, const std::vector<KernelPlan> &plans, RowPlan &R, std::string &why) {
+  for (auto &gp : fr.groups) {
+    const Group &g = *gp;
+    if (g.skeleton != SK_LOCAL && g.skeleton != SK_FOCAL) {
+      why = std::string("group of skeleton ") + skeleton_name(g.skeleton) + " (only Local and Focal groups run by rows)";
+      return false;
+    }
+    if (R.W < 0) {
+      R.W = g.W;
+      R.H = g.H;
+    } else if (g.W != R.W || g.H != R.H) {
+      why = "groups of different raster shapes";
+      return false;
+    }
+    const KernelPlan &K = plans[g.id];
+    R.th_max = std::max(R.th_max, K.tile_h);
+    R.hy_max = std::max(R.hy_max, K.halo_y);
+    for (Node *o : K.out_rasters) {
+      R.produced.insert(o);
+      R.producer[o] = &g;
+    }
+  }
+  if (R.W <= 0 || R.H <= 0) {
+    why = "no raster group";
+    return false;
+  }
+  for (auto &gp : fr.groups)
+    for (Node *n : plans[gp->id].in_rasters)
+      if (!R.produced.count(n)) R.inputs.insert(n);
+  for (auto it = fr.groups.rbegin(); it != fr.groups.rend(); ++it) {
+    const Group *c = it->get();
+    const KernelPlan &K = plans[c->id];
+    const int nc = R.need[c];
+    for (Node *n : K.in_rasters) {
+      auto p = R.producer.find(n);
+      if (p != R.producer.end()) R.need[p->second] = std::max(R.need[p->second], nc + K.halo_y);
+    }
+  }
+  for (auto &gp : fr.groups) R.M = std::max(R.M, R.need[gp.get()] + plans[gp->id].halo_y);
+  return true;
+}
+
+void Executor::evaluate_rows(const std::vector<Node *> &targets_in, const std::vector<Sink> &sinks, int y0, int y1) {
+  const double t0 = now_ms();
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  CudaEnv &env = CudaEnv::get();
+  if (rt.exec_mode != EXEC_FUSED) throw MapError("evalRows: row ranges run fused launches only");
+  std::vector<Node *> targets = targets_in;
+  for (auto &s : sinks) {
+    if (!s.dev || s.host) throw MapError("evalRows: every output goes to device memory");
+    targets.push_back(s.node);
+  }
+  for (Node *t : targets) {
+    if (!rt.owns(t)) throw MapError("evalRows: unknown node");
+    if (t->meta.numdim != D2) throw MapError("evalRows: every output is a 2-D raster");
+  }
+  std::set<Node *> tset(targets.begin(), targets.end());
+  std::shared_ptr<Prepared> PP = prepare_cached(targets, tset);
+  const Prepared &P = *PP;
+  for (Node *n : P.order)
+    if (n->kind == K_WRITE) throw MapError("evalRows: a program with file writes runs whole");
+  RowPlan R;
+  std::string why;
+  if (!row_plan(P.fr, P.plans, R, why)) throw MapError("evalRows: " + why);
+  const int W = R.W, H = R.H;
+  if (y0 < 0 || y1 > H || y0 >= y1)
+    throw MapError("evalRows: rows [" + std::to_string(y0) + ", " + std::to_string(y1) + ") are not a range of the " +
+                   std::to_string(H) + " rows");
+  for (const Sink &s : sinks) {
+    if (!R.produced.count(s.node)) throw MapError("evalRows: an output is not computed by a raster group");
+    if (s.dev_pitch < (long long)W * (long long)dt_size(s.node->meta.dtype)) throw MapError("evalRows: pitch smaller than a row");
+  }
+  const int ya = std::max(0, y0 - R.M), yb = std::min(H, y1 + R.M);
+  last = EvalStats();
+  last.groups = (int)P.fr.groups.size();
+  const int launches0 = env.launches();
+  env.ensure_device();
+  cudaStream_t st = (cudaStream_t)env.stream();
+  std::unordered_map<Node *, DevRaster> bufs;
+  for (Node *n : R.inputs) {
+    if (n->kind != K_DEVIN) throw MapError("evalRows: every input is a device raster (ma_fromDevice / ma_fromDeviceRows)");
+    if (n->meta.W() != W || n->meta.H() != H) throw MapError("evalRows: inputs of different raster shapes");
+    const DevData &d = *n->dev;
+    if (((uintptr_t)d.ptr & 15) != 0 || (d.pitch & 15) != 0)
+      throw MapError("evalRows: device inputs must start on 16 bytes with a pitch multiple of 16 bytes");
+    DevRaster r;
+    r.dtype = n->meta.dtype;
+    r.W = W;
+    r.H = H;
+    r.pitch = d.pitch;
+    if (d.rows) {
+      if (d.row0 > ya || d.row0 + d.rows < yb)
+        throw MapError("evalRows: an input holds rows [" + std::to_string(d.row0) + ", " + std::to_string(d.row0 + d.rows) +
+                       ") but rows [" + std::to_string(ya) + ", " + std::to_string(yb) + ") are read");
+      r.org = d.row0;
+      r.rows = d.rows;
+      r.ptr = (void *)((uintptr_t)d.ptr - (uintptr_t)((long long)d.row0 * d.pitch));
+    } else {
+      r.org = ya;
+      r.rows = H - ya;
+      r.ptr = d.ptr;
+    }
+    bufs[n] = r;
+  }
+  std::map<Node *, const Sink *> sink_of;
+  for (const Sink &s : sinks) sink_of[s.node] = &s;
+  std::vector<void *> allocs;
+  std::vector<std::pair<const Sink *, Node *>> copies;
+  try {
+    const int rows_alloc = (yb - ya) + R.th_max + R.hy_max + 1;
+    for (Node *n : R.produced) {
+      DevRaster r;
+      r.dtype = n->meta.dtype;
+      r.W = W;
+      r.H = H;
+      auto sk = sink_of.find(n);
+      if (sk != sink_of.end() && R.need[R.producer[n]] == 0 && ((uintptr_t)sk->second->dev & 15) == 0 &&
+          (sk->second->dev_pitch & 15) == 0) {
+        // written straight into the caller's rows [y0, y1)
+        r.pitch = sk->second->dev_pitch;
+        r.org = y0;
+        r.rows = y1 - y0;
+        r.ptr = (void *)((uintptr_t)sk->second->dev - (uintptr_t)((long long)y0 * r.pitch));
+      } else {
+        r.pitch = pitch_for(W, r.dtype);
+        void *p = nullptr;
+        cuda_check(cudaMallocAsync(&p, (size_t)r.pitch * rows_alloc, st), "cudaMallocAsync(rows)");
+        allocs.push_back(p);
+        r.org = ya;
+        r.rows = rows_alloc;
+        r.ptr = (void *)((uintptr_t)p - (uintptr_t)((long long)ya * r.pitch));
+        if (sk != sink_of.end()) copies.push_back({sk->second, n});
+      }
+      bufs[n] = r;
+    }
+    std::function<DevRaster &(Node *)> get = [&](Node *n) -> DevRaster & {
+      auto it = bufs.find(n);
+      if (it == bufs.end()) throw MapError("evalRows: raster not bound");
+      return it->second;
+    };
+    for (auto &gp : P.fr.groups) {
+      const Group &g = *gp;
+      const KernelPlan &K = P.plans[g.id];
+      const int ry0 = std::max(0, y0 - R.need[&g]), ry1 = std::min(H, y1 + R.need[&g]);
+      const int tx = (W + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+      KernelHandle kh = env.kernel(K.source, K.kname, K.smem_bytes);
+      uint64_t aux[4] = {0, 0, 0, 0};
+      auto a = pack_args(g, K, get, bufs, 0, ry0, W, ry1, aux);
+      env.launch(kh, tx * ty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+    }
+    for (auto &c : copies) {
+      const DevRaster &r = bufs.at(c.second);
+      const size_t row = (size_t)W * dt_size(c.second->meta.dtype);
+      cuda_check(cudaMemcpy2DAsync(c.first->dev, c.first->dev_pitch, (const char *)r.ptr + (long long)y0 * r.pitch, r.pitch,
+                                   row, y1 - y0, cudaMemcpyDeviceToDevice, st),
+                 "row copy");
+    }
+    for (void *p : allocs) cudaFreeAsync(p, st);
+    allocs.clear();
+    sync();
+  } catch (...) {
+    cudaStreamSynchronize(st);
+    for (void *p : allocs) cudaFreeAsync(p, st);
+    throw;
+  }
+  last.launches = env.launches() - launches0;
+  last.host_ms = now_ms() - t0;
+}
+
+int Executor::row_margin(const std::vector<Node *> &targets) {
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  for (Node *t : targets)
+    if (!rt.owns(t)) throw MapError("rowMargin: unknown node");
+  std::set<Node *> tset(targets.begin(), targets.end());
+  Prepared P = prepare(targets, tset, false);
+  RowPlan R;
+  std::string why;
+  if (!row_plan(P.fr, P.plans, R, why)) throw MapError("rowMargin: " + why);
+  return R.M;
+}
+
 bool Executor::evaluate_streamed(const Prepared &P, const std::vector<Node *> &targets, const std::vector<Sink> &sinks) {
   Runtime &rt = Runtime::get();
   if (rt.exec_mode != EXEC_FUSED || rt.stream_rows < 0 || sinks.empty()) return false;
@@ -695,40 +891,21 @@ bool Executor::evaluate_streamed(const Prepared &P, const std::vector<Node *> &t
     if (!sink_nodes.count(t)) return false;
   for (Node *n : P.order)
     if (n->kind == K_WRITE) return false;
-  int W = -1, H = -1, th_max = 1, hy_max = 0;
-  std::set<Node *> produced;
-  std::map<Node *, const Group *> producer;
-  for (auto &gp : P.fr.groups) {
-    const Group &g = *gp;
-    if (g.skeleton != SK_LOCAL && g.skeleton != SK_FOCAL) return false;
-    if (W < 0) {
-      W = g.W;
-      H = g.H;
-    } else if (g.W != W || g.H != H) {
-      return false;
-    }
-    const KernelPlan &K = P.plans[g.id];
-    th_max = std::max(th_max, K.tile_h);
-    hy_max = std::max(hy_max, K.halo_y);
-    for (Node *o : K.out_rasters) {
-      produced.insert(o);
-      producer[o] = &g;
-    }
-  }
-  if (W <= 0 || H <= 0) return false;
+  RowPlan R;
+  std::string why;
+  if (!row_plan(P.fr, P.plans, R, why)) return false;
+  const int W = R.W, H = R.H, th_max = R.th_max, hy_max = R.hy_max, M = R.M;
+  const std::set<Node *> &produced = R.produced;
+  std::map<const Group *, int> &need = R.need;
   for (Node *s : sink_nodes)
     if (!produced.count(s)) return false;
-  std::set<Node *> inputs;
-  for (auto &gp : P.fr.groups)
-    for (Node *n : P.plans[gp->id].in_rasters)
-      if (!produced.count(n)) inputs.insert(n);
   std::vector<Node *> host_in, dev_in;
-  for (Node *n : inputs) {
+  for (Node *n : R.inputs) {
     if (n->meta.W() != W || n->meta.H() != H) return false;
     if (n->kind == K_HOSTIN) {
       host_in.push_back(n);
     } else if (n->kind == K_DEVIN) {
-      if (((uintptr_t)n->dev->ptr & 127) != 0 || (n->dev->pitch & 15) != 0) return false;
+      if (n->dev->rows || ((uintptr_t)n->dev->ptr & 127) != 0 || (n->dev->pitch & 15) != 0) return false;
       dev_in.push_back(n);
     } else {
       return false;
@@ -746,19 +923,6 @@ bool Executor::evaluate_streamed(const Prepared &P, const std::vector<Node *> &t
     B = std::max(32, B / 32 * 32);
     if ((long long)H < 4LL * B) return false;
   }
-  // margins: rows beyond the band that each group must still produce
-  std::map<const Group *, int> need;
-  for (auto it = P.fr.groups.rbegin(); it != P.fr.groups.rend(); ++it) {
-    const Group *c = it->get();
-    const KernelPlan &K = P.plans[c->id];
-    const int nc = need[c];
-    for (Node *n : K.in_rasters) {
-      auto p = producer.find(n);
-      if (p != producer.end()) need[p->second] = std::max(need[p->second], nc + K.halo_y);
-    }
-  }
-  int M = 0;
-  for (auto &gp : P.fr.groups) M = std::max(M, need[gp.get()] + P.plans[gp->id].halo_y);
 
   CudaEnv &env = CudaEnv::get();
   cudaStream_t st = (cudaStream_t)env.stream();

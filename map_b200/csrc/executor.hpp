@@ -86,6 +86,16 @@ class Executor {
   // is set and nothing needs the host (no sinks with host memory, no writes,
   // no scalar read-backs).
   void evaluate(const std::vector<Node *> &targets, const std::vector<Sink> &sinks, bool async = false);
+  // Evaluates rows [y0, y1) of a program of Local / Focal groups over one raster
+  // shape: every sink goes to device memory holding those rows (its `dev` is the
+  // address of row y0), inputs are device rasters, whole or row bands holding at
+  // least the rows the range reads (the program's halo beyond it). Border
+  // decisions are made in whole-raster coordinates, so the rows equal those of a
+  // whole-raster evaluation. Blocks until done.
+  void evaluate_rows(const std::vector<Node *> &targets, const std::vector<Sink> &sinks, int y0, int y1);
+  // Rows beyond [y0, y1) (above and below, clipped to the raster) that
+  // evaluate_rows reads from the inputs of `targets`.
+  int row_margin(const std::vector<Node *> &targets);
   // Fusion + code generation + compilation only (no device needed).
   std::vector<std::string> compile_only(const std::vector<Node *> &targets, bool compile);
   std::string describe_groups(const std::vector<Node *> &targets);

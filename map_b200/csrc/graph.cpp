@@ -185,6 +185,17 @@ Node *Runtime::dev_input(void *ptr, long long pitch, Arr2 ds, int dt, Arr2 bs) {
   return add(std::move(n), "");
 }
 
+Node *Runtime::dev_input_rows(void *ptr, long long pitch, Arr2 ds, int dt, Arr2 bs, int row0, int rows) {
+  if (ds.n != 2 || ds.arr[0] <= 0 || ds.arr[1] <= 0) throw MapError("device input: data size must be 2-D and positive");
+  if (row0 < 0 || rows <= 0 || (long long)row0 + rows > (long long)ds.arr[1])
+    throw MapError("device row band: rows [" + std::to_string(row0) + ", " + std::to_string((long long)row0 + rows) +
+                   ") are not inside the raster's " + std::to_string(ds.arr[1]) + " rows");
+  Node *n = dev_input(ptr, pitch, ds, dt, bs);
+  n->dev->row0 = row0;
+  n->dev->rows = rows;
+  return n;
+}
+
 Node *Runtime::index(Node *arg, int dim) {
   check_node(arg, "index");
   if (dim != D1 && dim != D2) throw MapError("index: dimension must be D1 or D2");

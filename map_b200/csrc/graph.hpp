@@ -46,8 +46,12 @@ struct HostData {
 };
 
 struct DevData {
-  void *ptr = nullptr;    // caller-owned device memory
+  void *ptr = nullptr;    // caller-owned device memory (address of raster row `row0`)
   long long pitch = 0;    // bytes between rows
+  // Row band: the memory holds raster rows row0 .. row0 + rows - 1 only
+  // (rows == 0: the whole raster). Such an input is evaluated by row ranges
+  // (Executor::evaluate_rows) that read no row outside the band.
+  int row0 = 0, rows = 0;
 };
 
 struct Node {
@@ -98,6 +102,9 @@ struct Runtime {
   // Focal groups of float math compute two cells per thread step on packed
   // f32x2 instructions (bit-identical to one cell at a time); 0 turns it off.
   int paired_cells = 1;
+  // Hillshade compositions (python/hill.py:41-49) are generated through the
+  // shading identity of rewrite.hpp; 0 keeps the literal operator chain.
+  int algebraic_rewrite = 1;
   // incremented whenever nodes are destroyed (caches keyed by node ids check it)
   uint64_t epoch = 0;
   Arr2 default_bs{{256, 256}, 2};
@@ -110,6 +117,8 @@ struct Runtime {
   Node *scalar_param(Variant v);
   Node *host_input(const void *ptr, Arr2 ds, int dt, Arr2 bs, bool copy);
   Node *dev_input(void *ptr, long long pitch, Arr2 ds, int dt, Arr2 bs);
+  // Device input holding rows [row0, row0 + rows) of a ds raster; ptr is the address of row row0.
+  Node *dev_input_rows(void *ptr, long long pitch, Arr2 ds, int dt, Arr2 bs, int row0, int rows);
   Node *index(Node *arg, int dim);
   Node *rand(Node *seed, int dt, int mo);
   Node *cast(Node *arg, int dt);

@@ -64,6 +64,36 @@ template <class T> __device__ __forceinline__ void str(const RasterArg &r, int x
   ((T *)(r.p + (u64)(s64)y * (u64)r.pitch))[x] = v;
 }
 
+// Store of a Local / Focal result cell as an explicit global store that declares
+// no other memory effect, so the compiler keeps shared-memory taps (and other
+// loads) of one cell in registers for the next cells of the column instead of
+// reloading them after every store through a pointer that might alias them.
+// Only for kernels that never read, within the launch, what they write.
+template <int N> struct map_stg;
+template <> struct map_stg<1> {
+  static __device__ __forceinline__ void st(u64 p, u32 v) { asm volatile("st.global.u8 [%0], %1;" ::"l"(p), "r"(v)); }
+};
+template <> struct map_stg<2> {
+  static __device__ __forceinline__ void st(u64 p, u32 v) { asm volatile("st.global.u16 [%0], %1;" ::"l"(p), "r"(v)); }
+};
+template <> struct map_stg<4> {
+  static __device__ __forceinline__ void st(u64 p, u32 v) { asm volatile("st.global.u32 [%0], %1;" ::"l"(p), "r"(v)); }
+};
+template <> struct map_stg<8> {
+  static __device__ __forceinline__ void st(u64 p, u64 v) { asm volatile("st.global.u64 [%0], %1;" ::"l"(p), "l"(v)); }
+};
+template <int N> struct map_stg_word { typedef u32 type; };
+template <> struct map_stg_word<8> { typedef u64 type; };
+template <class T> __device__ __forceinline__ void str_out(const RasterArg &r, int x, int y, T v) {
+  const u64 p = r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x * sizeof(T);
+  typename map_stg_word<sizeof(T)>::type b = 0;
+  memcpy(&b, &v, sizeof(T));
+  map_stg<sizeof(T)>::st(p, b);
+}
+template <> __device__ __forceinline__ void str_out<bool>(const RasterArg &r, int x, int y, bool v) {
+  map_stg<1>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, v ? 1u : 0u);
+}
+
 // ------------------------------------------------------------------ atan2 (float)
 
 // Two-argument arctangent of float32 operands, at most 1.5 ulp from the
@@ -411,6 +441,68 @@ __device__ __forceinline__ PR<float> map_cosf(const PR<float> &x) {
   PR<float> sr, cr;
   map_sincos_reduced(x, qa, qb, sr, cr);
   return PR<float>(map_quadrant_cos(qa, sr.a, cr.a), map_quadrant_cos(qb, sr.b, cr.b));
+}
+
+// ------------------------------------------------------------------ shading identity
+
+#define MAP_INF_F __int_as_float(0x7f800000)
+
+// 1 / sqrt(v) for finite v >= 1: the hardware estimate (rsqrt.approx.f32) and one
+// Newton-Raphson step r' = r + (r / 2)(1 - v r^2), every operation rounded once.
+__device__ __forceinline__ float map_rsqrt_est(float v) {
+  float r;
+  asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
+__device__ __forceinline__ float map_rsqrt(float v) {
+  const float r = map_rsqrt_est(v);
+  const float e = __fmaf_rn(-__fmul_rn(v, r), r, 1.0f);
+  return __fmaf_rn(__fmul_rn(r, 0.5f), e, r);
+}
+__device__ __forceinline__ PR<float> map_rsqrt(const PR<float> &v) {
+  const float2 r = make_float2(map_rsqrt_est(v.a), map_rsqrt_est(v.b));
+  const float2 e = __ffma2_rn(__fmul2_rn(pr_f2(v), make_float2(-r.x, -r.y)), r, f2_of(1.0f));
+  return pr_of(__ffma2_rn(__fmul2_rn(r, f2_of(0.5f)), e, r));
+}
+
+// Hillshade through the shading identity (the host's rewrite of
+//   cz cos(s) + sz sin(s) cos(ar - aspect),  s = atan(k sqrt(x^2 + y^2)),
+//   aspect = atan2(y, -x) wrapped into [0, 2 PI'), x == 0 by its own branch):
+//   hs = (cz + szk (y S - x C)) / sqrt(1 + kk (x^2 + y^2)),  szk = sz k, kk = k^2.
+// (S, C) is the unit vector of the light direction the reference chain uses for
+// the cell: (S0, C0) where its atan2 is not negative, (S1, C1) where the atan2 is
+// negative and the wrap adds the script's 2 PI' (not 2 pi), SH / S3 for x == 0
+// (aspect PI'/2 or 3 PI'/2). atan2(y, -x) < 0 exactly when y < 0, or y is -0 and
+// -x < 0. Returns hs and q = x^2 + y^2; the caller takes the literal chain where
+// q is not finite. The pair form performs the same operations lane by lane
+// (packed where both lanes do the same), so its lanes equal the scalar form.
+template <bool K1>
+__device__ __forceinline__ float map_shade(float x, float y, float cz, float szk, float kk, float S0, float C0,
+                                           float S1, float C1, float SH, float S3, float &q) {
+  q = __fmaf_rn(x, x, __fmul_rn(y, y));
+  const bool nz = x != 0.0f;
+  const bool neg = y < 0.0f || ((__float_as_uint(y) >> 31) && x > 0.0f);
+  const float S = nz ? (neg ? S1 : S0) : (y > 0.0f ? SH : S3);
+  const float C = nz ? (neg ? C1 : C0) : 0.0f;
+  const float num = __fmaf_rn(y, S, __fmul_rn(x, -C));
+  const float v = K1 ? __fadd_rn(1.0f, q) : __fmaf_rn(kk, q, 1.0f);
+  return __fmul_rn(__fmaf_rn(szk, num, cz), map_rsqrt(v));
+}
+template <bool K1>
+__device__ __forceinline__ PR<float> map_shade(const PR<float> &x, const PR<float> &y, float cz, float szk, float kk,
+                                               float S0, float C0, float S1, float C1, float SH, float S3,
+                                               PR<float> &q) {
+  const float2 X = pr_f2(x), Y = pr_f2(y);
+  q = pr_of(__ffma2_rn(X, X, __fmul2_rn(Y, Y)));
+  const bool nza = x.a != 0.0f, nzb = x.b != 0.0f;
+  const bool nga = y.a < 0.0f || ((__float_as_uint(y.a) >> 31) && x.a > 0.0f);
+  const bool ngb = y.b < 0.0f || ((__float_as_uint(y.b) >> 31) && x.b > 0.0f);
+  const float2 S = make_float2(nza ? (nga ? S1 : S0) : (y.a > 0.0f ? SH : S3),
+                               nzb ? (ngb ? S1 : S0) : (y.b > 0.0f ? SH : S3));
+  const float2 nC = make_float2(nza ? (nga ? -C1 : -C0) : -0.0f, nzb ? (ngb ? -C1 : -C0) : -0.0f);
+  const float2 num = __ffma2_rn(Y, S, __fmul2_rn(X, nC));
+  const float2 v = K1 ? __fadd2_rn(f2_of(1.0f), pr_f2(q)) : __ffma2_rn(f2_of(kk), pr_f2(q), f2_of(1.0f));
+  return pr_of(__fmul2_rn(__ffma2_rn(f2_of(szk), num, f2_of(cz)), pr_f2(map_rsqrt(pr_of(v)))));
 }
 
 // ------------------------------------------------------------------ border rule

@@ -683,6 +683,27 @@ def from_device(ptr, pitch, ds, dt, bs=None):
     return Raster(_lib.ma_fromDevice(ct.c_void_p(ptr), pitch, Array(ds), dt, Array(bs or [])))
 
 
+def from_device_rows(ptr, pitch, ds, dt, row0, rows, bs=None):
+    """Raster input from device memory holding only rows [row0, row0 + rows) of a
+    ds = [x, y] raster (`ptr` is the address of row row0); evaluated by eval_rows."""
+    return Raster(_lib.ma_fromDeviceRows(ct.c_void_p(ptr), pitch, Array(ds), dt, Array(bs or []), row0, rows))
+
+
+def eval_rows(rasters, buffers, y0, y1):
+    """Evaluates rows [y0, y1) of `rasters` into device buffers: buffers[i] =
+    (address of row y0, pitch in bytes). Borders are decided in whole-raster
+    coordinates, so the rows equal a whole-raster evaluation's."""
+    n = len(rasters)
+    dst = (ct.c_void_p * n)(*[b[0] for b in buffers])
+    pitch = (ct.c_longlong * n)(*[b[1] for b in buffers])
+    _lib.ma_evalRows(_node_array(rasters), n, dst, pitch, y0, y1)
+
+
+def row_margin(*rasters):
+    """Rows beyond a row range that eval_rows of these rasters reads from their inputs."""
+    return _lib.ma_rowMargin(_node_array(rasters), len(rasters))
+
+
 def to_numpy(raster, out=None):
     """Evaluates a raster and returns it as a 2-D NumPy array."""
     import numpy as np
@@ -731,6 +752,17 @@ def set_paired_cells(on):
 
 def get_paired_cells():
     return bool(_lib.ma_getPairedCells())
+
+
+def set_algebraic_rewrite(on):
+    """Hillshade compositions through the shading identity (no per-cell
+    transcendental functions, results within the hillshade tolerance); False
+    generates the literal operator chain."""
+    _lib.ma_setAlgebraicRewrite(1 if on else 0)
+
+
+def get_algebraic_rewrite():
+    return bool(_lib.ma_getAlgebraicRewrite())
 
 
 def last_band_count():
@@ -941,6 +973,12 @@ _sig('ma_setStreamRows', [ct.c_int], None)
 _sig('ma_getStreamRows', [], ct.c_int, check=False)
 _sig('ma_setPairedCells', [ct.c_int], None)
 _sig('ma_getPairedCells', [], ct.c_int, check=False)
+_sig('ma_setAlgebraicRewrite', [ct.c_int], None)
+_sig('ma_fromDeviceRows', [ct.c_void_p, ct.c_longlong, Array, ct.c_int, Array, ct.c_int, ct.c_int], Node)
+_sig('ma_evalRows', [ct.POINTER(Node), ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_longlong), ct.c_int, ct.c_int],
+     ct.c_int)
+_sig('ma_rowMargin', [ct.POINTER(Node), ct.c_int], ct.c_int)
+_sig('ma_getAlgebraicRewrite', [], ct.c_int, check=False)
 _sig('ma_compileOnly', [ct.POINTER(Node), ct.c_int, ct.c_int], ct.c_int)
 _sig('ma_describeGroups', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_generatedSource', [ct.POINTER(Node), ct.c_int, ct.c_char_p, ct.c_size_t], ct.c_size_t)

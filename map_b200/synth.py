@@ -26,8 +26,11 @@ def _axis_weights(n, cells, xp, device=None):
     return i, f
 
 
-def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cells=4, xp=np, device=None):
-    """float32 (h, w) fractal Brownian value-noise DEM rescaled to [lo, hi], row-major."""
+def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cells=4, xp=np, device=None, threads=1):
+    """float32 (h, w) fractal Brownian value-noise DEM rescaled to [lo, hi], row-major.
+    threads > 1 (numpy only) computes row bands in parallel, with the same result."""
+    if xp is np and threads > 1 and h >= 64 * threads:
+        return _fbm_dem_bands(h, w, seed, octaves, persistence, lo, hi, base_cells, threads)
     rng = np.random.default_rng(seed)
     side = max(h, w)
     total = None
@@ -62,6 +65,49 @@ def fbm_dem(h, w, seed, octaves=8, persistence=0.5, lo=0.0, hi=3000.0, base_cell
     out = (total - mn) / (mx - mn) * (hi - lo) + lo
     # row-major (C-contiguous) like every raster the engine reads through raw pointers
     return np.ascontiguousarray(out, dtype=np.float32) if xp is np else out.float().contiguous()
+
+
+def _fbm_dem_bands(h, w, seed, octaves, persistence, lo, hi, base_cells, threads):
+    import concurrent.futures as cf
+    rng = np.random.default_rng(seed)
+    side = max(h, w)
+    lats = []
+    for o in range(octaves):
+        cells = base_cells * (2 ** o)
+        cx = max(1, int(round(cells * w / side)))
+        cy = max(1, int(round(cells * h / side)))
+        lats.append((rng.random((cy + 1, cx + 1)), cx, cy))
+    total = np.empty((h, w), np.float64)
+
+    def band(r0, r1):
+        amp = 1.0
+        acc = None
+        for lat, cx, cy in lats:
+            iy, fy = _axis_weights(h, cy, np)
+            ix, fx = _axis_weights(w, cx, np)
+            iy, fy = iy[r0:r1], fy[r0:r1]
+            top = lat[iy][:, ix] * (1 - fx)[None, :] + lat[iy][:, ix + 1] * fx[None, :]
+            bot = lat[iy + 1][:, ix] * (1 - fx)[None, :] + lat[iy + 1][:, ix + 1] * fx[None, :]
+            noise = top * (1 - fy)[:, None] + bot * fy[:, None]
+            acc = noise * amp if acc is None else acc + noise * amp
+            amp *= persistence
+        total[r0:r1] = acc
+        return acc.min(), acc.max()
+
+    step = (h + threads * 4 - 1) // (threads * 4)
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        mm = list(ex.map(lambda r: band(r, min(h, r + step)), range(0, h, step)))
+    mn = min(m[0] for m in mm)
+    mx = max(m[1] for m in mm)
+    out = np.empty((h, w), np.float32)
+
+    def rescale(r0):
+        r1 = min(h, r0 + step)
+        out[r0:r1] = (total[r0:r1] - mn) / (mx - mn) * (hi - lo) + lo
+
+    with cf.ThreadPoolExecutor(max_workers=threads) as ex:
+        list(ex.map(rescale, range(0, h, step)))
+    return out
 
 
 def bernoulli_u8(h, w, p, seed):

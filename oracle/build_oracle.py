@@ -15,7 +15,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("MAP_REFERENCE_DIR", "/root/reference")
+# The reference checkout: MAP_REFERENCE_DIR, else a `reference` directory beside
+# this repository's root (absent on machines that only run the prebuilt files).
+REF = os.environ.get("MAP_REFERENCE_DIR") or os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference")
 UTIL_SOURCES = ["DataType", "VariantType", "UnaryType", "BinaryType", "ReductionType", "NumDim", "MemOrder"]
 
 
@@ -33,12 +35,44 @@ def _stale(target, deps):
 
 
 def build_oracle():
+    """Portable build (the checker of the tests; travels with the repository)."""
     out_dir = os.path.join(HERE, "_build")
     os.makedirs(out_dir, exist_ok=True)
     lib = os.path.join(out_dir, "liboracle.so")
     src = os.path.join(HERE, "oracle.c")
     if _stale(lib, [src]):
         _run(["gcc", "-O2", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", src, "-lm", "-o", lib])
+    return lib
+
+
+def _host_cpu_tag():
+    import hashlib
+    import platform
+    info = platform.machine()
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith(("model name", "flags")):
+                    info += line
+                if line.strip() == "":
+                    break
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:10]
+
+
+def build_oracle_native():
+    """-O3 -march=native build for timing the CPU baseline, compiled on the
+    machine that runs it (the file name carries a digest of the host CPU model
+    and flags, so a build made elsewhere is never loaded). Same semantics:
+    -ffp-contract=off keeps every operation rounded once."""
+    out_dir = os.path.join(HERE, "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    lib = os.path.join(out_dir, "liboracle_native_%s.so" % _host_cpu_tag())
+    src = os.path.join(HERE, "oracle.c")
+    if _stale(lib, [src]):
+        _run(["gcc", "-O3", "-march=native", "-std=c11", "-fPIC", "-shared", "-ffp-contract=off", "-fno-fast-math", src,
+              "-lm", "-o", lib])
     return lib
 
 

@@ -112,30 +112,51 @@ static HillConst hill_const(double zenith, double azimuth) {
 static const int SOBEL_H[9] = {-1, 0, 1, -2, 0, 2, -1, 0, 1};
 static const int SOBEL_V[9] = {-1, -2, -1, 0, 0, 0, 1, 2, 1};
 
+/* One cell of the FP32 chain. */
+static float hill_cell_f32(const float *dem, int W, int H, int BS0, int BS1, int border, const HillConst *c, int x,
+                           int y, float *slope_v, float *aspect_v) {
+  float ch = 0.0f, cv = 0.0f;
+  for (int i1 = -1; i1 <= 1; i1++)
+    for (int i0 = -1; i0 <= 1; i0++) {
+      float t = tapf(dem, W, H, BS0, BS1, border, x, y, i0, i1);
+      ch = ch + t * SOBEL_H[(i1 + 1) * 3 + (i0 + 1)];
+      cv = cv + t * SOBEL_V[(i1 + 1) * 3 + (i0 + 1)];
+    }
+  float gx = ch / 8;
+  float gy = cv / 8;
+  float s = atanf(1 * sqrtf(gx * gx + gy * gy));
+  float z1 = (float)(uint8_t)(gx != 0) * atan2f(gy, -gx);
+  z1 = z1 + (float)(uint8_t)(z1 < 0) * c->pi2;
+  float z0 = (float)(uint8_t)(gx == 0) * ((float)(uint8_t)(gy > 0) * c->pih + (float)(uint8_t)(gy < 0) * c->pi32);
+  float asp = z1 + z0;
+  *slope_v = s;
+  *aspect_v = asp;
+  return c->cz * cosf(s) + c->sz * sinf(s) * cosf(c->ar - asp);
+}
+
 void orc_hillshade_f32(const float *dem, int W, int H, int BS0, int BS1, int border, double zenith, double azimuth,
                        float *out, float *slope_out, float *aspect_out) {
   HillConst c = hill_const(zenith, azimuth);
   for (int y = 0; y < H; y++)
     for (int x = 0; x < W; x++) {
-      float ch = 0.0f, cv = 0.0f;
-      for (int i1 = -1; i1 <= 1; i1++)
-        for (int i0 = -1; i0 <= 1; i0++) {
-          float t = tapf(dem, W, H, BS0, BS1, border, x, y, i0, i1);
-          ch = ch + t * SOBEL_H[(i1 + 1) * 3 + (i0 + 1)];
-          cv = cv + t * SOBEL_V[(i1 + 1) * 3 + (i0 + 1)];
-        }
-      float gx = ch / 8;
-      float gy = cv / 8;
-      float s = atanf(1 * sqrtf(gx * gx + gy * gy));
-      float z1 = (float)(uint8_t)(gx != 0) * atan2f(gy, -gx);
-      z1 = z1 + (float)(uint8_t)(z1 < 0) * c.pi2;
-      float z0 = (float)(uint8_t)(gx == 0) * ((float)(uint8_t)(gy > 0) * c.pih + (float)(uint8_t)(gy < 0) * c.pi32);
-      float asp = z1 + z0;
-      float hs = c.cz * cosf(s) + c.sz * sinf(s) * cosf(c.ar - asp);
+      float s, asp;
       size_t i = (size_t)y * W + x;
-      out[i] = hs;
+      out[i] = hill_cell_f32(dem, W, H, BS0, BS1, border, &c, x, y, &s, &asp);
       if (slope_out) slope_out[i] = s;
       if (aspect_out) aspect_out[i] = asp;
+    }
+}
+
+/* Rows [y0, y1) of the same computation over the whole raster (borders decided
+ * by the whole raster), written to out[y * W + x]: the CPU baseline runs row
+ * bands of one raster on several threads with this. */
+void orc_hillshade_f32_rows(const float *dem, int W, int H, int BS0, int BS1, int border, double zenith,
+                            double azimuth, int y0, int y1, float *out) {
+  HillConst c = hill_const(zenith, azimuth);
+  for (int y = y0; y < y1; y++)
+    for (int x = 0; x < W; x++) {
+      float s, asp;
+      out[(size_t)y * W + x] = hill_cell_f32(dem, W, H, BS0, BS1, border, &c, x, y, &s, &asp);
     }
 }
 
@@ -160,6 +181,49 @@ void orc_hillshade_f64(const float *dem, int W, int H, int BS0, int BS1, int bor
       double z0 = (gx == 0) * ((gy > 0) * (double)c.pih + (gy < 0) * (double)c.pi32);
       double asp = z1 + z0;
       out[(size_t)y * W + x] = (double)c.cz * cos(s) + (double)c.sz * sin(s) * cos((double)c.ar - asp);
+    }
+}
+
+/* Size of one float32 ulp at |v| (the spacing of floats there). */
+static double ulp32(double v) {
+  float f = fabsf((float)v);
+  if (!(f < INFINITY)) return INFINITY;
+  return (double)nextafterf(f, INFINITY) - (double)f;
+}
+
+/* First-order rounding-error scale of the FP32 hillshade chain at each cell,
+ * from FP64 values: the chain evaluates cos and sin at rounded angles, so its
+ * output moves by |d hs / d A| ulp(max(|aspect|, |A|)) for the azimuth
+ * difference A = ar - aspect and by |d hs / d s| ulp(s) for the slope s, and
+ * each of its two terms cz cos(s) and sz sin(s) cos(A) is itself rounded:
+ *   bound = sz sin(s) |sin A| ulp(max(|aspect|, |A|))
+ *         + (cz sin(s) + sz |cos(s) cos(A)|) ulp(s) + ulp(T1) + ulp(T2).
+ * Used by the tests to state the hillshade tolerance where the two terms
+ * cancel (there 4 ulp of the result is far below the chain's own error). */
+void orc_hillshade_bound(const float *dem, int W, int H, int BS0, int BS1, int border, double zenith, double azimuth,
+                         double *bound) {
+  HillConst c = hill_const(zenith, azimuth);
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      double ch = 0.0, cv = 0.0;
+      for (int i1 = -1; i1 <= 1; i1++)
+        for (int i0 = -1; i0 <= 1; i0++) {
+          double t = tapf(dem, W, H, BS0, BS1, border, x, y, i0, i1);
+          ch += t * SOBEL_H[(i1 + 1) * 3 + (i0 + 1)];
+          cv += t * SOBEL_V[(i1 + 1) * 3 + (i0 + 1)];
+        }
+      double gx = ch / 8, gy = cv / 8;
+      double s = atan(sqrt(gx * gx + gy * gy));
+      double z1 = (gx != 0) * atan2(gy, -gx);
+      z1 = z1 + (z1 < 0) * (double)c.pi2;
+      double z0 = (gx == 0) * ((gy > 0) * (double)c.pih + (gy < 0) * (double)c.pi32);
+      double asp = z1 + z0;
+      double A = (double)c.ar - asp;
+      double t1 = (double)c.cz * cos(s), t2 = (double)c.sz * sin(s) * cos(A);
+      double amax = fabs(asp) > fabs(A) ? fabs(asp) : fabs(A);
+      bound[(size_t)y * W + x] = (double)c.sz * sin(s) * fabs(sin(A)) * ulp32(amax) +
+                                 ((double)c.cz * sin(s) + (double)c.sz * fabs(cos(s) * cos(A))) * ulp32(s) +
+                                 ulp32(t1) + ulp32(t2);
     }
 }
 
@@ -189,6 +253,24 @@ void orc_life(const uint8_t *in, int W, int H, int BS0, int BS1, int border, int
   memcpy(out, a, n);
   free(a);
   free(b);
+}
+
+/* One generation of life.py for rows [y0, y1) only, reading the whole raster
+ * `in` (W x H) and writing out[y * W + x]: with in holding valid rows
+ * [y0 - 1, y1 + 1) only, this is what one rank of a row-band split computes. */
+void orc_life_rows(const uint8_t *in, int W, int H, int BS0, int BS1, int border, int y0, int y1, uint8_t *out) {
+  for (int y = y0; y < y1; y++)
+    for (int x = 0; x < W; x++) {
+      int32_t nbh = 0;
+      for (int i1 = -1; i1 <= 1; i1++)
+        for (int i0 = -1; i0 <= 1; i0++) {
+          int m = (i0 == 0 && i1 == 0) ? 0 : 1;
+          nbh = nbh + tapu8(in, W, H, BS0, BS1, border, x, y, i0, i1) * m;
+        }
+      uint8_t s = in[(size_t)y * W + x];
+      uint8_t e3 = (uint8_t)(nbh == 3), e2 = (uint8_t)(nbh == 2);
+      out[(size_t)y * W + x] = (uint8_t)(e3 + (uint8_t)(e2 * s));
+    }
 }
 
 /* ------------------------------------------------------------ weighted sum */

@@ -40,7 +40,10 @@ def lib():
         L.orc_conv_f32.argtypes = [f32p, I, I, I, I, I, f32p, I, I, f32p]
         L.orc_hillshade_f32.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f32p, ct.c_void_p, ct.c_void_p]
         L.orc_hillshade_f64.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f64p]
+        L.orc_hillshade_f32_rows.argtypes = [ct.c_void_p, I, I, I, I, I, ct.c_double, ct.c_double, I, I, ct.c_void_p]
+        L.orc_hillshade_bound.argtypes = [f32p, I, I, I, I, I, ct.c_double, ct.c_double, f64p]
         L.orc_life.argtypes = [u8p, I, I, I, I, I, I, u8p]
+        L.orc_life_rows.argtypes = [u8p, I, I, I, I, I, I, I, u8p]
         L.orc_rand_u8.argtypes = [ct.c_uint32, I, I, I, I, u8p]
         L.orc_d8.argtypes = [f32p, I, I, I, I, I, u8p]
         L.orc_flowacc_s32.argtypes = [i32p, u8p, I, I, i32p]
@@ -53,6 +56,32 @@ def lib():
         L.orc_focal_src.restype = I
         _lib = L
     return _lib
+
+
+_native = None
+
+
+def lib_native():
+    """The -O3 -march=native build of the same oracle, compiled on this host
+    (oracle/build_oracle.py:build_oracle_native), for timing the CPU baseline."""
+    global _native
+    with _lock:
+        if _native is None:
+            from oracle import build_oracle
+            L = ct.CDLL(build_oracle.build_oracle_native())
+            f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+            I = ct.c_int
+            L.orc_hillshade_f32_rows.argtypes = [ct.c_void_p, I, I, I, I, I, ct.c_double, ct.c_double, I, I, ct.c_void_p]
+            L.orc_wsum_f32.argtypes = [ct.POINTER(ct.c_void_p), f32p, I, ct.c_size_t, ct.c_void_p]
+            _native = L
+    return _native
+
+
+def hillshade_rows(L, dem, out, bs, border, y0, y1, zenith=45.0, azimuth=315.0):
+    """Rows [y0, y1) of the FP32 hillshade of the whole `dem` into `out` (both
+    C-contiguous float32 arrays of the raster's shape), with library L."""
+    L.orc_hillshade_f32_rows(dem.ctypes.data, dem.shape[1], dem.shape[0], bs[0], bs[1], border, zenith, azimuth,
+                             y0, y1, out.ctypes.data)
 
 
 def ref_util():
@@ -99,11 +128,40 @@ def hillshade_f64(dem, bs, border=0, zenith=45.0, azimuth=315.0):
     return out
 
 
+def hillshade_bound(dem, bs, border=0, zenith=45.0, azimuth=315.0):
+    """Per-cell first-order rounding-error scale of the FP32 hillshade chain
+    (angle roundings and the two terms' own roundings; see oracle.c)."""
+    dem = _c(dem, np.float32)
+    out = np.empty(dem.shape, np.float64)
+    lib().orc_hillshade_bound(dem, dem.shape[1], dem.shape[0], bs[0], bs[1], border, zenith, azimuth, out)
+    return out
+
+
+def hill_tolerance(gpu, ref32, bound):
+    """The hillshade tolerance against the FP32 oracle: within 4 ulp or 1e-5
+    relative of it, or, where its two terms cancel, within 4 times the chain's
+    own first-order rounding-error scale at that cell (hillshade_bound).
+    Returns (ok mask, |gpu - ref32|, mask of cells that pass only through the
+    cancellation clause)."""
+    d = np.abs(np.asarray(gpu, np.float64) - np.asarray(ref32, np.float64))
+    strict = (d <= 4 * ulp_f32(ref32)) | (d <= 1e-5 * np.abs(np.asarray(ref32, np.float64)))
+    cancel = d <= 4 * bound
+    nan_same = np.isnan(np.asarray(gpu, np.float64)) & np.isnan(np.asarray(ref32, np.float64))
+    ok = strict | cancel | nan_same
+    return ok, d, ok & ~strict & ~nan_same
+
+
 def life(state, bs, gens, border=0):
     s = _c(state, np.uint8)
     out = np.empty_like(s)
     lib().orc_life(s, s.shape[1], s.shape[0], bs[0], bs[1], border, gens, out)
     return out
+
+
+def life_rows(state, out, bs, border, y0, y1):
+    """One life.py generation for rows [y0, y1) of `state` (whole-raster
+    array; only rows [y0 - 1, y1 + 1) are read) into the same rows of `out`."""
+    lib().orc_life_rows(state, state.shape[1], state.shape[0], bs[0], bs[1], border, y0, y1, out)
 
 
 def rand_u8(seed, shape, bs):

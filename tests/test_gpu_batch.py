@@ -78,3 +78,42 @@ def test_batch_with_dependent_groups(M):
     for r, o in outs:
         assert np.array_equal(o.numpy(), M.to_numpy(r))
         o.free()
+
+
+def test_mix_rasters_against_oracle(fresh):
+    """Rasters of the 512-raster mix's kind at its large end, checked against the
+    oracle (not only against the engine itself): raster-edge mirror border,
+    sides of 1500 and more, sizes that are multiples of neither 256 nor 64,
+    aspect ratios near 0.5 and near 2, 256 x 256 blocks; hillshade within the
+    hillshade tolerance, the 6-layer overlay bit-exact."""
+    from oracle import oracle as O
+    M = fresh
+    M.set_border(M.BORDER_RASTER_MIRROR)
+    weights = [0.1, 0.2, 0.3, 0.15, 0.15, 0.1]
+    shapes = [(1537, 3070), (3001, 1501), (1999, 1999), (1500, 1700), (2047, 1503), (1601, 2900),
+              (1777, 1555), (2900, 1450)]   # (width, height)
+    b = M.Batch()
+    cases = []
+    for i, (w, h) in enumerate(shapes):
+        dem_np = synth.fbm_dem(h, w, seed=300 + i)
+        layers_np = [synth.uniform_f32(h, w, seed=400 + 10 * i + j) for j in range(6)]
+        dem = M.from_numpy(dem_np, bs=[256, 256])
+        layers = [M.from_numpy(l, bs=[256, 256]) for l in layers_np]
+        hs, ov = W.hillshade(dem), W.wsum(layers, weights)
+        o1, o2 = DevBuf(M, (h, w)), DevBuf(M, (h, w))
+        b.add([hs, ov], [(o1.ptr, o1.pitch), (o2.ptr, o2.pitch)])
+        cases.append((dem_np, layers_np, o1, o2))
+    b.prepare(autotune=True)
+    b.run()
+    only_total = 0
+    for dem_np, layers_np, o1, o2 in cases:
+        got = o1.numpy()
+        ref32 = O.hillshade_f32(dem_np, (256, 256), 1)
+        ok, d, only = O.hill_tolerance(got, ref32, O.hillshade_bound(dem_np, (256, 256), 1))
+        assert ok.all(), (dem_np.shape, int((~ok).sum()), float(d.max()))
+        only_total += int(only.sum())
+        ref_ov = O.wsum_f32(layers_np, np.array(weights, np.float32))
+        assert np.array_equal(o2.numpy().view(np.uint32), ref_ov.view(np.uint32))
+        o1.free()
+        o2.free()
+    assert only_total < 0.02 * sum(w * h for w, h in shapes)

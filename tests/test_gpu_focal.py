@@ -12,18 +12,25 @@ from oracle import oracle as O
 pytestmark = pytest.mark.gpu
 
 
-def hill_tolerance_ok(gpu, ref32, ref64):
-    """Float tolerance for hillshade: within 4 ulp or 1e-5 relative of the FP32
-    oracle; where the two O(1) terms of the formula cancel (|hs| small) the
-    bound is 4 ulp of 1.0, the magnitude of the cancelling terms."""
-    d = np.abs(gpu.astype(np.float64) - ref32.astype(np.float64))
-    ulp = O.ulp_f32(ref32)
-    ok = (d <= 4 * ulp) | (d <= 1e-5 * np.abs(ref32)) | (d <= 4 * float(np.spacing(np.float32(1.0))))
-    err_gpu = np.abs(gpu - ref64).max()
-    err_ref = np.abs(ref32 - ref64).max()
-    return ok, d, err_gpu, err_ref
+def hill_check(gpu, dem_np, bs, border):
+    """Hillshade against the oracle: within 4 ulp or 1e-5 relative of the FP32
+    oracle, or, where the formula's two terms cancel, within 4 times the FP32
+    chain's own first-order rounding-error scale at the cell (O.hill_tolerance);
+    and no further from the FP64 value than the FP32 restatement, up to 4 ulp of 1.
+    Returns the share of cells that pass only through the cancellation clause."""
+    ref32 = O.hillshade_f32(dem_np, bs, border)
+    ref64 = O.hillshade_f64(dem_np, bs, border)
+    ok, d, only = O.hill_tolerance(gpu, ref32, O.hillshade_bound(dem_np, bs, border))
+    bad = np.argwhere(~ok)
+    assert ok.all(), "%d cells out of tolerance, first %s: gpu %r ref %r" % (
+        len(bad), bad[:3].tolist(), gpu[tuple(bad[0])], ref32[tuple(bad[0])])
+    err_gpu = np.nanmax(np.abs(gpu - ref64))
+    err_ref = np.nanmax(np.abs(ref32 - ref64))
+    assert err_gpu <= err_ref + 4 * float(np.spacing(np.float32(1.0)))
+    return ref32, only.mean()
 
 
+@pytest.mark.parametrize("rewrite", [True, False])
 @pytest.mark.parametrize("shape,bs,border,mode", [
     ((1024, 1024), (256, 256), 0, 0),
     ((1024, 1024), (256, 256), 0, 1),
@@ -37,27 +44,53 @@ def hill_tolerance_ok(gpu, ref32, ref64):
     ((200, 270), (90, 70), 0, 1),     # plain launches from block origins not on a 16-byte boundary
     ((190, 333), (100, 60), 1, 1),
 ])
-def test_hillshade_matches_oracle(fresh, shape, bs, border, mode):
+def test_hillshade_matches_oracle(fresh, shape, bs, border, mode, rewrite):
     M = fresh
     M.set_border(border)
     M.set_exec_mode(mode)
+    M.set_algebraic_rewrite(rewrite)
     dem_np = synth.fbm_dem(shape[0], shape[1], seed=7)
     dem = M.from_numpy(dem_np, bs=list(bs))
     hs = W.hillshade(dem)
+    assert ("map_shade" in M.generated_source(hs)) == rewrite
     gpu = M.to_numpy(hs)
     assert M.last_launch_count() >= 1
-    ref32 = O.hillshade_f32(dem_np, bs, border)
-    ref64 = O.hillshade_f64(dem_np, bs, border)
-    ok, d, err_gpu, err_ref = hill_tolerance_ok(gpu, ref32, ref64)
-    bad = np.argwhere(~ok)
-    assert ok.all(), "%d cells out of tolerance, first %s: gpu %r ref %r" % (
-        len(bad), bad[:3].tolist(), gpu[tuple(bad[0])], ref32[tuple(bad[0])])
-    # the GPU result is no further from the FP64 value than the FP32 restatement, up to 4 ulp of 1
-    assert err_gpu <= err_ref + 4 * float(np.spacing(np.float32(1.0)))
-    # bit-identical on the large majority of cells (differences come only from
-    # transcendental-function implementations)
-    if gpu.size >= 4096:
+    ref32, only = hill_check(gpu, dem_np, bs, border)
+    # the literal chain is bit-identical to the FP32 restatement on the large
+    # majority of cells (differences come only from transcendental-function
+    # implementations); the rewrite evaluates none of them
+    if gpu.size >= 4096 and not rewrite:
         assert (gpu == ref32).mean() > 0.5
+    assert only < 0.02
+
+
+def test_hillshade_rewrite_literal_chain_where_not_finite(fresh):
+    """Cells whose x^2 + y^2 is not finite (NaN or infinite DEM cells, gradients
+    above 1.8e19) take the literal chain: identical to the switch turned off."""
+    M = fresh
+    dem_np = synth.fbm_dem(200, 300, seed=11)
+    dem_np.ravel()[::503] = np.nan
+    dem_np.ravel()[7::701] = np.inf
+    dem_np.ravel()[11::907] = -np.inf
+    dem_np.ravel()[13::1009] = 3e25
+    dem_np.ravel()[17::1103] = -1e30
+    out = {}
+    for rw in (True, False):
+        M.set_algebraic_rewrite(rw)
+        out[rw] = M.to_numpy(W.hillshade(M.from_numpy(dem_np, bs=[64, 64])))
+    x = O.conv_f32(dem_np, np.array([[-1, 0, 1], [-2, 0, 2], [-1, 0, 1]], np.float32), (64, 64)) * np.float32(0.125)
+    y = O.conv_f32(dem_np, np.array([[-1, -2, -1], [0, 0, 0], [1, 2, 1]], np.float32), (64, 64)) * np.float32(0.125)
+    with np.errstate(over="ignore", invalid="ignore"):
+        q = np.float32(x) * x + np.float32(y) * y
+    lit = ~(q < np.inf)
+    assert lit.sum() > 100
+    a, b = out[True][lit], out[False][lit]
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    fin = ~lit
+    ref32 = O.hillshade_f32(dem_np, (64, 64), 0)
+    bound = O.hillshade_bound(dem_np, (64, 64), 0)
+    ok, d, only = O.hill_tolerance(out[True][fin], ref32[fin], bound[fin])
+    assert ok.all()
 
 
 def test_hillshade_fused_and_plain_are_identical(fresh):

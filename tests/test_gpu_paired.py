@@ -51,10 +51,12 @@ def same(a, b):
     assert not diff.any(), int(diff.sum())
 
 
+@pytest.mark.parametrize("rewrite", [True, False])
 @pytest.mark.parametrize("border", [0, 1, 2])
-def test_hillshade_paired_bit_identical(P, border):
+def test_hillshade_paired_bit_identical(P, border, rewrite):
     M = P
     M.set_border(border)
+    M.set_algebraic_rewrite(rewrite)
     dem = synth.fbm_dem(777, 1000, seed=4)
     dem.ravel()[::997] = np.nan
     dem.ravel()[5::1999] = -0.0
@@ -121,13 +123,13 @@ def test_plain_mode_blocks(P, bs):
     same(a, b)
 
 
-def test_paired_hillshade_matches_oracle(P):
+@pytest.mark.parametrize("rewrite", [True, False])
+def test_paired_hillshade_matches_oracle(P, rewrite):
     from oracle import oracle as O
     M = P
+    M.set_algebraic_rewrite(rewrite)
     dem = synth.fbm_dem(300, 500, seed=6)
     got = M.to_numpy(W.hillshade(M.from_numpy(dem, bs=[128, 128])))
     ref = O.hillshade_f32(dem, (128, 128), 0)
-    d = np.abs(got.astype(np.float64) - ref)
-    ulp = O.ulp_f32(ref)
-    ok = (d <= 4 * ulp) | (d <= 1e-5 * np.abs(ref)) | (d <= 4 * float(np.spacing(np.float32(1.0))))
+    ok, d, only = O.hill_tolerance(got, ref, O.hillshade_bound(dem, (128, 128), 0))
     assert ok.all()
