@@ -367,6 +367,20 @@ struct Gen {
     return s.str();
   }
 
+  // the group's outputs as reference parameters (deferred stores): ", T &r0, ..."
+  std::string out_params(bool pair) const {
+    std::ostringstream s;
+    int k = 0;
+    for (auto &kv : outk) s << ", " << (pair ? "PR<" + T(kv.first) + ">" : T(kv.first)) << " &r" << k++;
+    return s.str();
+  }
+  std::string out_assigns() const {
+    std::ostringstream s;
+    int k = 0;
+    for (auto &kv : outk) s << "    r" << k++ << " = " << val(kv.first) << ";\n";
+    return s.str();
+  }
+
   std::string center_loads2() const {
     std::ostringstream s;
     for (Node *p : plan.in_rasters) {
@@ -489,11 +503,20 @@ struct Gen {
 
   // Literal chain of shading composition i as a separate function: cells whose
   // x^2 + y^2 is not finite take it.
+  // Whether the literal chain of composition i reads kernel arguments (scalar parameters).
+  bool shade_reads_args(int i) const {
+    for (Node *n : shades[i].pattern)
+      for (Node *p : n->prev)
+        if (sca.count(p)) return true;
+    return false;
+  }
   std::string shade_slow_decl(int i) const {
     const ShadeMatch &m = shades[i];
     std::ostringstream s;
-    s << "__device__ __noinline__ float shade_slow" << i << "(const Args &a, const float " << val(m.x) << ", const float "
-      << val(m.y) << ") {\n";
+    // without kernel arguments the function reads no memory, so the compiler
+    // may keep loads of the cells around its call sites in registers
+    s << "__device__ __noinline__ float shade_slow" << i << "(" << (shade_reads_args(i) ? "const Args &a, " : "")
+      << "const float " << val(m.x) << ", const float " << val(m.y) << ") {\n";
     for (Node *n : m.pattern) s << "  " << stmt(n, false) << "\n";
     s << "  return " << val(m.hs) << ";\n}\n";
     return s.str();
@@ -518,17 +541,18 @@ struct Gen {
     const ShadeMatch &m = shades[i];
     const std::string v = "v" + std::to_string(member.at(n)), q = v + "_q", si = std::to_string(i);
     const std::string tmpl = m.k_one ? "<true>" : "<false>";
+    const std::string aa = shade_reads_args(i) ? "a, " : "";
     std::ostringstream s;
     if (!pair) {
       s << "float " << q << "; float " << v << " = map_shade" << tmpl << "(" << val(m.x) << ", " << val(m.y) << ", "
-        << shade_args(m) << ", " << q << "); if (!(" << q << " < MAP_INF_F)) " << v << " = shade_slow" << si << "(a, "
+        << shade_args(m) << ", " << q << "); if (!(" << q << " < MAP_INF_F)) " << v << " = shade_slow" << si << "(" << aa
         << val(m.x) << ", " << val(m.y) << ");";
     } else {
       s << "PR<float> " << q << "; PR<float> " << v << " = map_shade" << tmpl << "(PR<float>(" << val(m.x)
         << "), PR<float>(" << val(m.y) << "), " << shade_args(m) << ", " << q << "); if (!(" << q << ".a < MAP_INF_F)) "
-        << v << ".a = shade_slow" << si << "(a, lane0(" << val(m.x) << "), lane0(" << val(m.y) << ")); if (!(" << q
-        << ".b < MAP_INF_F)) " << v << ".b = shade_slow" << si << "(a, lane1(" << val(m.x) << "), lane1(" << val(m.y)
-        << "));";
+        << v << ".a = shade_slow" << si << "(" << aa << "lane0(" << val(m.x) << "), lane0(" << val(m.y) << ")); if (!("
+        << q << ".b < MAP_INF_F)) " << v << ".b = shade_slow" << si << "(" << aa << "lane1(" << val(m.x) << "), lane1("
+        << val(m.y) << "));";
     }
     return s.str();
   }
@@ -865,8 +889,26 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << ", int x, int y, int lx, int ly) {\n";
     body << G.center_loads2() << G.body2() << G.stores2() << "}\n";
   }
-  const std::string unroll = heavy ? (pair ? "#pragma unroll 1\n" : "#pragma unroll 2\n") : "#pragma unroll\n";
+  const FocalTune &tune = focal_tune();
+  const bool full_unroll = tune.unroll ? tune.unroll >= rows : !heavy;
+  const std::string unroll = tune.unroll ? "#pragma unroll " + std::to_string(tune.unroll) + "\n"
+                                         : heavy ? (pair ? "#pragma unroll 1\n" : "#pragma unroll 2\n") : "#pragma unroll\n";
   const int step = pair ? 2 : 1;
+  // Interior tiles of a fully unrolled row loop keep the thread's results in
+  // registers and store them after the last cell: no store then lies between
+  // two loads of the same staged tap, which therefore load once per thread.
+  const int nout = (int)G.outk.size();
+  const bool defer = tune.defer && full_unroll && nout > 0 && rows * nout <= 32;
+  if (defer) {
+    for (int pf = 0; pf < (pair ? 2 : 1); pf++) {
+      body << "template <";
+      for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
+      body << ">\n__device__ __forceinline__ void " << (pf ? "focal_cell2r" : "focal_cellr") << "(const Args &a";
+      for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
+      body << ", int x, int y, int lx, int ly" << G.out_params(pf) << ") {\n";
+      body << (pf ? G.center_loads2() + G.body2() : G.center_loads(false) + G.body(false)) << G.out_assigns() << "}\n";
+    }
+  }
   std::ostringstream loop, loop_full;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
        << "    const int x = t.x0 + lx;\n"
@@ -883,12 +925,42 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   loop << "    }\n";
   // interior tiles are full: every cell of the tile is inside the raster
   loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
-            << "    const int x = t.x0 + lx;\n"
-            << unroll
-            << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
-            << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
-            << "      " << (pair ? call2.str() : call.str()) << ";\n"
-            << "    }\n";
+            << "    const int x = t.x0 + lx;\n";
+  if (defer) {
+    std::ostringstream callr, outs;
+    callr << (pair ? "focal_cell2r(a" : "focal_cellr(a");
+    for (int k = 0; k < nst; k++) callr << ", f" << k;
+    callr << ", x, y, lx, ly";
+    int k = 0;
+    for (auto &kv : G.outk) {
+      const std::string ty = G.T(kv.first);
+      loop_full << "    " << (pair ? "PR<" + ty + ">" : ty) << " r" << k << "[" << rows / step << "];\n";
+      callr << ", r" << k << "[k / " << step << "]";
+      if (pair)
+        outs << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y, lane0(r" << k << "[k / 2]));\n"
+             << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y + 1, lane1(r" << k << "[k / 2]));\n";
+      else
+        outs << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y, r" << k << "[k]);\n";
+      k++;
+    }
+    callr << ")";
+    loop_full << "#pragma unroll\n"
+              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
+              << "      " << callr.str() << ";\n"
+              << "    }\n"
+              << "#pragma unroll\n"
+              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "      const int y = t.y0 + ly0 + k;\n"
+              << outs.str()
+              << "    }\n";
+  } else {
+    loop_full << unroll
+              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
+              << "      " << (pair ? call2.str() : call.str()) << ";\n"
+              << "    }\n";
+  }
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
        << "                                         bool gdesc) {\n"
@@ -1526,6 +1598,34 @@ static std::string gen_spread(Gen &G) {
     << "  " << (packed ? "spread_walk_packed" : "spread_walk") << "(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
     << "}\n";
   return s.str();
+}
+
+const FocalTune &focal_tune() {
+  static FocalTune t = [] {
+    FocalTune r;
+    const char *e = std::getenv("MAP_B200_FOCAL_TUNE");
+    if (!e) return r;
+    std::string s(e);
+    size_t i = 0;
+    while (i < s.size()) {
+      size_t j = s.find(',', i);
+      if (j == std::string::npos) j = s.size();
+      std::string kv = s.substr(i, j - i);
+      size_t eq = kv.find('=');
+      if (eq != std::string::npos) {
+        const std::string k = kv.substr(0, eq);
+        const int v = std::atoi(kv.c_str() + eq + 1);
+        if (k == "unroll") r.unroll = v;
+        else if (k == "defer") r.defer = v;
+        else if (k == "nt") r.nt = v;
+        else if (k == "tw") r.tw = v;
+        else if (k == "th") r.th = v;
+      }
+      i = j + 1;
+    }
+    return r;
+  }();
+  return t;
 }
 
 bool tile_cfg_valid(const TileCfg &c) {

@@ -58,6 +58,17 @@ struct KernelPlan {
 
 KernelPlan generate_kernel(const Group &g, TileCfg cfg = TileCfg());
 
+// Tuning overrides of the standalone focal skeleton, read once from the
+// environment variable MAP_B200_FOCAL_TUNE ("key=value,..."; keys unroll, defer,
+// nt, tw, th; 0 or absent = the built-in choice). Used to measure variants;
+// every variant computes the same cells with the same operations.
+struct FocalTune {
+  int unroll = 0;   // unroll factor of the per-thread row loop (0: by body weight)
+  int defer = 1;    // interior tiles keep a thread's results in registers and store them last
+  int nt = 0, tw = 0, th = 0;
+};
+const FocalTune &focal_tune();
+
 // Dynamic shared memory of a radial scan launch over a W x H raster: two front
 // buffers when they fit (0 otherwise: the kernel then re-reads fronts from its output).
 size_t radial_front_smem(int W, int H, int dtype);

@@ -261,7 +261,13 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
     // standalone focal kernels: 128 threads on a 64 x 32 tile (16 rows per thread),
     // measured 1.5% faster than 256 threads on the hillshade and 2% on life
     TileCfg cfg;
-    if (g->skeleton == SK_FOCAL) cfg.nt = 128;
+    if (g->skeleton == SK_FOCAL) {
+      cfg.nt = 128;
+      const FocalTune &ft = focal_tune();
+      if (ft.nt) cfg.nt = ft.nt;
+      if (ft.tw) cfg.tw = ft.tw;
+      if (ft.th) cfg.th = ft.th;
+    }
     P.plans[g->id] = generate_kernel(*g, cfg);
     if (compile && seen.insert(P.plans[g->id].source).second) {
       const std::string *src = &P.plans[g->id].source;

@@ -5,13 +5,19 @@
  * workloads of the hot path, used by tests and by the CPU baseline leg of
  * bench.py as the checker. Nothing in the product links or calls it.
  *
- * Parity status: the reference (OpenCL kernels generated at run time) cannot be
- * built or run in this environment (no OpenCL headers or platform), and it
- * ships no tests, fixtures or golden vectors. This oracle is therefore pinned
- * only by the code semantics it restates (cited per function) and, for the
- * host-side scalar operator tables, by the reference's own util/ sources
- * compiled under oracle/ref_util (see oracle/build_oracle.py):
- * PARITY UNPINNED against reference outputs.
+ * Parity status: the reference ships no tests, fixtures or golden vectors, and
+ * its OpenCL kernels cannot run here (no OpenCL platform). What is pinned on the
+ * reference's own artefacts:
+ *  - the per-cell operations, their order, the focal masks and loop nesting,
+ *    the Philox counter / key, and the scalar constants the kernels receive,
+ *    for hill.py, life.py and wsum.py: the reference's DAG, fusion compiler and
+ *    kernel generators, built from its sources with stand-in OpenCL entry
+ *    points (oracle/ref_codegen), print the kernels they generate, and
+ *    tests/test_ref_codegen.py checks this file's restatements against them;
+ *  - the host-side scalar operator tables, against the reference's util/
+ *    sources compiled under oracle/ref_util (oracle/build_oracle.py).
+ * Not pinned: cell VALUES computed by the reference's kernels (its OpenCL
+ * implementation's transcendental functions have no fixed accuracy).
  *
  * Floating point: compiled with -ffp-contract=off and no fast-math so each
  * operation rounds once, in the order the reference's generated code writes

@@ -1,0 +1,121 @@
+// Driver of the reference's runtime for the kernel dump (TEST INFRASTRUCTURE
+// ONLY). Builds the programs of the reference's example scripts through the
+// reference's own C ABI (front/bindings.hpp), creating scalar constants the way
+// its Python bindings do (python/map.py: a Python float becomes an F32 Variant,
+// an int an S32 one), and evaluates them with ma_write, which makes the
+// reference fuse, generate and print its OpenCL kernels (the stand-in OpenCL of
+// stubs.cpp runs nothing).
+//
+// usage: ref_codegen hill|life|wsum <work dir>
+#include "front/bindings.hpp"
+#include "util/util.hpp"
+
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace map::detail;
+
+namespace {
+
+Node *fconst(double v) {   // Variant(float) (python/map.py:113-115)
+  VariantType var((float)v);
+  return ma_constant(var, DataSize(), F32, ROW + BLK, BlockSize());
+}
+Node *iconst(int v) {      // Variant(int) (python/map.py:119-121)
+  VariantType var((int32_t)v);
+  return ma_constant(var, DataSize(), S32, ROW + BLK, BlockSize());
+}
+Node *bin(Node *l, Node *r, BinaryEnum op) { return ma_binary(l, r, op); }
+Node *un(Node *a, UnaryEnum op) { return ma_unary(a, op); }
+
+Node *convolve(Node *a, const std::vector<int> &m, int side) {
+  std::vector<VariantType> v;
+  for (int x : m) v.push_back(VariantType((int32_t)x));   // convolve(raster, list of ints)
+  return ma_convolution(a, v.data(), (int)v.size(), DataSize{side, side});
+}
+
+void write_bin(const std::string &path, int w, int h, int bs, DataTypeEnum dt) {
+  // a zero raster of the given shape in the reference's .bin layout is written
+  // by the reference itself: zeros -> write
+  VariantType zero = VariantType(0).convert(DataType(dt));
+  Node *z = ma_constant(zero, DataSize{w, h}, dt, ROW + BLK, BlockSize{bs, bs});
+  ma_increaseRef(z);
+  ma_write(z, path.c_str());
+  ma_decreaseRef(z);
+}
+
+// python/hill.py:15-54
+Node *hill(Node *dem) {
+  const double PI = 3.141593;
+  auto hori = [&](Node *d) {
+    return bin(convolve(d, {-1, 0, 1, -2, 0, 2, -1, 0, 1}, 3), iconst(8 * 1), DIV);
+  };
+  auto vert = [&](Node *d) {
+    return bin(convolve(d, {-1, -2, -1, 0, 0, 0, 1, 2, 1}, 3), iconst(8 * 1), DIV);
+  };
+  auto slope = [&](Node *d) {
+    Node *x = hori(d), *y = vert(d);
+    return un(bin(iconst(1), un(bin(bin(x, x, MUL), bin(y, y, MUL), ADD), SQRT), MUL), ATAN);
+  };
+  auto aspect = [&](Node *d) {
+    Node *x = hori(d), *y = vert(d);
+    Node *z1 = bin(bin(x, iconst(0), NE), ma_binary(y, un(x, NEG), ATAN2), MUL);
+    z1 = bin(z1, bin(bin(z1, iconst(0), LT), fconst(PI * 2), MUL), ADD);
+    Node *z0 = bin(bin(x, iconst(0), EQ),
+                   bin(bin(bin(y, iconst(0), GT), fconst(PI / 2), MUL), bin(bin(y, iconst(0), LT), fconst(PI * 2 - PI / 2), MUL), ADD),
+                   MUL);
+    return bin(z1, z0, ADD);
+  };
+  const double zr = (90 - 45.0) / 180 * PI;
+  double ar = 360 - 315.0 + 90;
+  ar = ar > 360 ? ar - 360 : ar;
+  ar = ar / 180 * PI;
+  Node *a = bin(fconst(std::cos(zr)), un(slope(dem), COS), MUL);
+  Node *b = bin(bin(fconst(std::sin(zr)), un(slope(dem), SIN), MUL), un(bin(fconst(ar), aspect(dem), SUB), COS), MUL);
+  return bin(a, b, ADD);
+}
+
+}  // namespace
+
+int main(int argc, char **argv) {
+  if (argc < 3) {
+    std::fprintf(stderr, "usage: %s hill|life|wsum <work dir>\n", argv[0]);
+    return 2;
+  }
+  const std::string what = argv[1], dir = argv[2];
+  ma_setupDevices("", DEV_GPU, "");
+  Node *out = nullptr;
+  if (what == "hill") {
+    write_bin(dir + "/dem.bin", 512, 512, 256, F32);
+    Node *dem = ma_read((dir + "/dem.bin").c_str());
+    out = hill(dem);
+  } else if (what == "life") {
+    // python/life.py:24-34, two generations of a rand(N, ds, U8, ROW+BLK, bs) > 128 state
+    VariantType seed = VariantType((int32_t)16).convert(DataType(U8));
+    Node *s = ma_constant(seed, DataSize{512, 512}, U8, ROW + BLK, BlockSize{256, 256});
+    Node *state = bin(ma_rand(s, U8, ROW + BLK), iconst(128), GT);
+    for (int g = 0; g < 2; g++) {
+      Node *nbh = convolve(state, {1, 1, 1, 1, 0, 1, 1, 1, 1}, 3);
+      state = bin(bin(nbh, iconst(3), EQ), bin(bin(nbh, iconst(2), EQ), state, MUL), ADD);
+    }
+    out = state;
+  } else if (what == "wsum") {
+    // python/wsum.py:11
+    Node *r[4];
+    for (int i = 0; i < 4; i++) write_bin(dir + "/r" + std::to_string(i) + ".bin", 512, 512, 256, F32);
+    for (int i = 0; i < 4; i++) r[i] = ma_read((dir + "/r" + std::to_string(i) + ".bin").c_str());
+    Node *o = bin(iconst(0), bin(fconst(0.1), r[0], MUL), ADD);
+    o = bin(o, bin(r[1], fconst(0.2), MUL), ADD);
+    o = bin(o, bin(fconst(0.3), r[2], MUL), ADD);
+    o = bin(o, bin(r[3], fconst(0.4), MUL), ADD);
+    out = bin(o, iconst(0), ADD);
+  } else {
+    std::fprintf(stderr, "unknown program %s\n", what.c_str());
+    return 2;
+  }
+  ma_increaseRef(out);
+  std::fflush(stdout);
+  return ma_write(out, (dir + "/out.bin").c_str());
+}

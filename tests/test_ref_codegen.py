@@ -1,0 +1,152 @@
+"""The oracle pinned on the reference's own code generator.
+
+tests/golden/ref_kernel_facts.json holds facts of the OpenCL kernels that the
+reference's runtime generates for the example programs (hill.py, life.py,
+wsum.py), and of the scalar values it launches them with, produced by running
+the reference's DAG, fusion compiler and kernel generators built from its own
+sources (oracle/ref_codegen: build_ref_codegen.py, dump_kernels.py). These
+tests check that the oracle's restatement (oracle/oracle.c) performs the same
+operations in the same order with the same constants, and, where the
+reference checkout is present, that the facts are what the reference
+generates today."""
+import json
+import math
+import os
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+FACTS = os.path.join(ROOT, "tests", "golden", "ref_kernel_facts.json")
+
+
+@pytest.fixture(scope="module")
+def facts():
+    with open(FACTS) as f:
+        return json.load(f)
+
+
+def core(kernels, n_loops):
+    ks = [k for k in kernels if len(k["focal_loops"]) == n_loops]
+    assert len(ks) >= 1
+    return ks[0]
+
+
+# hill_cell_f32 of oracle/oracle.c, statement by statement, in the facts'
+# canonical names: t0 / t3 the two correlations, t5 the centre cell (unused),
+# t6..t14 the scalar arguments (8, 1, cz, 0, 2 PI', 3 PI'/2, PI'/2, ar, sz)
+HILL_ORACLE = [
+    "t0f = 0", "t3f = 0", "t5f = LOAD_L_F32(IN)",
+    "t6i = a0", "t7i = a1", "t8f = a2", "t9i = a3", "t10f = a4", "t11f = a5", "t12f = a6", "t13f = a7", "t14f = a8",
+    "t15f = t0f / t6i",            # gx = ch / 8
+    "t16f = t3f / t6i",            # gy = cv / 8
+    "t17f = t16f * t16f",          # gy * gy
+    "t18f = t15f * t15f",          # gx * gx
+    "t19f = t18f + t17f",          # gx * gx + gy * gy
+    "t20f = sqrt(t19f)",
+    "t21f = t7i * t20f",           # 1 * sqrt(...)
+    "t22f = atan(t21f)",           # s
+    "t23f = cos(t22f)",
+    "t24f = t8f * t23f",           # cz * cos(s)
+    "t25f = -t15f",
+    "t26f = atan2(t16f,t25f)",     # atan2(gy, -gx)
+    "t27u8 = t15f != t9i",
+    "t28f = t27u8 * t26f",         # z1
+    "t29u8 = t28f < t9i",
+    "t30f = t29u8 * t10f",
+    "t31f = t28f + t30f",          # z1 += (z1 < 0) * 2 PI'
+    "t32u8 = t16f < t9i",
+    "t33f = t32u8 * t11f",         # (gy < 0) * 3 PI'/2
+    "t34u8 = t16f > t9i",
+    "t35f = t34u8 * t12f",         # (gy > 0) * PI'/2
+    "t36f = t35f + t33f",
+    "t37u8 = t15f == t9i",
+    "t38f = t37u8 * t36f",         # z0
+    "t39f = t31f + t38f",          # aspect
+    "t40f = t13f - t39f",          # ar - aspect
+    "t41f = cos(t40f)",
+    "t42f = sin(t22f)",
+    "t43f = t14f * t42f",          # sz * sin(s)
+    "t44f = t43f * t41f",
+    "t45f = t24f + t44f",          # hs
+]
+
+
+def strip_ids(stmts):
+    import re
+    return [re.sub(r"\(IN_\d+\)", "(IN)", s) for s in stmts]
+
+
+def test_hillshade_restatement_matches_reference_kernel(facts):
+    k = core(facts["hill"], 2)
+    assert strip_ids(k["statements"]) == HILL_ORACLE
+    # correlation: acc += tap * mask, rows (i1) outer, columns (i0) inner, integer masks
+    assert k["loop_nesting"] == ["i1", "i0"]
+    assert k["focal_loops"] == ["t0f += t1f[tap(i0,i1)] * t2i[i1][i0]", "t3f += t1f[tap(i0,i1)] * t4i[i1][i0]"]
+    assert k["masks"]["t2i"] == [[-1, 0, 1], [-2, 0, 2], [-1, 0, 1]]
+    assert k["masks"]["t4i"] == [[-1, -2, -1], [0, 0, 0], [1, 2, 1]]
+
+
+def test_hillshade_constants_are_the_oracles(facts):
+    """The script's constants reach the reference kernel as exact float32 kernel
+    arguments, equal to oracle.c's hill_const (Python double arithmetic, then
+    float32)."""
+    k = core(facts["hill"], 2)
+    args = k["scalar_args"]
+    assert [a["type"] for a in args] == ["int", "int", "float", "int", "float", "float", "float", "float", "float"]
+    assert [args[i]["value"] for i in (0, 1, 3)] == [8, 1, 0]
+    PI = 3.141593
+    zr = (90 - 45.0) / 180 * PI
+    ar = (360 - 315.0 + 90) / 180 * PI
+    want = [math.cos(zr), PI * 2, PI * 2 - PI / 2, PI / 2, ar, math.sin(zr)]
+    got = [args[i]["bits"] for i in (2, 4, 5, 6, 7, 8)]
+    assert got == ["%08x" % np.float32(v).view(np.uint32) for v in want]
+
+
+def test_life_restatement_matches_reference_kernel(facts):
+    gens = [k for k in facts["life"] if len(k["focal_loops"]) == 1]
+    assert len(gens) == 2       # two generations, one focal kernel each
+    for k in gens:
+        assert k["masks"]["t2i"] == [[1, 1, 1], [1, 0, 1], [1, 1, 1]]
+        assert k["focal_loops"] == ["t0i += t1u8[tap(i0,i1)] * t2i[i1][i0]"]   # U8 taps, S32 accumulator
+        assert k["loop_nesting"] == ["i1", "i0"]
+        assert [a["value"] for a in k["scalar_args"]] == [2, 3]
+        st = strip_ids(k["statements"])
+        # (nbh == 3) + (nbh == 2) * state, all U8 (oracle.c orc_life)
+        assert st[-4:] in (["t6u8 = t0i == t4i", "t7u8 = t6u8 * t3u8", "t8u8 = t0i == t5i", "t9u8 = t8u8 + t7u8"],
+                           ["t6u8 = t0i == t3i", "t7u8 = t6u8 * t5u8", "t8u8 = t0i == t4i", "t9u8 = t8u8 + t7u8"])
+
+
+def test_rand_key_and_counter_match_the_oracle(facts):
+    """rand(seed, ...) > 128: Philox2x32 counter {seed}, key BS1*BC1 + BS0*BC0 +
+    bc1*BS0 + bc0 (oracle.c orc_rand_u8), U8 draw = low byte of the counter."""
+    k = [k for k in facts["life"] if k["rng"]][0]
+    assert k["rng"] == ["philox2x32_ctr_t ctr = {{t1u8}};",
+                        "philox2x32_key_t key = {{BS1*BC1+BS0*BC0+(bc1)*BS0+bc0}};",
+                        "ctr = philox2x32(ctr,key);"]
+    assert any(s.startswith("t2u8 = *(uchar*)& ctr") for s in k["statements"])
+    assert [a["value"] for a in k["scalar_args"]] == [128]
+
+
+def test_wsum_left_to_right(facts):
+    k = facts["wsum"][0]
+    st = strip_ids(k["statements"])
+    # 0 + 0.1*r1 + r2*0.2 + 0.3*r3 + r4*0.4 + 0, left to right (oracle.c orc_wsum_f32)
+    assert st[9:] == ["t9f = t4f * t0f", "t10f = t5i + t9f", "t11f = t1f * t6f", "t12f = t10f + t11f",
+                      "t13f = t7f * t2f", "t14f = t12f + t13f", "t15f = t3f * t8f", "t16f = t14f + t15f",
+                      "t17f = t16f + t5i"]
+    vals = [a["value"] for a in k["scalar_args"]]
+    assert vals == [np.float32(0.1), 0, np.float32(0.2), np.float32(0.3), np.float32(0.4)]
+
+
+def test_facts_are_what_the_reference_generates():
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref_codegen"))
+    import build_ref_codegen as B
+    import dump_kernels as D
+    if not os.path.isfile(os.path.join(B.REF, "Makefile")):
+        pytest.skip("reference checkout not available")
+    exe = B.build()
+    with open(FACTS) as f:
+        committed = json.load(f)
+    assert json.loads(json.dumps(D.facts(exe), sort_keys=True)) == committed
