@@ -353,20 +353,27 @@ def bench_batched(M, W, synth, torch, dev, n_rasters=512, steps=5, seed=5):
             "programs": "fused hillshade + 6-layer weighted overlay per raster"}
 
 
-def bench_serving(M, synth, torch, dev, size=32768, rates=(200, 1000, 2000), seconds=3.0):
-    """Requests over a device-resident size^2 DEM: Poisson arrivals, windows
-    256^2/512^2/1024^2 at uniform offsets, mix 50% hillshade / 20% slope / 15%
-    viewshed (observer height 10 m, radius 167 cells = 5 km at 30 m) / 15% D8 +
-    flow accumulation; admission by an HBM budget of 8 GiB."""
+def bench_serving(M, synth, torch, dev, size=32768, rates=(200, 1000, 2000, 5000, 10000), outstanding=(4, 16, 64),
+                  seconds=3.0):
+    """Requests over a device-resident size^2 DEM: windows 256^2/512^2/1024^2 at
+    uniform offsets, mix 50% hillshade / 20% slope / 15% viewshed (observer
+    height 10 m, radius 167 cells = 5 km at 30 m) / 15% D8 + flow accumulation;
+    admission by an HBM budget of 8 GiB. Open loop: Poisson arrivals at each
+    rate (up to past saturation); closed loop: a fixed number of requests kept
+    in flight (the throughput ceiling). mean_batch is per run."""
     dem = synth.fbm_dem(size, size, seed=4242, xp=torch, device=dev).contiguous()
     torch.cuda.synchronize()
     srv = M.Server(dem.data_ptr(), size * 4, size, size, budget_bytes=8 << 30, max_batch=512)
     srv.load(rate=200, seconds=0.5, seed=99)            # warm-up: compiles every program kind
     out = {"dem": "%dx%d F32 fBm, resident" % (size, size), "mix": [0.5, 0.2, 0.15, 0.15], "runs": []}
+    keys = ("mode", "requests", "throughput_req_s", "gcells_s", "p50_ms", "p99_ms", "batches", "mean_batch",
+            "by_window", "by_program")
     for r in rates:
         res = srv.load(rate=r, seconds=seconds, seed=r)
-        out["runs"].append({k: res[k] for k in ("rate_req_s", "requests", "throughput_req_s", "gcells_s", "p50_ms",
-                                                "p99_ms", "by_window", "by_program")} | {"mean_batch": res["server"]["mean_batch"]})
+        out["runs"].append({"rate_req_s": r} | {k: res[k] for k in keys})
+    for n in outstanding:
+        res = srv.load_closed(n, seconds, seed=1000 + n)
+        out["runs"].append({"outstanding": n} | {k: res[k] for k in keys})
     srv.close()
     del dem
     return out

@@ -130,6 +130,15 @@ int ma_getPairedCells(void);
  * the hillshade tolerance of the literal chain; cells where x^2 + y^2 is not
  * finite take the literal chain. on = 0 generates the literal chain
  * everywhere. Engine option with no counterpart in the reference. */
+/* Prediction (runtime/visitor/Predictor.cpp:22-200, runtime/Worker.cpp:83-91):
+ * a Local / Focal group whose every output holds one value known on the host
+ * (constants, element-wise operators of them, focal operators of them under a
+ * mirror border rule) is written with a fill instead of a kernel launch. On by
+ * default; ma_lastPredictedCount() counts the groups of the last evaluation
+ * that were filled. */
+void ma_setPrediction(int on);
+int ma_getPrediction(void);
+int ma_lastPredictedCount(void);
 void ma_setAlgebraicRewrite(int on);
 int ma_getAlgebraicRewrite(void);
 /* Block size given to rasters created without one (default 256 x 256). */
@@ -172,6 +181,17 @@ ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Arra
 ma_Node *ma_fromDeviceRows(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs, int row0, int rows);
 int ma_evalRows(ma_Node **nodes, int n, void **dst, const long long *pitch, int y0, int y1);
 int ma_rowMargin(ma_Node **nodes, int n);
+
+/* `.bin` raster files (file/binary.cpp:221-404) on the host, no device needed:
+ * ma_binInfo fills info7 with data type, number of dimensions, data size
+ * (x, y), memory order and block size (x, y) from the header; ma_binReadHost
+ * reads the cells as a dense row-major array; ma_binWriteHost writes one
+ * (memory order ROW + BLK: block by block, edge blocks padded; ROW: dense).
+ * Engine extension: the reference reads and writes these files only inside
+ * evaluations (Read / Write nodes). Return 0 on success. */
+int ma_binInfo(const char *path, int *info7);
+int ma_binReadHost(const char *path, void *dst, size_t bytes);
+int ma_binWriteHost(const char *path, const void *src, ma_Array ds, int dt, int mo, ma_Array bs);
 
 /* Evaluate `node` and copy the raster to dense row-major host memory of
  * `bytes` bytes. Returns 0 on success. */
@@ -232,6 +252,11 @@ double ma_serverLatency(ma_Server *s, long long id);
 size_t ma_serverStats(ma_Server *s, char *buf, size_t len);
 size_t ma_serverLoad(ma_Server *s, double rate, double seconds, const double *mix, unsigned seed, double obs_h,
                      double radius, char *buf, size_t len);
+/* Closed-loop load: `outstanding` requests kept in flight for `seconds`, each
+ * completion replaced at once by a new request of the mix (the throughput
+ * ceiling and latency under saturation); same JSON report as ma_serverLoad. */
+size_t ma_serverLoadClosed(ma_Server *s, int outstanding, double seconds, const double *mix, unsigned seed,
+                           double obs_h, double radius, char *buf, size_t len);
 void ma_serverDestroy(ma_Server *s);
 
 /* Per-zone statistics (no counterpart in the reference, whose zonal skeleton

@@ -7,6 +7,7 @@
 #include "zonestats.hpp"
 #include "codegen.hpp"
 #include "cuda_env.hpp"
+#include "binfile.hpp"
 #include "executor.hpp"
 #include "graph.hpp"
 
@@ -283,8 +284,10 @@ ma_Node *ma_focalFunc(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array ma
     return Runtime::get().focal_func(checked(node), reinterpret_cast<Variant *>(mask_v), mask_s, A(mask_ds), type);
   });
 }
-ma_Node *ma_focalPercent(ma_Node *, ma_Variant *, int, ma_Array, int) {
-  return node_call([&]() -> Node * { throw MapError("focalPercent is not supported by this engine"); });
+ma_Node *ma_focalPercent(ma_Node *node, ma_Variant *mask_v, int mask_s, ma_Array mask_ds, int type) {
+  return node_call([&] {
+    return Runtime::get().focal_percent(checked(node), reinterpret_cast<Variant *>(mask_v), mask_s, A(mask_ds), type);
+  });
 }
 ma_Node *ma_zonalReduc(ma_Node *node, int type) {
   return node_call([&] { return Runtime::get().zonal_reduc(checked(node), type); });
@@ -357,6 +360,12 @@ void ma_setPairedCells(int on) {
 }
 int ma_getPairedCells(void) { return Runtime::get().paired_cells; }
 
+void ma_setPrediction(int on) {
+  void_call([&] { Runtime::get().prediction = on ? 1 : 0; });
+}
+int ma_getPrediction(void) { return Runtime::get().prediction; }
+int ma_lastPredictedCount(void) { return Executor::get().last.predicted; }
+
 void ma_setAlgebraicRewrite(int on) {
   void_call([&] { Runtime::get().algebraic_rewrite = on ? 1 : 0; });
 }
@@ -402,6 +411,46 @@ int ma_evalRows(ma_Node **nodes, int n, void **dst, const long long *pitch, int 
 
 int ma_rowMargin(ma_Node **nodes, int n) {
   return int_call([&] { return Executor::get().row_margin(node_vec(nodes, n)); });
+}
+
+int ma_binInfo(const char *path, int *info7) {
+  return int_call([&] {
+    if (!path || !info7) throw MapError("binInfo: null argument");
+    BinHeader h = bin_read_header(path);
+    const int v[7] = {h.dtype, h.numdim, h.ds0, h.ds1, h.memorder, h.bs0, h.bs1};
+    std::memcpy(info7, v, sizeof v);
+    return 0;
+  });
+}
+
+int ma_binReadHost(const char *path, void *dst, size_t bytes) {
+  return int_call([&] {
+    if (!path || !dst) throw MapError("binRead: null argument");
+    BinHeader h = bin_read_header(path);
+    const size_t need = (size_t)h.ds0 * h.ds1 * dt_size(h.dtype);
+    if (bytes < need) throw MapError("binRead: destination holds " + std::to_string(bytes) + " bytes, " +
+                                     std::to_string(need) + " needed");
+    bin_read_dense(path, h, dst);
+    return 0;
+  });
+}
+
+int ma_binWriteHost(const char *path, const void *src, ma_Array ds, int dt, int mo, ma_Array bs) {
+  return int_call([&] {
+    if (!path || !src) throw MapError("binWrite: null argument");
+    BinHeader h;
+    h.dtype = dt;
+    h.numdim = D2;
+    h.ds0 = ds.arr[0];
+    h.ds1 = ds.arr[1];
+    h.memorder = mo;
+    h.bs0 = mo == ROW ? h.ds0 : bs.arr[0];
+    h.bs1 = mo == ROW ? h.ds1 : bs.arr[1];
+    if (h.ds0 <= 0 || h.ds1 <= 0 || h.bs0 <= 0 || h.bs1 <= 0) throw MapError("binWrite: invalid sizes");
+    dt_size(dt);
+    bin_write_dense(path, h, src);
+    return 0;
+  });
 }
 
 int ma_toHost(ma_Node *node, void *dst, size_t bytes) {
@@ -691,6 +740,19 @@ size_t ma_serverLoad(ma_Server *h, double rate, double seconds, const double *mi
   try {
     if (!h || !mix) throw MapError("server: null argument");
     std::string j = h->s->run_load(rate, seconds, mix, seed, obs_h, radius);
+    ok();
+    return copy_out(j, buf, len);
+  } catch (const std::exception &e) {
+    fail(e.what());
+    return 0;
+  }
+}
+
+size_t ma_serverLoadClosed(ma_Server *h, int outstanding, double seconds, const double *mix, unsigned seed, double obs_h,
+                           double radius, char *buf, size_t len) {
+  try {
+    if (!h || !mix) throw MapError("server: null argument");
+    std::string j = h->s->run_closed(outstanding, seconds, mix, seed, obs_h, radius);
     ok();
     return copy_out(j, buf, len);
   } catch (const std::exception &e) {

@@ -421,7 +421,8 @@ struct Gen {
       }
     }
     for (Node *n : g.nodes) {
-      bool focal = n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW;
+      bool focal = n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW ||
+                   n->kind == K_FOCALPERCENT;
       for (size_t j = 0; j < n->prev.size(); j++) {
         Node *p = n->prev[j];
         if (!rin.count(p)) continue;
@@ -681,6 +682,22 @@ struct Gen {
               << tap(n->prev[0], i0, i1) << ");";
         break;
       }
+      case K_FOCALPERCENT: {
+        // FocalSkeleton.cpp:375-403: var = 0; var += (centre OP cell) over the
+        // window; var /= window size, in the argument's type (OP: == for AGE,
+        // > for ILE, util/PercentType.cpp). The window is centred on the cell and
+        // the divisor is (2 hx + 1)(2 hy + 1): the reference's loop starts at the
+        // centre (i = 0 .. 2h) and its divisor lacks parentheses, both defects.
+        int hx = n->halo_x(), hy = n->halo_y();
+        const char *cmp = n->op == 1 ? "==" : ">";
+        s << t << " " << v << "_c = " << tap(n->prev[0], 0, 0) << "; " << t << " " << v << " = (" << t << ")0;";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++)
+            s << "\n    " << v << " = (" << t << ")(" << v << " + (" << t << ")(" << v << "_c " << cmp << " "
+              << tap(n->prev[0], i0, i1) << "));";
+        s << "\n    " << v << " = (" << t << ")(" << v << " / (" << t << ")" << (2 * hx + 1) * (2 * hy + 1) << ");";
+        break;
+      }
       case K_FOCALFLOW: {
         // FocalSkeleton.cpp:405-443: steepest descent among the 8 neighbours in the order
         // E, SE, S, SW, W, NW, N, NE; drop = (self - nbh) / dist with dist 1 or 1.414213f;
@@ -791,10 +808,86 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   body << "}\n";
   body << "__device__ __forceinline__ void compute_cell(const Args &a, const In &in, int x, int y) {\n";
   body << G.center_loads(true) << G.body(false) << G.stores(true) << "}\n";
+  // 16-byte vector form: every raster of the group has one element size es,
+  // V = 16 / es consecutive cells of a row per vector; full tiles whose rows start
+  // on 16-byte boundaries load and store whole vectors and evaluate the cells
+  // from their lanes (the same per-cell code), other tiles take the scalar path
+  int es = 0;
+  bool vec = !P.out_rasters.empty();
+  for (Node *p : P.in_rasters) {
+    const int s = (int)dt_size(p->meta.dtype);
+    if (es && s != es) vec = false;
+    es = s;
+  }
+  for (Node *p : P.out_rasters) {
+    const int s = (int)dt_size(p->meta.dtype);
+    if (es && s != es) vec = false;
+    es = s;
+  }
+  const int V = es ? 16 / es : 0;
+  const int TV = V ? TW / V : 0;                // threads per tile row
+  if (!V || TW % V || TV == 0 || NT % TV || TH % (NT / TV)) vec = false;
+  const int RV = vec ? TH / (NT / TV) : 0;      // vectors per thread
+  if (vec) {
+    body << "__device__ __forceinline__ void compute_cellr(const Args &a, const In &in, int x, int y" << G.out_params(false)
+         << ") {\n" << G.center_loads(true) << G.body(false) << G.out_assigns() << "}\n";
+  }
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
        << "                                         bool gdesc) {\n"
-       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
-       << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
+       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n";
+  if (vec) {
+    std::ostringstream align;
+    align << "(t.x0 * " << es << ")";
+    for (size_t k = 0; k < P.in_rasters.size(); k++) align << " | a.in[" << k << "].p | a.in[" << k << "].pitch";
+    for (size_t k = 0; k < P.out_rasters.size(); k++) align << " | a.out[" << k << "].p | a.out[" << k << "].pitch";
+    body << "  if (t.xe - t.x0 == " << TW << " && t.ye - t.y0 == " << TH << " && ((" << align.str() << ") & 15) == 0) {\n"
+         << "    const int x = t.x0 + (threadIdx.x % " << TV << ") * " << V << ", ly0 = threadIdx.x / " << TV << ";\n";
+    for (Node *p : P.in_rasters) body << "    uint4 w" << G.rin.at(p) << "[" << RV << "];\n";
+    body << "#pragma unroll\n"
+         << "    for (int r = 0; r < " << RV << "; ++r) {\n"
+         << "      const int y = t.y0 + ly0 + r * " << NT / TV << ";\n";
+    for (Node *p : P.in_rasters) {
+      const int k = G.rin.at(p);
+      body << "      w" << k << "[r] = __ldg((const uint4 *)(row_ptr<" << G.T(p) << ">(a.in[" << k << "], y) + x));\n";
+    }
+    body << "    }\n"
+         << "#pragma unroll\n"
+         << "    for (int r = 0; r < " << RV << "; ++r) {\n"
+         << "      const int y = t.y0 + ly0 + r * " << NT / TV << ";\n";
+    int o = 0;
+    for (auto &kv : G.outk) body << "      uint4 q" << o++ << ";\n";
+    body << "#pragma unroll\n"
+         << "      for (int j = 0; j < " << V << "; ++j) {\n"
+         << "        In in;\n";
+    for (Node *p : P.in_rasters) {
+      const int k = G.rin.at(p);
+      body << "        in.i" << k << " = vlane<" << G.T(p) << ">(w" << k << "[r], j);\n";
+    }
+    o = 0;
+    std::ostringstream rargs;
+    for (auto &kv : G.outk) {
+      body << "        " << G.T(kv.first) << " r" << o << ";\n";
+      rargs << ", r" << o;
+      o++;
+    }
+    body << "        compute_cellr(a, in, x + j, y" << rargs.str() << ");\n";
+    o = 0;
+    for (auto &kv : G.outk) {
+      body << "        vset<" << G.T(kv.first) << ">(q" << o << ", j, r" << o << ");\n";
+      o++;
+    }
+    body << "      }\n";
+    o = 0;
+    for (auto &kv : G.outk) {
+      body << "      *(uint4 *)((" << G.T(kv.first) << " *)(a.out[" << kv.second << "].p + (u64)(s64)y * (u64)a.out[" << kv.second
+           << "].pitch) + x) = q" << o << ";\n";
+      o++;
+    }
+    body << "    }\n"
+         << "    return true;\n"
+         << "  }\n";
+  }
+  body << "  const int lx = threadIdx.x % " << TW << ", ly0 = threadIdx.x / " << TW << ";\n"
        << "  const int x = t.x0 + lx;\n"
        << "  In in[" << R << "];\n"
        << "#pragma unroll\n"
@@ -1620,6 +1713,9 @@ const FocalTune &focal_tune() {
         else if (k == "nt") r.nt = v;
         else if (k == "tw") r.tw = v;
         else if (k == "th") r.th = v;
+        else if (k == "lnt") r.lnt = v;
+        else if (k == "ltw") r.ltw = v;
+        else if (k == "lth") r.lth = v;
       }
       i = j + 1;
     }

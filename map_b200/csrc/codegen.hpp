@@ -60,12 +60,13 @@ KernelPlan generate_kernel(const Group &g, TileCfg cfg = TileCfg());
 
 // Tuning overrides of the standalone focal skeleton, read once from the
 // environment variable MAP_B200_FOCAL_TUNE ("key=value,..."; keys unroll, defer,
-// nt, tw, th; 0 or absent = the built-in choice). Used to measure variants;
+// nt, tw, th, and lnt, ltw, lth for Local kernels; 0 or absent = the built-in choice). Used to measure variants;
 // every variant computes the same cells with the same operations.
 struct FocalTune {
   int unroll = 0;   // unroll factor of the per-thread row loop (0: by body weight)
   int defer = 1;    // interior tiles keep a thread's results in registers and store them last
   int nt = 0, tw = 0, th = 0;
+  int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
 };
 const FocalTune &focal_tune();
 

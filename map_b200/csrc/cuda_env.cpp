@@ -11,6 +11,7 @@
 #include <unistd.h>
 
 #include <cstdio>
+#include <cstring>
 #include <cstdlib>
 #include <fstream>
 #include <map>
@@ -35,6 +36,9 @@ typedef CUresult (*PFN_TensorMapEncodeTiled)(CUtensorMap *, CUtensorMapDataType,
                                              CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 typedef CUresult (*PFN_GetErrorString)(CUresult, const char **);
 typedef CUresult (*PFN_Occupancy)(int *, CUfunction, int, size_t);
+typedef CUresult (*PFN_MemsetD2D8)(CUdeviceptr, size_t, unsigned char, size_t, size_t, CUstream);
+typedef CUresult (*PFN_MemsetD2D16)(CUdeviceptr, size_t, unsigned short, size_t, size_t, CUstream);
+typedef CUresult (*PFN_MemsetD2D32)(CUdeviceptr, size_t, unsigned int, size_t, size_t, CUstream);
 
 struct Driver {
   PFN_ModuleLoadData moduleLoadData = nullptr;
@@ -45,6 +49,9 @@ struct Driver {
   PFN_TensorMapEncodeTiled tensorMapEncodeTiled = nullptr;
   PFN_GetErrorString getErrorString = nullptr;
   PFN_Occupancy occupancy = nullptr;
+  PFN_MemsetD2D8 memsetD2D8 = nullptr;
+  PFN_MemsetD2D16 memsetD2D16 = nullptr;
+  PFN_MemsetD2D32 memsetD2D32 = nullptr;
 };
 
 Driver g_drv;
@@ -207,6 +214,9 @@ void CudaEnv::ensure_device() {
   load_entry(g_drv.tensorMapEncodeTiled, "cuTensorMapEncodeTiled");
   load_entry(g_drv.getErrorString, "cuGetErrorString");
   load_entry(g_drv.occupancy, "cuOccupancyMaxActiveBlocksPerMultiprocessor");
+  load_entry(g_drv.memsetD2D8, "cuMemsetD2D8Async");
+  load_entry(g_drv.memsetD2D16, "cuMemsetD2D16Async");
+  load_entry(g_drv.memsetD2D32, "cuMemsetD2D32Async");
   cuda_check(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking), "cudaStreamCreate");
   cuda_check(cudaMalloc(&err_word_, sizeof(uint32_t)), "cudaMalloc(error word)");
   cuda_check(cudaMemset(err_word_, 0, sizeof(uint32_t)), "cudaMemset");
@@ -320,6 +330,28 @@ void CudaEnv::encode_tma_2d(void *desc128, int dtype, const void *base, uint64_t
                                        box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE),
             "cuTensorMapEncodeTiled");
+}
+
+bool CudaEnv::fill_2d(void *dst, size_t pitch, const void *value, int elem_size, size_t width, size_t height,
+                      CUstream_st *stream) {
+  if (width == 0 || height == 0) return true;
+  const CUdeviceptr d = (CUdeviceptr)(uintptr_t)dst;
+  if (elem_size == 1) {
+    unsigned char v;
+    std::memcpy(&v, value, 1);
+    drv_check(g_drv.memsetD2D8(d, pitch, v, width, height, (CUstream)stream), "cuMemsetD2D8Async");
+  } else if (elem_size == 2) {
+    unsigned short v;
+    std::memcpy(&v, value, 2);
+    drv_check(g_drv.memsetD2D16(d, pitch, v, width, height, (CUstream)stream), "cuMemsetD2D16Async");
+  } else if (elem_size == 4) {
+    unsigned int v;
+    std::memcpy(&v, value, 4);
+    drv_check(g_drv.memsetD2D32(d, pitch, v, width, height, (CUstream)stream), "cuMemsetD2D32Async");
+  } else {
+    return false;
+  }
+  return true;
 }
 
 }  // namespace mapb

@@ -43,6 +43,10 @@ class CudaEnv {
   void launch(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args, size_t args_size);
   void launch_cluster(const KernelHandle &k, int grid, int block, int cluster, size_t smem, CUstream_st *stream, void *args);
   int occupancy(const KernelHandle &k, int block, size_t smem);   // resident CTAs per SM
+  // Writes `value` (elem_size bytes: 1, 2 or 4) into every element of a width x
+  // height 2-D array; false (nothing done) for other element sizes.
+  bool fill_2d(void *dst, size_t pitch, const void *value, int elem_size, size_t width, size_t height,
+               CUstream_st *stream);
   void encode_tma_2d(void *desc128, int dtype, const void *base, uint64_t width, uint64_t height, uint64_t pitch_bytes,
                      uint32_t box_w, uint32_t box_h);
   CUstream_st *stream() const { return stream_; }

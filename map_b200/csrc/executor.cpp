@@ -65,7 +65,8 @@ bool per_block(int sk) { return sk == SK_LOCAL || sk == SK_FOCAL || sk == SK_ZON
 
 bool reads_focal(const Group &g, Node *in) {
   for (Node *n : g.nodes)
-    if ((n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW) &&
+    if ((n->kind == K_NEIGHBOR || n->kind == K_CONVOLUTION || n->kind == K_FOCALFUNC || n->kind == K_FOCALFLOW ||
+         n->kind == K_FOCALPERCENT) &&
         n->prev[0] == in)
       return true;
   return false;
@@ -89,6 +90,80 @@ Variant host_eval(Node *n) {
 
 double now_ms() {
   return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Whole-raster form of the reference's Predictor (runtime/visitor/Predictor.cpp:22-200,
+// called before every block's computation, runtime/Worker.cpp:83-91): a node is
+// fixed when every cell holds the same value, known on the host. Constants are
+// fixed; element-wise nodes of fixed operands are evaluated with the host
+// operator tables; a focal node over a fixed raster is fixed under the mirror
+// border rules (every tap reads the same value) and is folded in the kernel's
+// order; an integer product with a fixed zero operand is zero. Cell-dependent
+// nodes (index, rand, flow directions, percentages) and raster inputs are not
+// fixed. Returns whether every raster output of the group is fixed (and how
+// many bytes each holds: 1, 2 or 4, the sizes a fill writes without a kernel).
+bool predict_group(const Group &g, const KernelPlan &K, std::unordered_map<Node *, Variant> &fixed, int border) {
+  if (g.skeleton != SK_LOCAL && g.skeleton != SK_FOCAL) return false;
+  auto known = [&](Node *p, Variant &v) {
+    auto it = fixed.find(p);
+    if (it != fixed.end()) { v = it->second; return true; }
+    if (p->meta.numdim == D0 && p->kind == K_CONSTANT) { v = p->cnst; return true; }
+    if (p->meta.numdim == D0 && p->has_value) { v = p->value; return true; }
+    return false;
+  };
+  const bool mirror = border == BORDER_BLOCK_MIRROR || border == BORDER_RASTER_MIRROR;
+  for (Node *n : g.nodes) {
+    Variant a, b, c;
+    const int dt = n->meta.dtype;
+    switch (n->kind) {
+      case K_CONSTANT: fixed[n] = var_convert(n->cnst, dt); break;
+      case K_CAST: case K_BARRIER:
+        if (known(n->prev[0], a)) fixed[n] = var_convert(a, dt);
+        break;
+      case K_UNARY:
+        if (known(n->prev[0], a)) fixed[n] = var_convert(host_unary(n->op, a), dt);
+        break;
+      case K_BINARY: {
+        const bool la = known(n->prev[0], a), lb = known(n->prev[1], b);
+        if (la && lb) fixed[n] = var_convert(host_binary(n->op, a, b), dt);
+        else if (n->op == MUL && !dt_is_float(dt) && ((la && var_is_zero(a)) || (lb && var_is_zero(b))))
+          fixed[n] = var_make_f64(0.0, dt);
+        break;
+      }
+      case K_CONDITIONAL:
+        if (known(n->prev[0], c)) {
+          Node *pick = var_as_f64(c) != 0.0 ? n->prev[1] : n->prev[2];
+          if (known(pick, a)) fixed[n] = var_convert(a, dt);
+        }
+        break;
+      case K_NEIGHBOR:
+        if (mirror && known(n->prev[0], a)) fixed[n] = var_convert(a, dt);
+        break;
+      case K_CONVOLUTION:
+        if (mirror && known(n->prev[0], a)) {   // acc = acc + tap * w, rows outer, columns inner
+          Variant acc = var_make_f64(0.0, dt);
+          for (const Variant &w : n->mask) acc = var_convert(host_binary(ADD, acc, host_binary(MUL, a, w)), dt);
+          fixed[n] = acc;
+        }
+        break;
+      case K_FOCALFUNC:
+        if (mirror && known(n->prev[0], a)) {
+          Variant acc = reduction_neutral(n->op, dt);
+          for (size_t i = 0; i < n->mask.size(); i++) acc = host_reduce(n->op, acc, var_convert(a, dt));
+          fixed[n] = acc;
+        }
+        break;
+      default:
+        break;
+    }
+  }
+  if (K.out_rasters.empty()) return false;
+  for (Node *o : K.out_rasters) {
+    if (!fixed.count(o)) return false;
+    const size_t s = dt_size(o->meta.dtype);
+    if (s != 1 && s != 2 && s != 4) return false;
+  }
+  return true;
 }
 
 }  // namespace
@@ -267,6 +342,11 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
       if (ft.nt) cfg.nt = ft.nt;
       if (ft.tw) cfg.tw = ft.tw;
       if (ft.th) cfg.th = ft.th;
+    } else if (g->skeleton == SK_LOCAL) {
+      const FocalTune &ft = focal_tune();
+      if (ft.lnt) cfg.nt = ft.lnt;
+      if (ft.ltw) cfg.tw = ft.ltw;
+      if (ft.lth) cfg.th = ft.lth;
     }
     P.plans[g->id] = generate_kernel(*g, cfg);
     if (compile && seen.insert(P.plans[g->id].source).second) {
@@ -282,7 +362,7 @@ std::shared_ptr<Executor::Prepared> Executor::prepare_cached(const std::vector<N
                                                              const std::set<Node *> &tset) {
   Runtime &rt = Runtime::get();
   std::string key = std::to_string(rt.exec_mode) + "," + std::to_string(rt.paired_cells) + "," +
-                    std::to_string(rt.algebraic_rewrite) + ";";
+                    std::to_string(rt.algebraic_rewrite) + ";";   // prediction runs per evaluation (not cached)
   for (Node *t : targets) key += std::to_string(t->id) + ",";
   key += ";";
   for (Node *t : tset) key += std::to_string(t->id) + ",";
@@ -564,12 +644,31 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
     n->has_value = true;
   };
 
+  // groups whose every output is one known value (Predictor): filled, not launched
+  std::unordered_map<Node *, Variant> fixed;
+  std::vector<char> predicted(P.fr.groups.size(), 0), filled(P.fr.groups.size(), 0);
+  if (rt.prediction)
+    for (auto &gp : P.fr.groups)
+      predicted[gp->id] = predict_group(*gp, P.plans[gp->id], fixed, rt.border) ? 1 : 0;
+  auto fill_predicted = [&](const Group &g, const KernelPlan &K) {
+    ensure_outputs(g, K);
+    for (Node *o : K.out_rasters) {
+      DevRaster &r = bufs.at(o);
+      const Variant v = fixed.at(o);
+      const int es = (int)dt_size(o->meta.dtype);
+      if (!env.fill_2d(r.ptr, (size_t)r.pitch, &v.u, es, (size_t)o->meta.W(), (size_t)o->meta.H(), (CUstream_st *)st))
+        throw MapError("prediction: no fill for this element size");
+    }
+    last.predicted++;
+  };
+
   try {
     if (rt.exec_mode == EXEC_FUSED) {
       for (auto &gp : P.fr.groups) {
         const Group &g = *gp;
         const KernelPlan &K = P.plans[g.id];
         if (g.skeleton == SK_HOST) { run_host(g); continue; }
+        if (predicted[g.id]) { fill_predicted(g, K); continue; }
         if (g.skeleton == SK_RADIAL || g.skeleton == SK_SPREAD) {
           run_scan_group(g, K, bufs, get, alloc_out);
           continue;
@@ -589,6 +688,11 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
           case 1: run_scan_group(g, K, bufs, get, alloc_out); break;
           case 2: zonal_finish(g, K); break;
           default: {
+            if (predicted[g.id]) {
+              if (!filled[g.id]) fill_predicted(g, K);   // one fill, at the group's first block, for all its blocks
+              filled[g.id] = 1;
+              break;
+            }
             ensure_outputs(g, K);
             if (g.skeleton == SK_ZONAL) zonal_begin(g, K);
             const int rx0 = j.bx * g.BS0, ry0 = j.by * g.BS1;

@@ -76,6 +76,7 @@ struct EvalStats {
   int groups = 0;
   int compiled = 0;
   int bands = 0;     // row bands of a streamed evaluation (0: whole rasters)
+  int predicted = 0; // groups filled with their one known value instead of launched
   double host_ms = 0;
 };
 

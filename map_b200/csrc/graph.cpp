@@ -12,8 +12,8 @@ namespace mapb {
 const char *kind_name(int k) {
   static const char *n[] = {"Constant", "Read", "HostInput", "DeviceInput", "Index", "Rand", "Cast", "Unary", "Binary",
                             "Conditional", "Neighbor", "Convolution", "FocalFunc", "FocalFlow", "ZonalReduc",
-                            "RadialScan", "SpreadScan", "Write", "Barrier"};
-  return (k >= 0 && k <= K_BARRIER) ? n[k] : "?";
+                            "RadialScan", "SpreadScan", "Write", "Barrier", "FocalPercent"};
+  return (k >= 0 && k <= K_FOCALPERCENT) ? n[k] : "?";
 }
 
 std::string arr_str(const Arr2 &a) {
@@ -22,7 +22,7 @@ std::string arr_str(const Arr2 &a) {
 
 int Node::halo_x() const {
   switch (kind) {
-    case K_CONVOLUTION: case K_FOCALFUNC: return mask_ds.arr[0] / 2;   // Convolution.cpp:85 (size/2)
+    case K_CONVOLUTION: case K_FOCALFUNC: case K_FOCALPERCENT: return mask_ds.arr[0] / 2;   // Convolution.cpp:85 (size/2)
     case K_NEIGHBOR: return std::abs(coord.arr[0]);                     // Neighbor.cpp:86
     case K_FOCALFLOW: return 1;                                         // FocalFlow.cpp:75
     default: return 0;
@@ -30,7 +30,7 @@ int Node::halo_x() const {
 }
 int Node::halo_y() const {
   switch (kind) {
-    case K_CONVOLUTION: case K_FOCALFUNC: return mask_ds.arr[1] / 2;
+    case K_CONVOLUTION: case K_FOCALFUNC: case K_FOCALPERCENT: return mask_ds.arr[1] / 2;
     case K_NEIGHBOR: return std::abs(coord.arr[1]);
     case K_FOCALFLOW: return 1;
     default: return 0;
@@ -344,6 +344,24 @@ Node *Runtime::focal_func(Node *arg, const Variant *mask, int cnt, Arr2 mds, int
   n->meta = arg->meta;   // FocalFunc.cpp: keeps the argument's type
   n->prev = {arg};
   return add(std::move(n), "FF|" + std::to_string(red) + "|" + mask_key(n->mask, mds) + "|" + pid(arg));
+}
+
+// FocalPercent (runtime/dag/FocalPercent.cpp Factory, runtime/skeleton/FocalSkeleton.cpp:375-403,
+// util/PercentType.cpp): the result keeps the argument's type; the mask gives
+// the window's extent only (its values are not read, as in the reference).
+Node *Runtime::focal_percent(Node *arg, const Variant *mask, int cnt, Arr2 mds, int type) {
+  check_focal_arg(arg, "focalPercent");
+  check_mask(mask, cnt, mds, "focalPercent");
+  if (type != 1 && type != 2) throw MapError("focalPercent: type must be AGE (1) or ILE (2)");
+  auto n = std::make_unique<Node>();
+  n->kind = K_FOCALPERCENT;
+  n->pattern = P_FOCAL;
+  n->op = type;
+  n->mask.assign(mask, mask + cnt);
+  n->mask_ds = mds;
+  n->meta = arg->meta;
+  n->prev = {arg};
+  return add(std::move(n), "FP|" + std::to_string(type) + "|" + mask_key(n->mask, mds) + "|" + pid(arg));
 }
 
 Node *Runtime::focal_flow(Node *arg) {

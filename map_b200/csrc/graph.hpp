@@ -21,7 +21,7 @@ namespace mapb {
 enum NodeKind : int {
   K_CONSTANT, K_READ, K_HOSTIN, K_DEVIN, K_INDEX, K_RAND, K_CAST, K_UNARY, K_BINARY, K_CONDITIONAL,
   K_NEIGHBOR, K_CONVOLUTION, K_FOCALFUNC, K_FOCALFLOW, K_ZONALREDUC, K_RADIALSCAN, K_SPREADSCAN,
-  K_WRITE, K_BARRIER
+  K_WRITE, K_BARRIER, K_FOCALPERCENT
 };
 
 const char *kind_name(int k);
@@ -105,6 +105,9 @@ struct Runtime {
   // Hillshade compositions (python/hill.py:41-49) are generated through the
   // shading identity of rewrite.hpp; 0 keeps the literal operator chain.
   int algebraic_rewrite = 1;
+  // Local / Focal groups whose every output is one known value are filled, not
+  // launched (the reference's Predictor, runtime/visitor/Predictor.cpp); 0 turns it off.
+  int prediction = 1;
   // incremented whenever nodes are destroyed (caches keyed by node ids check it)
   uint64_t epoch = 0;
   Arr2 default_bs{{256, 256}, 2};
@@ -128,6 +131,9 @@ struct Runtime {
   Node *neighbor(Node *arg, Arr2 coord);
   Node *convolution(Node *arg, const Variant *mask, int n, Arr2 mask_ds);
   Node *focal_func(Node *arg, const Variant *mask, int n, Arr2 mask_ds, int red);
+  // type 1 (AGE): fraction of the window's cells equal to the centre cell;
+  // type 2 (ILE): fraction of the window's cells the centre cell exceeds
+  Node *focal_percent(Node *arg, const Variant *mask, int n, Arr2 mask_ds, int type);
   Node *focal_flow(Node *arg);
   Node *zonal_reduc(Node *arg, int red);
   Node *radial_scan(Node *arg, int red, Arr2 start, double radius = 0);

@@ -779,36 +779,37 @@ double pct(std::vector<double> v, double p) {
 }
 }  // namespace
 
-std::string Server::run_load(double rate, double seconds, const double *mix, unsigned seed, double obs_h, double radius) {
-  Impl &I = *impl_;
-  std::mt19937_64 rng(seed);
-  std::exponential_distribution<double> gap(rate);
-  std::discrete_distribution<int> pick(mix, mix + 4);
-  const int sizes[3] = {256, 512, 1024};
-  std::uniform_int_distribution<int> pick_size(0, 2);
-  std::vector<long long> ids;
-  std::vector<int> types, wsz;
-  const double t0 = now_s();
-  double t = 0;
-  long long cells = 0;
-  while (true) {
-    t += gap(rng);
-    if (t > seconds) break;
-    const int type = pick(rng);
-    const int w = sizes[pick_size(rng)];
-    const int h = w;
-    std::uniform_int_distribution<int> px(0, I.W - w), py(0, I.H - h), po(0, w - 1);
-    const int x0 = px(rng), y0 = py(rng), ox = po(rng), oy = po(rng);
-    const double target = t0 + t;
-    double dt = target - now_s();
-    if (dt > 0) std::this_thread::sleep_for(std::chrono::duration<double>(dt));
-    ids.push_back(submit(type, x0, y0, w, h, ox, oy, (float)obs_h, radius, true));
-    types.push_back(type);
-    wsz.push_back(w);
-    cells += (long long)w * h;
+namespace {
+// one generated request of the synthetic load (program, window, observer)
+struct GenReq {
+  int type, w, h, x0, y0, ox, oy;
+};
+struct LoadGen {
+  std::mt19937_64 rng;
+  std::discrete_distribution<int> pick;
+  std::uniform_int_distribution<int> pick_size{0, 2};
+  int W, H;
+  LoadGen(unsigned seed, const double *mix, int W, int H) : rng(seed), pick(mix, mix + 4), W(W), H(H) {}
+  GenReq next() {
+    static const int sizes[3] = {256, 512, 1024};
+    GenReq r;
+    r.type = pick(rng);
+    r.w = r.h = sizes[pick_size(rng)];
+    std::uniform_int_distribution<int> px(0, W - r.w), py(0, H - r.h), po(0, r.w - 1);
+    r.x0 = px(rng);
+    r.y0 = py(rng);
+    r.ox = po(rng);
+    r.oy = po(rng);
+    return r;
   }
-  for (long long id : ids) wait(id, 120.0);
-  const double t_end = now_s();
+};
+}  // namespace
+
+std::string Server::load_report(const std::vector<long long> &ids, const std::vector<int> &types,
+                                const std::vector<int> &wsz, double t0, double t_end, long long cells,
+                                long long batches0, long long batched0, const std::string &head) {
+  Impl &I = *impl_;
+  const int sizes[3] = {256, 512, 1024};
   std::vector<double> all, by_size[3], by_type[4];
   for (size_t i = 0; i < ids.size(); i++) {
     double l = latency_ms(ids[i]);
@@ -817,14 +818,20 @@ std::string Server::run_load(double rate, double seconds, const double *mix, uns
     by_size[wsz[i] == 256 ? 0 : wsz[i] == 512 ? 1 : 2].push_back(l);
     by_type[types[i]].push_back(l);
   }
+  long long nb, nr;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    nb = I.batches - batches0;
+    nr = I.batched_requests - batched0;
+  }
   std::ostringstream s;
   s.setf(std::ios::fixed);
   s.precision(3);
   const double wall = t_end - t0;
-  s << "{\"rate_req_s\": " << rate << ", \"seconds\": " << seconds << ", \"requests\": " << ids.size()
-    << ", \"completed\": " << all.size() << ", \"wall_s\": " << wall << ", \"throughput_req_s\": " << ids.size() / wall
-    << ", \"gcells_s\": " << cells / wall / 1e9 << ", \"p50_ms\": " << pct(all, 50) << ", \"p99_ms\": " << pct(all, 99)
-    << ", \"by_window\": {";
+  s << "{" << head << ", \"requests\": " << ids.size() << ", \"completed\": " << all.size() << ", \"wall_s\": " << wall
+    << ", \"throughput_req_s\": " << ids.size() / wall << ", \"gcells_s\": " << cells / wall / 1e9
+    << ", \"p50_ms\": " << pct(all, 50) << ", \"p99_ms\": " << pct(all, 99) << ", \"batches\": " << nb
+    << ", \"mean_batch\": " << (nb ? (double)nr / nb : 0.0) << ", \"by_window\": {";
   for (int k = 0; k < 3; k++)
     s << (k ? ", " : "") << "\"" << sizes[k] << "\": {\"n\": " << by_size[k].size() << ", \"p50_ms\": " << pct(by_size[k], 50)
       << ", \"p99_ms\": " << pct(by_size[k], 99) << "}";
@@ -835,6 +842,86 @@ std::string Server::run_load(double rate, double seconds, const double *mix, uns
       << ", \"p99_ms\": " << pct(by_type[k], 99) << "}";
   s << "}, \"server\": " << stats_json() << "}";
   return s.str();
+}
+
+std::string Server::run_load(double rate, double seconds, const double *mix, unsigned seed, double obs_h, double radius) {
+  Impl &I = *impl_;
+  LoadGen gen(seed, mix, I.W, I.H);
+  std::exponential_distribution<double> gap(rate);
+  std::vector<long long> ids;
+  std::vector<int> types, wsz;
+  long long batches0, batched0;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    batches0 = I.batches;
+    batched0 = I.batched_requests;
+  }
+  const double t0 = now_s();
+  double t = 0;
+  long long cells = 0;
+  while (true) {
+    t += gap(gen.rng);
+    if (t > seconds) break;
+    const GenReq r = gen.next();
+    const double target = t0 + t;
+    double dt = target - now_s();
+    if (dt > 0) std::this_thread::sleep_for(std::chrono::duration<double>(dt));
+    ids.push_back(submit(r.type, r.x0, r.y0, r.w, r.h, r.ox, r.oy, (float)obs_h, radius, true));
+    types.push_back(r.type);
+    wsz.push_back(r.w);
+    cells += (long long)r.w * r.h;
+  }
+  for (long long id : ids) wait(id, 120.0);
+  std::ostringstream head;
+  head.setf(std::ios::fixed);
+  head.precision(3);
+  head << "\"mode\": \"open\", \"rate_req_s\": " << rate << ", \"seconds\": " << seconds;
+  return load_report(ids, types, wsz, t0, now_s(), cells, batches0, batched0, head.str());
+}
+
+std::string Server::run_closed(int outstanding, double seconds, const double *mix, unsigned seed, double obs_h,
+                               double radius) {
+  Impl &I = *impl_;
+  if (outstanding < 1) throw MapError("server: a closed-loop load needs at least one outstanding request");
+  LoadGen gen(seed, mix, I.W, I.H);
+  std::vector<long long> ids;
+  std::vector<int> types, wsz;
+  std::vector<size_t> inflight;   // indices into ids
+  long long batches0, batched0;
+  {
+    std::lock_guard<std::mutex> lk(I.m);
+    batches0 = I.batches;
+    batched0 = I.batched_requests;
+  }
+  const double t0 = now_s();
+  long long cells = 0;
+  while (now_s() - t0 < seconds) {
+    while ((int)inflight.size() < outstanding) {
+      const GenReq r = gen.next();
+      inflight.push_back(ids.size());
+      ids.push_back(submit(r.type, r.x0, r.y0, r.w, r.h, r.ox, r.oy, (float)obs_h, radius, true));
+      types.push_back(r.type);
+      wsz.push_back(r.w);
+      cells += (long long)r.w * r.h;
+    }
+    bool any = false;
+    for (size_t k = 0; k < inflight.size();) {
+      if (wait(ids[inflight[k]], 0.0) == 0) {
+        inflight[k] = inflight.back();
+        inflight.pop_back();
+        any = true;
+      } else {
+        k++;
+      }
+    }
+    if (!any) std::this_thread::sleep_for(std::chrono::microseconds(20));
+  }
+  for (size_t k : inflight) wait(ids[k], 120.0);
+  std::ostringstream head;
+  head.setf(std::ios::fixed);
+  head.precision(3);
+  head << "\"mode\": \"closed\", \"outstanding\": " << outstanding << ", \"seconds\": " << seconds;
+  return load_report(ids, types, wsz, t0, now_s(), cells, batches0, batched0, head.str());
 }
 
 }  // namespace mapb

@@ -24,6 +24,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <vector>
 
 namespace mapb {
 
@@ -49,8 +50,14 @@ class Server {
   // mix weights mix[4], windows 256^2 / 512^2 / 1024^2 uniformly, offsets and
   // observers uniform; returns latency percentiles and throughput as JSON.
   std::string run_load(double rate, double seconds, const double *mix, unsigned seed, double obs_h, double radius);
+  // Closed-loop load: `outstanding` requests are kept in flight for `seconds`
+  // (each completion is replaced at once by a new request of the same mix).
+  std::string run_closed(int outstanding, double seconds, const double *mix, unsigned seed, double obs_h, double radius);
 
  private:
+  std::string load_report(const std::vector<long long> &ids, const std::vector<int> &types, const std::vector<int> &wsz,
+                          double t0, double t_end, long long cells, long long batches0, long long batched0,
+                          const std::string &head);
   struct Impl;
   std::unique_ptr<Impl> impl_;
 };

@@ -94,6 +94,16 @@ template <> __device__ __forceinline__ void str_out<bool>(const RasterArg &r, in
   map_stg<1>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, v ? 1u : 0u);
 }
 
+// Lane j of a 16-byte vector of cells of type T, and its assignment.
+template <class T> __device__ __forceinline__ T vlane(const uint4 &v, int j) {
+  T r;
+  memcpy(&r, (const char *)&v + j * sizeof(T), sizeof(T));
+  return r;
+}
+template <class T> __device__ __forceinline__ void vset(uint4 &v, int j, T x) {
+  memcpy((char *)&v + j * sizeof(T), &x, sizeof(T));
+}
+
 // ------------------------------------------------------------------ atan2 (float)
 
 // Two-argument arctangent of float32 operands, at most 1.5 ulp from the

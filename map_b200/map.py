@@ -506,6 +506,23 @@ def fmax(raster, lst):
     return Raster(_lib.ma_focalFunc(raster, varptr, size, ds, MAX))
 
 
+# Focal percentages (front/Raster.cpp:437-448, no Python binding in the
+# reference): the fraction of the mask-sized window around each cell whose
+# cells the centre equals (percentage, AGE) or exceeds (percentile, ILE), in
+# the raster's own type; the mask's values are not used, only its extent.
+AGE, ILE = 1, 2
+
+
+def percentage(raster, lst):
+    varptr, size, ds, _keep = _mask(lst)
+    return Raster(_lib.ma_focalPercent(raster, varptr, size, ds, AGE))
+
+
+def percentile(raster, lst):
+    varptr, size, ds, _keep = _mask(lst)
+    return Raster(_lib.ma_focalPercent(raster, varptr, size, ds, ILE))
+
+
 def zsum(raster):
     return Raster(_lib.ma_zonalReduc(raster, SUM))
 
@@ -704,6 +721,27 @@ def row_margin(*rasters):
     return _lib.ma_rowMargin(_node_array(rasters), len(rasters))
 
 
+def bin_read_numpy(path):
+    """The cells of a `.bin` file as a 2-D NumPy array (host only, no device)."""
+    import numpy as np
+    info = (ct.c_int * 7)()
+    _lib.ma_binInfo(path.encode(), info)
+    dt, _, w, h = info[0], info[1], info[2], info[3]
+    out = np.empty((h, w), dtype=np.dtype(_np_dtype[dt]))
+    _lib.ma_binReadHost(path.encode(), out.ctypes.data_as(ct.c_void_p), out.nbytes)
+    return out
+
+
+def bin_write_numpy(path, a, bs=(256, 256), mo=None):
+    """Writes a 2-D NumPy array as a `.bin` file (ROW+BLK blocks of bs, or ROW)."""
+    import numpy as np
+    a = np.ascontiguousarray(a)
+    dt = _dt_of_np[a.dtype.name]
+    mo = ROW + BLK if mo is None else mo
+    _lib.ma_binWriteHost(path.encode(), a.ctypes.data_as(ct.c_void_p), Array([a.shape[1], a.shape[0]]), dt, mo,
+                         Array(list(bs)))
+
+
 def to_numpy(raster, out=None):
     """Evaluates a raster and returns it as a 2-D NumPy array."""
     import numpy as np
@@ -752,6 +790,15 @@ def set_paired_cells(on):
 
 def get_paired_cells():
     return bool(_lib.ma_getPairedCells())
+
+
+def set_prediction(on):
+    """Groups whose every output is one known value are filled without a launch."""
+    _lib.ma_setPrediction(1 if on else 0)
+
+
+def last_predicted_count():
+    return _lib.ma_lastPredictedCount()
 
 
 def set_algebraic_rewrite(on):
@@ -943,6 +990,7 @@ _sig('ma_neighbor', [Raster, Array], Node)
 _sig('ma_boundedNbh', [Raster, Raster, Raster], Node)
 _sig('ma_convolution', [Raster, ct.POINTER(Variant), ct.c_int, Array], Node)
 _sig('ma_focalFunc', [Raster, ct.POINTER(Variant), ct.c_int, Array, ct.c_int], Node)
+_sig('ma_focalPercent', [Raster, ct.POINTER(Variant), ct.c_int, Array, ct.c_int], Node)
 _sig('ma_zonalReduc', [Raster, ct.c_int], Node)
 _sig('ma_radialScan', [Raster, ct.c_int, Array], Node)
 _sig('ma_spreadScan', [Raster, Raster, ct.c_int], Node)
@@ -974,6 +1022,12 @@ _sig('ma_getStreamRows', [], ct.c_int, check=False)
 _sig('ma_setPairedCells', [ct.c_int], None)
 _sig('ma_getPairedCells', [], ct.c_int, check=False)
 _sig('ma_setAlgebraicRewrite', [ct.c_int], None)
+_sig('ma_setPrediction', [ct.c_int], None)
+_sig('ma_binInfo', [ct.c_char_p, ct.POINTER(ct.c_int)], ct.c_int)
+_sig('ma_binReadHost', [ct.c_char_p, ct.c_void_p, ct.c_size_t], ct.c_int)
+_sig('ma_binWriteHost', [ct.c_char_p, ct.c_void_p, Array, ct.c_int, ct.c_int, Array], ct.c_int)
+_sig('ma_getPrediction', [], ct.c_int, check=False)
+_sig('ma_lastPredictedCount', [], ct.c_int, check=False)
 _sig('ma_fromDeviceRows', [ct.c_void_p, ct.c_longlong, Array, ct.c_int, Array, ct.c_int, ct.c_int], Node)
 _sig('ma_evalRows', [ct.POINTER(Node), ct.c_int, ct.POINTER(ct.c_void_p), ct.POINTER(ct.c_longlong), ct.c_int, ct.c_int],
      ct.c_int)
@@ -1086,6 +1140,15 @@ class Server:
         n = _lib.ma_serverLoad(self._h, rate, seconds, m, seed, obs_h, radius, buf, cap)
         return json.loads(buf.value.decode())
 
+    def load_closed(self, outstanding, seconds, mix=(0.5, 0.2, 0.15, 0.15), seed=0, obs_h=10.0, radius=167.0):
+        """Closed loop: `outstanding` requests in flight for `seconds`."""
+        import json
+        m = (ct.c_double * 4)(*mix)
+        cap = 1 << 16
+        buf = ct.create_string_buffer(cap)
+        _lib.ma_serverLoadClosed(self._h, outstanding, seconds, m, seed, obs_h, radius, buf, cap)
+        return json.loads(buf.value.decode())
+
     def close(self):
         if getattr(self, "_h", None):
             _lib.ma_serverDestroy(self._h)
@@ -1108,4 +1171,6 @@ _sig('ma_serverLatency', [ct.c_void_p, ct.c_longlong], ct.c_double)
 _sig('ma_serverStats', [ct.c_void_p, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_serverLoad', [ct.c_void_p, ct.c_double, ct.c_double, ct.POINTER(ct.c_double), ct.c_uint, ct.c_double,
                        ct.c_double, ct.c_char_p, ct.c_size_t], ct.c_size_t)
+_sig('ma_serverLoadClosed', [ct.c_void_p, ct.c_int, ct.c_double, ct.POINTER(ct.c_double), ct.c_uint, ct.c_double,
+                             ct.c_double, ct.c_char_p, ct.c_size_t], ct.c_size_t)
 _sig('ma_serverDestroy', [ct.c_void_p], None)

@@ -279,6 +279,39 @@ void orc_life_rows(const uint8_t *in, int W, int H, int BS0, int BS1, int border
     }
 }
 
+/* FocalPercent (runtime/skeleton/FocalSkeleton.cpp:375-403, util/PercentType.cpp):
+ * count, in the argument's type, the cells of the (2hx+1) x (2hy+1) window
+ * around the cell for which `centre OP cell` holds (OP: == for type 1 AGE,
+ * > for type 2 ILE), then divide by the window size in that type. The window
+ * is centred and the divisor is the window size (the reference's kernel starts
+ * its loop at the centre and drops the parentheses of its divisor). */
+void orc_focal_percent_f32(const float *in, int W, int H, int BS0, int BS1, int border, int hx, int hy, int type,
+                           float *out) {
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      float c = in[(size_t)y * W + x], v = 0.0f;
+      for (int i1 = -hy; i1 <= hy; i1++)
+        for (int i0 = -hx; i0 <= hx; i0++) {
+          float t = tapf(in, W, H, BS0, BS1, border, x, y, i0, i1);
+          v = v + (float)(type == 1 ? (c == t) : (c > t));
+        }
+      out[(size_t)y * W + x] = v / (float)((2 * hx + 1) * (2 * hy + 1));
+    }
+}
+void orc_focal_percent_u8(const uint8_t *in, int W, int H, int BS0, int BS1, int border, int hx, int hy, int type,
+                          uint8_t *out) {
+  for (int y = 0; y < H; y++)
+    for (int x = 0; x < W; x++) {
+      uint8_t c = in[(size_t)y * W + x], v = 0;
+      for (int i1 = -hy; i1 <= hy; i1++)
+        for (int i0 = -hx; i0 <= hx; i0++) {
+          uint8_t t = tapu8(in, W, H, BS0, BS1, border, x, y, i0, i1);
+          v = (uint8_t)(v + (uint8_t)(type == 1 ? (c == t) : (c > t)));
+        }
+      out[(size_t)y * W + x] = (uint8_t)(v / (uint8_t)((2 * hx + 1) * (2 * hy + 1)));
+    }
+}
+
 /* ------------------------------------------------------------ weighted sum */
 
 /* wsum.py (python/wsum.py:11) generalised to k layers:

@@ -7,10 +7,17 @@
 // stubs.cpp runs nothing).
 //
 // usage: ref_codegen hill|life|wsum <work dir>
+//        ref_codegen binwrite <path> <W> <H> <BS> <dtype>
+//        ref_codegen binread <path> <out>
 #include "front/bindings.hpp"
 #include "util/util.hpp"
+#include "file/File.hpp"
+#include "file/binary.hpp"
+#include "runtime/Block.hpp"
+#include "runtime/Entry.hpp"
 
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -77,9 +84,77 @@ Node *hill(Node *dem) {
   return bin(a, b, ADD);
 }
 
+// .bin files through the reference's own File<binary> (file/binary.cpp):
+// bin_write creates a W x H raster of dtype dt (F32, U8 or S32) in BS x BS
+// blocks whose cell (x, y) holds pattern(x, y), block by block with writeBlock
+// (cells of edge blocks beyond the raster hold pattern of their padded
+// coordinate); bin_read reads a file block by block with readBlock and writes
+// its cells as dense row-major bytes to `out`.
+double pattern(int x, int y) { return (double)((x * 7 + y * 13) % 251) + 0.25 * (x % 4); }
+
+int bin_write(const std::string &path, int W, int H, int BS, int dt) {
+  MetaData meta(DataSize{W, H}, DataType((DataTypeEnum)dt), MemOrder(ROW + BLK), BlockSize{BS, BS});
+  File<binary> f(meta);
+  f.open(path, OUT);
+  const int es = DataType((DataTypeEnum)dt).sizeOf();
+  std::vector<char> buf((size_t)BS * BS * es);
+  Entry entry(nullptr);
+  entry.host_mem = buf.data();
+  for (int by = 0; by * BS < H; by++)
+    for (int bx = 0; bx * BS < W; bx++) {
+      for (int j = 0; j < BS; j++)
+        for (int i = 0; i < BS; i++) {
+          const double v = pattern(bx * BS + i, by * BS + j);
+          char *c = buf.data() + ((size_t)j * BS + i) * es;
+          if (dt == F32) { float t = (float)v; std::memcpy(c, &t, 4); }
+          else if (dt == S32) { int32_t t = (int32_t)v; std::memcpy(c, &t, 4); }
+          else { uint8_t t = (uint8_t)v; std::memcpy(c, &t, 1); }
+        }
+      Block blk(Key(nullptr, Coord{bx, by}));
+      blk.entry = &entry;
+      f.writeBlock(blk);
+      blk.entry = nullptr;
+    }
+  f.close();
+  return 0;
+}
+
+int bin_read(const std::string &path, const std::string &out) {
+  File<binary> f;
+  f.open(path, IN);
+  const DataSize ds = f.getDataSize();
+  const BlockSize bs = f.getBlockSize();
+  const int es = f.getDataType().sizeOf();
+  const int W = ds[0], H = ds[1];
+  std::vector<char> buf((size_t)bs[0] * bs[1] * es), dense((size_t)W * H * es);
+  Entry entry(nullptr);
+  entry.host_mem = buf.data();
+  for (int by = 0; by * bs[1] < H; by++)
+    for (int bx = 0; bx * bs[0] < W; bx++) {
+      Block blk(Key(nullptr, Coord{bx, by}));
+      blk.entry = &entry;
+      f.readBlock(blk);
+      blk.entry = nullptr;
+      for (int j = 0; j < bs[1] && by * bs[1] + j < H; j++)
+        for (int i = 0; i < bs[0] && bx * bs[0] + i < W; i++)
+          std::memcpy(dense.data() + ((size_t)(by * bs[1] + j) * W + bx * bs[0] + i) * es,
+                      buf.data() + ((size_t)j * bs[0] + i) * es, es);
+    }
+  f.close();
+  FILE *o = std::fopen(out.c_str(), "wb");
+  if (!o) return 1;
+  std::fprintf(o, "%d %d %d %d %d %d\n", (int)f.getDataType().get(), W, H, (int)f.getMemOrder().get(), bs[0], bs[1]);
+  std::fwrite(dense.data(), 1, dense.size(), o);
+  std::fclose(o);
+  return 0;
+}
+
 }  // namespace
 
 int main(int argc, char **argv) {
+  if (argc >= 7 && std::string(argv[1]) == "binwrite")
+    return bin_write(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]));
+  if (argc >= 4 && std::string(argv[1]) == "binread") return bin_read(argv[2], argv[3]);
   if (argc < 3) {
     std::fprintf(stderr, "usage: %s hill|life|wsum <work dir>\n", argv[0]);
     return 2;

@@ -43,4 +43,5 @@ def fresh(M):
     M.set_exec_mode(M.EXEC_FUSED)
     M.set_paired_cells(True)
     M.set_algebraic_rewrite(True)
+    M.set_prediction(True)
     M.set_default_blocksize([256, 256])

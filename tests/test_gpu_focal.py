@@ -223,3 +223,21 @@ def test_block_mirror_corner_rule(fresh):
     M.set_border(M.BORDER_RASTER_MIRROR)
     got = M.to_numpy(r([-1, -1]))
     assert got[0, 32] == a[0, 31]
+
+
+@pytest.mark.parametrize("typ", [1, 2])
+@pytest.mark.parametrize("dtype,border", [(np.float32, 0), (np.float32, 1), (np.uint8, 2), (np.uint8, 0)])
+def test_focal_percent_matches_oracle(fresh, typ, dtype, border):
+    """FocalPercent (percentage: share of the window equal to the centre;
+    percentile: share below it), 3x3 and 5x3 windows, bit-exact."""
+    M = fresh
+    M.set_border(border)
+    rng = np.random.default_rng(31 + typ)
+    a_np = (rng.integers(0, 6, size=(150, 211))).astype(dtype)     # few values: many ties
+    a = M.from_numpy(a_np, bs=[64, 64])
+    fn = M.percentage if typ == 1 else M.percentile
+    for mask, (hx, hy) in (([[1, 1, 1]] * 3, (1, 1)), ([[1, 2, 3, 4, 5]] * 3, (2, 1))):
+        got = M.to_numpy(fn(a, mask))
+        ref = O.focal_percent(a_np, hx, hy, typ, (64, 64), border)
+        assert got.dtype == ref.dtype
+        assert np.array_equal(got, ref), (mask, int((got != ref).sum()))

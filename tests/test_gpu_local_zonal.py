@@ -154,3 +154,30 @@ def test_sincos_pairing_is_bit_identical(M):
     assert "sincosf(" in src
     ab = M.to_numpy(a + b)
     assert np.array_equal(ab, only_s + only_c)
+
+
+@pytest.mark.parametrize("mode", [0, 1])
+def test_prediction_fills_fixed_groups_without_launches(fresh, mode):
+    """A program of constants only (element-wise and focal operators of a
+    constant raster, block-mirror border) is written by fills, with no kernel
+    launch, in fused and plain mode; switching prediction off launches kernels
+    and gives the same cells."""
+    M = fresh
+    M.set_exec_mode(mode)
+    c = M.zeros((300, 200), M.F32, M.ROW + M.BLK, [64, 64]) + 2.5
+    prog = M.convolve(c * 3.0 - 1.0, [[1, 2, 1], [0, 1, 0], [1, 2, 1]]) + (c > 1.0)
+    got = M.to_numpy(prog)
+    assert M.last_launch_count() == 0 and M.last_predicted_count() >= 1
+    want = np.float32(0)
+    for w in (1, 2, 1, 0, 1, 0, 1, 2, 1):
+        want = np.float32(want + np.float32(6.5) * np.float32(w))
+    assert np.all(got == np.float32(want + np.float32(1)))
+    M.set_prediction(False)
+    again = M.to_numpy(prog)
+    assert M.last_launch_count() >= 1
+    assert np.array_equal(got, again)
+    # a cell-dependent node keeps the launch
+    M.set_prediction(True)
+    idx = M.to_numpy(c + M.index(c, M.D1))
+    assert M.last_launch_count() >= 1
+    assert np.array_equal(idx, np.float32(2.5) + np.arange(300, dtype=np.float32)[None, :] + np.zeros((200, 1), np.float32))

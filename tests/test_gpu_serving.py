@@ -126,3 +126,15 @@ def test_window_sizes_beyond_the_template_cache_still_work(served):
         got = srv.result(rid, (h, w), np.float32)
         want = window_expected(M, dem_np, M.Server.SLOPE, 11 * k, 5 * k, w, h)
         assert np.array_equal(got, want)
+
+
+def test_closed_loop_load_batches_requests(served):
+    """With many requests kept in flight the dispatcher admits several per batch
+    (continuous batching), every request completes, and the report counts the
+    batches of this run only."""
+    M, srv, _ = served
+    res = srv.load_closed(32, 1.0, seed=5)
+    assert res["mode"] == "closed" and res["requests"] >= 32
+    assert res["completed"] == res["requests"]
+    assert res["batches"] >= 1 and res["mean_batch"] > 1.0
+    assert res["p99_ms"] >= res["p50_ms"] > 0

@@ -150,3 +150,51 @@ def test_facts_are_what_the_reference_generates():
     with open(FACTS) as f:
         committed = json.load(f)
     assert json.loads(json.dumps(D.facts(exe), sort_keys=True)) == committed
+
+
+def _ref_exe():
+    sys.path.insert(0, os.path.join(ROOT, "oracle", "ref_codegen"))
+    import build_ref_codegen as B
+    if not os.path.isfile(os.path.join(B.REF, "Makefile")):
+        pytest.skip("reference checkout not available")
+    return B.build()
+
+
+def _pattern(w, h, dtype):
+    y, x = np.mgrid[0:h, 0:w]
+    v = ((x * 7 + y * 13) % 251).astype(np.float64) + 0.25 * (x % 4)
+    return v.astype(dtype)
+
+
+@pytest.mark.parametrize("w,h,bs,dt", [(300, 200, 128, 1), (256, 256, 256, 4), (257, 130, 64, 10)])
+def test_bin_files_written_by_the_reference_read_here(M, tmp_path, w, h, bs, dt):
+    """The reference's own .bin writer (file/binary.cpp File<binary>, block by
+    block) produces files this engine reads cell for cell."""
+    import subprocess
+    exe = _ref_exe()
+    path = str(tmp_path / "ref.bin")
+    subprocess.run([exe, "binwrite", path, str(w), str(h), str(bs), str(dt)], check=True, timeout=60,
+                   stdout=subprocess.DEVNULL)
+    np_dt = {1: np.float32, 4: np.uint8, 10: np.int32}[dt]
+    got = M.bin_read_numpy(path)
+    assert got.dtype == np_dt and got.shape == (h, w)
+    assert np.array_equal(got, _pattern(w, h, np_dt))
+
+
+@pytest.mark.parametrize("w,h,bs,dtype", [(300, 200, (128, 128), np.float32), (257, 130, (64, 32), np.uint8),
+                                          (100, 100, (100, 100), np.int32)])
+def test_bin_files_written_here_read_by_the_reference(M, tmp_path, w, h, bs, dtype):
+    """Files this engine writes are read back by the reference's own reader
+    (File<binary>::readBlock) with the same header and cells."""
+    import subprocess
+    exe = _ref_exe()
+    a = (np.random.default_rng(3).random((h, w)) * 200).astype(dtype)
+    path, dense = str(tmp_path / "ours.bin"), str(tmp_path / "dense")
+    M.bin_write_numpy(path, a, bs=bs)
+    subprocess.run([exe, "binread", path, dense], check=True, timeout=60, stdout=subprocess.DEVNULL)
+    raw = open(dense, "rb").read()
+    head, body = raw.split(b"\n", 1)
+    dt, W, H, mo, b0, b1 = map(int, head.split())
+    assert (W, H, b0, b1) == (w, h) + tuple(bs)
+    assert mo == M.ROW + M.BLK and dt == M._dt_of_np[np.dtype(dtype).name]
+    assert np.array_equal(np.frombuffer(body, dtype=dtype).reshape(h, w), a)
