@@ -388,6 +388,7 @@ def bench_life(M, W, synth, torch, dev, size=4096, gens=100, steps=5, warmup=3, 
     grid = synth.bernoulli_u8(size, size, 0.3, seed=2024)
     g_t = torch.from_numpy(grid).to(dev)
     out = torch.empty_like(g_t)
+    torch.cuda.synchronize()   # the engine's stream does not wait for torch's
     M.set_border(M.BORDER_DEAD)
     try:
         src = M.from_device(g_t.data_ptr(), size, [size, size], M.U8, [block, block])
@@ -529,6 +530,7 @@ def bench_parity(M, W, torch, dem_t, out_t, block, win=2048):
     try:
         M.set_algebraic_rewrite(not prev)
         wt = torch.from_numpy(dem_win).to(dem_t.device)
+        torch.cuda.synchronize()
         d = M.from_device(wt.data_ptr(), win * 4, [win, win], M.F32, [block, block])
         other = M.to_numpy(W.hillshade(d))[1:-1, 1:-1]
         res["gpu_rewrite_off" if prev else "gpu_rewrite_on"] = stats(other)
@@ -547,6 +549,7 @@ def bench_plain(M, W, synth, torch, dev, block=256, steps=10, warmup=3):
     for S, k in ((1024, steps * 5), (16384, 3)):
         dem_t = synth.fbm_dem(S, S, seed=77, xp=torch, device=dev).contiguous()
         o_t = torch.empty_like(dem_t)
+        torch.cuda.synchronize()   # the engine's stream does not wait for torch's
         dem = M.from_device(dem_t.data_ptr(), S * 4, [S, S], M.F32, [block, block])
         hs = W.hillshade(dem)
         r = {}
@@ -591,6 +594,7 @@ def bench_wsum(M, W, torch, dev, size=16384, steps=10, warmup=3):
     g.manual_seed(17)
     lay = [torch.rand((size, size), generator=g, device=dev) for _ in range(6)]
     o_t = torch.empty((size, size), dtype=torch.float32, device=dev)
+    torch.cuda.synchronize()   # the engine's stream does not wait for torch's
     ln = [M.from_device(l.data_ptr(), size * 4, [size, size], M.F32, [256, 256]) for l in lay]
     prog = W.wsum(ln, weights)
     st = torch.cuda.ExternalStream(M.stream(), device=dev)

@@ -160,7 +160,11 @@ ma_Node *ma_radialScanRadius(ma_Node *node, int type, ma_Array coord, double rad
  * otherwise it keeps the pointer, which must stay valid while the node is used
  * (pinned memory from ma_hostAlloc makes the upload asynchronous). */
 ma_Node *ma_fromHost(const void *data, ma_Array ds, int dt, ma_Array bs, int copy);
-/* Device-resident raster input (pitch in bytes); the memory is not copied. */
+/* Device-resident raster input (pitch in bytes); the memory is not copied.
+ * The library works on its own CUDA stream (ma_stream), which does not wait for
+ * other streams: work that writes the memory (or an output buffer it is given)
+ * must be complete, or ordered before ma_stream() by an event, when the
+ * evaluation is enqueued. */
 ma_Node *ma_fromDevice(void *dptr, long long pitch, ma_Array ds, int dt, ma_Array bs);
 
 /* Row bands (splitting one raster over several devices or processes; no

@@ -125,6 +125,9 @@ def run_rows(M, split, build, inputs, out, bs=None):
     (rows [y0, y1)); bs: the raster's block size (the reference's block-mirror
     border rule depends on it). The band inputs must hold the program's halo,
     that is split.margin >= M.row_margin(program)."""
+    import torch
+    if out.is_cuda:
+        torch.cuda.current_stream(out.device).synchronize()   # the engine's stream does not wait for torch's
     nodes = []
     for t, dt in inputs:
         pitch = t.stride(0) * t.element_size()

@@ -42,6 +42,7 @@ def test_unaligned_device_pitch_takes_the_scalar_path(M):
     rng = np.random.default_rng(9)
     h, w = 96, 128
     base = torch.from_numpy(rng.standard_normal((h, w + 1)).astype(np.float32)).cuda()   # pitch 516 bytes
+    torch.cuda.synchronize()   # the engine's stream does not wait for torch's
     a = M.from_device(base.data_ptr(), (w + 1) * 4, [w, h], M.F32)
     got = M.to_numpy(a * 3.0 + 1.0)
     ref = base[:, :w].cpu().numpy() * np.float32(3.0) + np.float32(1.0)

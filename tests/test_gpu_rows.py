@@ -35,6 +35,7 @@ def band_eval(M, arrays, dts, build, y0, y1):
     wpo = (Wd * es_out + 127) // 128 * 128 // es_out
     out = torch.zeros((y1 - y0, wpo), dtype=torch.from_numpy(np.zeros(1, M._np_dtype[prog.datatype()])).dtype,
                       device="cuda")
+    torch.cuda.synchronize()   # the engine's stream does not wait for torch's
     M.eval_rows([prog], [(out.data_ptr(), out.stride(0) * es_out)], y0, y1)
     return out[:, :Wd].cpu().numpy()
 
@@ -85,6 +86,7 @@ def test_row_band_errors(fresh):
     band = M.from_device_rows(t.data_ptr(), 128 * 4, [128, 200], M.F32, 40, 50)
     hs = W.hillshade(band)
     out = torch.zeros((10, 128), device="cuda")
+    torch.cuda.synchronize()
     with pytest.raises(M.MapError):     # rows [59, 71) read, but [40, 90) held: fine; rows [30, 40) are not
         M.eval_rows([hs], [(out.data_ptr(), 512)], 30, 40)
     M.eval_rows([hs], [(out.data_ptr(), 512)], 60, 70)
