@@ -128,8 +128,12 @@ int ma_getPairedCells(void);
  * script's wrap constants (its PI = 3.141593) folded into S and C, so the
  * kernel evaluates no transcendental function per cell. Results stay within
  * the hillshade tolerance of the literal chain; cells where x^2 + y^2 is not
- * finite take the literal chain. on = 0 generates the literal chain
- * everywhere. Engine option with no counterpart in the reference. */
+ * finite take the literal chain. When the derivatives are correlations of
+ * one input with weights 0 or +-2^k scaled by a power of two (hill.py's
+ * Sobel / 8), they are also computed without their zero-weight terms and
+ * folded into the constants (bit-identical on finite cells; on = 2 turns this
+ * part off). on = 0 generates the literal chain everywhere. Engine option
+ * with no counterpart in the reference. */
 /* Prediction (runtime/visitor/Predictor.cpp:22-200, runtime/Worker.cpp:83-91):
  * a Local / Focal group whose every output holds one value known on the host
  * (constants, element-wise operators of them, focal operators of them under a

@@ -367,7 +367,7 @@ int ma_getPrediction(void) { return Runtime::get().prediction; }
 int ma_lastPredictedCount(void) { return Executor::get().last.predicted; }
 
 void ma_setAlgebraicRewrite(int on) {
-  void_call([&] { Runtime::get().algebraic_rewrite = on ? 1 : 0; });
+  void_call([&] { Runtime::get().algebraic_rewrite = on < 0 ? 0 : on > 2 ? 2 : on; });
 }
 int ma_getAlgebraicRewrite(void) { return Runtime::get().algebraic_rewrite; }
 void ma_setDefaultBlockSize(ma_Array bs) {

@@ -115,6 +115,18 @@ struct Gen {
   std::vector<ShadeMatch> shades;
   std::map<Node *, int> shade_at;    // rewritten node -> index in `shades`
   std::set<Node *> replaced;         // nodes only the rewritten values needed: not emitted
+  // Fast form of a composition whose derivatives are private, exactly weighted
+  // correlations of one staged input: x = s * xc, y = s * yc (s a power of two),
+  // every mask weight 0 or +-2^k (exact products), same mask extent.
+  struct ShadeFast {
+    bool on = false;
+    Node *xc = nullptr, *yc = nullptr, *in = nullptr;
+    double s = 1;
+    bool arith = false;                                   // exact arithmetic choice of S / C
+    float szks = 0, kks = 0, S0 = 0, dS = 0, nC0 = 0, dnC = 0, SH = 0, dSx = 0;
+    float S1 = 0, S3 = 0, nC1 = 0;                        // for the selecting form
+  };
+  std::vector<ShadeFast> fast;
 
   Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
 
@@ -500,6 +512,81 @@ struct Gen {
           replaced.erase(kv.second);
         }
     }
+    fast.assign(shades.size(), ShadeFast());
+    if (g.skeleton == SK_FOCAL && Runtime::get().algebraic_rewrite == 1)
+      for (size_t i = 0; i < shades.size(); i++) find_fast((int)i, outs);
+  }
+
+  // x (or y) = scale * conv: DIV by / MUL with a literal power of two
+  bool scaled_conv(Node *x, Node *&c, double &s) const {
+    if (x->kind != K_BINARY || x->meta.dtype != F32) return false;
+    double rc = 0;
+    if (x->op == DIV && pow2_reciprocal(x->prev[1], rc)) { c = x->prev[0]; s = rc; }
+    else if (x->op == MUL && literal.count(x->prev[1]) && pow2_reciprocal(x->prev[1], rc)) { c = x->prev[0]; s = 1.0 / rc; }
+    else if (x->op == MUL && literal.count(x->prev[0]) && pow2_reciprocal(x->prev[0], rc)) { c = x->prev[1]; s = 1.0 / rc; }
+    else return false;
+    if (c->kind != K_CONVOLUTION || c->meta.dtype != F32 || c->prev[0]->meta.dtype != F32) return false;
+    if (!rin.count(c->prev[0]) || !staged.count(c->prev[0])) return false;
+    for (const Variant &w : c->mask) {
+      const double v = var_as_f64(w);
+      if (v == 0.0) continue;
+      int e = 0;
+      const double mnt = std::frexp(std::fabs(v), &e);
+      if (mnt != 0.5 || e < -20 || e > 20) return false;   // +-2^k: every product is exact
+    }
+    return true;
+  }
+  // a node computed only for the rewritten values (every consumer in the group replaced)
+  bool private_to_rewrite(Node *n, const std::set<Node *> &outs) const {
+    if (outs.count(n) || !member.count(n)) return false;
+    for (Node *c : n->next)
+      if (member.count(c) && !shade_at.count(c) && !replaced.count(c)) return false;
+    return true;
+  }
+  void find_fast(int i, const std::set<Node *> &outs) {
+    const ShadeMatch &m = shades[i];
+    ShadeFast f;
+    double sx = 0, sy = 0;
+    if (!scaled_conv(m.x, f.xc, sx) || !scaled_conv(m.y, f.yc, sy) || sx != sy) return;
+    if (f.xc->prev[0] != f.yc->prev[0] || f.xc->mask_ds.arr[0] != f.yc->mask_ds.arr[0] ||
+        f.xc->mask_ds.arr[1] != f.yc->mask_ds.arr[1] || f.xc == f.yc)
+      return;
+    if (!private_to_rewrite(m.x, outs) || !private_to_rewrite(m.y, outs)) return;
+    replaced.insert(m.x);
+    replaced.insert(m.y);
+    if (!private_to_rewrite(f.xc, outs) || !private_to_rewrite(f.yc, outs)) {
+      replaced.erase(m.x);
+      replaced.erase(m.y);
+      return;
+    }
+    replaced.insert(f.xc);
+    replaced.insert(f.yc);
+    f.in = f.xc->prev[0];
+    f.s = sx;
+    f.on = true;
+    f.szks = (float)((double)m.szk * f.s);
+    f.kks = (float)((double)m.kk * f.s * f.s);
+    f.S0 = m.S0;
+    f.S1 = m.S1;
+    f.SH = m.SH;
+    f.S3 = m.S3;
+    f.nC0 = -m.C0;
+    f.nC1 = -m.C1;
+    // the arithmetic choice needs S1 - S0, -C1 + C0 and S3 - SH exact in float32
+    auto exact = [](float a, float b, float &d) {
+      d = a - b;
+      return (double)d == (double)a - (double)b;
+    };
+    f.arith = exact(f.S1, f.S0, f.dS) && exact(f.nC1, f.nC0, f.dnC) && exact(f.S3, f.SH, f.dSx) &&
+              (double)f.szks == (double)m.szk * f.s && (double)f.kks == (double)m.kk * f.s * f.s;
+    if (!f.arith) {   // keep the general form
+      replaced.erase(f.xc);
+      replaced.erase(f.yc);
+      replaced.erase(m.x);
+      replaced.erase(m.y);
+      return;
+    }
+    fast[i] = f;
   }
 
   // Literal chain of shading composition i as a separate function: cells whose
@@ -536,9 +623,79 @@ struct Gen {
     return fl(m.cz) + ", " + fl(m.szk) + ", " + fl(m.kk) + ", " + fl(m.S0) + ", " + fl(m.C0) + ", " + fl(m.S1) + ", " +
            fl(m.C1) + ", " + fl(m.SH) + ", " + fl(m.S3);
   }
+  // tap of focal input `in` at offset (dx, dy) of the cell (x, y + dr), as a scalar
+  std::string tap_row(Node *in, int dx, int dy, int dr) const {
+    const int k = staged.at(in);
+    const std::string yo = dr ? " + " + std::to_string(dr) : "";
+    return "f" + std::to_string(k) + ".tap(x, y" + yo + ", lx, ly" + yo + ", " + std::to_string(dx) + ", " +
+           std::to_string(dy) + ")";
+  }
+  // Fast statement of composition i (see ShadeFast / map_shade_fast): the two
+  // correlations as fused multiply-adds over their non-zero weights (exact
+  // products, so each term rounds like the literal add of the product), zero
+  // weights dropped; cells where a tap that neither reads, or x^2 + y^2, is not
+  // finite recompute the literal derivatives (the dropped terms added back as
+  // fma(tap, 0, acc)) and take the literal chain.
+  std::string shade_fast_stmt(Node *n, bool pair) const {
+    const int i = shade_at.at(n);
+    const ShadeFast &f = fast[i];
+    const std::string v = "v" + std::to_string(member.at(n)), si = std::to_string(i);
+    const std::string T = pair ? "PR<float>" : "float", fma = pair ? "pr_fmaf(" : "__fmaf_rn(";
+    const int hx = f.xc->halo_x(), hy = f.xc->halo_y(), mw = f.xc->mask_ds.arr[0];
+    auto tapv = [&](int dx, int dy) { return pair ? tap2(f.in, dx, dy) : tap(f.in, dx, dy); };
+    std::ostringstream s;
+    for (int c = 0; c < 2; c++) {
+      Node *cv = c ? f.yc : f.xc;
+      const std::string acc = v + (c ? "_yc" : "_xc");
+      s << T << " " << acc << " = " << T << "(0.0f);";
+      for (int i1 = -hy; i1 <= hy; i1++)
+        for (int i0 = -hx; i0 <= hx; i0++) {
+          const double w = var_as_f64(cv->mask[(i1 + hy) * mw + (i0 + hx)]);
+          if (w == 0.0) continue;
+          s << " " << acc << " = " << fma << tapv(i0, i1) << ", " << fl((float)w) << ", " << acc << ");";
+        }
+    }
+    s << " " << T << " " << v << "_z = " << T << "(0.0f);";
+    for (int i1 = -hy; i1 <= hy; i1++)
+      for (int i0 = -hx; i0 <= hx; i0++) {
+        const int k = (i1 + hy) * mw + (i0 + hx);
+        if (var_as_f64(f.xc->mask[k]) == 0.0 && var_as_f64(f.yc->mask[k]) == 0.0)
+          s << " " << v << "_z = " << fma << tapv(i0, i1) << ", 0.0f, " << v << "_z);";
+      }
+    s << " " << T << " " << v << "_q; " << T << " " << v << " = map_shade_fast(" << v << "_xc, " << v << "_yc, " << v
+      << "_z, " << fl(shades[i].cz) << ", " << fl(f.szks) << ", " << fl(f.kks) << ", " << fl(f.S0) << ", " << fl(f.dS)
+      << ", " << fl(f.nC0) << ", " << fl(f.dnC) << ", " << fl(f.SH) << ", " << fl(f.dSx) << ", " << v << "_q);";
+    // literal derivatives and chain of one lane (dr: row offset of the lane)
+    auto slow_lane = [&](const std::string &lane, int dr) {
+      std::ostringstream t;
+      const std::string sel = lane.empty() ? "" : "." + lane;
+      for (int c = 0; c < 2; c++) {
+        Node *cv = c ? f.yc : f.xc;
+        const std::string acc = v + (c ? "_yl" : "_xl");
+        t << " float " << acc << " = " << v << (c ? "_yc" : "_xc") << sel << ";";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++)
+            if (var_as_f64(cv->mask[(i1 + hy) * mw + (i0 + hx)]) == 0.0)
+              t << " " << acc << " = __fmaf_rn(" << tap_row(f.in, i0, i1, dr) << ", 0.0f, " << acc << ");";
+      }
+      t << " " << v << sel << " = shade_slow" << si << "(" << (shade_reads_args(i) ? "a, " : "") << "__fmul_rn(" << v
+        << "_xl, " << fl((float)f.s) << "), __fmul_rn(" << v << "_yl, " << fl((float)f.s) << "));";
+      return t.str();
+    };
+    if (!pair) {
+      s << " if (!(" << v << "_q < MAP_INF_F)) {" << slow_lane("", 0) << " }";
+    } else {
+      s << " if (!(" << v << "_q.a < MAP_INF_F) || !(" << v << "_q.b < MAP_INF_F)) {";
+      s << " if (!(" << v << "_q.a < MAP_INF_F)) {" << slow_lane("a", 0) << " }";
+      s << " if (!(" << v << "_q.b < MAP_INF_F)) {" << slow_lane("b", 1) << " } }";
+    }
+    return s.str();
+  }
+
   // statement of a rewritten node (scalar or pair form)
   std::string shade_stmt(Node *n, bool pair) const {
     const int i = shade_at.at(n);
+    if (fast[i].on) return shade_fast_stmt(n, pair);
     const ShadeMatch &m = shades[i];
     const std::string v = "v" + std::to_string(member.at(n)), q = v + "_q", si = std::to_string(i);
     const std::string tmpl = m.k_one ? "<true>" : "<false>";

@@ -103,7 +103,8 @@ struct Runtime {
   // f32x2 instructions (bit-identical to one cell at a time); 0 turns it off.
   int paired_cells = 1;
   // Hillshade compositions (python/hill.py:41-49) are generated through the
-  // shading identity of rewrite.hpp; 0 keeps the literal operator chain.
+  // shading identity of rewrite.hpp; 0 keeps the literal operator chain; 2 uses
+  // the identity without its fast form (derivatives computed as written).
   int algebraic_rewrite = 1;
   // Local / Focal groups whose every output is one known value are filled, not
   // launched (the reference's Predictor, runtime/visitor/Predictor.cpp); 0 turns it off.

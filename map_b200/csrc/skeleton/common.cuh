@@ -515,6 +515,40 @@ __device__ __forceinline__ PR<float> map_shade(const PR<float> &x, const PR<floa
   return pr_of(__fmul2_rn(__ffma2_rn(f2_of(szk), num, f2_of(cz)), pr_f2(map_rsqrt(pr_of(v)))));
 }
 
+// The same identity on unscaled derivatives: x = s xc, y = s yc for a power of
+// two s folded into the constants (szks = sz k s, kks = k^2 s^2), y never -0
+// (the derivatives are sums that start from +0), and the light direction chosen
+// arithmetically: with negf = (yc < 0), S = S0 + negf (S1 - S0) and -C = -C0 +
+// negf (C0 - C1) for xc != 0, S = SH + negf (S3 - SH) for xc == 0, where the
+// differences are exact in float32 (the host checks this before choosing this
+// form), so S and -C are exactly S0 / S1 / SH / S3 and -C0 / -C1. z is +-0, or
+// NaN when a cell the derivatives do not read (weight 0 in both) is not finite;
+// q = xc^2 + yc^2 + z, and the caller takes the literal chain where q is not
+// finite. Every operation rounds once; the pair form performs the same
+// operations lane by lane.
+__device__ __forceinline__ float map_shade_fast(float xc, float yc, float z, float cz, float szks, float kks, float S0,
+                                                float dS, float nC0, float dnC, float SH, float dSx, float &q) {
+  q = __fadd_rn(__fmaf_rn(xc, xc, __fmul_rn(yc, yc)), z);
+  const float negf = yc < 0.0f ? 1.0f : 0.0f;
+  const float Sn = __fmaf_rn(negf, dS, S0), nC = __fmaf_rn(negf, dnC, nC0), Sx = __fmaf_rn(negf, dSx, SH);
+  const float S = xc != 0.0f ? Sn : Sx;
+  const float num = __fmaf_rn(yc, S, __fmul_rn(xc, nC));
+  return __fmul_rn(__fmaf_rn(szks, num, cz), map_rsqrt(__fmaf_rn(kks, q, 1.0f)));
+}
+__device__ __forceinline__ PR<float> map_shade_fast(const PR<float> &xc, const PR<float> &yc, const PR<float> &z, float cz,
+                                                    float szks, float kks, float S0, float dS, float nC0, float dnC,
+                                                    float SH, float dSx, PR<float> &q) {
+  const float2 X = pr_f2(xc), Y = pr_f2(yc);
+  q = pr_of(__fadd2_rn(__ffma2_rn(X, X, __fmul2_rn(Y, Y)), pr_f2(z)));
+  const float2 negf = make_float2(yc.a < 0.0f ? 1.0f : 0.0f, yc.b < 0.0f ? 1.0f : 0.0f);
+  const float2 Sn = __ffma2_rn(negf, f2_of(dS), f2_of(S0)), nC = __ffma2_rn(negf, f2_of(dnC), f2_of(nC0));
+  const float2 Sx = __ffma2_rn(negf, f2_of(dSx), f2_of(SH));
+  const float2 S = make_float2(xc.a != 0.0f ? Sn.x : Sx.x, xc.b != 0.0f ? Sn.y : Sx.y);
+  const float2 num = __ffma2_rn(Y, S, __fmul2_rn(X, nC));
+  const PR<float> r = map_rsqrt(pr_of(__ffma2_rn(f2_of(kks), pr_f2(q), f2_of(1.0f))));
+  return pr_of(__fmul2_rn(__ffma2_rn(f2_of(szks), num, f2_of(cz)), pr_f2(r)));
+}
+
 // ------------------------------------------------------------------ border rule
 
 // Reflection used by the reference's focal loads: invert(i,d) = i<0 ? -i-1 : i>=d ? d-(i-d+1) : i

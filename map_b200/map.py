@@ -804,12 +804,12 @@ def last_predicted_count():
 def set_algebraic_rewrite(on):
     """Hillshade compositions through the shading identity (no per-cell
     transcendental functions, results within the hillshade tolerance); False
-    generates the literal operator chain."""
-    _lib.ma_setAlgebraicRewrite(1 if on else 0)
+    generates the literal operator chain; 2 the identity without its fast form."""
+    _lib.ma_setAlgebraicRewrite(on if isinstance(on, int) and not isinstance(on, bool) else (1 if on else 0))
 
 
 def get_algebraic_rewrite():
-    return bool(_lib.ma_getAlgebraicRewrite())
+    return _lib.ma_getAlgebraicRewrite()
 
 
 def last_band_count():

@@ -241,3 +241,24 @@ def test_focal_percent_matches_oracle(fresh, typ, dtype, border):
         ref = O.focal_percent(a_np, hx, hy, typ, (64, 64), border)
         assert got.dtype == ref.dtype
         assert np.array_equal(got, ref), (mask, int((got != ref).sum()))
+
+
+@pytest.mark.parametrize("shape,bs,border", [((1024, 1024), (256, 256), 0), ((300, 500), (128, 128), 1),
+                                              ((190, 333), (64, 64), 2), ((257, 129), (64, 64), 0)])
+def test_hillshade_fast_form_equals_general_form(fresh, shape, bs, border):
+    """The fast form of the rewrite (Sobel sums without zero weights, 1/8 and the
+    light direction folded into constants) is bit-identical to the general
+    rewritten form, including flat cells, NaN and infinite DEM cells."""
+    M = fresh
+    M.set_border(border)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=17)
+    dem_np[::29, ::31] = 100.0
+    dem_np[5::97, 3::89] = np.nan
+    dem_np[7::113, 11::101] = np.inf
+    out = {}
+    for mode in (1, 2):
+        M.set_algebraic_rewrite(mode)
+        r = W.hillshade(M.from_numpy(dem_np, bs=list(bs)))
+        assert ("map_shade_fast" in M.generated_source(r)) == (mode == 1)
+        out[mode] = M.to_numpy(r)
+    assert np.array_equal(out[1].view(np.uint32), out[2].view(np.uint32))

@@ -28,11 +28,15 @@ def test_hill_script_is_rewritten(R):
     M = R
     hs = W.hillshade(dem(M))
     src = M.generated_source(hs)
-    assert "map_shade<true>" in src and "shade_slow0" in src
+    # hill.py's derivatives (Sobel / 8) take the fast form
+    assert "map_shade_fast(" in src and "shade_slow0" in src
     # the group body computes no transcendental function outside the fallback
     body = src[src.index("focal_cell("):]
     assert "map_atan2f" not in body and "atanf" not in body and "map_sincosf" not in body
     assert M.compile_only(hs) == 1
+    M.set_algebraic_rewrite(2)
+    src = M.generated_source(W.hillshade(dem(M)))
+    assert "map_shade<true>" in src and "map_shade_fast" not in src
     M.set_algebraic_rewrite(False)
     hs = W.hillshade(dem(M))
     src = M.generated_source(hs)
@@ -50,8 +54,10 @@ def test_operand_orders_and_zfactor(R):
     asp = z0 + z1
     hs = M.sin(s) * (M.cos(asp - 2.1) * 0.6) + M.cos(s) * 0.8
     src = M.generated_source(hs)
-    assert "map_shade<false>" in src
+    assert "map_shade_fast(" in src
     assert M.compile_only(hs) == 1
+    M.set_algebraic_rewrite(2)
+    assert "map_shade<false>" in M.generated_source(hs)
 
 
 PI2, PIH, PI32 = 3.141593 * 2, 3.141593 / 2, 3.141593 * 2 - 3.141593 / 2
@@ -93,7 +99,7 @@ def test_two_azimuths_share_one_group(R):
     d = dem(M)
     a, b = W.hillshade(d, 45, 315), W.hillshade(d, 30, 200)
     src = M.generated_source(a, b)
-    assert src.count("= map_shade<true>") >= 2 and "shade_slow1" in src
+    assert src.count("= map_shade_fast(") >= 2 and "shade_slow1" in src
     body = src[src.index("focal_cell("):]
     assert "map_sincosf" not in body
     assert M.compile_only(a, b) >= 1
@@ -154,3 +160,44 @@ def test_rewrite_replay_within_tolerance(n, seed, scale, border):
     assert only.mean() < 0.01
     # no further from FP64 than the FP32 chain (both carry the same float Sobel sums)
     assert np.abs(hs - ref64).max() <= np.abs(ref32 - ref64).max() + 4 * float(np.spacing(f32(1)))
+
+
+def test_fast_form_equals_general_form_replay():
+    """map_shade_fast on the unscaled Sobel sums (zero weights dropped, products
+    by +-1 / +-2 as fused multiply-adds, 1/8 and the light direction folded into
+    the constants) replayed in float32 equals map_shade on the derivatives /8,
+    bit for bit, on every cell."""
+    k = shade_constants()
+    d = synth.fbm_dem(300, 400, seed=12)
+    d[::37, ::41] = 0.0                     # flat spots: x == 0 / y == 0 cells
+    H = np.array([[-1, 0, 1], [-2, 0, 2], [-1, 0, 1]], f32)
+    V = np.array([[-1, -2, -1], [0, 0, 0], [1, 2, 1]], f32)
+    xl = O.conv_f32(d, H, (128, 128), 0)
+    yl = O.conv_f32(d, V, (128, 128), 0)
+    # the fast sums: fma(tap, w, acc) over non-zero weights, from +0
+    p = np.pad(d, 1, mode="symmetric")      # interior cells only are compared below
+    def fast_sum(m):
+        acc = np.zeros(d.shape, f32)
+        for i1 in range(3):
+            for i0 in range(3):
+                if m[i1, i0] != 0:
+                    acc = fma32(p[i1:i1 + d.shape[0], i0:i0 + d.shape[1]], m[i1, i0], acc)
+        return acc
+    xc, yc = fast_sum(H), fast_sum(V)
+    inner = (slice(1, -1), slice(1, -1))
+    assert np.array_equal(xc[inner].view(np.uint32), xl[inner].view(np.uint32))
+    assert np.array_equal(yc[inner].view(np.uint32), yl[inner].view(np.uint32))
+    general = replay_shade((xl * f32(0.125)).astype(f32), (yl * f32(0.125)).astype(f32), k)
+    # fast: q = fma(xc, xc, yc*yc) + 0; choice by arithmetic; constants scaled
+    q = fma32(xc, xc, (yc * yc).astype(f32))
+    negf = (yc < 0).astype(f32)
+    dS, dnC, dSx = f32(k["S1"] - k["S0"]), f32(-k["C1"] + k["C0"]), f32(k["S3"] - k["SH"])
+    Sn = fma32(negf, dS, k["S0"])
+    nC = fma32(negf, dnC, -k["C0"])
+    Sx = fma32(negf, dSx, k["SH"])
+    S = np.where(xc != 0, Sn, Sx).astype(f32)
+    num = fma32(yc, S, (xc * nC).astype(f32))
+    v = fma32(f32(2.0 ** -6), q, f32(1))
+    r = (1.0 / np.sqrt(v.astype(np.float64))).astype(f32)
+    fast = (fma32(f32(k["sz"] / 8), num, k["cz"]) * r).astype(f32)
+    assert np.array_equal(fast[inner].view(np.uint32), general[inner].view(np.uint32))
