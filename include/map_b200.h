@@ -227,7 +227,10 @@ int ma_memcpy(void *dst, const void *src, size_t bytes, int kind); /* kind as cu
  * buffers (16-byte aligned base and pitch).
  * ma_batchAdd returns the instance index; ma_batchPrepare fuses, autotunes tile
  * shapes (autotune != 0), compiles and captures the graph (called by the first
- * ma_batchRun when omitted); ma_batchInfo writes a JSON description. */
+ * ma_batchRun when omitted); ma_batchInfo writes a JSON description.
+ * ma_batchRun with sync != 0 returns non-zero when any tile reported a device
+ * error (a staging wait that timed out): every output of that run is then void,
+ * not only the failing tile's. */
 typedef struct ma_Batch ma_Batch;
 ma_Batch *ma_batchCreate(void);
 int ma_batchAdd(ma_Batch *b, ma_Node **outs, int num, void **dst, const long long *pitch);
@@ -291,9 +294,12 @@ int ma_zoneStats(const void *value, long long value_pitch, const void *zone, lon
  * where an allocation may synchronise the device or grow the memory pool.
  * The working bins are one fixed array per device in the library's own device
  * memory, so nzones may be at most 16384; larger counts return an error. Runs
- * on the calling thread's current device. The first call on a device does the
- * set-up (looks up the array, loads the kernels): make it before any stream
- * capture begins. All calls on a device share the array: calls whose work can
+ * on the calling thread's current device, checked like every other entry
+ * point. The first call on a device does the set-up (loads the kernels): make
+ * it before any stream capture begins. The array's address is looked up in the
+ * current context on every call, so a device or context reset between calls is
+ * safe, but the first call after a reset loads the kernels again (which may
+ * allocate once). All calls on a device share the array: calls whose work can
  * overlap on the device (several streams or host threads) race and corrupt each
  * other's results, so order them on one stream. Same arguments, rules and
  * results as ma_zoneStats. */

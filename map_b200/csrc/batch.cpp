@@ -508,7 +508,15 @@ void Batch::run(bool sync) {
   CudaEnv &env = CudaEnv::get();
   cuda_check(cudaGraphLaunch(impl_->exec, (cudaStream_t)env.stream()), "cudaGraphLaunch");
   env.count_launch();
-  if (sync) Executor::get().sync();
+  if (!sync) return;
+  try {
+    Executor::get().sync();
+  } catch (const MapError &e) {
+    // A CTA that gave up on its staging wait left its tile's copy in flight; the
+    // copy can land in shared memory that another CTA reuses, so no output of
+    // this run can be trusted, not only the tile that failed.
+    throw MapError(std::string(e.what()) + " every output of this batch run is void");
+  }
 }
 
 std::string Batch::info() const {

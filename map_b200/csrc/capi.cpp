@@ -797,6 +797,7 @@ int ma_zoneStatsNoAlloc(const void *value, long long value_pitch, const void *zo
                         int H, int nzones, unsigned long long *count, float *vmin, float *vmax, float *sum,
                         float *mean, void *stream) {
   return int_call([&] {
+    CudaEnv::get().ensure_device();
     ZoneStatsArgs a;
     a.value = value;
     a.value_pitch = value_pitch;

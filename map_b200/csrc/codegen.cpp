@@ -715,6 +715,273 @@ struct Gen {
     return s.str();
   }
 
+  // ---- packed byte cells (Q4 in skeleton/common.cuh): four cells of a row per step
+
+  // Value range of a node of the packed form; `wrap`: its type reduces the
+  // computed value mod 256 (the lanes are masked after the operation).
+  struct QRange {
+    long long lo = 0, hi = 0;
+    bool wrap = false;
+  };
+  std::map<Node *, QRange> qr;
+
+  // Conversion to type dt of a value in r (0 <= lo, hi <= 0xFFFF); false when the
+  // converted value could leave [0, 0x7FFF] or the type is not an integer.
+  static bool q_type(int dt, QRange &r) {
+    r.wrap = false;
+    switch (dt) {
+      case U8:
+        if (r.hi > 255) { r.lo = 0; r.hi = 255; r.wrap = true; }
+        return true;
+      case B8: return r.hi <= 1;
+      case S8: return r.hi <= 127;
+      case U16: case S16: case U32: case S32: case U64: case S64: return r.hi <= 0x7FFF;
+      default: return false;
+    }
+  }
+  bool q_literal(Node *p, long long &c) const {
+    double v = 0;
+    if (literal.count(p)) v = var_as_f64(p->cnst);
+    else if (member.count(p) && p->kind == K_CONSTANT) v = var_as_f64(reference_literal_value(p->cnst));
+    else return false;
+    if (dt_is_float(p->meta.dtype) || !(v >= 0 && v <= 0x7FFF) || v != std::floor(v)) return false;
+    c = (long long)v;
+    return true;
+  }
+  bool q_range(Node *p, QRange &r) const {
+    long long c = 0;
+    if (q_literal(p, c)) { r.lo = r.hi = c; r.wrap = false; return true; }
+    auto it = qr.find(p);
+    if (it == qr.end()) return false;
+    r = it->second;
+    return true;
+  }
+  static bool zero_one_range(const QRange &r) { return r.lo >= 0 && r.hi <= 1; }
+
+  // Whether every node of the group has a packed form whose lanes provably stay
+  // in range: integer arithmetic on byte rasters staged in shared memory
+  // (correlations with non-negative integer weights, sums, differences that stay
+  // non-negative, products, relations, logical and bitwise operations, selects,
+  // minimum and maximum), every value in [0, 0x7FFF] after its type's conversion,
+  // every output an 8-bit cell. Fills qr.
+  bool quadable() {
+    qr.clear();
+    if (!shades.empty() || outk.empty()) return false;
+    for (Node *in : g.inputs) {
+      long long c = 0;
+      if (sca.count(in)) return false;
+      if (literal.count(in)) {
+        if (!q_literal(in, c)) return false;
+        continue;
+      }
+      if (rin.count(in)) {
+        if (in->meta.dtype != U8) return false;
+        qr[in] = QRange{0, 255, false};
+      }
+    }
+    for (auto &kv : outk)
+      if (kv.first->meta.dtype != U8 && kv.first->meta.dtype != B8) return false;
+    for (Node *n : g.nodes) {
+      if (replaced.count(n)) return false;
+      QRange r, a, b;
+      switch (n->kind) {
+        case K_CONSTANT: {
+          long long c = 0;
+          if (!q_literal(n, c)) return false;
+          r.lo = r.hi = c;
+          break;
+        }
+        case K_CAST: case K_BARRIER:
+          if (!q_range(n->prev[0], r)) return false;
+          break;
+        case K_NEIGHBOR:
+          if (n->prev[0]->meta.dtype != U8 || !staged.count(n->prev[0])) return false;
+          r = QRange{0, 255, false};
+          break;
+        case K_CONVOLUTION: {
+          if (n->prev[0]->meta.dtype != U8 || !staged.count(n->prev[0]) || dt_is_float(n->meta.dtype)) return false;
+          for (const Variant &w : n->mask) {
+            const double v = var_as_f64(w);
+            if (!(v >= 0 && v <= 0xFFFF) || v != std::floor(v)) return false;
+            r.hi += (long long)v * 255;
+          }
+          if (r.hi > 0xFFFF) return false;
+          break;
+        }
+        case K_UNARY:
+          if (n->op == POS) {
+            if (!q_range(n->prev[0], r)) return false;
+          } else if (n->op == NOT) {
+            if (!q_range(n->prev[0], a)) return false;
+            r = QRange{0, 1, false};
+          } else {
+            return false;
+          }
+          break;
+        case K_BINARY: {
+          if (!q_range(n->prev[0], a) || !q_range(n->prev[1], b)) return false;
+          switch (n->op) {
+            case ADD: r.lo = a.lo + b.lo; r.hi = a.hi + b.hi; break;
+            case SUB: r.lo = a.lo - b.hi; r.hi = a.hi - b.lo; if (r.lo < 0) return false; break;
+            case MUL:
+              r.lo = a.lo * b.lo;
+              r.hi = a.hi * b.hi;
+              break;
+            case EQ: case NE: case LT: case GT: case LE: case GE: case AND: case OR: r = QRange{0, 1, false}; break;
+            case bAND: r = QRange{0, std::min(a.hi, b.hi), false}; break;
+            case bOR: case bXOR: {
+              long long m = 1;
+              while (m <= std::max(a.hi, b.hi)) m <<= 1;
+              r = QRange{0, m - 1, false};
+              break;
+            }
+            case MAX2: r = QRange{std::max(a.lo, b.lo), std::max(a.hi, b.hi), false}; break;
+            case MIN2: r = QRange{std::min(a.lo, b.lo), std::min(a.hi, b.hi), false}; break;
+            default: return false;
+          }
+          if (r.hi > 0xFFFF) return false;
+          break;
+        }
+        case K_CONDITIONAL: {
+          QRange c;
+          if (!q_range(n->prev[0], c) || !q_range(n->prev[1], a) || !q_range(n->prev[2], b)) return false;
+          r = QRange{std::min(a.lo, b.lo), std::max(a.hi, b.hi), false};
+          break;
+        }
+        default:
+          return false;
+      }
+      if (!q_type(n->meta.dtype, r) || r.lo < 0 || r.hi > 0x7FFF) return false;
+      qr[n] = r;
+    }
+    return true;
+  }
+
+  std::string val4(Node *p) const {
+    long long c = 0;
+    if (q_literal(p, c) && !member.count(p)) return "q4_splat(" + std::to_string(c) + "u)";
+    auto m = member.find(p);
+    if (m != member.end()) return "v" + std::to_string(m->second);
+    auto r = rin.find(p);
+    if (r != rin.end()) return "i" + std::to_string(r->second);
+    throw MapError("codegen: packed value of a node that is not available");
+  }
+  std::string tap4(Node *in, int dx, int dy) const {
+    return "f" + std::to_string(staged.at(in)) + ".tap4(lx, ly, " + std::to_string(dx) + ", " + std::to_string(dy) + ")";
+  }
+  // a value as lanes 0 / 1 (a relation's result already is)
+  std::string bool4(Node *p) const {
+    QRange r;
+    if (q_range(p, r) && zero_one_range(r)) return val4(p);
+    return "q4_ne0(" + val4(p) + ")";
+  }
+  std::string stmt4(Node *n) const {
+    const QRange &R = qr.at(n);
+    const std::string v = "v" + std::to_string(member.at(n));
+    std::string e;
+    switch (n->kind) {
+      case K_CONSTANT: {
+        long long c = 0;
+        q_literal(n, c);
+        e = "q4_splat(" + std::to_string(c) + "u)";
+        break;
+      }
+      case K_CAST: case K_BARRIER: e = val4(n->prev[0]); break;
+      case K_NEIGHBOR: e = tap4(n->prev[0], n->coord.arr[0], n->coord.arr[1]); break;
+      case K_CONVOLUTION: {
+        int hx = n->halo_x(), hy = n->halo_y(), mw = n->mask_ds.arr[0];
+        std::ostringstream s;
+        s << "Q4 " << v << " = q4_splat(0u);";
+        for (int i1 = -hy; i1 <= hy; i1++)
+          for (int i0 = -hx; i0 <= hx; i0++) {
+            const long long w = (long long)var_as_f64(n->mask[(i1 + hy) * mw + (i0 + hx)]);
+            if (w == 0) continue;
+            const std::string t = tap4(n->prev[0], i0, i1);
+            s << "\n    " << v << " = q4_add(" << v << ", " << (w == 1 ? t : "q4_mulc(" + t + ", " + std::to_string(w) + "u)")
+              << ");";
+          }
+        if (R.wrap) s << "\n    " << v << " = q4_wrap8(" << v << ");";
+        return s.str();
+      }
+      case K_UNARY: e = n->op == NOT ? "q4_eq0(" + val4(n->prev[0]) + ")" : val4(n->prev[0]); break;
+      case K_BINARY: {
+        Node *p0 = n->prev[0], *p1 = n->prev[1];
+        const std::string l = val4(p0), r = val4(p1);
+        QRange a, b;
+        q_range(p0, a);
+        q_range(p1, b);
+        long long c = 0;
+        switch (n->op) {
+          case ADD: e = "q4_add(" + l + ", " + r + ")"; break;
+          case SUB: e = "q4_sub(" + l + ", " + r + ")"; break;
+          case MUL:
+            if (q_literal(p1, c)) e = "q4_mulc(" + l + ", " + std::to_string(c) + "u)";
+            else if (q_literal(p0, c)) e = "q4_mulc(" + r + ", " + std::to_string(c) + "u)";
+            else if (zero_one_range(a)) e = "q4_mul01(" + l + ", " + r + ")";
+            else if (zero_one_range(b)) e = "q4_mul01(" + r + ", " + l + ")";
+            else e = "q4_mul(" + l + ", " + r + ")";
+            break;
+          case EQ: e = "q4_eq(" + l + ", " + r + ")"; break;
+          case NE: e = "q4_ne(" + l + ", " + r + ")"; break;
+          case LT: e = "q4_lt(" + l + ", " + r + ")"; break;
+          case GT: e = "q4_gt(" + l + ", " + r + ")"; break;
+          case LE: e = "q4_le(" + l + ", " + r + ")"; break;
+          case GE: e = "q4_ge(" + l + ", " + r + ")"; break;
+          case AND: e = "q4_and(" + bool4(p0) + ", " + bool4(p1) + ")"; break;
+          case OR: e = "q4_or(" + bool4(p0) + ", " + bool4(p1) + ")"; break;
+          case bAND: e = "q4_and(" + l + ", " + r + ")"; break;
+          case bOR: e = "q4_or(" + l + ", " + r + ")"; break;
+          case bXOR: e = "q4_xor(" + l + ", " + r + ")"; break;
+          case MAX2: e = "q4_max(" + l + ", " + r + ")"; break;
+          case MIN2: e = "q4_min(" + l + ", " + r + ")"; break;
+          default: throw MapError("codegen: binary op without a packed form");
+        }
+        break;
+      }
+      case K_CONDITIONAL:
+        e = "q4_sel(" + bool4(n->prev[0]) + ", " + val4(n->prev[1]) + ", " + val4(n->prev[2]) + ")";
+        break;
+      default:
+        throw MapError(std::string("codegen: node kind ") + kind_name(n->kind) + " has no packed form");
+    }
+    if (R.wrap) e = "q4_wrap8(" + e + ")";
+    return "const Q4 " + v + " = " + e + ";";
+  }
+  // inputs read at the centre cell only come from global memory as one word
+  // (4-byte aligned rows, checked by quad_aligned)
+  std::string center_loads4() const {
+    std::ostringstream s;
+    for (Node *p : plan.in_rasters) {
+      if (!center_read.count(p)) continue;
+      const int k = rin.at(p);
+      if (staged.count(p)) s << "    const Q4 i" << k << " = " << tap4(p, 0, 0) << ";\n";
+      else s << "    const Q4 i" << k << " = q4_bytes(ldr_q4_u8(a.in[" << k << "], x, y));\n";
+    }
+    return s.str();
+  }
+  std::string body4() const {
+    std::ostringstream s;
+    for (Node *n : g.nodes) s << "    " << stmt4(n) << "\n";
+    return s.str();
+  }
+  std::string stores4() const {
+    std::ostringstream s;
+    for (auto &kv : outk) s << "    str_out_q4_u8(a.out[" << kv.second << "], x, y, " << val4(kv.first) << ");\n";
+    return s.str();
+  }
+  // every output row, and every row of an input read from global memory, starts
+  // on a 4-byte boundary (base and pitch)
+  std::string quad_aligned() const {
+    std::ostringstream s;
+    s << "((0";
+    for (auto &kv : outk) s << " | a.out[" << kv.second << "].p | (u64)a.out[" << kv.second << "].pitch";
+    for (Node *p : plan.in_rasters)
+      if (center_read.count(p) && !staged.count(p))
+        s << " | a.in[" << rin.at(p) << "].p | (u64)a.in[" << rin.at(p) << "].pitch";
+    s << ") & 3) == 0";
+    return s.str();
+  }
+
   // ---- per-node statements
 
   std::string stmt(Node *n, bool zonal_acc) const {
@@ -1012,7 +1279,7 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
          << "    for (int r = 0; r < " << RV << "; ++r) {\n"
          << "      const int y = t.y0 + ly0 + r * " << NT / TV << ";\n";
     int o = 0;
-    for (auto &kv : G.outk) body << "      uint4 q" << o++ << ";\n";
+    for (size_t k = 0; k < G.outk.size(); k++) body << "      uint4 q" << k << ";\n";
     body << "#pragma unroll\n"
          << "      for (int j = 0; j < " << V << "; ++j) {\n"
          << "        In in;\n";
@@ -1140,6 +1407,21 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << G.center_loads2() << G.body2() << G.stores2() << "}\n";
   }
   const FocalTune &tune = focal_tune();
+  // Integer bodies on byte rasters compute four cells of a row per thread step as
+  // 16-bit lanes (Q4) on interior tiles: one shared-memory word holds the taps of
+  // four cells and one operation serves two cells.
+  const int qw = TW / 4;
+  const bool quad = !pair && use_tma && Runtime::get().paired_cells && TW % 4 == 0 && qw <= NT && NT % qw == 0 &&
+                    (TH * qw) % NT == 0 && G.quadable();
+  const int qrows = quad ? TH * qw / NT : 0;
+  if (quad) {
+    body << "template <";
+    for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
+    body << ">\n__device__ __forceinline__ void focal_cell4(const Args &a";
+    for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
+    body << ", int x, int y, int lx, int ly) {\n";
+    body << G.center_loads4() << G.body4() << G.stores4() << "}\n";
+  }
   const bool full_unroll = tune.unroll ? tune.unroll >= rows : !heavy;
   const std::string unroll = tune.unroll ? "#pragma unroll " + std::to_string(tune.unroll) + "\n"
                                          : heavy ? (pair ? "#pragma unroll 1\n" : "#pragma unroll 2\n") : "#pragma unroll\n";
@@ -1210,6 +1492,31 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
               << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
               << "      " << (pair ? call2.str() : call.str()) << ";\n"
               << "    }\n";
+  }
+  if (quad) {
+    // thread t: cells 4 (t % qw) .. + 3 of rows (t / qw) * qrows .. + qrows - 1;
+    // outputs whose rows are not 4-byte aligned take the one-cell form
+    std::ostringstream q;
+    q << "    const int lx = 4 * (threadIdx.x % " << qw << "), ly0 = (threadIdx.x / " << qw << ") * " << qrows << ";\n"
+      << "    const int x = t.x0 + lx;\n"
+      << "    if (" << G.quad_aligned() << ") {\n"
+      << "#pragma unroll\n"
+      << "      for (int k = 0; k < " << qrows << "; k++) {\n"
+      << "        const int ly = ly0 + k, y = t.y0 + ly;\n"
+      << "        focal_cell4(a";
+    for (int k = 0; k < nst; k++) q << ", f" << k;
+    q << ", x, y, lx, ly);\n"
+      << "      }\n"
+      << "    } else {\n"
+      << "      for (int k = 0; k < " << qrows << "; k++)\n"
+      << "        for (int c = 0; c < 4; c++) {\n"
+      << "          const int ly = ly0 + k, y = t.y0 + ly;\n"
+      << "          focal_cell(a";
+    for (int k = 0; k < nst; k++) q << ", f" << k;
+    q << ", x + c, y, lx + c, ly);\n"
+      << "        }\n"
+      << "    }\n";
+    loop_full.str(q.str());
   }
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
@@ -1873,12 +2180,23 @@ const FocalTune &focal_tune() {
         else if (k == "lnt") r.lnt = v;
         else if (k == "ltw") r.ltw = v;
         else if (k == "lth") r.lth = v;
+        else if (k == "qnt") r.qnt = v;
+        else if (k == "qtw") r.qtw = v;
+        else if (k == "qth") r.qth = v;
       }
       i = j + 1;
     }
     return r;
   }();
   return t;
+}
+
+bool focal_quad_form(const Group &g) {
+  if (g.skeleton != SK_FOCAL || !Runtime::get().paired_cells) return false;
+  KernelPlan P;
+  Gen G(g, P);
+  G.classify();
+  return G.quadable();
 }
 
 bool tile_cfg_valid(const TileCfg &c) {

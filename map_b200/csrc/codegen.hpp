@@ -30,6 +30,9 @@ struct TileCfg {
   int tw = 64, th = 32, nt = 256;
 };
 bool tile_cfg_valid(const TileCfg &c);
+// Whether a focal group's interior tiles compute four byte cells of a row per
+// thread step (packed 16-bit lanes; integer bodies on byte rasters).
+bool focal_quad_form(const Group &g);
 
 struct KernelPlan {
   int skeleton = SK_LOCAL;
@@ -67,6 +70,7 @@ struct FocalTune {
   int defer = 1;    // interior tiles keep a thread's results in registers and store them last
   int nt = 0, tw = 0, th = 0;
   int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
+  int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
 };
 const FocalTune &focal_tune();
 

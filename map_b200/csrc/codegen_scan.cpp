@@ -5,7 +5,12 @@
 // sweeps the octant's fronts d0 = 1, 2, ... in order; the cells of a front are
 // independent and are spread over the CTA's threads. A cell's scan value is
 // op(LIT(prev front at d1, prev front at d1-1), in) when `in` is finite; the
-// start cell holds the neutral value. The previous front is read back from the
+// start cell holds the neutral value. The previous and current fronts are kept in
+// the CTA's shared memory when both fit (radial_front_smem, up to 200 KiB); for
+// rasters at least kRadialClusterDim cells across, the octant runs on a cluster of
+// kRadialCluster CTAs, each holding one segment of both fronts in its shared
+// memory and reading the value left of its segment from its neighbour's
+// (distributed shared memory). Fronts too long for either are read back from the
 // scan's own output raster (written by this CTA one step earlier; cells on an
 // octant boundary are written by both adjacent octants with identical values).
 // The group's local nodes before the scan are evaluated per cell to produce
@@ -17,7 +22,7 @@
 // strictly-upstream cells. Here the same fixed point is reached without
 // iterating to convergence. In-degrees are counted by pulling from the 8
 // neighbours; then either one CTA sweeps frontier by frontier (topological
-// order; rasters up to 64 K cells) or, for larger rasters, a thread per source
+// order; rasters up to kSpreadKahnCells = 64 K cells) or, for larger rasters, a thread per source
 // walks down its flow path pushing (accumulation + water) with atomic adds and
 // continues into a cell only when its push was the cell's last pending one, so
 // each cell is completed exactly once after all its upstream cells. Integer
@@ -95,7 +100,7 @@ void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node
                      (uint64_t)(uintptr_t)((int32_t *)work + 4 * N), (uint64_t)(N + 1)};
   auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
   if (N <= kSpreadKahnCells) {
-    // one CTA, frontier by frontier: the lowest latency for rasters of a few million cells
+    // one CTA, frontier by frontier: the lowest latency up to 64 K cells
     env.launch(env.kernel(P.source, P.kname + "_kahn", 0), 1, 1024, 0, (CUstream_st *)st, a.data(), a.size());
   } else {
     const int grid = (int)std::max<size_t>(1, std::min<size_t>((N + 255) / 256, (size_t)env.sm_count() * 8));

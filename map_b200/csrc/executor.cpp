@@ -336,7 +336,14 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
     // standalone focal kernels: 128 threads on a 64 x 32 tile (16 rows per thread),
     // measured 1.5% faster than 256 threads on the hillshade and 2% on life
     TileCfg cfg;
-    if (g->skeleton == SK_FOCAL) {
+    if (g->skeleton == SK_FOCAL && focal_quad_form(*g)) {
+      // packed byte form: a warp's 32 threads cover the 128 cells of one tile row
+      // (32 consecutive shared-memory words, no bank conflict), 8 rows per thread
+      const FocalTune &ft = focal_tune();
+      cfg.tw = ft.qtw ? ft.qtw : 128;
+      cfg.th = ft.qth ? ft.qth : 32;
+      cfg.nt = ft.qnt ? ft.qnt : 128;
+    } else if (g->skeleton == SK_FOCAL) {
       cfg.nt = 128;
       const FocalTune &ft = focal_tune();
       if (ft.nt) cfg.nt = ft.nt;

@@ -619,6 +619,71 @@ template <class T> struct GatherTap {
 
 // Focal tap served from a tile staged in shared memory (interior tiles).
 // The tile's element (0,0) is raster cell (x0 - PX, y0 - HY).
+// ------------------------------------------------------------------ packed byte cells
+
+// Four consecutive cells of a row (x .. x + 3) of an integer expression whose
+// every value lies in [0, 0x7FFF], as 16-bit lanes of two words: lo holds the
+// cells x (bits 0-15) and x + 1 (bits 16-31), hi the cells x + 2 and x + 3.
+// Sums, differences and products by non-negative constants of such lanes are
+// plain 32-bit operations as long as no lane leaves [0, 0xFFFF], which the code
+// generator proves by interval arithmetic before it uses this form; results of
+// an 8-bit unsigned type are reduced mod 256 lane by lane (q4_wrap8).
+struct Q4 { u32 lo, hi; };
+__device__ __forceinline__ Q4 q4_splat(u32 c) { return Q4{c * 0x00010001u, c * 0x00010001u}; }
+// four bytes (cells x .. x + 3) as lanes
+__device__ __forceinline__ Q4 q4_bytes(u32 w) { return Q4{__byte_perm(w, 0u, 0x4140), __byte_perm(w, 0u, 0x4342)}; }
+// the four lanes (each < 256) as the bytes of one word, cell x in the low byte
+__device__ __forceinline__ u32 q4_pack_u8(Q4 v) { return __byte_perm(v.lo, v.hi, 0x6420); }
+__device__ __forceinline__ Q4 q4_add(Q4 a, Q4 b) { return Q4{a.lo + b.lo, a.hi + b.hi}; }
+__device__ __forceinline__ Q4 q4_sub(Q4 a, Q4 b) { return Q4{a.lo - b.lo, a.hi - b.hi}; }
+__device__ __forceinline__ Q4 q4_mulc(Q4 a, u32 c) { return Q4{a.lo * c, a.hi * c}; }
+__device__ __forceinline__ Q4 q4_and(Q4 a, Q4 b) { return Q4{a.lo & b.lo, a.hi & b.hi}; }
+__device__ __forceinline__ Q4 q4_or(Q4 a, Q4 b) { return Q4{a.lo | b.lo, a.hi | b.hi}; }
+__device__ __forceinline__ Q4 q4_xor(Q4 a, Q4 b) { return Q4{a.lo ^ b.lo, a.hi ^ b.hi}; }
+__device__ __forceinline__ Q4 q4_wrap8(Q4 a) { return Q4{a.lo & 0x00FF00FFu, a.hi & 0x00FF00FFu}; }
+// lane products: m has lanes 0 or 1 (a mask times a value)
+__device__ __forceinline__ u32 q4_mul01_w(u32 m, u32 b) { return (m * 0xFFFFu) & b; }
+__device__ __forceinline__ Q4 q4_mul01(Q4 m, Q4 b) { return Q4{q4_mul01_w(m.lo, b.lo), q4_mul01_w(m.hi, b.hi)}; }
+// general lane products (each product below 2^16)
+__device__ __forceinline__ u32 q4_mul_w(u32 a, u32 b) {
+  return ((a & 0xFFFFu) * (b & 0xFFFFu)) | (((a >> 16) * (b >> 16)) << 16);
+}
+__device__ __forceinline__ Q4 q4_mul(Q4 a, Q4 b) { return Q4{q4_mul_w(a.lo, b.lo), q4_mul_w(a.hi, b.hi)}; }
+// relations of lanes in [0, 0x7FFF], as lanes 0 / 1: a lane plus 0x7FFF sets its
+// bit 15 exactly when it is not zero, and 0x8000 + a - b keeps bit 15 exactly when
+// a >= b; neither carries nor borrows across lanes
+__device__ __forceinline__ u32 q4_ne0_w(u32 a) { return ((a + 0x7FFF7FFFu) & 0x80008000u) >> 15; }
+__device__ __forceinline__ u32 q4_ge_w(u32 a, u32 b) { return (((a | 0x80008000u) - b) & 0x80008000u) >> 15; }
+__device__ __forceinline__ Q4 q4_ne(Q4 a, Q4 b) { return Q4{q4_ne0_w(a.lo ^ b.lo), q4_ne0_w(a.hi ^ b.hi)}; }
+__device__ __forceinline__ Q4 q4_eq(Q4 a, Q4 b) {
+  return Q4{q4_ne0_w(a.lo ^ b.lo) ^ 0x00010001u, q4_ne0_w(a.hi ^ b.hi) ^ 0x00010001u};
+}
+__device__ __forceinline__ Q4 q4_ge(Q4 a, Q4 b) { return Q4{q4_ge_w(a.lo, b.lo), q4_ge_w(a.hi, b.hi)}; }
+__device__ __forceinline__ Q4 q4_lt(Q4 a, Q4 b) {
+  return Q4{q4_ge_w(a.lo, b.lo) ^ 0x00010001u, q4_ge_w(a.hi, b.hi) ^ 0x00010001u};
+}
+__device__ __forceinline__ Q4 q4_gt(Q4 a, Q4 b) { return q4_lt(b, a); }
+__device__ __forceinline__ Q4 q4_le(Q4 a, Q4 b) { return q4_ge(b, a); }
+__device__ __forceinline__ Q4 q4_ne0(Q4 a) { return Q4{q4_ne0_w(a.lo), q4_ne0_w(a.hi)}; }
+__device__ __forceinline__ Q4 q4_eq0(Q4 a) { return Q4{q4_ne0_w(a.lo) ^ 0x00010001u, q4_ne0_w(a.hi) ^ 0x00010001u}; }
+// lanes of t where m (lanes 0 / 1) is 1, else of f
+__device__ __forceinline__ Q4 q4_sel(Q4 m, Q4 t, Q4 f) {
+  const u32 ml = m.lo * 0xFFFFu, mh = m.hi * 0xFFFFu;
+  return Q4{(t.lo & ml) | (f.lo & ~ml), (t.hi & mh) | (f.hi & ~mh)};
+}
+__device__ __forceinline__ Q4 q4_max(Q4 a, Q4 b) { return q4_sel(q4_ge(a, b), a, b); }
+__device__ __forceinline__ Q4 q4_min(Q4 a, Q4 b) { return q4_sel(q4_ge(b, a), a, b); }
+// the four U8 cells x .. x + 3 of row y of a raster as one 32-bit load (the row
+// address plus x must be 4-byte aligned)
+__device__ __forceinline__ u32 ldr_q4_u8(const RasterArg &r, int x, int y) {
+  return __ldg((const u32 *)(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x));
+}
+// the four U8 result cells x .. x + 3 of row y as one 32-bit store (the row
+// address plus x must be 4-byte aligned)
+__device__ __forceinline__ void str_out_q4_u8(const RasterArg &r, int x, int y, Q4 v) {
+  map_stg<4>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, q4_pack_u8(v));
+}
+
 template <class T, int SW, int PX, int HY> struct SmemTap {
   const T *s;
   __device__ __forceinline__ T tap(int x, int y, int lx, int ly, int dx, int dy) const {
@@ -626,6 +691,16 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   }
   __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
     return PR<T>(s[(ly + HY + dy) * SW + (lx + PX + dx)], s[(ly + 1 + HY + dy) * SW + (lx + PX + dx)]);
+  }
+  // the taps at (dx, dy) of the byte cells lx .. lx + 3 (lx a multiple of 4, the
+  // row stride SW and pad PX multiples of 4, |dx| <= PX): the aligned words that
+  // hold them, funnel-shifted when dx is not a multiple of 4
+  __device__ __forceinline__ Q4 tap4(int lx, int ly, int dx, int dy) const {
+    static_assert(sizeof(T) == 1 && SW % 4 == 0 && PX % 4 == 0, "tap4: byte cells, word-aligned rows");
+    const u32 *row = (const u32 *)(s + (ly + HY + dy) * SW + lx + PX);
+    const int o = dx & 3, w = (dx - o) / 4;
+    const u32 v = o ? __funnelshift_r(row[w], row[w + 1], 8 * o) : row[w];
+    return q4_bytes(v);
   }
 };
 

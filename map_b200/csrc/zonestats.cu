@@ -425,27 +425,32 @@ void zone_stats(const ZoneStatsArgs &a, cudaStream_t st) {
 constexpr int kStaticZones = 16384;   // 16384 x 24 B = 384 KiB per device
 static __device__ __align__(256) Bin zs_static_bins[kStaticZones];
 
-// Address of the array on the current device (set-up on the first call there).
+// Address of the array in the current device's context. The address is looked
+// up on every call (a host-side lookup, no allocation), so a device or context
+// reset by the application between calls is harmless: the next call finds the
+// array in the new context. The kernels are loaded on the first call per device
+// so that later calls load nothing; after a reset the runtime loads them again
+// on the next call.
 static void *static_bins() {
   static std::mutex m;
-  static void *addr[64] = {};
+  static bool loaded[64] = {};
   int d = 0;
   check(cudaGetDevice(&d), "cudaGetDevice");
   if (d < 0 || d >= 64) throw MapError("zone statistics: device ordinal out of range");
+  void *p = nullptr;
+  const cudaError_t e = cudaGetSymbolAddress(&p, zs_static_bins);
+  if (e != cudaSuccess || !p)
+    throw MapError(std::string("zone statistics: cudaGetSymbolAddress of the static bins failed: ") +
+                   cudaGetErrorString(e));
   std::lock_guard<std::mutex> lk(m);
-  if (!addr[d]) {
-    void *p = nullptr;
-    const cudaError_t e = cudaGetSymbolAddress(&p, zs_static_bins);
-    if (e != cudaSuccess || !p)
-      throw MapError(std::string("zone statistics: cudaGetSymbolAddress of the static bins failed: ") +
-                     cudaGetErrorString(e));
+  if (!loaded[d]) {
     dev_info();   // loads the shared-bin accumulation kernel
     cudaFuncAttributes fa;
     check(cudaFuncGetAttributes(&fa, zs_accumulate<false>), "cudaFuncGetAttributes");
     check(cudaFuncGetAttributes(&fa, zs_finalize), "cudaFuncGetAttributes");
-    addr[d] = p;
+    loaded[d] = true;
   }
-  return addr[d];
+  return p;
 }
 
 void zone_stats_no_alloc(const ZoneStatsArgs &a, cudaStream_t st) {
