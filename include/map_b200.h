@@ -115,13 +115,26 @@ int ma_getExecMode(void);
  * identical to whole-raster evaluation. */
 void ma_setStreamRows(int rows);
 int ma_getStreamRows(void);
-/* Paired cells: focal groups with float math compute the cells of two rows per
+/* Packed cells: focal groups with float math compute the cells of two rows per
  * thread step, their float additions, subtractions, multiplications and the
- * polynomial parts of sin, cos and atan2 as packed f32x2 instructions. Results
- * are bit-identical either way; on = 0 computes one cell at a time. Engine
- * option with no counterpart in the reference. */
+ * polynomial parts of sin, cos and atan2 as packed f32x2 instructions; focal
+ * groups of integer arithmetic on byte rasters whose values provably stay in
+ * [0, 0x7FFF] (Life, thresholds of small-weight correlations) compute four
+ * cells of a row per step as 16-bit lanes of two words. Results are
+ * bit-identical either way; on = 0 computes one cell at a time. Engine option
+ * with no counterpart in the reference. */
 void ma_setPairedCells(int on);
 int ma_getPairedCells(void);
+/* Flow accumulations (spreadScan) of integer water over more than 64 K cells
+ * and at most `cells` cells run as pointer jumping over the Euler tour of the
+ * D8 forest: about log2(2N) rounds whatever the length of the longest flow
+ * path, O(N log N) work. Larger rasters walk the flow paths (O(N) work, one
+ * atomic step per cell of the longest path). Results are identical (integer
+ * sums). cells < 0 restores the default (2^21, or MAP_B200_SPREAD_PJ), 0 never
+ * jumps. A direction raster with a cycle makes the jumping form fail with an
+ * error. Engine option with no counterpart in the reference. */
+void ma_setFlowJumpCells(long long cells);
+long long ma_getFlowJumpCells(void);
 /* Algebraic rewrite of hillshade compositions (python/hill.py:41-49):
  * cz cos(atan(k sqrt(x^2+y^2))) + sz sin(...) cos(ar - aspect(x, y)) is
  * generated as (cz + sz k (y S - x C)) / sqrt(1 + k^2 (x^2 + y^2)), with the

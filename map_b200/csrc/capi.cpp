@@ -359,6 +359,10 @@ void ma_setPairedCells(int on) {
   void_call([&] { Runtime::get().paired_cells = on ? 1 : 0; });
 }
 int ma_getPairedCells(void) { return Runtime::get().paired_cells; }
+void ma_setFlowJumpCells(long long cells) {
+  void_call([&] { Runtime::get().flow_jump_cells = cells < 0 ? -1 : cells; });
+}
+long long ma_getFlowJumpCells(void) { return (long long)spread_pj_cells(); }
 
 void ma_setPrediction(int on) {
   void_call([&] { Runtime::get().prediction = on ? 1 : 0; });

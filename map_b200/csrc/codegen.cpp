@@ -127,6 +127,8 @@ struct Gen {
     float S1 = 0, S3 = 0, nC1 = 0;                        // for the selecting form
   };
   std::vector<ShadeFast> fast;
+  // fast shading statements record non-finite cells in `bad` instead of branching
+  mutable bool fast_flag = false;
 
   Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
 
@@ -609,9 +611,35 @@ struct Gen {
     s << "  return " << val(m.hs) << ";\n}\n";
     return s.str();
   }
+  // The fallback of fast composition i for one cell: the literal derivatives
+  // (every tap in the correlation's order, as the general form computes them,
+  // scaled by s) and the literal chain.
+  std::string shade_cell_slow_decl(int i) const {
+    const ShadeFast &f = fast[i];
+    const int hx = f.xc->halo_x(), hy = f.xc->halo_y(), mw = f.xc->mask_ds.arr[0];
+    const std::string fk = "f" + std::to_string(staged.at(f.in));
+    std::ostringstream s;
+    s << "template <class F>\n__device__ __noinline__ float shade_cell_slow" << i << "("
+      << (shade_reads_args(i) ? "const Args &a, " : "") << "const F &" << fk << ", int x, int y, int lx, int ly) {\n";
+    for (int c = 0; c < 2; c++) {
+      Node *cv = c ? f.yc : f.xc;
+      const std::string acc = c ? "yl" : "xl";
+      s << "  float " << acc << " = 0.0f;\n";
+      for (int i1 = -hy; i1 <= hy; i1++)
+        for (int i0 = -hx; i0 <= hx; i0++)
+          s << "  " << conv_term(acc, "(float)", tap(f.in, i0, i1), F32, F32, cv->mask[(i1 + hy) * mw + (i0 + hx)], false)
+            << "\n";
+    }
+    s << "  return shade_slow" << i << "(" << (shade_reads_args(i) ? "a, " : "") << "__fmul_rn(xl, " << fl((float)f.s)
+      << "), __fmul_rn(yl, " << fl((float)f.s) << "));\n}\n";
+    return s.str();
+  }
   std::string shade_decls() const {
     std::string s;
-    for (size_t i = 0; i < shades.size(); i++) s += shade_slow_decl((int)i);
+    for (size_t i = 0; i < shades.size(); i++) {
+      s += shade_slow_decl((int)i);
+      if (fast[i].on) s += shade_cell_slow_decl((int)i);
+    }
     return s;
   }
   static std::string fl(float f) {
@@ -622,13 +650,6 @@ struct Gen {
   std::string shade_args(const ShadeMatch &m) const {
     return fl(m.cz) + ", " + fl(m.szk) + ", " + fl(m.kk) + ", " + fl(m.S0) + ", " + fl(m.C0) + ", " + fl(m.S1) + ", " +
            fl(m.C1) + ", " + fl(m.SH) + ", " + fl(m.S3);
-  }
-  // tap of focal input `in` at offset (dx, dy) of the cell (x, y + dr), as a scalar
-  std::string tap_row(Node *in, int dx, int dy, int dr) const {
-    const int k = staged.at(in);
-    const std::string yo = dr ? " + " + std::to_string(dr) : "";
-    return "f" + std::to_string(k) + ".tap(x, y" + yo + ", lx, ly" + yo + ", " + std::to_string(dx) + ", " +
-           std::to_string(dy) + ")";
   }
   // Fast statement of composition i (see ShadeFast / map_shade_fast): the two
   // correlations as fused multiply-adds over their non-zero weights (exact
@@ -644,10 +665,21 @@ struct Gen {
     const int hx = f.xc->halo_x(), hy = f.xc->halo_y(), mw = f.xc->mask_ds.arr[0];
     auto tapv = [&](int dx, int dy) { return pair ? tap2(f.in, dx, dy) : tap(f.in, dx, dy); };
     std::ostringstream s;
+    // z: the taps both correlations weight by zero, as fma(tap, 0, z) (zero for
+    // finite taps, NaN otherwise); the x sum starts from it, so a non-finite
+    // such tap makes x, hence x^2 + y^2, NaN (the sign of a zero x does not
+    // change the result)
+    s << T << " " << v << "_xc = " << T << "(0.0f);";
+    for (int i1 = -hy; i1 <= hy; i1++)
+      for (int i0 = -hx; i0 <= hx; i0++) {
+        const int k = (i1 + hy) * mw + (i0 + hx);
+        if (var_as_f64(f.xc->mask[k]) == 0.0 && var_as_f64(f.yc->mask[k]) == 0.0)
+          s << " " << v << "_xc = " << fma << tapv(i0, i1) << ", 0.0f, " << v << "_xc);";
+      }
     for (int c = 0; c < 2; c++) {
       Node *cv = c ? f.yc : f.xc;
       const std::string acc = v + (c ? "_yc" : "_xc");
-      s << T << " " << acc << " = " << T << "(0.0f);";
+      if (c) s << " " << T << " " << acc << " = " << T << "(0.0f);";
       for (int i1 = -hy; i1 <= hy; i1++)
         for (int i0 = -hx; i0 <= hx; i0++) {
           const double w = var_as_f64(cv->mask[(i1 + hy) * mw + (i0 + hx)]);
@@ -655,32 +687,24 @@ struct Gen {
           s << " " << acc << " = " << fma << tapv(i0, i1) << ", " << fl((float)w) << ", " << acc << ");";
         }
     }
-    s << " " << T << " " << v << "_z = " << T << "(0.0f);";
-    for (int i1 = -hy; i1 <= hy; i1++)
-      for (int i0 = -hx; i0 <= hx; i0++) {
-        const int k = (i1 + hy) * mw + (i0 + hx);
-        if (var_as_f64(f.xc->mask[k]) == 0.0 && var_as_f64(f.yc->mask[k]) == 0.0)
-          s << " " << v << "_z = " << fma << tapv(i0, i1) << ", 0.0f, " << v << "_z);";
-      }
-    s << " " << T << " " << v << "_q; " << T << " " << v << " = map_shade_fast(" << v << "_xc, " << v << "_yc, " << v
-      << "_z, " << fl(shades[i].cz) << ", " << fl(f.szks) << ", " << fl(f.kks) << ", " << fl(f.S0) << ", " << fl(f.dS)
-      << ", " << fl(f.nC0) << ", " << fl(f.dnC) << ", " << fl(f.SH) << ", " << fl(f.dSx) << ", " << v << "_q);";
-    // literal derivatives and chain of one lane (dr: row offset of the lane)
+    s << " " << T << " " << v << "_q; " << T << " " << v << " = map_shade_fast(" << v << "_xc, " << v << "_yc, "
+      << fl(shades[i].cz) << ", " << fl(f.szks) << ", " << fl(f.kks) << ", " << fl(f.S0) << ", " << fl(f.dS) << ", "
+      << fl(f.nC0) << ", " << fl(f.dnC) << ", " << fl(f.SH) << ", " << fl(f.dSx) << ", " << v << "_q);";
+    // Cells whose x^2 + y^2 is not finite take the literal derivatives and chain
+    // (shade_cell_slow, a function of its own: no code in the unrolled row loop).
+    // In the flag form the row loop only records that some cell needs it, and
+    // recomputes the thread's cells with the checks when one did.
+    if (fast_flag) {
+      if (!pair) s << " bad |= !(" << v << "_q < MAP_INF_F);";
+      else s << " bad |= !(" << v << "_q.a < MAP_INF_F) | !(" << v << "_q.b < MAP_INF_F);";
+      return s.str();
+    }
+    const std::string fk = "f" + std::to_string(staged.at(f.in));
     auto slow_lane = [&](const std::string &lane, int dr) {
-      std::ostringstream t;
       const std::string sel = lane.empty() ? "" : "." + lane;
-      for (int c = 0; c < 2; c++) {
-        Node *cv = c ? f.yc : f.xc;
-        const std::string acc = v + (c ? "_yl" : "_xl");
-        t << " float " << acc << " = " << v << (c ? "_yc" : "_xc") << sel << ";";
-        for (int i1 = -hy; i1 <= hy; i1++)
-          for (int i0 = -hx; i0 <= hx; i0++)
-            if (var_as_f64(cv->mask[(i1 + hy) * mw + (i0 + hx)]) == 0.0)
-              t << " " << acc << " = __fmaf_rn(" << tap_row(f.in, i0, i1, dr) << ", 0.0f, " << acc << ");";
-      }
-      t << " " << v << sel << " = shade_slow" << si << "(" << (shade_reads_args(i) ? "a, " : "") << "__fmul_rn(" << v
-        << "_xl, " << fl((float)f.s) << "), __fmul_rn(" << v << "_yl, " << fl((float)f.s) << "));";
-      return t.str();
+      const std::string yo = dr ? " + " + std::to_string(dr) : "";
+      return " " + v + sel + " = shade_cell_slow" + si + "(" + (shade_reads_args(i) ? "a, " : "") + fk + ", x, y" + yo +
+             ", lx, ly" + yo + ");";
     };
     if (!pair) {
       s << " if (!(" << v << "_q < MAP_INF_F)) {" << slow_lane("", 0) << " }";
@@ -690,6 +714,11 @@ struct Gen {
       s << " if (!(" << v << "_q.b < MAP_INF_F)) {" << slow_lane("b", 1) << " } }";
     }
     return s.str();
+  }
+  bool any_fast() const {
+    for (auto &f : fast)
+      if (f.on) return true;
+    return false;
   }
 
   // statement of a rewritten node (scalar or pair form)
@@ -889,19 +918,26 @@ struct Gen {
       case K_CAST: case K_BARRIER: e = val4(n->prev[0]); break;
       case K_NEIGHBOR: e = tap4(n->prev[0], n->coord.arr[0], n->coord.arr[1]); break;
       case K_CONVOLUTION: {
+        // Sums of lanes are exact in any order (no lane leaves its range), so the
+        // correlation is summed mask row by mask row: the sum of one mask row
+        // over one tap row is the same expression for every output row that
+        // uses it, and the compiler computes it once for the unrolled rows.
         int hx = n->halo_x(), hy = n->halo_y(), mw = n->mask_ds.arr[0];
-        std::ostringstream s;
-        s << "Q4 " << v << " = q4_splat(0u);";
-        for (int i1 = -hy; i1 <= hy; i1++)
+        std::vector<std::string> rows;
+        for (int i1 = -hy; i1 <= hy; i1++) {
+          std::string r;
           for (int i0 = -hx; i0 <= hx; i0++) {
             const long long w = (long long)var_as_f64(n->mask[(i1 + hy) * mw + (i0 + hx)]);
             if (w == 0) continue;
             const std::string t = tap4(n->prev[0], i0, i1);
-            s << "\n    " << v << " = q4_add(" << v << ", " << (w == 1 ? t : "q4_mulc(" + t + ", " + std::to_string(w) + "u)")
-              << ");";
+            const std::string term = w == 1 ? t : "q4_mulc(" + t + ", " + std::to_string(w) + "u)";
+            r = r.empty() ? term : "q4_add(" + r + ", " + term + ")";
           }
-        if (R.wrap) s << "\n    " << v << " = q4_wrap8(" << v << ");";
-        return s.str();
+          if (!r.empty()) rows.push_back(r);
+        }
+        e = rows.empty() ? "q4_splat(0u)" : rows[0];
+        for (size_t k = 1; k < rows.size(); k++) e = "q4_add(" + e + ", " + rows[k] + ")";
+        break;
       }
       case K_UNARY: e = n->op == NOT ? "q4_eq0(" + val4(n->prev[0]) + ")" : val4(n->prev[0]); break;
       case K_BINARY: {
@@ -1431,15 +1467,23 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   // two loads of the same staged tap, which therefore load once per thread.
   const int nout = (int)G.outk.size();
   const bool defer = tune.defer && full_unroll && nout > 0 && rows * nout <= 32;
+  // with fast shading compositions, interior tiles first compute their cells
+  // recording only whether one needs the literal chain (flag form), and redo
+  // the thread's cells with the per-cell checks when one did
+  const bool flagged = defer && G.any_fast();
   if (defer) {
-    for (int pf = 0; pf < (pair ? 2 : 1); pf++) {
-      body << "template <";
-      for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
-      body << ">\n__device__ __forceinline__ void " << (pf ? "focal_cell2r" : "focal_cellr") << "(const Args &a";
-      for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
-      body << ", int x, int y, int lx, int ly" << G.out_params(pf) << ") {\n";
-      body << (pf ? G.center_loads2() + G.body2() : G.center_loads(false) + G.body(false)) << G.out_assigns() << "}\n";
-    }
+    for (int nc = 0; nc < (flagged ? 2 : 1); nc++)
+      for (int pf = 0; pf < (pair ? 2 : 1); pf++) {
+        body << "template <";
+        for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
+        body << ">\n__device__ __forceinline__ void " << (pf ? "focal_cell2r" : "focal_cellr") << (nc ? "_nc" : "")
+             << "(const Args &a";
+        for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
+        body << ", int x, int y, int lx, int ly" << G.out_params(pf) << (nc ? ", bool &bad" : "") << ") {\n";
+        G.fast_flag = nc == 1;
+        body << (pf ? G.center_loads2() + G.body2() : G.center_loads(false) + G.body(false)) << G.out_assigns() << "}\n";
+        G.fast_flag = false;
+      }
   }
   std::ostringstream loop, loop_full;
   loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
@@ -1476,12 +1520,25 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       k++;
     }
     callr << ")";
+    if (flagged) {
+      std::string cnc = callr.str();
+      cnc.insert(cnc.find('('), "_nc");
+      cnc.insert(cnc.size() - 1, ", bad");
+      loop_full << "    bool bad = false;\n"
+                << "#pragma unroll\n"
+                << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+                << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
+                << "      " << cnc << ";\n"
+                << "    }\n"
+                << "    if (bad) {\n";
+    }
     loop_full << "#pragma unroll\n"
               << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
               << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
               << "      " << callr.str() << ";\n"
-              << "    }\n"
-              << "#pragma unroll\n"
+              << "    }\n";
+    if (flagged) loop_full << "    }\n";
+    loop_full << "#pragma unroll\n"
               << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
               << "      const int y = t.y0 + ly0 + k;\n"
               << outs.str()
@@ -1575,7 +1632,9 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
   }
   body << loop.str() << "  }\n  return true;\n}\n";
-  wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
+  wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT;
+  if (tune.minb > 0) wrap << ", " << tune.minb;
+  wrap << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  extern __shared__ __align__(128) unsigned char smem[];\n"
        << "  u32 phase = 0;\n";
   if (use_tma)
@@ -2123,6 +2182,128 @@ static std::string gen_spread(Gen &G) {
       << "  }\n"
       << "}\n";
   }
+  // Integer accumulations: pointer jumping over the Euler tour of the D8 forest,
+  // a fixed number of rounds (ceil(log2(2N)) + 1) whatever the length of the
+  // longest flow path. Every non-root cell c (one whose D8 code leads to a cell
+  // of the raster, its parent) owns two tour elements: D(c) = 2c, the step down
+  // from its parent into c, carrying c's water, and U(c) = 2c + 1, the step back
+  // up, carrying 0. The children of a cell are its neighbours whose codes point
+  // at it, in direction order (E, SE, S, SW, W, NW, N, NE), so the tour's
+  // successor function is local: after D(c) comes D(first child of c), or U(c)
+  // for a leaf; after U(c) comes D(next sibling of c), or U(parent) unless the
+  // parent is a root (end of the tour). Each round sets sum[e] += sum[next[e]]
+  // and next[e] = next[next[e]] (Wyllie); afterwards sum[e] is the water from e
+  // to the end of its tour, so the subtree of c holds
+  // sum[D(c)] - sum[successor of U(c)], and the accumulation (strictly upstream
+  // water) is that minus c's own water; a root's is sum[D(first child)].
+  // Integer sums are exact modulo the type's width, so the result equals any
+  // other order of additions bit for bit. A list still linked after the last
+  // round lies on a cycle of codes: the error flag is set.
+  // Scratch at aux[0]: next[2][2N] (s32), then sum[2][2N] (the sum type).
+  const bool pj = dt == S32 || dt == U32 || dt == S64 || dt == U64;
+  if (pj) {
+    const std::string ST = dt_size(dt) == 4 ? "u32" : "u64";
+    s << "#define PJ_END (-1)\n"
+      << "struct PjArgs { u64 args; s64 n; s64 slices; s64 round; };\n"
+      << "__device__ __forceinline__ s32 pj_child(const RasterArg &D, int W, int H, int x, int y, int j0) {\n"
+      << "  for (int j = j0; j < 8; ++j) {\n"
+      << "    const int nx = x + d8_dx(j), ny = y + d8_dy(j);\n"
+      << "    if (nx < 0 || ny < 0 || nx >= W || ny >= H) continue;\n"
+      << "    if (d8_index(ldr<u8>(D, nx, ny)) == ((j + 4) & 7)) return ny * W + nx;\n"
+      << "  }\n"
+      << "  return -1;\n"
+      << "}\n"
+      // successor of U(c) for a non-root cell (x, y) whose code has index d
+      << "__device__ __forceinline__ s32 pj_after_up(const RasterArg &D, int W, int H, int x, int y, int d) {\n"
+      << "  const int px = x + d8_dx(d), py = y + d8_dy(d);\n"
+      << "  const s32 sib = pj_child(D, W, H, px, py, ((d + 4) & 7) + 1);\n"
+      << "  if (sib >= 0) return 2 * sib;\n"
+      << "  return d8_down(D, W, H, px, py) >= 0 ? 2 * (py * W + px) + 1 : PJ_END;\n"
+      << "}\n"
+      << "__device__ __forceinline__ void pj_init(const Args &a, s64 first, s64 step) {\n"
+      << "  const int W = a.g.W, H = a.g.H;\n"
+      << "  const s64 N = (s64)W * H;\n"
+      << "  s32 *nx0 = (s32 *)a.aux[0];\n"
+      << "  " << ST << " *sm0 = (" << ST << " *)(nx0 + 4 * N);\n"
+      << "  const RasterArg D = a.in[" << kd << "];\n"
+      << "  for (s64 c = first; c < N; c += step) {\n"
+      << "    const int x = (int)(c % W), y = (int)(c / W);\n"
+      << "    s32 nd = PJ_END, nu = PJ_END;\n"
+      << "    " << ST << " w = 0;\n"
+      << "    if (d8_down(D, W, H, x, y) >= 0) {\n"
+      << "      const s32 fc = pj_child(D, W, H, x, y, 0);\n"
+      << "      nd = fc >= 0 ? 2 * fc : (s32)(2 * c + 1);\n"
+      << "      nu = pj_after_up(D, W, H, x, y, d8_index(ldr<u8>(D, x, y)));\n"
+      << "      w = (" << ST << ")water_at(a, x, y);\n"
+      << "    }\n"
+      << "    nx0[2 * c] = nd;\n"
+      << "    nx0[2 * c + 1] = nu;\n"
+      << "    sm0[2 * c] = w;\n"
+      << "    sm0[2 * c + 1] = 0;\n"
+      << "  }\n"
+      << "}\n"
+      << "__device__ __forceinline__ void pj_step(const Args &a, s64 first, s64 step, int round) {\n"
+      << "  const s64 N = (s64)a.g.W * a.g.H;\n"
+      << "  s32 *nxs = (s32 *)a.aux[0] + (round & 1) * 2 * N, *nxd = (s32 *)a.aux[0] + ((round + 1) & 1) * 2 * N;\n"
+      << "  " << ST << " *sm = (" << ST << " *)((s32 *)a.aux[0] + 4 * N);\n"
+      << "  const " << ST << " *sms = sm + (round & 1) * 2 * N;\n"
+      << "  " << ST << " *smd = sm + ((round + 1) & 1) * 2 * N;\n"
+      << "  for (s64 e = first; e < 2 * N; e += step) {\n"
+      << "    const s32 n = nxs[e];\n"
+      << "    if (n == PJ_END) { nxd[e] = PJ_END; smd[e] = sms[e]; }\n"
+      << "    else { smd[e] = sms[e] + sms[n]; nxd[e] = nxs[n]; }\n"
+      << "  }\n"
+      << "}\n"
+      << "__device__ __forceinline__ void pj_final(const Args &a, s64 first, s64 step, int rounds) {\n"
+      << "  const int W = a.g.W, H = a.g.H;\n"
+      << "  const s64 N = (s64)W * H;\n"
+      << "  const s32 *nx = (const s32 *)a.aux[0] + (rounds & 1) * 2 * N;\n"
+      << "  const " << ST << " *sm = (const " << ST << " *)((const s32 *)a.aux[0] + 4 * N) + (rounds & 1) * 2 * N;\n"
+      << "  const RasterArg D = a.in[" << kd << "];\n"
+      << "  const RasterArg O = a.out[" << ko << "];\n"
+      << "  for (s64 c = first; c < N; c += step) {\n"
+      << "    const int x = (int)(c % W), y = (int)(c / W);\n"
+      << "    " << ST << " acc;\n"
+      << "    if (d8_down(D, W, H, x, y) < 0) {\n"
+      << "      const s32 fc = pj_child(D, W, H, x, y, 0);\n"
+      << "      acc = fc >= 0 ? sm[2 * fc] : (" << ST << ")0;\n"
+      << "    } else {\n"
+      << "      if (nx[2 * c] != PJ_END) skel_fail(a.err, ERR_ITER_LIMIT);   // a cycle of codes\n"
+      << "      const s32 nu = pj_after_up(D, W, H, x, y, d8_index(ldr<u8>(D, x, y)));\n"
+      << "      acc = sm[2 * c] - (nu == PJ_END ? (" << ST << ")0 : sm[nu]) - (" << ST << ")water_at(a, x, y);\n"
+      << "    }\n"
+      << "    *cell_ptr<" << T << ">(O, x, y) = (" << T << ")acc;\n"
+      << "  }\n"
+      << "}\n"
+      // one raster (aux[1]: round of a step launch)
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_init(const __grid_constant__ Args a) {\n"
+      << "  pj_init(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x);\n"
+      << "}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_step(const __grid_constant__ Args a) {\n"
+      << "  pj_step(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x, (int)a.aux[1]);\n"
+      << "}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_final(const __grid_constant__ Args a) {\n"
+      << "  pj_final(a, (s64)blockIdx.x * blockDim.x + threadIdx.x, (s64)gridDim.x * blockDim.x, (int)a.aux[1]);\n"
+      << "}\n"
+      // many rasters (serving windows): `slices` CTAs per raster
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_init_many(const __grid_constant__ PjArgs m) {\n"
+      << "  const s64 r = blockIdx.x / m.slices;\n"
+      << "  if (r >= m.n) return;\n"
+      << "  pj_init(((const Args *)m.args)[r], (blockIdx.x % m.slices) * blockDim.x + threadIdx.x, m.slices * blockDim.x);\n"
+      << "}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_step_many(const __grid_constant__ PjArgs m) {\n"
+      << "  const s64 r = blockIdx.x / m.slices;\n"
+      << "  if (r >= m.n) return;\n"
+      << "  pj_step(((const Args *)m.args)[r], (blockIdx.x % m.slices) * blockDim.x + threadIdx.x, m.slices * blockDim.x,\n"
+      << "          (int)m.round);\n"
+      << "}\n"
+      << "extern \"C\" __global__ void __launch_bounds__(256) KNAME_pj_final_many(const __grid_constant__ PjArgs m) {\n"
+      << "  const s64 r = blockIdx.x / m.slices;\n"
+      << "  if (r >= m.n) return;\n"
+      << "  pj_final(((const Args *)m.args)[r], (blockIdx.x % m.slices) * blockDim.x + threadIdx.x, m.slices * blockDim.x,\n"
+      << "           (int)m.round);\n"
+      << "}\n";
+  }
   const std::string kahn_fn = packed ? "spread_kahn_packed" : "spread_kahn";
   const std::string init_fn = packed ? "spread_init_packed" : "spread_init";
   s
@@ -2183,6 +2364,7 @@ const FocalTune &focal_tune() {
         else if (k == "qnt") r.qnt = v;
         else if (k == "qtw") r.qtw = v;
         else if (k == "qth") r.qth = v;
+        else if (k == "minb") r.minb = v;
       }
       i = j + 1;
     }

@@ -71,12 +71,19 @@ struct FocalTune {
   int nt = 0, tw = 0, th = 0;
   int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
   int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
+  int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
 };
 const FocalTune &focal_tune();
 
 // Dynamic shared memory of a radial scan launch over a W x H raster: two front
 // buffers when they fit (0 otherwise: the kernel then re-reads fronts from its output).
 size_t radial_front_smem(int W, int H, int dtype);
+// Pointer-jumping flow accumulation (integer types): cell limit, rounds for N
+// cells, whether a type qualifies, and the scratch bytes for N cells.
+size_t spread_pj_cells();
+int spread_pj_rounds(size_t N);
+bool spread_pj_type(int dt);
+size_t spread_pj_scratch(size_t N, int dt);
 
 // Reference float-constant rounding: constants written into kernel text by the
 // reference go through std::to_string ("%f", six decimals) before the device

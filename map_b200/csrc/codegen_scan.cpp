@@ -35,6 +35,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <unordered_map>
@@ -46,6 +47,27 @@ namespace mapb {
 // which spread over every SM (measured at 1024²: 1.7 ms against 5.6 ms for one
 // CTA). Serving runs one CTA per window instead, many windows side by side.
 constexpr size_t kSpreadKahnCells = (size_t)1 << 16;
+// Integer flow accumulations of more cells than kSpreadKahnCells and at most this
+// many run as pointer jumping over the Euler tour of the D8 forest (a fixed
+// number of rounds, independent of the longest flow path; O(N log N) work, so
+// the downstream walks take over for larger rasters). ma_setFlowJumpCells, or
+// MAP_B200_SPREAD_PJ for the default, sets the limit (0: never).
+size_t spread_pj_cells() {
+  static const size_t dflt = [] {
+    const char *e = std::getenv("MAP_B200_SPREAD_PJ");
+    return e ? (size_t)std::strtoull(e, nullptr, 10) : ((size_t)1 << 21);
+  }();
+  const long long v = Runtime::get().flow_jump_cells;
+  return v < 0 ? dflt : (size_t)v;
+}
+// rounds of pointer jumping for N cells: 2^rounds exceeds 2N, the longest tour
+int spread_pj_rounds(size_t N) {
+  int r = 1;
+  while (((size_t)1 << r) <= 2 * N) r++;
+  return r;
+}
+bool spread_pj_type(int dt) { return dt == S32 || dt == U32 || dt == S64 || dt == U64; }
+size_t spread_pj_scratch(size_t N, int dt) { return 4 * N * (sizeof(int32_t) + dt_size(dt)); }
 // radial scans of rasters at least this wide or tall use CTA clusters per octant
 constexpr int kRadialClusterDim = 2048;
 constexpr int kRadialCluster = 8;
@@ -94,6 +116,26 @@ void run_scan_group(const Group &g, const KernelPlan &P, std::unordered_map<Node
   }
   const size_t N = (size_t)g.W * g.H;
   if (N >= (size_t)1 << 31) throw MapError("spreadScan: raster too large");
+  if (N > kSpreadKahnCells && N <= spread_pj_cells() && spread_pj_type(scan->meta.dtype)) {
+    void *work = nullptr;
+    cuda_check(cudaMallocAsync(&work, spread_pj_scratch(N, scan->meta.dtype), st), "cudaMallocAsync(spread work)");
+    const int rounds = spread_pj_rounds(N);
+    const int grid = (int)std::max<size_t>(1, std::min<size_t>((2 * N + 255) / 256, (size_t)env.sm_count() * 8));
+    uint64_t aux[4] = {(uint64_t)(uintptr_t)work, 0, 0, 0};
+    auto a = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+    env.launch(env.kernel(P.source, P.kname + "_pj_init", 0), grid, 256, 0, (CUstream_st *)st, a.data(), a.size());
+    KernelHandle ks = env.kernel(P.source, P.kname + "_pj_step", 0);
+    for (int r = 0; r < rounds; r++) {
+      aux[1] = (uint64_t)r;
+      auto ar = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+      env.launch(ks, grid, 256, 0, (CUstream_st *)st, ar.data(), ar.size());
+    }
+    aux[1] = (uint64_t)rounds;
+    auto af = pack_args(g, P, get, bufs, 0, 0, g.W, g.H, aux);
+    env.launch(env.kernel(P.source, P.kname + "_pj_final", 0), grid, 256, 0, (CUstream_st *)st, af.data(), af.size());
+    cuda_check(cudaFreeAsync(work, st), "cudaFreeAsync");
+    return;
+  }
   void *work = nullptr;
   cuda_check(cudaMallocAsync(&work, 6 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
   uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + 2 * N),

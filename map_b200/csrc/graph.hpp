@@ -102,6 +102,7 @@ struct Runtime {
   // Focal groups of float math compute two cells per thread step on packed
   // f32x2 instructions (bit-identical to one cell at a time); 0 turns it off.
   int paired_cells = 1;
+  long long flow_jump_cells = -1;   // < 0: the default limit of pointer-jumping flow accumulation
   // Hillshade compositions (python/hill.py:41-49) are generated through the
   // shading identity of rewrite.hpp; 0 keeps the literal operator chain; 2 uses
   // the identity without its fast form (derivatives computed as written).

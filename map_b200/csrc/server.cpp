@@ -14,6 +14,7 @@
 #include <chrono>
 #include <cmath>
 #include <condition_variable>
+#include <cstdlib>
 #include <cstring>
 #include <deque>
 #include <map>
@@ -60,9 +61,19 @@ struct Req {
   std::vector<void *> scratch;
 };
 
+// Flow windows above 64 K cells with integer accumulations use pointer jumping
+// (MAP_B200_SERVE_PJ=0: the one-CTA frontier sweep instead).
+bool serve_pj() {
+  static const bool v = [] {
+    const char *e = std::getenv("MAP_B200_SERVE_PJ");
+    return !(e && e[0] == '0');
+  }();
+  return v;
+}
+
 size_t request_bytes(int type, int w, int h) {
   size_t b = (size_t)pitch_for(w, F32) * h * 2;   // window copy + output
-  if (type == REQ_FLOW) b += (size_t)pitch_for(w, U8) * h + (size_t)w * h * 24;   // directions + sweep scratch
+  if (type == REQ_FLOW) b += (size_t)pitch_for(w, U8) * h + (size_t)w * h * 32;   // directions + sweep scratch
   return b;
 }
 
@@ -216,6 +227,8 @@ Template &Server::Impl::template_for(int type, int w, int h, bool compile) {
     } else if (g.skeleton == SK_SPREAD) {
       env.kernel(P.source, P.kname + "_prep_many", 0);
       env.kernel(P.source, P.kname + "_kahnp_many", 0);
+      if (spread_pj_type(P.core->meta.dtype))
+        for (const char *k : {"_pj_init_many", "_pj_step_many", "_pj_final_many"}) env.kernel(P.source, P.kname + k, 0);
       T->last_phase = std::max(T->last_phase, (int)PH_SPREAD);
     } else {
       throw MapError("serving: zonal groups are not served");
@@ -259,6 +272,8 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     std::vector<unsigned char> args;
     int n = 0;
     int max_dim = 0;   // largest window side (radial front buffers)
+    size_t max_cells = 0;
+    bool pj = false;   // flow accumulation by pointer jumping (integer type, windows above 64 K cells)
   };
   std::map<std::string, Many> radial, spread;
   std::vector<Req *> ok;
@@ -352,11 +367,16 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
           mn.n++;
           mn.max_dim = std::max(mn.max_dim, std::max(g.W, g.H));
         } else {   // SK_SPREAD
-          Many &mn = spread[P.source];
-          mn.plan = &P;
           const size_t N = (size_t)g.W * g.H;
+          const bool pj = serve_pj() && N > ((size_t)1 << 16) && spread_pj_type(P.core->meta.dtype);
+          // windows of one template share one launch per phase, so each form keys its own
+          Many &mn = spread[P.source + (pj ? "#pj" : "")];
+          mn.plan = &P;
+          mn.pj = pj;
+          mn.max_cells = std::max(mn.max_cells, N);
           void *work = nullptr;
-          cuda_check(cudaMallocAsync(&work, 6 * N * sizeof(int32_t), st), "cudaMallocAsync(spread work)");
+          const size_t wbytes = pj ? spread_pj_scratch(N, P.core->meta.dtype) : 6 * N * sizeof(int32_t);
+          cuda_check(cudaMallocAsync(&work, wbytes, st), "cudaMallocAsync(spread work)");
           r->scratch.push_back(work);
           uint64_t aux[4] = {(uint64_t)(uintptr_t)work, (uint64_t)(uintptr_t)((int32_t *)work + 2 * N),
                              (uint64_t)(uintptr_t)((int32_t *)work + 4 * N), (uint64_t)(N + 1)};
@@ -458,6 +478,24 @@ void Server::Impl::run_batch(std::vector<Req *> &batch) {
     cuda_check(cudaStreamWaitEvent(sp, ev[PH_LEVEL1], 0), "cudaStreamWaitEvent");
     for (auto &kv : spread) {
       Many &mn = kv.second;
+      if (mn.pj) {
+        // pointer jumping: a fixed number of rounds, `slices` CTAs per window
+        const int rounds = spread_pj_rounds(mn.max_cells);
+        const int64_t slices = std::max<int64_t>(32, std::min<int64_t>(256, (int64_t)(2 * mn.max_cells / 8192)));
+        struct { uint64_t args; int64_t n, slices, round; } pa{(uint64_t)(uintptr_t)dptr[bi++], mn.n, slices, 0};
+        const int grid = (int)(mn.n * slices);
+        env.launch(env.kernel(mn.plan->source, mn.plan->kname + "_pj_init_many", 0), grid, 256, 0, (CUstream_st *)sp,
+                   &pa, sizeof pa);
+        KernelHandle ks = env.kernel(mn.plan->source, mn.plan->kname + "_pj_step_many", 0);
+        for (int k = 0; k < rounds; k++) {
+          pa.round = k;
+          env.launch(ks, grid, 256, 0, (CUstream_st *)sp, &pa, sizeof pa);
+        }
+        pa.round = rounds;
+        env.launch(env.kernel(mn.plan->source, mn.plan->kname + "_pj_final_many", 0), grid, 256, 0, (CUstream_st *)sp,
+                   &pa, sizeof pa);
+        continue;
+      }
       // in-degrees by 32 CTAs per window, then one CTA per window sweeps the
       // frontiers (the lowest latency at window sizes)
       KernelHandle kp = env.kernel(mn.plan->source, mn.plan->kname + "_prep_many", 0);

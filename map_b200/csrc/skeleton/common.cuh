@@ -521,25 +521,25 @@ __device__ __forceinline__ PR<float> map_shade(const PR<float> &x, const PR<floa
 // arithmetically: with negf = (yc < 0), S = S0 + negf (S1 - S0) and -C = -C0 +
 // negf (C0 - C1) for xc != 0, S = SH + negf (S3 - SH) for xc == 0, where the
 // differences are exact in float32 (the host checks this before choosing this
-// form), so S and -C are exactly S0 / S1 / SH / S3 and -C0 / -C1. z is +-0, or
-// NaN when a cell the derivatives do not read (weight 0 in both) is not finite;
-// q = xc^2 + yc^2 + z, and the caller takes the literal chain where q is not
-// finite. Every operation rounds once; the pair form performs the same
-// operations lane by lane.
-__device__ __forceinline__ float map_shade_fast(float xc, float yc, float z, float cz, float szks, float kks, float S0,
+// form), so S and -C are exactly S0 / S1 / SH / S3 and -C0 / -C1. The caller's
+// xc starts from the taps neither derivative weights (fma(tap, 0, .): +-0, or
+// NaN when such a tap is not finite); q = xc^2 + yc^2, and the caller takes the
+// literal chain where q is not finite. Every operation rounds once; the pair
+// form performs the same operations lane by lane.
+__device__ __forceinline__ float map_shade_fast(float xc, float yc, float cz, float szks, float kks, float S0,
                                                 float dS, float nC0, float dnC, float SH, float dSx, float &q) {
-  q = __fadd_rn(__fmaf_rn(xc, xc, __fmul_rn(yc, yc)), z);
+  q = __fmaf_rn(xc, xc, __fmul_rn(yc, yc));
   const float negf = yc < 0.0f ? 1.0f : 0.0f;
   const float Sn = __fmaf_rn(negf, dS, S0), nC = __fmaf_rn(negf, dnC, nC0), Sx = __fmaf_rn(negf, dSx, SH);
   const float S = xc != 0.0f ? Sn : Sx;
   const float num = __fmaf_rn(yc, S, __fmul_rn(xc, nC));
   return __fmul_rn(__fmaf_rn(szks, num, cz), map_rsqrt(__fmaf_rn(kks, q, 1.0f)));
 }
-__device__ __forceinline__ PR<float> map_shade_fast(const PR<float> &xc, const PR<float> &yc, const PR<float> &z, float cz,
+__device__ __forceinline__ PR<float> map_shade_fast(const PR<float> &xc, const PR<float> &yc, float cz,
                                                     float szks, float kks, float S0, float dS, float nC0, float dnC,
                                                     float SH, float dSx, PR<float> &q) {
   const float2 X = pr_f2(xc), Y = pr_f2(yc);
-  q = pr_of(__fadd2_rn(__ffma2_rn(X, X, __fmul2_rn(Y, Y)), pr_f2(z)));
+  q = pr_of(__ffma2_rn(X, X, __fmul2_rn(Y, Y)));
   const float2 negf = make_float2(yc.a < 0.0f ? 1.0f : 0.0f, yc.b < 0.0f ? 1.0f : 0.0f);
   const float2 Sn = __ffma2_rn(negf, f2_of(dS), f2_of(S0)), nC = __ffma2_rn(negf, f2_of(dnC), f2_of(nC0));
   const float2 Sx = __ffma2_rn(negf, f2_of(dSx), f2_of(SH));
@@ -622,8 +622,11 @@ template <class T> struct GatherTap {
 // ------------------------------------------------------------------ packed byte cells
 
 // Four consecutive cells of a row (x .. x + 3) of an integer expression whose
-// every value lies in [0, 0x7FFF], as 16-bit lanes of two words: lo holds the
-// cells x (bits 0-15) and x + 1 (bits 16-31), hi the cells x + 2 and x + 3.
+// every value lies in [0, 0x7FFF], as 16-bit lanes of two words, interleaved:
+// lo holds the cells x (bits 0-15) and x + 2 (bits 16-31), hi the cells x + 1
+// and x + 3. With this layout the taps of neighbouring offsets share words
+// (the lanes of offset +1 are hi and the even lanes of offset +2), so a row of
+// byte cells costs one byte permute per word of taps (see SmemTap::tap4).
 // Sums, differences and products by non-negative constants of such lanes are
 // plain 32-bit operations as long as no lane leaves [0, 0xFFFF], which the code
 // generator proves by interval arithmetic before it uses this form; results of
@@ -631,9 +634,11 @@ template <class T> struct GatherTap {
 struct Q4 { u32 lo, hi; };
 __device__ __forceinline__ Q4 q4_splat(u32 c) { return Q4{c * 0x00010001u, c * 0x00010001u}; }
 // four bytes (cells x .. x + 3) as lanes
-__device__ __forceinline__ Q4 q4_bytes(u32 w) { return Q4{__byte_perm(w, 0u, 0x4140), __byte_perm(w, 0u, 0x4342)}; }
+__device__ __forceinline__ u32 q4_even(u32 w) { return __byte_perm(w, 0u, 0x4240); }   // bytes 0, 2
+__device__ __forceinline__ u32 q4_odd(u32 w) { return __byte_perm(w, 0u, 0x4341); }    // bytes 1, 3
+__device__ __forceinline__ Q4 q4_bytes(u32 w) { return Q4{q4_even(w), q4_odd(w)}; }
 // the four lanes (each < 256) as the bytes of one word, cell x in the low byte
-__device__ __forceinline__ u32 q4_pack_u8(Q4 v) { return __byte_perm(v.lo, v.hi, 0x6420); }
+__device__ __forceinline__ u32 q4_pack_u8(Q4 v) { return __byte_perm(v.lo, v.hi, 0x6240); }
 __device__ __forceinline__ Q4 q4_add(Q4 a, Q4 b) { return Q4{a.lo + b.lo, a.hi + b.hi}; }
 __device__ __forceinline__ Q4 q4_sub(Q4 a, Q4 b) { return Q4{a.lo - b.lo, a.hi - b.hi}; }
 __device__ __forceinline__ Q4 q4_mulc(Q4 a, u32 c) { return Q4{a.lo * c, a.hi * c}; }
@@ -692,15 +697,32 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
     return PR<T>(s[(ly + HY + dy) * SW + (lx + PX + dx)], s[(ly + 1 + HY + dy) * SW + (lx + PX + dx)]);
   }
-  // the taps at (dx, dy) of the byte cells lx .. lx + 3 (lx a multiple of 4, the
-  // row stride SW and pad PX multiples of 4, |dx| <= PX): the aligned words that
-  // hold them, funnel-shifted when dx is not a multiple of 4
+  // The taps at (dx, dy) of the byte cells lx .. lx + 3 (lx a multiple of 4, the
+  // row stride SW and pad PX multiples of 4, |dx| <= PX), in the interleaved
+  // lane layout of Q4. With dx = 4 m + o and W_m the m-th aligned word from the
+  // cell lx: the even and odd bytes of W_m (q4_even / q4_odd) are the lanes of
+  // o = 0; lanes (4m + 2, 4m + 4) take byte 2 of W_m and byte 0 of W_m+1
+  // beside the zero bytes of q4_even(W_m); lanes (4m + 3, 4m + 5) take byte 3 of
+  // W_m and the odd lanes of W_m+1. Each piece is one byte permute of loaded
+  // words, and the pieces of neighbouring offsets are the same expressions.
+  __device__ __forceinline__ u32 word(int lx, int ly, int dy, int m) const {
+    return ((const u32 *)(s + (ly + HY + dy) * SW + lx + PX))[m];
+  }
+  __device__ __forceinline__ u32 tap4_e(int lx, int ly, int dy, int m) const {   // lanes 4m + 2, 4m + 4
+    return __byte_perm(q4_even(word(lx, ly, dy, m)), word(lx, ly, dy, m + 1), 0x1412);
+  }
+  __device__ __forceinline__ u32 tap4_o(int lx, int ly, int dy, int m) const {   // lanes 4m + 3, 4m + 5
+    return __byte_perm(word(lx, ly, dy, m), q4_odd(word(lx, ly, dy, m + 1)), 0x5453);
+  }
   __device__ __forceinline__ Q4 tap4(int lx, int ly, int dx, int dy) const {
     static_assert(sizeof(T) == 1 && SW % 4 == 0 && PX % 4 == 0, "tap4: byte cells, word-aligned rows");
-    const u32 *row = (const u32 *)(s + (ly + HY + dy) * SW + lx + PX);
-    const int o = dx & 3, w = (dx - o) / 4;
-    const u32 v = o ? __funnelshift_r(row[w], row[w + 1], 8 * o) : row[w];
-    return q4_bytes(v);
+    const int o = dx & 3, m = (dx - o) / 4;
+    switch (o) {
+      case 0: return q4_bytes(word(lx, ly, dy, m));
+      case 1: return Q4{q4_odd(word(lx, ly, dy, m)), tap4_e(lx, ly, dy, m)};
+      case 2: return Q4{tap4_e(lx, ly, dy, m), tap4_o(lx, ly, dy, m)};
+      default: return Q4{tap4_o(lx, ly, dy, m), q4_even(word(lx, ly, dy, m + 1))};
+    }
   }
 };
 

@@ -782,6 +782,16 @@ def get_stream_rows():
     return _lib.ma_getStreamRows()
 
 
+def set_flow_jump_cells(cells):
+    """Largest integer flow accumulation (cells) computed by pointer jumping;
+    0 never, < 0 the default."""
+    _lib.ma_setFlowJumpCells(int(cells))
+
+
+def get_flow_jump_cells():
+    return _lib.ma_getFlowJumpCells()
+
+
 def set_paired_cells(on):
     """Two cells per thread step on packed f32x2 instructions in float focal groups
     (bit-identical results); False computes one cell at a time."""
@@ -1020,6 +1030,8 @@ _sig('ma_lastBandCount', [], ct.c_int, check=False)
 _sig('ma_setStreamRows', [ct.c_int], None)
 _sig('ma_getStreamRows', [], ct.c_int, check=False)
 _sig('ma_setPairedCells', [ct.c_int], None)
+_sig('ma_setFlowJumpCells', [ct.c_longlong], None)
+_sig('ma_getFlowJumpCells', [], ct.c_longlong, check=False)
 _sig('ma_getPairedCells', [], ct.c_int, check=False)
 _sig('ma_setAlgebraicRewrite', [ct.c_int], None)
 _sig('ma_setPrediction', [ct.c_int], None)

@@ -42,6 +42,7 @@ def fresh(M):
     M.set_border(M.BORDER_BLOCK_MIRROR)
     M.set_exec_mode(M.EXEC_FUSED)
     M.set_paired_cells(True)
+    M.set_flow_jump_cells(-1)
     M.set_algebraic_rewrite(True)
     M.set_prediction(True)
     M.set_default_blocksize([256, 256])

@@ -162,3 +162,60 @@ def test_flow_accumulation_large_raster_float_water(M):
     got = M.to_numpy(M.flow_accumulation(M.from_numpy(water, bs=[512, 512]), dirs))
     ref, _ = O.flowacc_s32(np.ones(shape, np.int32), M.to_numpy(dirs))
     assert np.array_equal(got, ref.astype(np.float32) * np.float32(0.5))
+
+
+@pytest.mark.parametrize("shape,dtype", [((300, 260), np.int32), ((517, 333), np.uint32), ((1024, 1024), np.int32),
+                                         ((700, 650), np.int64)])
+def test_flow_accumulation_pointer_jumping_equals_walk_and_oracle(fresh, shape, dtype):
+    # rasters above 64 K cells: the Euler-tour pointer jumping (fixed rounds) and
+    # the downstream walks give the same integer sums, equal to the oracle's
+    M = fresh
+    rng = np.random.default_rng(41)
+    dem_np = synth.fbm_dem(shape[0], shape[1], seed=42)
+    dem = M.from_numpy(dem_np, bs=[256, 256])
+    dirs = M.flow_direction(dem)
+    lo = -700 if np.issubdtype(dtype, np.signedinteger) else 0
+    water_np = rng.integers(lo, 700, shape).astype(dtype)
+    out = {}
+    for cells in (1 << 30, 0):
+        M.set_flow_jump_cells(cells)
+        out[cells] = M.to_numpy(M.flow_accumulation(M.from_numpy(water_np, bs=[256, 256]), dirs))
+    M.set_flow_jump_cells(-1)
+    assert np.array_equal(out[1 << 30], out[0])
+    d = M.to_numpy(dirs)
+    if dtype != np.int64:
+        ref, cyclic = O.flowacc_s32(water_np.astype(np.int32), d)
+        assert not cyclic
+        assert np.array_equal(out[0].astype(np.int32), ref)
+
+
+def test_flow_accumulation_pointer_jumping_roots_and_edges(fresh):
+    # zero codes (pits), invalid codes (several bits) and codes leading out of
+    # the raster are roots. Codes E, SE, S, SW never decrease y and E alone
+    # keeps it, so the random direction raster is acyclic.
+    M = fresh
+    rng = np.random.default_rng(43)
+    shape = (400, 300)
+    codes = np.array([0, 1, 2, 4, 8, 1, 2, 4, 8, 3, 6], np.uint8)
+    d = codes[rng.integers(0, len(codes), shape)]
+    ref, cyclic = O.flowacc_s32(np.ones(shape, np.int32), d)
+    assert not cyclic
+    M.set_flow_jump_cells(1 << 30)
+    got = M.to_numpy(M.flow_accumulation(M.ones_like(M.from_numpy(d), M.S32), M.from_numpy(d)))
+    assert np.array_equal(got, ref)
+
+
+def test_flow_accumulation_pointer_jumping_reports_a_cycle(fresh):
+    # two cells draining into each other: the tour never ends, the kernel sets
+    # the error flag after its fixed rounds and the call fails
+    M = fresh
+    shape = (300, 300)
+    d = np.full(shape, 1, np.uint8)         # everything drains east
+    d[100, 100], d[100, 101] = 1, 16        # (100,100) -> E, (100,101) -> W: a 2-cycle
+    M.set_flow_jump_cells(1 << 30)
+    with pytest.raises(M.MapError):
+        M.to_numpy(M.flow_accumulation(M.ones_like(M.from_numpy(d), M.S32), M.from_numpy(d)))
+    # the engine stays usable
+    d[100, 101] = 1
+    got = M.to_numpy(M.flow_accumulation(M.ones_like(M.from_numpy(d), M.S32), M.from_numpy(d)))
+    assert got[0, 299] == 299

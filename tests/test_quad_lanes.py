@@ -92,20 +92,42 @@ def byte_perm(x, y, s):
     return out.astype(u32)
 
 
+def q4_even(w):
+    return byte_perm(w, 0, 0x4240)
+
+
+def q4_odd(w):
+    return byte_perm(w, 0, 0x4341)
+
+
+def tap4(words, lx, dx):
+    """SmemTap::tap4 restated: the interleaved lanes (lo: cells 0 and 2, hi:
+    cells 1 and 3 of lx + dx .. lx + dx + 3) from the aligned words."""
+    o, m = dx & 3, (dx - (dx & 3)) // 4
+    W = lambda k: u32(words[lx // 4 + k])
+    e = lambda k: byte_perm(q4_even(W(k)), W(k + 1), 0x1412)
+    od = lambda k: byte_perm(W(k), q4_odd(W(k + 1)), 0x5453)
+    if o == 0:
+        return q4_even(W(m)), q4_odd(W(m))
+    if o == 1:
+        return q4_odd(W(m)), e(m)
+    if o == 2:
+        return e(m), od(m)
+    return od(m), q4_even(W(m + 1))
+
+
 def test_byte_lanes_round_trip_and_taps():
     rng = np.random.default_rng(3)
-    row = rng.integers(0, 256, 64, dtype=np.uint8)
+    row = rng.integers(0, 256, 96, dtype=np.uint8)
     words = row.view("<u4")
-    for lx in range(8, 48, 4):
-        for dx in range(-8, 9):
-            o, w = dx & 3, (dx - (dx & 3)) // 4
-            i = lx // 4 + w
-            lo64 = np.uint64(words[i]) | (np.uint64(words[i + 1]) << np.uint64(32)) if o else np.uint64(words[i])
-            v = u32((int(lo64) >> (8 * o)) & 0xFFFFFFFF)          # __funnelshift_r(row[w], row[w+1], 8 o)
-            l, h = byte_perm(v, 0, 0x4140), byte_perm(v, 0, 0x4342)
-            cells = [int(l) & 0xFFFF, int(l) >> 16, int(h) & 0xFFFF, int(h) >> 16]
-            assert cells == row[lx + dx:lx + dx + 4].tolist()
-            assert int(byte_perm(l, h, 0x6420)) == int(v)         # q4_pack_u8 undoes q4_bytes
+    for lx in range(16, 64, 4):
+        for dx in range(-16, 17):
+            lo, hi = tap4(words, lx, dx)
+            cells = [int(lo) & 0xFFFF, int(hi) & 0xFFFF, int(lo) >> 16, int(hi) >> 16]
+            assert cells == row[lx + dx:lx + dx + 4].tolist(), (lx, dx)
+            v = words[(lx + dx) // 4] if dx % 4 == 0 else None
+            if v is not None:                                     # q4_pack_u8 undoes q4_bytes
+                assert int(byte_perm(lo, hi, 0x6240)) == int(v)
 
 
 def test_life_takes_the_packed_form(M):
