@@ -128,11 +128,14 @@ int ma_getPairedCells(void);
 /* Flow accumulations (spreadScan) of integer water over more than 64 K cells
  * and at most `cells` cells run as pointer jumping over the Euler tour of the
  * D8 forest: about log2(2N) rounds whatever the length of the longest flow
- * path, O(N log N) work. Larger rasters walk the flow paths (O(N) work, one
- * atomic step per cell of the longest path). Results are identical (integer
- * sums). cells < 0 restores the default (2^21, or MAP_B200_SPREAD_PJ), 0 never
- * jumps. A direction raster with a cycle makes the jumping form fail with an
- * error. Engine option with no counterpart in the reference. */
+ * path, O(N log N) work. Other rasters walk the flow paths (O(N) work, one
+ * atomic step per cell of the longest path), which is faster for a whole
+ * raster on an idle GPU; serving windows above 64 K cells always jump (they
+ * run beside other requests, where the fixed rounds cut the latency tail).
+ * Results are identical (integer sums). cells < 0 restores the default (0, or
+ * MAP_B200_SPREAD_PJ), 0 never jumps. A direction raster with a cycle makes the
+ * jumping form fail with an error. Engine option with no counterpart in the
+ * reference. */
 void ma_setFlowJumpCells(long long cells);
 long long ma_getFlowJumpCells(void);
 /* Algebraic rewrite of hillshade compositions (python/hill.py:41-49):

@@ -1645,6 +1645,99 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   else
     wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
   wrap << "}\n";
+  if (use_tma) {
+    // Pipelined form (KNAME_p): a grid of resident CTAs walks the tiles with
+    // stride gridDim.x, two staging buffers, the copy of the tile after next
+    // issued as soon as a buffer is free, so a tile's copy lands while the one
+    // before it computes. Same cells, same operations as one tile per CTA.
+    size_t total = 0;
+    for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
+    int align_e = 1;
+    for (auto &t : P.tma) align_e = std::max(align_e, 16 / (int)dt_size(t.dtype));
+    const size_t stage = (bar_off + 127) / 128 * 128;
+    P.smem_pipe = 2 * stage + 16;
+    wrap << "__device__ __forceinline__ bool tile_staged(const Args &a, const Tile &t, bool &inner) {\n"
+         << "  inner = tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ");\n"
+         << "  return t.x0 % " << align_e << " == 0 && (inner || edge_staging(a.g));\n"
+         << "}\n"
+         << "__device__ __forceinline__ void issue_tile(const Args &a, int tile, unsigned char *buf, u64 *bar) {\n"
+         << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
+         << "  bool inner;\n"
+         << "  if (!tile_staged(a, t, inner)) return;\n"
+         << "  fence_proxy_async();\n"
+         << "  mbar_arrive_expect_tx(bar, " << total << "u);\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      wrap << "  tma_load_2d(buf + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
+           << " - a.g.oy);\n";
+    }
+    wrap << "}\n"
+         << "__device__ __forceinline__ bool compute_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 parity,\n"
+         << "                                             bool &used) {\n"
+         << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
+         << "  bool inner;\n"
+         << "  used = tile_staged(a, t, inner);\n"
+         << "  if (used) {\n"
+         << "    if (!mbar_wait_bounded(bar, parity, 1u << 26)) { skel_fail(a.err, ERR_TMA_TIMEOUT); return false; }\n"
+         << "    if (!inner) {\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      std::string ty = dt_ctype(t.dtype);
+      wrap << "      stage_fix_border<" << ty << ", " << t.box_w << ", " << t.box_h << ">((" << ty << " *)(smem + " << t.smem_off
+           << "), a.g, t.x0 - " << t.pad_x << ", t.y0 - " << hy << ", " << hx << ", " << hy << ");\n";
+    }
+    wrap << "      __syncthreads();\n"
+         << "    }\n";
+    for (int k = 0; k < nst; k++) {
+      auto &t = P.tma[k];
+      std::string ty = dt_ctype(t.dtype);
+      wrap << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
+           << " *)(smem + " << t.smem_off << ")};\n";
+    }
+    wrap << "    if (inner) {\n" << loop_full.str() << "    } else {\n" << loop.str() << "    }\n"
+         << "    return true;\n  }\n  {\n";
+    for (int k = 0; k < nst; k++) {
+      std::string ty = G.T(staged_nodes[k]);
+      wrap << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
+    }
+    wrap << loop.str() << "  }\n  return true;\n}\n";
+    wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT;
+    if (tune.minb > 0) wrap << ", " << tune.minb;
+    wrap << ") KNAME_p(const __grid_constant__ Args a) {\n"
+         << "  extern __shared__ __align__(128) unsigned char smem[];\n"
+         << "  unsigned char *buf0 = smem, *buf1 = smem + " << stage << ";\n"
+         << "  u64 *bar = (u64 *)(smem + " << 2 * stage << ");\n"
+         << "  if (threadIdx.x == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); fence_mbar_init(); }\n"
+         << "  __syncthreads();\n"
+         << "  const int n = a.g.tiles, G = (int)gridDim.x;\n"
+         << "  if (threadIdx.x == 0) {\n"
+         << "    if ((int)blockIdx.x < n) issue_tile(a, (int)blockIdx.x, buf0, &bar[0]);\n"
+         << "    if ((int)blockIdx.x + G < n) issue_tile(a, (int)blockIdx.x + G, buf1, &bar[1]);\n"
+         << "  }\n"
+         << "  u32 ph0 = 0, ph1 = 0;\n"
+         << "  int i = 0;\n"
+         << "  for (int tile = (int)blockIdx.x; tile < n; tile += G, i++) {\n"
+         << "    const int s = i & 1;\n"
+         << "    bool used = false;\n"
+         << "    const u32 par = s ? ph1 : ph0;\n"
+         << "    const bool ok = compute_tile(a, tile, s ? buf1 : buf0, &bar[s], par, used);\n"
+         << "    if (used) { if (s) ph1 ^= 1u; else ph0 ^= 1u; }\n"
+         // every thread is done with buffer s (and a failed wait ends the CTA, after
+         // a bounded wait for the copy still in flight into the other buffer)
+         << "    if (__syncthreads_or(!ok)) {\n"
+         << "      if (threadIdx.x == 0) {\n"
+         << "        if (used) mbar_wait_bounded(&bar[s], par, 1u << 26);\n"
+         << "        const int nx = tile + G;\n"
+         << "        bool in2;\n"
+         << "        if (nx < n && tile_staged(a, tile_of<" << TW << ", " << TH << ">(a.g, nx), in2))\n"
+         << "          mbar_wait_bounded(&bar[s ^ 1], s ? ph0 : ph1, 1u << 26);\n"
+         << "      }\n"
+         << "      return;\n"
+         << "    }\n"
+         << "    if (threadIdx.x == 0 && tile + 2 * G < n) issue_tile(a, tile + 2 * G, s ? buf1 : buf0, &bar[s]);\n"
+         << "  }\n"
+         << "}\n";
+  }
   if (!use_tma) P.tma.clear();
 }
 
@@ -2365,6 +2458,7 @@ const FocalTune &focal_tune() {
         else if (k == "qtw") r.qtw = v;
         else if (k == "qth") r.qth = v;
         else if (k == "minb") r.minb = v;
+        else if (k == "pipe") r.pipe = v;
       }
       i = j + 1;
     }

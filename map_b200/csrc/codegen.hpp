@@ -54,6 +54,7 @@ struct KernelPlan {
   int tile_w = 64, tile_h = 32;
   int halo_x = 0, halo_y = 0;
   size_t smem_bytes = 0;
+  size_t smem_pipe = 0;     // Focal: dynamic shared memory of the pipelined kernel KNAME_p (0: none)
   int aux_count = 0;
   // radial / spreading specifics
   Node *core = nullptr;
@@ -72,6 +73,7 @@ struct FocalTune {
   int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
   int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
   int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
+  int pipe = -1;                    // focal kernels: pipelined form (1), one tile per CTA (0), built-in choice (-1)
 };
 const FocalTune &focal_tune();
 

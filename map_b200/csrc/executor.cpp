@@ -324,6 +324,14 @@ Executor &Executor::get() {
   return e;
 }
 
+// Whether a focal launch over `tiles` tiles uses the pipelined kernel (MAP_B200_FOCAL_TUNE pipe=0/1 forces it).
+bool focal_pipelined(int tiles) {
+  const FocalTune &ft = focal_tune();
+  if (ft.pipe >= 0) return ft.pipe == 1;
+  (void)tiles;
+  return false;
+}
+
 Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const std::set<Node *> &tset, bool compile) {
   Prepared P;
   P.order = collect(targets);
@@ -597,6 +605,13 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
       env.launch(kh, grid, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
       z.slots += grid;
       (void)nz;
+    } else if (g.skeleton == SK_FOCAL && K.smem_pipe > 0 && focal_pipelined(tiles)) {
+      // pipelined focal kernel: resident CTAs walk the tiles with two staging buffers
+      KernelHandle kp = env.kernel(K.source, K.kname + "_p", K.smem_pipe);
+      const int per_sm = std::max(1, env.occupancy(kp, K.threads, K.smem_pipe));
+      const int grid = std::min(tiles, env.sm_count() * per_sm);
+      auto a = build_args(g, K, rx0, ry0, rx1, ry1, 0, 0);
+      env.launch(kp, grid, K.threads, K.smem_pipe, (CUstream_st *)st, a.data(), a.size());
     } else {
       auto a = build_args(g, K, rx0, ry0, rx1, ry1, 0, 0);
       env.launch(kh, tiles, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
