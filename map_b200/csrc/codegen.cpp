@@ -619,8 +619,10 @@ struct Gen {
     const int hx = f.xc->halo_x(), hy = f.xc->halo_y(), mw = f.xc->mask_ds.arr[0];
     const std::string fk = "f" + std::to_string(staged.at(f.in));
     std::ostringstream s;
+    // the tap object by value: a reference would take its address and keep it
+    // (and the loop's loads of its pointer) in local memory
     s << "template <class F>\n__device__ __noinline__ float shade_cell_slow" << i << "("
-      << (shade_reads_args(i) ? "const Args &a, " : "") << "const F &" << fk << ", int x, int y, int lx, int ly) {\n";
+      << (shade_reads_args(i) ? "const Args &a, " : "") << "const F " << fk << ", int x, int y, int lx, int ly) {\n";
     for (int c = 0; c < 2; c++) {
       Node *cv = c ? f.yc : f.xc;
       const std::string acc = c ? "yl" : "xl";
@@ -1433,7 +1435,10 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   // Float-heavy bodies, and bodies with a rewritten shading composition, compute
   // the cells of two consecutive rows together (PR<T> pairs: packed f32x2
   // arithmetic, one issue slot for both cells).
-  const bool pair = (heavy || !G.shades.empty()) && rows % 2 == 0 && Runtime::get().paired_cells && G.pairable();
+  // (the fast shading form runs one cell at a time: paired it measured no faster,
+  // 434 against 437 Gcells/s on the 16384^2 hillshade)
+  const bool pair = (heavy || (!G.shades.empty() && !G.any_fast())) && rows % 2 == 0 && Runtime::get().paired_cells &&
+                    G.pairable();
   if (pair) {
     body << "template <";
     for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
@@ -1550,6 +1555,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
               << "      " << (pair ? call2.str() : call.str()) << ";\n"
               << "    }\n";
   }
+  std::string loop_edge;   // staged edge tiles (default: the one-cell loop)
   if (quad) {
     // thread t: cells 4 (t % qw) .. + 3 of rows (t / qw) * qrows .. + qrows - 1;
     // outputs whose rows are not 4-byte aligned take the one-cell form
@@ -1574,6 +1580,28 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       << "        }\n"
       << "    }\n";
     loop_full.str(q.str());
+    // staged edge tiles: whole quads inside the region in the packed form, the
+    // cells of a quad that crosses the region's end one at a time
+    std::ostringstream e;
+    e << "    const int lx = 4 * (threadIdx.x % " << qw << "), ly0 = (threadIdx.x / " << qw << ") * " << qrows << ";\n"
+      << "    const int x = t.x0 + lx;\n"
+      << "    const bool al = " << G.quad_aligned() << ";\n"
+      << "#pragma unroll\n"
+      << "    for (int k = 0; k < " << qrows << "; k++) {\n"
+      << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
+      << "      if (y >= t.ye) continue;\n"
+      << "      if (al && x + 3 < t.xe) {\n"
+      << "        focal_cell4(a";
+    for (int k = 0; k < nst; k++) e << ", f" << k;
+    e << ", x, y, lx, ly);\n"
+      << "      } else {\n"
+      << "        for (int c = 0; c < 4; c++)\n"
+      << "          if (x + c < t.xe) focal_cell(a";
+    for (int k = 0; k < nst; k++) e << ", f" << k;
+    e << ", x + c, y, lx + c, ly);\n"
+      << "      }\n"
+      << "    }\n";
+    loop_edge = e.str();
   }
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
   body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
@@ -1582,15 +1610,15 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   if (use_tma) {
     size_t total = 0;
     for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
-    // interior tiles, and edge tiles whose out-of-raster halo has one value per
-    // cell, are staged by TMA (zero fill outside the map, then the border rule)
-    // a tiled TMA copy must start on a 16-byte boundary in x: tiles whose origin is
-    // not a multiple of the staged types' alignment (plain-mode blocks of odd
-    // widths) take the gather path
+    // interior and edge tiles are staged by TMA (zero fill outside the map, then
+    // the border rule: dead, raster mirror, or the raster mirror plus the
+    // block-mirror exceptions recomputed afterwards); a tiled TMA copy must start
+    // on a 16-byte boundary in x: tiles whose origin is not a multiple of the
+    // staged types' alignment (plain-mode blocks of odd widths) take the gather path
     int align_e = 1;
     for (auto &t : P.tma) align_e = std::max(align_e, 16 / (int)dt_size(t.dtype));
     body << "  const bool inner = tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ");\n"
-         << "  if (t.x0 % " << align_e << " == 0 && (inner || edge_staging(a.g))) {\n"
+         << "  if (t.x0 % " << align_e << " == 0) {\n"
          << "    __syncthreads();   // earlier readers of the staging buffer are done\n"
          << "    if (threadIdx.x == 0) {\n"
          << "      fence_proxy_async();\n";
@@ -1623,7 +1651,39 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       body << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
            << " *)(smem + " << t.smem_off << ")};\n";
     }
-    body << "    if (inner) {\n" << loop_full.str() << "    } else {\n" << loop.str() << "    }\n"
+    if (loop_edge.empty()) loop_edge = loop.str();
+    // block-mirror exceptions of staged edge tiles, recomputed by the same
+    // threads (after their own stores of the same cells) from global memory
+    {
+      std::ostringstream fx;
+      fx << "      if (block_fixup(a.g)) {\n";
+      for (int k = 0; k < nst; k++) {
+        std::string ty = G.T(staged_nodes[k]);
+        fx << "        const GatherTap<" << ty << "> g" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
+      }
+      std::string call1 = "focal_cell(a";
+      for (int k = 0; k < nst; k++) call1 += ", g" + std::to_string(k);
+      if (quad) {
+        fx << "        const int lx = 4 * (threadIdx.x % " << qw << "), ly0 = (threadIdx.x / " << qw << ") * " << qrows << ";\n"
+           << "        for (int k = 0; k < " << qrows << "; k++)\n"
+           << "          for (int c = 0; c < 4; c++) {\n"
+           << "            const int x = t.x0 + lx + c, y = t.y0 + ly0 + k;\n"
+           << "            if (x < t.xe && y < t.ye && block_exception(a.g, x, y, " << hx << ", " << hy << "))\n"
+           << "              " << call1 << ", x, y, lx + c, ly0 + k);\n"
+           << "          }\n";
+      } else {
+        fx << "        const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
+           << "        const int x = t.x0 + lx;\n"
+           << "        for (int k = 0; k < " << rows << "; k++) {\n"
+           << "          const int y = t.y0 + ly0 + k;\n"
+           << "          if (x < t.xe && y < t.ye && block_exception(a.g, x, y, " << hx << ", " << hy << "))\n"
+           << "            " << call1 << ", x, y, lx, ly0 + k);\n"
+           << "        }\n";
+      }
+      fx << "      }\n";
+      loop_edge += fx.str();
+    }
+    body << "    if (inner) {\n" << loop_full.str() << "    } else {\n" << loop_edge << "    }\n"
          << "    return true;\n  }\n";
   }
   body << "  {\n";
@@ -1645,99 +1705,6 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   else
     wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
   wrap << "}\n";
-  if (use_tma) {
-    // Pipelined form (KNAME_p): a grid of resident CTAs walks the tiles with
-    // stride gridDim.x, two staging buffers, the copy of the tile after next
-    // issued as soon as a buffer is free, so a tile's copy lands while the one
-    // before it computes. Same cells, same operations as one tile per CTA.
-    size_t total = 0;
-    for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
-    int align_e = 1;
-    for (auto &t : P.tma) align_e = std::max(align_e, 16 / (int)dt_size(t.dtype));
-    const size_t stage = (bar_off + 127) / 128 * 128;
-    P.smem_pipe = 2 * stage + 16;
-    wrap << "__device__ __forceinline__ bool tile_staged(const Args &a, const Tile &t, bool &inner) {\n"
-         << "  inner = tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ");\n"
-         << "  return t.x0 % " << align_e << " == 0 && (inner || edge_staging(a.g));\n"
-         << "}\n"
-         << "__device__ __forceinline__ void issue_tile(const Args &a, int tile, unsigned char *buf, u64 *bar) {\n"
-         << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
-         << "  bool inner;\n"
-         << "  if (!tile_staged(a, t, inner)) return;\n"
-         << "  fence_proxy_async();\n"
-         << "  mbar_arrive_expect_tx(bar, " << total << "u);\n";
-    for (int k = 0; k < nst; k++) {
-      auto &t = P.tma[k];
-      wrap << "  tma_load_2d(buf + " << t.smem_off << ", &a.tm[" << k << "], bar, t.x0 - " << t.pad_x << ", t.y0 - " << hy
-           << " - a.g.oy);\n";
-    }
-    wrap << "}\n"
-         << "__device__ __forceinline__ bool compute_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 parity,\n"
-         << "                                             bool &used) {\n"
-         << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n"
-         << "  bool inner;\n"
-         << "  used = tile_staged(a, t, inner);\n"
-         << "  if (used) {\n"
-         << "    if (!mbar_wait_bounded(bar, parity, 1u << 26)) { skel_fail(a.err, ERR_TMA_TIMEOUT); return false; }\n"
-         << "    if (!inner) {\n";
-    for (int k = 0; k < nst; k++) {
-      auto &t = P.tma[k];
-      std::string ty = dt_ctype(t.dtype);
-      wrap << "      stage_fix_border<" << ty << ", " << t.box_w << ", " << t.box_h << ">((" << ty << " *)(smem + " << t.smem_off
-           << "), a.g, t.x0 - " << t.pad_x << ", t.y0 - " << hy << ", " << hx << ", " << hy << ");\n";
-    }
-    wrap << "      __syncthreads();\n"
-         << "    }\n";
-    for (int k = 0; k < nst; k++) {
-      auto &t = P.tma[k];
-      std::string ty = dt_ctype(t.dtype);
-      wrap << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
-           << " *)(smem + " << t.smem_off << ")};\n";
-    }
-    wrap << "    if (inner) {\n" << loop_full.str() << "    } else {\n" << loop.str() << "    }\n"
-         << "    return true;\n  }\n  {\n";
-    for (int k = 0; k < nst; k++) {
-      std::string ty = G.T(staged_nodes[k]);
-      wrap << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
-    }
-    wrap << loop.str() << "  }\n  return true;\n}\n";
-    wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT;
-    if (tune.minb > 0) wrap << ", " << tune.minb;
-    wrap << ") KNAME_p(const __grid_constant__ Args a) {\n"
-         << "  extern __shared__ __align__(128) unsigned char smem[];\n"
-         << "  unsigned char *buf0 = smem, *buf1 = smem + " << stage << ";\n"
-         << "  u64 *bar = (u64 *)(smem + " << 2 * stage << ");\n"
-         << "  if (threadIdx.x == 0) { mbar_init(&bar[0], 1); mbar_init(&bar[1], 1); fence_mbar_init(); }\n"
-         << "  __syncthreads();\n"
-         << "  const int n = a.g.tiles, G = (int)gridDim.x;\n"
-         << "  if (threadIdx.x == 0) {\n"
-         << "    if ((int)blockIdx.x < n) issue_tile(a, (int)blockIdx.x, buf0, &bar[0]);\n"
-         << "    if ((int)blockIdx.x + G < n) issue_tile(a, (int)blockIdx.x + G, buf1, &bar[1]);\n"
-         << "  }\n"
-         << "  u32 ph0 = 0, ph1 = 0;\n"
-         << "  int i = 0;\n"
-         << "  for (int tile = (int)blockIdx.x; tile < n; tile += G, i++) {\n"
-         << "    const int s = i & 1;\n"
-         << "    bool used = false;\n"
-         << "    const u32 par = s ? ph1 : ph0;\n"
-         << "    const bool ok = compute_tile(a, tile, s ? buf1 : buf0, &bar[s], par, used);\n"
-         << "    if (used) { if (s) ph1 ^= 1u; else ph0 ^= 1u; }\n"
-         // every thread is done with buffer s (and a failed wait ends the CTA, after
-         // a bounded wait for the copy still in flight into the other buffer)
-         << "    if (__syncthreads_or(!ok)) {\n"
-         << "      if (threadIdx.x == 0) {\n"
-         << "        if (used) mbar_wait_bounded(&bar[s], par, 1u << 26);\n"
-         << "        const int nx = tile + G;\n"
-         << "        bool in2;\n"
-         << "        if (nx < n && tile_staged(a, tile_of<" << TW << ", " << TH << ">(a.g, nx), in2))\n"
-         << "          mbar_wait_bounded(&bar[s ^ 1], s ? ph0 : ph1, 1u << 26);\n"
-         << "      }\n"
-         << "      return;\n"
-         << "    }\n"
-         << "    if (threadIdx.x == 0 && tile + 2 * G < n) issue_tile(a, tile + 2 * G, s ? buf1 : buf0, &bar[s]);\n"
-         << "  }\n"
-         << "}\n";
-  }
   if (!use_tma) P.tma.clear();
 }
 
@@ -2458,13 +2425,20 @@ const FocalTune &focal_tune() {
         else if (k == "qtw") r.qtw = v;
         else if (k == "qth") r.qth = v;
         else if (k == "minb") r.minb = v;
-        else if (k == "pipe") r.pipe = v;
       }
       i = j + 1;
     }
     return r;
   }();
   return t;
+}
+
+bool focal_fast_shade(const Group &g) {
+  if (g.skeleton != SK_FOCAL) return false;
+  KernelPlan P;
+  Gen G(g, P);
+  G.classify();
+  return G.any_fast();
 }
 
 bool focal_quad_form(const Group &g) {

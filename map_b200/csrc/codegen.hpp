@@ -33,6 +33,8 @@ bool tile_cfg_valid(const TileCfg &c);
 // Whether a focal group's interior tiles compute four byte cells of a row per
 // thread step (packed 16-bit lanes; integer bodies on byte rasters).
 bool focal_quad_form(const Group &g);
+// Whether a focal group holds a hillshade composition in the fast rewritten form.
+bool focal_fast_shade(const Group &g);
 
 struct KernelPlan {
   int skeleton = SK_LOCAL;
@@ -54,7 +56,6 @@ struct KernelPlan {
   int tile_w = 64, tile_h = 32;
   int halo_x = 0, halo_y = 0;
   size_t smem_bytes = 0;
-  size_t smem_pipe = 0;     // Focal: dynamic shared memory of the pipelined kernel KNAME_p (0: none)
   int aux_count = 0;
   // radial / spreading specifics
   Node *core = nullptr;
@@ -73,7 +74,6 @@ struct FocalTune {
   int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
   int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
   int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
-  int pipe = -1;                    // focal kernels: pipelined form (1), one tile per CTA (0), built-in choice (-1)
 };
 const FocalTune &focal_tune();
 

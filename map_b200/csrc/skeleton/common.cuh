@@ -577,18 +577,29 @@ __device__ __forceinline__ bool focal_src(const Geom &g, int x, int y, int dx, i
   return true;
 }
 
-// Whether a tile at the raster edge can be staged like an interior one: its halo
-// cells outside the raster then hold the same value for every centre cell that
-// reads them (dead border: zero; raster mirror: the mirrored cell; block mirror:
-// only when the raster is one block, where it is the raster mirror).
-__device__ __forceinline__ bool edge_staging(const Geom &g) {
-  return g.border == 2 || g.border == 1 || (g.BS0 >= g.W && g.BS1 >= g.H);
+// Block mirror on a raster of several blocks: an out-of-raster tap takes the
+// raster mirror's value (what stage_fix_border writes) except where its other
+// coordinate crosses the reading cell's block boundary (the reference reflects
+// both coordinates inside the reading cell's block). That happens only for cells
+// within the halo of a raster edge and of a block boundary across it; staged
+// edge tiles recompute those cells from global memory afterwards.
+__device__ __forceinline__ bool block_fixup(const Geom &g) {
+  return g.border == 0 && !(g.BS0 >= g.W && g.BS1 >= g.H);
+}
+__device__ __forceinline__ bool block_exception(const Geom &g, int x, int y, int hx, int hy) {
+  const int bx = x % g.BS0, by = y % g.BS1;
+  const bool near_bx = bx < hx || bx >= g.BS0 - hx || x >= g.W - hx;
+  const bool near_by = by < hy || by >= g.BS1 - hy || y >= g.H - hy;
+  const bool edge_y = y < hy || y >= g.H - hy, edge_x = x < hx || x >= g.W - hx;
+  return (edge_y && near_bx) || (edge_x && near_by);
 }
 
 // After a staged box of an edge tile has landed (raster cell (ox + bx, oy + by) at
 // s[by * SW + bx]), overwrites its cells outside the raster that a centre cell can
-// reach (within hx / hy of the edge) with the border rule's value. The sources
-// are inside the raster, so no cell is both read and written.
+// reach (within hx / hy of the edge) with the border rule's value: zero (dead) or
+// the cell mirrored at the raster edge (raster mirror; block mirror, whose
+// exceptions block_exception names). The sources are inside the raster, so no
+// cell is both read and written.
 template <class T, int SW, int SH>
 __device__ __forceinline__ void stage_fix_border(T *s, const Geom &g, int ox, int oy, int hx, int hy) {
   for (int i = threadIdx.x; i < SW * SH; i += blockDim.x) {

@@ -144,11 +144,14 @@ def test_sin_cos_pairs_share_sincosf(M):
 
 def test_paired_cells_codegen(M):
     """Float focal groups get the two-rows-per-step form (focal_cell2) unless it is
-    switched off; integer focal groups (life) keep one cell per step. Both forms
-    compile."""
+    switched off, except the fast rewritten hillshade (one cell per step);
+    integer focal groups on bytes (life) take the four-cell packed form. Every
+    form compiles."""
     from map_b200 import workloads as W
     dem = M.from_numpy(np.zeros((64, 64), np.float32), bs=[32, 32])
     try:
+        assert "focal_cell2" not in M.generated_source(W.hillshade(dem))     # fast form
+        M.set_algebraic_rewrite(2)
         hs = W.hillshade(dem)
         assert "focal_cell2" in M.generated_source(hs)
         assert M.compile_only(hs) == 1
@@ -159,8 +162,10 @@ def test_paired_cells_codegen(M):
         assert M.compile_only(hs) == 1
     finally:
         M.set_paired_cells(True)
+        M.set_algebraic_rewrite(1)
     grid = M.from_numpy(np.zeros((64, 64), np.uint8), bs=[32, 32])
-    assert "focal_cell2" not in M.generated_source(W.life(grid, 1))
+    src = M.generated_source(W.life(grid, 1))
+    assert "focal_cell2" not in src and "focal_cell4" in src
 
 
 def test_scan_kernel_forms_codegen(M):

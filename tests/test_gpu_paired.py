@@ -51,7 +51,9 @@ def same(a, b):
     assert not diff.any(), int(diff.sum())
 
 
-@pytest.mark.parametrize("rewrite", [True, False])
+# the fast rewritten form (mode 1, the default) runs one cell at a time; the
+# general rewritten form (2) and the literal chain (0) have pair forms
+@pytest.mark.parametrize("rewrite", [2, 0])
 @pytest.mark.parametrize("border", [0, 1, 2])
 def test_hillshade_paired_bit_identical(P, border, rewrite):
     M = P
@@ -118,6 +120,7 @@ def test_integer_and_boolean_outputs(P):
 def test_plain_mode_blocks(P, bs):
     M = P
     M.set_exec_mode(M.EXEC_PLAIN)
+    M.set_algebraic_rewrite(2)
     dem = synth.fbm_dem(333, 517, seed=8)
     a, b = both(M, lambda: W.hillshade(M.from_numpy(dem, bs=bs)))
     same(a, b)
