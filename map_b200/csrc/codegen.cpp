@@ -620,7 +620,7 @@ struct Gen {
     const std::string fk = "f" + std::to_string(staged.at(f.in));
     std::ostringstream s;
     // the tap object by value: a reference would take its address and keep it
-    // (and the loop's loads of its pointer) in local memory
+    // (and the row loop's loads of its pointer) in local memory
     s << "template <class F>\n__device__ __noinline__ float shade_cell_slow" << i << "("
       << (shade_reads_args(i) ? "const Args &a, " : "") << "const F " << fk << ", int x, int y, int lx, int ly) {\n";
     for (int c = 0; c < 2; c++) {
@@ -1364,8 +1364,11 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
        << "  }\n"
        << "  return true;\n"
        << "}\n";
+  // launched as a dependent launch: no global access before griddep_wait
   wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  u32 phase = 0;\n"
+       << "  griddep_launch();\n"
+       << "  griddep_wait();\n"
        << "  run_tile(a, blockIdx.x, nullptr, nullptr, phase, false);\n"
        << "}\n";
 }
@@ -1697,13 +1700,19 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   wrap << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  extern __shared__ __align__(128) unsigned char smem[];\n"
        << "  u32 phase = 0;\n";
+  // launched as a dependent launch: the barrier set-up overlaps the previous
+  // kernel's last CTAs, and no global access comes before griddep_wait
   if (use_tma)
     wrap << "  u64 *bar = (u64 *)(smem + " << bar_off << ");\n"
          << "  if (threadIdx.x == 0) { mbar_init(bar, 1); fence_mbar_init(); }\n"
+         << "  griddep_launch();\n"
          << "  __syncthreads();\n"
+         << "  griddep_wait();\n"
          << "  run_tile(a, blockIdx.x, smem, bar, phase, false);\n";
   else
-    wrap << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
+    wrap << "  griddep_launch();\n"
+         << "  griddep_wait();\n"
+         << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
   wrap << "}\n";
   if (!use_tma) P.tma.clear();
 }
@@ -2425,6 +2434,7 @@ const FocalTune &focal_tune() {
         else if (k == "qtw") r.qtw = v;
         else if (k == "qth") r.qth = v;
         else if (k == "minb") r.minb = v;
+        else if (k == "pdl") r.pdl = v;
       }
       i = j + 1;
     }

@@ -74,6 +74,7 @@ struct FocalTune {
   int lnt = 0, ltw = 0, lth = 0;   // the same for standalone Local kernels
   int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
   int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
+  int pdl = 1;                      // Local / Focal kernels as programmatic dependent launches (0: plain launches)
 };
 const FocalTune &focal_tune();
 

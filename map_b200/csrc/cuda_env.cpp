@@ -270,6 +270,33 @@ void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CU
   launches_++;
 }
 
+// A launch that may begin while the previous kernel of the stream is still
+// running (programmatic dependent launch): its CTAs become resident as the
+// previous grid's CTAs exit and run their prologue; the kernel must execute
+// griddepcontrol.wait (map_common.cuh griddep_wait) before it touches global
+// memory, which waits for the previous grid to complete and its writes to be
+// visible. Used for the generated Local / Focal kernels, which all do.
+void CudaEnv::launch_pdl(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args) {
+  if (grid <= 0) return;
+  void *params[] = {args};
+  CUlaunchAttribute attr;
+  attr.id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
+  attr.value.programmaticStreamSerializationAllowed = 1;
+  CUlaunchConfig cfg = {};
+  cfg.gridDimX = (unsigned)grid;
+  cfg.gridDimY = 1;
+  cfg.gridDimZ = 1;
+  cfg.blockDimX = (unsigned)block;
+  cfg.blockDimY = 1;
+  cfg.blockDimZ = 1;
+  cfg.sharedMemBytes = (unsigned)smem;
+  cfg.hStream = reinterpret_cast<CUstream>(stream);
+  cfg.attrs = &attr;
+  cfg.numAttrs = 1;
+  drv_check(g_drv.launchKernelEx(&cfg, reinterpret_cast<CUfunction>(k.fn), params, nullptr), "cuLaunchKernelEx");
+  launches_++;
+}
+
 // A launch whose CTAs form 1-D thread-block clusters of `cluster` CTAs (grid a
 // multiple of it): the CTAs of a cluster run at once on one GPC and share
 // their shared memory.

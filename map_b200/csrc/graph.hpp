@@ -103,6 +103,7 @@ struct Runtime {
   // f32x2 instructions (bit-identical to one cell at a time); 0 turns it off.
   int paired_cells = 1;
   long long flow_jump_cells = -1;   // < 0: the default limit of pointer-jumping flow accumulation
+  int dependent_launch = 1;           // Local / Focal kernels as programmatic dependent launches
   // Hillshade compositions (python/hill.py:41-49) are generated through the
   // shading identity of rewrite.hpp; 0 keeps the literal operator chain; 2 uses
   // the identity without its fast form (derivatives computed as written).

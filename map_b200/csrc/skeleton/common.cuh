@@ -737,6 +737,16 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   }
 };
 
+// ------------------------------------------------------------------ dependent launches
+
+// Programmatic dependent launch: a kernel launched with it may start before the
+// previous kernel of its stream has finished. griddep_launch lets the next
+// kernel's CTAs start as this grid's CTAs leave; griddep_wait blocks until the
+// previous grid has completed and its memory is visible (immediately when the
+// launch had no such dependency). Every global access comes after the wait.
+__device__ __forceinline__ void griddep_launch() { asm volatile("griddepcontrol.launch_dependents;" ::: "memory"); }
+__device__ __forceinline__ void griddep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // ------------------------------------------------------------------ TMA + mbarrier
 
 __device__ __forceinline__ u32 smem_u32(const void *p) { return (u32)__cvta_generic_to_shared(p); }
