@@ -1440,8 +1440,8 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   // arithmetic, one issue slot for both cells).
   // (the fast shading form runs one cell at a time: paired it measured no faster,
   // 434 against 437 Gcells/s on the 16384^2 hillshade)
-  const bool pair = (heavy || (!G.shades.empty() && !G.any_fast())) && rows % 2 == 0 && Runtime::get().paired_cells &&
-                    G.pairable();
+  const bool pair = (heavy || (!G.shades.empty() && (!G.any_fast() || focal_tune().fpair))) && rows % 2 == 0 &&
+                    Runtime::get().paired_cells && G.pairable();
   if (pair) {
     body << "template <";
     for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
@@ -2435,6 +2435,7 @@ const FocalTune &focal_tune() {
         else if (k == "qth") r.qth = v;
         else if (k == "minb") r.minb = v;
         else if (k == "pdl") r.pdl = v;
+        else if (k == "fpair") r.fpair = v;
       }
       i = j + 1;
     }

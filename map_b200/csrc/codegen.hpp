@@ -75,6 +75,7 @@ struct FocalTune {
   int qnt = 0, qtw = 0, qth = 0;   // the same for focal kernels of the packed byte form
   int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
   int pdl = 1;                      // Local / Focal kernels as programmatic dependent launches (0: plain launches)
+  int fpair = 0;                    // the fast hillshade form in the paired (f32x2) form as well
 };
 const FocalTune &focal_tune();
 

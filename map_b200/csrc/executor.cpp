@@ -337,12 +337,12 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
     // measured 1.5% faster than 256 threads on the hillshade and 2% on life
     TileCfg cfg;
     if (g->skeleton == SK_FOCAL && focal_quad_form(*g)) {
-      // packed byte form: 64 x 32 tiles of 128 threads, 16 quads per row and 8 rows
-      // per thread (measured on Life at 4096^2: 896 Gcell-updates/s, against 794
-      // for 128 x 32 and 875 for 128 x 16)
+      // packed byte form: 128 x 16 tiles of 128 threads, a warp on the 32 words of
+      // one tile row, 4 rows per thread (Life at 4096^2 with dependent launches:
+      // 1021 Gcell-updates/s, against 996 for 64 x 32 and 981 for 128 x 32 of 256)
       const FocalTune &ft = focal_tune();
-      cfg.tw = ft.qtw ? ft.qtw : 64;
-      cfg.th = ft.qth ? ft.qth : 32;
+      cfg.tw = ft.qtw ? ft.qtw : 128;
+      cfg.th = ft.qth ? ft.qth : 16;
       cfg.nt = ft.qnt ? ft.qnt : 128;
     } else if (g->skeleton == SK_FOCAL) {
       cfg.nt = 128;
