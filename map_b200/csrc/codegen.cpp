@@ -129,6 +129,13 @@ struct Gen {
   std::vector<ShadeFast> fast;
   // fast shading statements record non-finite cells in `bad` instead of branching
   mutable bool fast_flag = false;
+  // where the second cell of a pair lies: (x, y + 1) for row pairs, (x + 1, y)
+  // for column pairs
+  int pdx = 0, pdy = 1;
+  std::string x2() const { return pdx ? "x + 1" : "x"; }
+  std::string y2() const { return pdy ? "y + 1" : "y"; }
+  std::string lx2() const { return pdx ? "lx + 1" : "lx"; }
+  std::string ly2() const { return pdy ? "ly + 1" : "ly"; }
 
   Gen(const Group &g, KernelPlan &p) : g(g), plan(p) {}
 
@@ -161,7 +168,8 @@ struct Gen {
   std::string tap2(Node *in, int dx, int dy) const {
     auto s = staged.find(in);
     if (s == staged.end()) throw MapError("codegen: focal read of a raster that is not staged");
-    return "f" + std::to_string(s->second) + ".tap2(x, y, lx, ly, " + std::to_string(dx) + ", " + std::to_string(dy) + ")";
+    return "f" + std::to_string(s->second) + (pdx ? ".tap2c" : ".tap2") + "(x, y, lx, ly, " + std::to_string(dx) + ", " +
+           std::to_string(dy) + ")";
   }
 
   // One term acc = acc + tap * w of a float convolution. A zero weight gives an
@@ -260,8 +268,8 @@ struct Gen {
         s << decl << pt_ << "(" << var_literal(reference_literal_value(n->cnst)) << ");";
         break;
       case K_INDEX:
-        if (n->op == D1) s << decl << pt_ << "((" << t << ")(x), (" << t << ")(x));";
-        else s << decl << pt_ << "((" << t << ")(y), (" << t << ")(y + 1));";
+        if (n->op == D1) s << decl << pt_ << "((" << t << ")(x), (" << t << ")(" << x2() << "));";
+        else s << decl << pt_ << "((" << t << ")(y), (" << t << ")(" << y2() << "));";
         break;
       case K_CAST: case K_BARRIER:
         s << decl << pt_ << "(" << val(n->prev[0]) << ");";
@@ -375,8 +383,12 @@ struct Gen {
     std::ostringstream s;
     for (auto &kv : outk) {
       Node *o = kv.first;
-      s << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "));\n"
-        << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y + 1, lane1(" << val(o) << "));\n";
+      if (pdx)
+        s << "    str_out2x<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "), lane1(" << val(o)
+          << "));\n";
+      else
+        s << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y, lane0(" << val(o) << "));\n"
+          << "    str_out<" << T(o) << ">(a.out[" << kv.second << "], x, y + 1, lane1(" << val(o) << "));\n";
     }
     return s.str();
   }
@@ -404,7 +416,7 @@ struct Gen {
       if (staged.count(p)) s << "    const PR<" << t << "> i" << k << " = " << tap2(p, 0, 0) << ";\n";
       else
         s << "    const PR<" << t << "> i" << k << "(ldr<" << t << ">(a.in[" << k << "], x, y), ldr<" << t << ">(a.in[" << k
-          << "], x, y + 1));\n";
+          << "], " << x2() << ", " << y2() << "));\n";
     }
     return s.str();
   }
@@ -702,11 +714,10 @@ struct Gen {
       return s.str();
     }
     const std::string fk = "f" + std::to_string(staged.at(f.in));
-    auto slow_lane = [&](const std::string &lane, int dr) {
+    auto slow_lane = [&](const std::string &lane, int second) {
       const std::string sel = lane.empty() ? "" : "." + lane;
-      const std::string yo = dr ? " + " + std::to_string(dr) : "";
-      return " " + v + sel + " = shade_cell_slow" + si + "(" + (shade_reads_args(i) ? "a, " : "") + fk + ", x, y" + yo +
-             ", lx, ly" + yo + ");";
+      return " " + v + sel + " = shade_cell_slow" + si + "(" + (shade_reads_args(i) ? "a, " : "") + fk + ", " +
+             (second ? x2() + ", " + y2() + ", " + lx2() + ", " + ly2() : std::string("x, y, lx, ly")) + ");";
     };
     if (!pair) {
       s << " if (!(" << v << "_q < MAP_INF_F)) {" << slow_lane("", 0) << " }";
@@ -1442,6 +1453,23 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   // 434 against 437 Gcells/s on the 16384^2 hillshade)
   const bool pair = (heavy || (!G.shades.empty() && (!G.any_fast() || focal_tune().fpair))) && rows % 2 == 0 &&
                     Runtime::get().paired_cells && G.pairable();
+  // Column pairs: the two cells of a pair are (x, y) and (x + 1, y) of one row,
+  // so one 8-byte shared-memory load serves both cells' taps (tap2c) and their
+  // results leave in one 8-byte store; each thread then covers two columns and
+  // R = TH * TW / (2 NT) rows. For staged float inputs.
+  bool all_f32 = nst > 0;
+  for (Node *in : staged_nodes) all_f32 = all_f32 && in->meta.dtype == F32;
+  const int cw = TW / 2;
+  const bool cpair = pair && focal_tune().cpair && all_f32 && TW % 2 == 0 && cw <= NT && NT % cw == 0 && (TH * cw) % NT == 0;
+  if (cpair) {
+    G.pdx = 1;
+    G.pdy = 0;
+  }
+  const int R = cpair ? TH * cw / NT : rows;   // rows per thread
+  const std::string tmap = cpair ? "    const int lx = 2 * (threadIdx.x % " + std::to_string(cw) + "), ly0 = (threadIdx.x / " +
+                                       std::to_string(cw) + ") * " + std::to_string(R) + ";\n"
+                                 : "    const int lx = threadIdx.x % " + std::to_string(TW) + ", ly0 = (threadIdx.x / " +
+                                       std::to_string(TW) + ") * " + std::to_string(rows) + ";\n";
   if (pair) {
     body << "template <";
     for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
@@ -1466,15 +1494,15 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << ", int x, int y, int lx, int ly) {\n";
     body << G.center_loads4() << G.body4() << G.stores4() << "}\n";
   }
-  const bool full_unroll = tune.unroll ? tune.unroll >= rows : !heavy;
+  const bool full_unroll = tune.unroll ? tune.unroll >= R : !heavy;
   const std::string unroll = tune.unroll ? "#pragma unroll " + std::to_string(tune.unroll) + "\n"
                                          : heavy ? (pair ? "#pragma unroll 1\n" : "#pragma unroll 2\n") : "#pragma unroll\n";
-  const int step = pair ? 2 : 1;
+  const int step = pair && !cpair ? 2 : 1;
   // Interior tiles of a fully unrolled row loop keep the thread's results in
   // registers and store them after the last cell: no store then lies between
   // two loads of the same staged tap, which therefore load once per thread.
   const int nout = (int)G.outk.size();
-  const bool defer = tune.defer && full_unroll && nout > 0 && rows * nout <= 32;
+  const bool defer = tune.defer && full_unroll && nout > 0 && R * nout <= 32;
   // with fast shading compositions, interior tiles first compute their cells
   // recording only whether one needs the literal chain (flag form), and redo
   // the thread's cells with the per-cell checks when one did
@@ -1494,12 +1522,17 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       }
   }
   std::ostringstream loop, loop_full;
-  loop << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
+  loop << tmap
        << "    const int x = t.x0 + lx;\n"
        << unroll
-       << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+       << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
        << "      const int ly = ly0 + k, y = t.y0 + ly;\n";
-  if (pair)
+  if (cpair)
+    loop << "      if (y < t.ye) {\n"
+         << "        if (x + 1 < t.xe) " << call2.str() << ";\n"
+         << "        else if (x < t.xe) " << call.str() << ";\n"
+         << "      }\n";
+  else if (pair)
     loop << "      if (x < t.xe) {\n"
          << "        if (y + 1 < t.ye) " << call2.str() << ";\n"
          << "        else if (y < t.ye) " << call.str() << ";\n"
@@ -1508,8 +1541,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     loop << "      if (x < t.xe && y < t.ye) " << call.str() << ";\n";
   loop << "    }\n";
   // interior tiles are full: every cell of the tile is inside the raster
-  loop_full << "    const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
-            << "    const int x = t.x0 + lx;\n";
+  loop_full << tmap << "    const int x = t.x0 + lx;\n";
   if (defer) {
     std::ostringstream callr, outs;
     callr << (pair ? "focal_cell2r(a" : "focal_cellr(a");
@@ -1518,9 +1550,12 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     int k = 0;
     for (auto &kv : G.outk) {
       const std::string ty = G.T(kv.first);
-      loop_full << "    " << (pair ? "PR<" + ty + ">" : ty) << " r" << k << "[" << rows / step << "];\n";
+      loop_full << "    " << (pair ? "PR<" + ty + ">" : ty) << " r" << k << "[" << R / step << "];\n";
       callr << ", r" << k << "[k / " << step << "]";
-      if (pair)
+      if (cpair)
+        outs << "      str_out2x<" << ty << ">(a.out[" << kv.second << "], x, y, lane0(r" << k << "[k]), lane1(r" << k
+             << "[k]));\n";
+      else if (pair)
         outs << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y, lane0(r" << k << "[k / 2]));\n"
              << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y + 1, lane1(r" << k << "[k / 2]));\n";
       else
@@ -1534,26 +1569,26 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       cnc.insert(cnc.size() - 1, ", bad");
       loop_full << "    bool bad = false;\n"
                 << "#pragma unroll\n"
-                << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+                << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
                 << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
                 << "      " << cnc << ";\n"
                 << "    }\n"
                 << "    if (bad) {\n";
     }
     loop_full << "#pragma unroll\n"
-              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
               << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
               << "      " << callr.str() << ";\n"
               << "    }\n";
     if (flagged) loop_full << "    }\n";
     loop_full << "#pragma unroll\n"
-              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
               << "      const int y = t.y0 + ly0 + k;\n"
               << outs.str()
               << "    }\n";
   } else {
     loop_full << unroll
-              << "    for (int k = 0; k < " << rows << "; k += " << step << ") {\n"
+              << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
               << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
               << "      " << (pair ? call2.str() : call.str()) << ";\n"
               << "    }\n";
@@ -1674,8 +1709,16 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
            << "            if (x < t.xe && y < t.ye && block_exception(a.g, x, y, " << hx << ", " << hy << "))\n"
            << "              " << call1 << ", x, y, lx + c, ly0 + k);\n"
            << "          }\n";
+      } else if (cpair) {
+        fx << tmap
+           << "        for (int k = 0; k < " << R << "; k++)\n"
+           << "          for (int c = 0; c < 2; c++) {\n"
+           << "            const int x = t.x0 + lx + c, y = t.y0 + ly0 + k;\n"
+           << "            if (x < t.xe && y < t.ye && block_exception(a.g, x, y, " << hx << ", " << hy << "))\n"
+           << "              " << call1 << ", x, y, lx + c, ly0 + k);\n"
+           << "          }\n";
       } else {
-        fx << "        const int lx = threadIdx.x % " << TW << ", ly0 = (threadIdx.x / " << TW << ") * " << rows << ";\n"
+        fx << tmap
            << "        const int x = t.x0 + lx;\n"
            << "        for (int k = 0; k < " << rows << "; k++) {\n"
            << "          const int y = t.y0 + ly0 + k;\n"
@@ -2436,6 +2479,7 @@ const FocalTune &focal_tune() {
         else if (k == "minb") r.minb = v;
         else if (k == "pdl") r.pdl = v;
         else if (k == "fpair") r.fpair = v;
+        else if (k == "cpair") r.cpair = v;
       }
       i = j + 1;
     }

@@ -76,6 +76,7 @@ struct FocalTune {
   int minb = 0;                     // focal kernels: minimum resident CTAs per SM (register cap)
   int pdl = 1;                      // Local / Focal kernels as programmatic dependent launches (0: plain launches)
   int fpair = 0;                    // the fast hillshade form in the paired (f32x2) form as well
+  int cpair = 0;                    // pairs of cells (x, x + 1) of one row instead of (y, y + 1) of one column
 };
 const FocalTune &focal_tune();
 

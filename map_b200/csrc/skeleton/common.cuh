@@ -93,6 +93,22 @@ template <class T> __device__ __forceinline__ void str_out(const RasterArg &r, i
 template <> __device__ __forceinline__ void str_out<bool>(const RasterArg &r, int x, int y, bool v) {
   map_stg<1>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, v ? 1u : 0u);
 }
+// the cells (x, y) and (x + 1, y): one 8-byte store for 4-byte cells whose row
+// and x allow it (x even, base and pitch 8-byte aligned), else two stores
+template <class T> __device__ __forceinline__ void str_out2x(const RasterArg &r, int x, int y, T v0, T v1) {
+  if constexpr (sizeof(T) == 4) {
+    if (((r.p | (u64)r.pitch) & 7) == 0 && (x & 1) == 0) {
+      u32 a, b;
+      memcpy(&a, &v0, 4);
+      memcpy(&b, &v1, 4);
+      const u64 p = r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x * 4;
+      asm volatile("st.global.v2.u32 [%0], {%1, %2};" ::"l"(p), "r"(a), "r"(b));
+      return;
+    }
+  }
+  str_out<T>(r, x, y, v0);
+  str_out<T>(r, x + 1, y, v1);
+}
 
 // Lane j of a 16-byte vector of cells of type T, and its assignment.
 template <class T> __device__ __forceinline__ T vlane(const uint4 &v, int j) {
@@ -626,6 +642,10 @@ template <class T> struct GatherTap {
   __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
     return PR<T>(tap(x, y, lx, ly, dx, dy), tap(x, y + 1, lx, ly + 1, dx, dy));
   }
+  // the same tap of the cells (x, y) and (x + 1, y)
+  __device__ __forceinline__ PR<T> tap2c(int x, int y, int lx, int ly, int dx, int dy) const {
+    return PR<T>(tap(x, y, lx, ly, dx, dy), tap(x + 1, y, lx + 1, ly, dx, dy));
+  }
 };
 
 // Focal tap served from a tile staged in shared memory (interior tiles).
@@ -700,6 +720,13 @@ __device__ __forceinline__ void str_out_q4_u8(const RasterArg &r, int x, int y, 
   map_stg<4>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, q4_pack_u8(v));
 }
 
+// a 4-byte cell value carried in a float register, as its own type
+template <class T> __device__ __forceinline__ T __float_as_raw(float f) {
+  T r;
+  memcpy(&r, &f, sizeof(T));
+  return r;
+}
+
 template <class T, int SW, int PX, int HY> struct SmemTap {
   const T *s;
   __device__ __forceinline__ T tap(int x, int y, int lx, int ly, int dx, int dy) const {
@@ -707,6 +734,19 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   }
   __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
     return PR<T>(s[(ly + HY + dy) * SW + (lx + PX + dx)], s[(ly + 1 + HY + dy) * SW + (lx + PX + dx)]);
+  }
+  // The tap at (dx, dy) of the cells lx and lx + 1 of a row (4-byte cells, lx +
+  // PX and SW even): aligned pairs of the staged row, one 8-byte load each; an
+  // odd dx takes the second cell of one pair and the first of the next, so the
+  // three taps of a 3-wide window come from three loads for both cells.
+  __device__ __forceinline__ PR<T> tap2c(int x, int y, int lx, int ly, int dx, int dy) const {
+    static_assert(sizeof(T) == 4 && SW % 2 == 0 && PX % 2 == 0, "tap2c: 4-byte cells, even row stride and pad");
+    const float2 *row = (const float2 *)(s + (ly + HY + dy) * SW + lx + PX);
+    const int o = dx & 1, m = (dx - o) / 2;
+    const float2 p = row[m];
+    if (!o) return PR<T>(__float_as_raw<T>(p.x), __float_as_raw<T>(p.y));
+    const float2 q = row[m + 1];
+    return PR<T>(__float_as_raw<T>(p.y), __float_as_raw<T>(q.x));
   }
   // The taps at (dx, dy) of the byte cells lx .. lx + 3 (lx a multiple of 4, the
   // row stride SW and pad PX multiples of 4, |dx| <= PX), in the interleaved
