@@ -708,9 +708,12 @@ struct Gen {
     // (shade_cell_slow, a function of its own: no code in the unrolled row loop).
     // In the flag form the row loop only records that some cell needs it, and
     // recomputes the thread's cells with the checks when one did.
+    // (flag form: q is +0 or more, +inf or NaN; as unsigned bits it reaches
+    // 0x7f800000 exactly when it is not finite, so one unsigned maximum per cell
+    // records it)
     if (fast_flag) {
-      if (!pair) s << " bad |= !(" << v << "_q < MAP_INF_F);";
-      else s << " bad |= !(" << v << "_q.a < MAP_INF_F) | !(" << v << "_q.b < MAP_INF_F);";
+      if (!pair) s << " bad = max(bad, __float_as_uint(" << v << "_q));";
+      else s << " bad = max(bad, max(__float_as_uint(" << v << "_q.a), __float_as_uint(" << v << "_q.b)));";
       return s.str();
     }
     const std::string fk = "f" + std::to_string(staged.at(f.in));
@@ -1515,7 +1518,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
         body << ">\n__device__ __forceinline__ void " << (pf ? "focal_cell2r" : "focal_cellr") << (nc ? "_nc" : "")
              << "(const Args &a";
         for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
-        body << ", int x, int y, int lx, int ly" << G.out_params(pf) << (nc ? ", bool &bad" : "") << ") {\n";
+        body << ", int x, int y, int lx, int ly" << G.out_params(pf) << (nc ? ", u32 &bad" : "") << ") {\n";
         G.fast_flag = nc == 1;
         body << (pf ? G.center_loads2() + G.body2() : G.center_loads(false) + G.body(false)) << G.out_assigns() << "}\n";
         G.fast_flag = false;
@@ -1567,13 +1570,13 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       std::string cnc = callr.str();
       cnc.insert(cnc.find('('), "_nc");
       cnc.insert(cnc.size() - 1, ", bad");
-      loop_full << "    bool bad = false;\n"
+      loop_full << "    u32 bad = 0u;\n"
                 << "#pragma unroll\n"
                 << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
                 << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
                 << "      " << cnc << ";\n"
                 << "    }\n"
-                << "    if (bad) {\n";
+                << "    if (bad >= 0x7f800000u) {\n";
     }
     loop_full << "#pragma unroll\n"
               << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
