@@ -594,11 +594,13 @@ __device__ __forceinline__ bool focal_src(const Geom &g, int x, int y, int dx, i
 }
 
 // Block mirror on a raster of several blocks: an out-of-raster tap takes the
-// raster mirror's value (what stage_fix_border writes) except where its other
-// coordinate crosses the reading cell's block boundary (the reference reflects
-// both coordinates inside the reading cell's block). That happens only for cells
-// within the halo of a raster edge and of a block boundary across it; staged
-// edge tiles recompute those cells from global memory afterwards.
+// raster mirror's value (what stage_fix_border writes) except where the
+// reference's reflection inside the reading cell's block differs from it: the
+// tap's other coordinate crosses the reading cell's block boundary, or the tap
+// leaves the raster past the right / bottom edge from a block that is not the
+// last one, or from a last block narrower than the halo (the reflection inside
+// it is clamped). Only cells within the halo of a raster edge qualify; staged
+// edge tiles recompute them from global memory afterwards.
 __device__ __forceinline__ bool block_fixup(const Geom &g) {
   return g.border == 0 && !(g.BS0 >= g.W && g.BS1 >= g.H);
 }
@@ -607,7 +609,10 @@ __device__ __forceinline__ bool block_exception(const Geom &g, int x, int y, int
   const bool near_bx = bx < hx || bx >= g.BS0 - hx || x >= g.W - hx;
   const bool near_by = by < hy || by >= g.BS1 - hy || y >= g.H - hy;
   const bool edge_y = y < hy || y >= g.H - hy, edge_x = x < hx || x >= g.W - hx;
-  return (edge_y && near_bx) || (edge_x && near_by);
+  const int lastx = (g.W - 1) / g.BS0, lasty = (g.H - 1) / g.BS1;
+  const bool inner_last_x = x >= g.W - hx && (x / g.BS0 != lastx || g.W - lastx * g.BS0 < hx);
+  const bool inner_last_y = y >= g.H - hy && (y / g.BS1 != lasty || g.H - lasty * g.BS1 < hy);
+  return (edge_y && near_bx) || (edge_x && near_by) || inner_last_x || inner_last_y;
 }
 
 // After a staged box of an edge tile has landed (raster cell (ox + bx, oy + by) at

@@ -262,3 +262,20 @@ def test_hillshade_fast_form_equals_general_form(fresh, shape, bs, border):
         assert ("map_shade_fast" in M.generated_source(r)) == (mode == 1)
         out[mode] = M.to_numpy(r)
     assert np.array_equal(out[1].view(np.uint32), out[2].view(np.uint32))
+
+
+@pytest.mark.parametrize("shape,bs", [((47, 65), (16, 16)), ((50, 49), (8, 16)), ((34, 97), (32, 8)),
+                                      ((300, 257), (128, 128))])
+@pytest.mark.parametrize("border", [0, 1, 2])
+def test_wide_halo_edges_bit_exact(fresh, shape, bs, border):
+    """A 5 x 5 correlation on rasters whose last block is narrower than the halo
+    (the reference's in-block reflection clamps there): staged edge tiles plus
+    the recomputed block-mirror cells equal the oracle cell for cell."""
+    M = fresh
+    M.set_border(border)
+    rng = np.random.default_rng(44)
+    a = rng.integers(-50, 50, shape).astype(np.float32)
+    mask = rng.integers(-3, 4, (5, 5)).astype(np.float32)
+    got = M.to_numpy(M.convolve(M.from_numpy(a, bs=list(bs)), mask.tolist()))
+    ref = O.conv_f32(a, mask, bs, border)
+    assert np.array_equal(got, ref)
