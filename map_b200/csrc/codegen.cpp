@@ -712,8 +712,13 @@ struct Gen {
     // 0x7f800000 exactly when it is not finite, so one unsigned maximum per cell
     // records it)
     if (fast_flag) {
-      if (!pair) s << " bad = max(bad, __float_as_uint(" << v << "_q));";
-      else s << " bad = max(bad, max(__float_as_uint(" << v << "_q.a), __float_as_uint(" << v << "_q.b)));";
+      if (focal_tune().fflag) {
+        if (!pair) s << " bad = max(bad, __float_as_uint(" << v << "_q));";
+        else s << " bad = max(bad, max(__float_as_uint(" << v << "_q.a), __float_as_uint(" << v << "_q.b)));";
+      } else {
+        if (!pair) s << " bad |= !(" << v << "_q < MAP_INF_F) ? 0x7f800000u : 0u;";
+        else s << " bad |= (!(" << v << "_q.a < MAP_INF_F) | !(" << v << "_q.b < MAP_INF_F)) ? 0x7f800000u : 0u;";
+      }
       return s.str();
     }
     const std::string fk = "f" + std::to_string(staged.at(f.in));
@@ -2483,6 +2488,7 @@ const FocalTune &focal_tune() {
         else if (k == "pdl") r.pdl = v;
         else if (k == "fpair") r.fpair = v;
         else if (k == "cpair") r.cpair = v;
+        else if (k == "fflag") r.fflag = v;
       }
       i = j + 1;
     }

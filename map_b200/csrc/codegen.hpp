@@ -77,6 +77,7 @@ struct FocalTune {
   int pdl = 1;                      // Local / Focal kernels as programmatic dependent launches (0: plain launches)
   int fpair = 0;                    // the fast hillshade form in the paired (f32x2) form as well
   int cpair = 0;                    // pairs of cells (x, x + 1) of one row instead of (y, y + 1) of one column
+  int fflag = 1;                    // fast form's non-finite record: unsigned maximum (1) or comparison (0)
 };
 const FocalTune &focal_tune();
 
