@@ -708,9 +708,9 @@ struct Gen {
     // (shade_cell_slow, a function of its own: no code in the unrolled row loop).
     // In the flag form the row loop only records that some cell needs it, and
     // recomputes the thread's cells with the checks when one did.
-    // (flag form: q is +0 or more, +inf or NaN; as unsigned bits it reaches
-    // 0x7f800000 exactly when it is not finite, so one unsigned maximum per cell
-    // records it)
+    // (flag form: `bad` reaches 0x7f800000 when some cell's q is not finite;
+    // either by a comparison per cell, or, as q is +0 or more, +inf or NaN, by
+    // an unsigned maximum of its bits, measured 2.5% slower on the hillshade)
     if (fast_flag) {
       if (focal_tune().fflag) {
         if (!pair) s << " bad = max(bad, __float_as_uint(" << v << "_q));";
