@@ -1665,7 +1665,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     for (auto &t : P.tma) align_e = std::max(align_e, 16 / (int)dt_size(t.dtype));
     body << "  const bool inner = tile_interior<" << TW << ", " << TH << ">(a.g, t, " << hx << ", " << hy << ");\n"
          << "  if (t.x0 % " << align_e << " == 0) {\n"
-         << "    __syncthreads();   // earlier readers of the staging buffer are done\n"
+         << "    if (gdesc) __syncthreads();   // a persistent CTA: earlier readers of the staging buffer are done\n"
          << "    if (threadIdx.x == 0) {\n"
          << "      fence_proxy_async();\n";
     for (int k = 0; k < nst; k++) body << "      if (gdesc) tensormap_acquire(&a.tm[" << k << "]);\n";

@@ -545,9 +545,10 @@ __device__ __forceinline__ PR<float> map_shade(const PR<float> &x, const PR<floa
 __device__ __forceinline__ float map_shade_fast(float xc, float yc, float cz, float szks, float kks, float S0,
                                                 float dS, float nC0, float dnC, float SH, float dSx, float &q) {
   q = __fmaf_rn(xc, xc, __fmul_rn(yc, yc));
-  const float negf = yc < 0.0f ? 1.0f : 0.0f;
-  const float Sn = __fmaf_rn(negf, dS, S0), nC = __fmaf_rn(negf, dnC, nC0), Sx = __fmaf_rn(negf, dSx, SH);
-  const float S = xc != 0.0f ? Sn : Sx;
+  // the same values chosen by selects (S0 + dS etc. are exact, folded on the host)
+  const bool neg = yc < 0.0f;
+  const float S = xc != 0.0f ? (neg ? S0 + dS : S0) : (neg ? SH + dSx : SH);
+  const float nC = neg ? nC0 + dnC : nC0;
   const float num = __fmaf_rn(yc, S, __fmul_rn(xc, nC));
   return __fmul_rn(__fmaf_rn(szks, num, cz), map_rsqrt(__fmaf_rn(kks, q, 1.0f)));
 }
