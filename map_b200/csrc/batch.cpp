@@ -93,7 +93,7 @@ TileCfg autotune_kind(const std::vector<const Group *> &members, const std::func
   }
   CudaEnv &env = CudaEnv::get();
   cudaStream_t st = (cudaStream_t)env.stream();
-  static const int cand[][2] = {{64, 32}, {128, 16}, {32, 32}, {64, 16}, {128, 32}, {32, 64}, {64, 64}};
+  static const int cand[][2] = {{64, 32}, {128, 16}, {32, 32}, {64, 16}, {128, 32}, {32, 64}, {64, 64}, {32, 128}};
   TileCfg best;
   float best_ms = 1e30f;
   cudaEvent_t e0, e1;
