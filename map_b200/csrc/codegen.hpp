@@ -63,10 +63,11 @@ struct KernelPlan {
 
 KernelPlan generate_kernel(const Group &g, TileCfg cfg = TileCfg());
 
-// Tuning overrides of the standalone focal skeleton, read once from the
-// environment variable MAP_B200_FOCAL_TUNE ("key=value,..."; keys unroll, defer,
-// nt, tw, th, and lnt, ltw, lth for Local kernels; 0 or absent = the built-in choice). Used to measure variants;
-// every variant computes the same cells with the same operations.
+// Tuning overrides of the standalone Local / Focal skeletons, read once from the
+// environment variable MAP_B200_FOCAL_TUNE ("key=value,..."; the keys are the
+// field names below; absent = the built-in choice, which the measured defaults
+// in executor.cpp set). Used to measure variants: every variant computes the
+// same cells with the same operations, so results are identical.
 struct FocalTune {
   int unroll = 0;   // unroll factor of the per-thread row loop (0: by body weight)
   int defer = 1;    // interior tiles keep a thread's results in registers and store them last
