@@ -1676,9 +1676,9 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
            << " - a.g.oy);\n";
     }
     body << "    }\n"
-         << "    if (!mbar_wait_bounded(bar, phase, 1u << 26)) {\n"
+         << "    if (!mbar_wait_bounded(bar, phase, 1u << 14)) {\n"
          << "      skel_fail(a.err, ERR_TMA_TIMEOUT);\n"
-         << "      mbar_wait_bounded(bar, phase, 1u << 26);\n"
+         << "      mbar_wait_bounded(bar, phase, 1u << 14);\n"
          << "      return false;\n"
          << "    }\n"
          << "    phase ^= 1u;\n"

@@ -820,11 +820,26 @@ __device__ __forceinline__ bool mbar_try_wait(u64 *bar, u32 parity) {
       : "memory");
   return ok != 0;
 }
-// Bounded wait: gives up after `limit` polls (each poll may itself suspend for a
-// while), so a copy that never lands ends the CTA with an error instead of a hang.
+// The same test with a suspend-time hint: a thread whose phase has not completed
+// sleeps until it completes or `ns` nanoseconds pass, instead of returning at
+// once, so waiting warps take no issue slots from the warps that compute.
+__device__ __forceinline__ bool mbar_try_wait_sleep(u64 *bar, u32 parity, u32 ns) {
+  u32 ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity), "r"(ns)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait: gives up after `limit` polls of at most about 0.26 ms each
+// (about 4 s for the skeletons' 2^14), so a copy that never lands ends the CTA
+// with an error instead of a hang.
 __device__ __forceinline__ bool mbar_wait_bounded(u64 *bar, u32 parity, u32 limit) {
   for (u32 i = 0; i < limit; ++i)
-    if (mbar_try_wait(bar, parity)) return true;
+    if (mbar_try_wait_sleep(bar, parity, 1u << 18)) return true;
   return false;
 }
 
