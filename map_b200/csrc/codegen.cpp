@@ -1021,10 +1021,34 @@ struct Gen {
     for (Node *n : g.nodes) s << "    " << stmt4(n) << "\n";
     return s.str();
   }
+  // each output's address of the thread's first quad (ob<k>, pitch op<k>) is a
+  // parameter; the quad of row kr below it takes one multiply-add
   std::string stores4() const {
     std::ostringstream s;
-    for (auto &kv : outk) s << "    str_out_q4_u8(a.out[" << kv.second << "], x, y, " << val4(kv.first) << ");\n";
+    int k = 0;
+    for (auto &kv : outk)
+      s << "    str_out_row<u32>(ob" << k << ", op" << k << ", kr, q4_pack_u8(" << val4(kv.first) << "));\n", k++;
     return s.str();
+  }
+  std::string out_params4() const {
+    std::string s;
+    for (size_t k = 0; k < outk.size(); k++) s += ", u64 ob" + std::to_string(k) + ", u32 op" + std::to_string(k);
+    return s + ", int kr";
+  }
+  std::string out_bases4(const std::string &indent) const {
+    std::ostringstream s;
+    int k = 0;
+    for (auto &kv : outk) {
+      s << indent << "const u64 ob" << k << " = out_addr<u8>(a.out[" << kv.second << "], x, t.y0 + ly0);\n"
+        << indent << "const u32 op" << k << " = (u32)a.out[" << kv.second << "].pitch;\n";
+      k++;
+    }
+    return s.str();
+  }
+  std::string out_args4() const {
+    std::string s;
+    for (size_t k = 0; k < outk.size(); k++) s += ", ob" + std::to_string(k) + ", op" + std::to_string(k);
+    return s;
   }
   // every output row, and every row of an input read from global memory, starts
   // on a 4-byte boundary (base and pitch)
@@ -1499,7 +1523,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
     body << ">\n__device__ __forceinline__ void focal_cell4(const Args &a";
     for (int k = 0; k < nst; k++) body << ", const F" << k << " &f" << k;
-    body << ", int x, int y, int lx, int ly) {\n";
+    body << ", int x, int y, int lx, int ly" << G.out_params4() << ") {\n";
     body << G.center_loads4() << G.body4() << G.stores4() << "}\n";
   }
   const bool full_unroll = tune.unroll ? tune.unroll >= R : !heavy;
@@ -1556,18 +1580,25 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     for (int k = 0; k < nst; k++) callr << ", f" << k;
     callr << ", x, y, lx, ly";
     int k = 0;
+    std::ostringstream bases;   // each output's address of the thread's first cell
     for (auto &kv : G.outk) {
       const std::string ty = G.T(kv.first);
       loop_full << "    " << (pair ? "PR<" + ty + ">" : ty) << " r" << k << "[" << R / step << "];\n";
       callr << ", r" << k << "[k / " << step << "]";
+      const std::string o = std::to_string(kv.second);
       if (cpair)
-        outs << "      str_out2x<" << ty << ">(a.out[" << kv.second << "], x, y, lane0(r" << k << "[k]), lane1(r" << k
+        outs << "      str_out2x<" << ty << ">(a.out[" << o << "], x, y, lane0(r" << k << "[k]), lane1(r" << k
              << "[k]));\n";
-      else if (pair)
-        outs << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y, lane0(r" << k << "[k / 2]));\n"
-             << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y + 1, lane1(r" << k << "[k / 2]));\n";
-      else
-        outs << "      str_out<" << ty << ">(a.out[" << kv.second << "], x, y, r" << k << "[k]);\n";
+      else if (pair) {
+        bases << "    const u64 ob" << k << " = out_addr<" << ty << ">(a.out[" << o << "], x, t.y0 + ly0);\n"
+              << "    const u32 op" << k << " = (u32)a.out[" << o << "].pitch;\n";
+        outs << "      str_out_row<" << ty << ">(ob" << k << ", op" << k << ", k, lane0(r" << k << "[k / 2]));\n"
+             << "      str_out_row<" << ty << ">(ob" << k << ", op" << k << ", k + 1, lane1(r" << k << "[k / 2]));\n";
+      } else {
+        bases << "    const u64 ob" << k << " = out_addr<" << ty << ">(a.out[" << o << "], x, t.y0 + ly0);\n"
+              << "    const u32 op" << k << " = (u32)a.out[" << o << "].pitch;\n";
+        outs << "      str_out_row<" << ty << ">(ob" << k << ", op" << k << ", k, r" << k << "[k]);\n";
+      }
       k++;
     }
     callr << ")";
@@ -1589,7 +1620,8 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
               << "      " << callr.str() << ";\n"
               << "    }\n";
     if (flagged) loop_full << "    }\n";
-    loop_full << "#pragma unroll\n"
+    loop_full << bases.str()
+              << "#pragma unroll\n"
               << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
               << "      const int y = t.y0 + ly0 + k;\n"
               << outs.str()
@@ -1609,12 +1641,13 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     q << "    const int lx = 4 * (threadIdx.x % " << qw << "), ly0 = (threadIdx.x / " << qw << ") * " << qrows << ";\n"
       << "    const int x = t.x0 + lx;\n"
       << "    if (" << G.quad_aligned() << ") {\n"
+      << G.out_bases4("      ")
       << "#pragma unroll\n"
       << "      for (int k = 0; k < " << qrows << "; k++) {\n"
       << "        const int ly = ly0 + k, y = t.y0 + ly;\n"
       << "        focal_cell4(a";
     for (int k = 0; k < nst; k++) q << ", f" << k;
-    q << ", x, y, lx, ly);\n"
+    q << ", x, y, lx, ly" << G.out_args4() << ", k);\n"
       << "      }\n"
       << "    } else {\n"
       << "      for (int k = 0; k < " << qrows << "; k++)\n"
@@ -1632,6 +1665,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     e << "    const int lx = 4 * (threadIdx.x % " << qw << "), ly0 = (threadIdx.x / " << qw << ") * " << qrows << ";\n"
       << "    const int x = t.x0 + lx;\n"
       << "    const bool al = " << G.quad_aligned() << ";\n"
+      << G.out_bases4("    ")
       << "#pragma unroll\n"
       << "    for (int k = 0; k < " << qrows << "; k++) {\n"
       << "      const int ly = ly0 + k, y = t.y0 + ly;\n"
@@ -1639,7 +1673,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
       << "      if (al && x + 3 < t.xe) {\n"
       << "        focal_cell4(a";
     for (int k = 0; k < nst; k++) e << ", f" << k;
-    e << ", x, y, lx, ly);\n"
+    e << ", x, y, lx, ly" << G.out_args4() << ", k);\n"
       << "      } else {\n"
       << "        for (int c = 0; c < 4; c++)\n"
       << "          if (x + c < t.xe) focal_cell(a";

@@ -93,6 +93,22 @@ template <class T> __device__ __forceinline__ void str_out(const RasterArg &r, i
 template <> __device__ __forceinline__ void str_out<bool>(const RasterArg &r, int x, int y, bool v) {
   map_stg<1>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, v ? 1u : 0u);
 }
+// Address of cell (x, y) of an output, computed once per thread: the rows of a
+// thread's cells are then reached with one 32 x 32 -> 64-bit multiply-add each
+// (str_out_row) instead of a 64-bit product per store.
+template <class T> __device__ __forceinline__ u64 out_addr(const RasterArg &r, int x, int y) {
+  return r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x * sizeof(T);
+}
+// the cell k rows below the one at `base` (pitch below 4 GiB)
+template <class T> __device__ __forceinline__ void str_out_row(u64 base, u32 pitch, u32 k, T v) {
+  typename map_stg_word<sizeof(T)>::type b = 0;
+  memcpy(&b, &v, sizeof(T));
+  map_stg<sizeof(T)>::st(base + (u64)k * (u64)pitch, b);
+}
+template <> __device__ __forceinline__ void str_out_row<bool>(u64 base, u32 pitch, u32 k, bool v) {
+  map_stg<1>::st(base + (u64)k * (u64)pitch, v ? 1u : 0u);
+}
+
 // the cells (x, y) and (x + 1, y): one 8-byte store for 4-byte cells whose row
 // and x allow it (x even, base and pitch 8-byte aligned), else two stores
 template <class T> __device__ __forceinline__ void str_out2x(const RasterArg &r, int x, int y, T v0, T v1) {
@@ -720,11 +736,7 @@ __device__ __forceinline__ Q4 q4_min(Q4 a, Q4 b) { return q4_sel(q4_ge(b, a), a,
 __device__ __forceinline__ u32 ldr_q4_u8(const RasterArg &r, int x, int y) {
   return __ldg((const u32 *)(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x));
 }
-// the four U8 result cells x .. x + 3 of row y as one 32-bit store (the row
-// address plus x must be 4-byte aligned)
-__device__ __forceinline__ void str_out_q4_u8(const RasterArg &r, int x, int y, Q4 v) {
-  map_stg<4>::st(r.p + (u64)(s64)y * (u64)r.pitch + (u64)(s64)x, q4_pack_u8(v));
-}
+
 
 // a 4-byte cell value carried in a float register, as its own type
 template <class T> __device__ __forceinline__ T __float_as_raw(float f) {

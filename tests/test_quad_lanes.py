@@ -133,7 +133,7 @@ def test_byte_lanes_round_trip_and_taps():
 def test_life_takes_the_packed_form(M):
     s = M.from_numpy(np.zeros((256, 512), np.uint8), bs=[256, 256])
     src = M.generated_source(W.life_step(s))
-    assert "focal_cell4(" in src and "q4_eq(" in src and "str_out_q4_u8" in src
+    assert "focal_cell4(" in src and "q4_eq(" in src and "str_out_row<u32>" in src
     assert M.compile_only(W.life_step(s)) == 1
 
 
