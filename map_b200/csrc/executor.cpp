@@ -347,12 +347,12 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
     } else if (g->skeleton == SK_FOCAL) {
       cfg.nt = 128;
       if (focal_fast_shade(*g)) {
-        // fast hillshade form: 32 x 128 tiles of 128 threads, 32 rows per thread
-        // (512 Gcells/s at 16384^2, against 506 for 32 x 128 of 256 threads and
-        // 505 for 64 x 64 of 256, the same box, three runs each)
-        cfg.tw = 32;
-        cfg.th = 128;
-        cfg.nt = 128;
+        // fast hillshade form: 64 x 64 tiles of 256 threads, 16 rows per thread
+        // (532 Gcells/s at 16384^2, against 530 for 32 x 128 of 256 threads and
+        // 513 for 32 x 128 of 128, the same box, with per-thread store addresses)
+        cfg.tw = 64;
+        cfg.th = 64;
+        cfg.nt = 256;
       }
       const FocalTune &ft = focal_tune();
       if (ft.nt) cfg.nt = ft.nt;
