@@ -1728,8 +1728,8 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     for (int k = 0; k < nst; k++) {
       auto &t = P.tma[k];
       std::string ty = dt_ctype(t.dtype);
-      body << "    const auto f" << k << " = make_smem_tap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy
-           << ">(smem + " << t.smem_off << ");\n";
+      body << "    const SmemTap<" << ty << ", " << t.box_w << ", " << t.pad_x << ", " << hy << "> f" << k << "{(const " << ty
+           << " *)(smem + " << t.smem_off << ")};\n";
     }
     if (loop_edge.empty()) loop_edge = loop.str();
     // block-mirror exceptions of staged edge tiles, recomputed by the same

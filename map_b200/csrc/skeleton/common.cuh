@@ -745,58 +745,13 @@ template <class T> __device__ __forceinline__ T __float_as_raw(float f) {
   return r;
 }
 
-// Loads from the shared window at a 32-bit shared address: the address of a tap
-// is the staged tile's base plus a constant offset, so each load is one
-// instruction with an immediate offset. Not volatile and without a memory
-// clobber, so equal loads merge; they cannot move above the point where the
-// tile's base address is taken (make_smem_tap, after the staging wait).
-template <int N> struct lds_bits;
-template <> struct lds_bits<1> {
-  static __device__ __forceinline__ u32 ld(u32 a) {
-    u32 v;
-    asm("ld.shared.u8 %0, [%1];" : "=r"(v) : "r"(a));
-    return v;
-  }
-};
-template <> struct lds_bits<2> {
-  static __device__ __forceinline__ u32 ld(u32 a) {
-    u32 v;
-    asm("ld.shared.u16 %0, [%1];" : "=r"(v) : "r"(a));
-    return v;
-  }
-};
-template <> struct lds_bits<4> {
-  static __device__ __forceinline__ u32 ld(u32 a) {
-    u32 v;
-    asm("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(a));
-    return v;
-  }
-};
-template <> struct lds_bits<8> {
-  static __device__ __forceinline__ u64 ld(u32 a) {
-    u64 v;
-    asm("ld.shared.u64 %0, [%1];" : "=l"(v) : "r"(a));
-    return v;
-  }
-};
-template <class T> __device__ __forceinline__ T lds_val(u32 a) {
-  const auto b = lds_bits<sizeof(T)>::ld(a);
-  T v;
-  memcpy(&v, &b, sizeof(T));
-  return v;
-}
-template <> __device__ __forceinline__ bool lds_val<bool>(u32 a) { return lds_bits<1>::ld(a) != 0; }
-
 template <class T, int SW, int PX, int HY> struct SmemTap {
-  u32 sa;   // shared address of the staged tile's element (0, 0)
-  __device__ __forceinline__ u32 at(int lx, int ly, int dx, int dy) const {
-    return sa + (u32)(((ly + HY + dy) * SW + (lx + PX + dx)) * (int)sizeof(T));
-  }
+  const T *s;
   __device__ __forceinline__ T tap(int x, int y, int lx, int ly, int dx, int dy) const {
-    return lds_val<T>(at(lx, ly, dx, dy));
+    return s[(ly + HY + dy) * SW + (lx + PX + dx)];
   }
   __device__ __forceinline__ PR<T> tap2(int x, int y, int lx, int ly, int dx, int dy) const {
-    return PR<T>(lds_val<T>(at(lx, ly, dx, dy)), lds_val<T>(at(lx, ly + 1, dx, dy)));
+    return PR<T>(s[(ly + HY + dy) * SW + (lx + PX + dx)], s[(ly + 1 + HY + dy) * SW + (lx + PX + dx)]);
   }
   // The tap at (dx, dy) of the cells lx and lx + 1 of a row (4-byte cells, lx +
   // PX and SW even): aligned pairs of the staged row, one 8-byte load each; an
@@ -804,11 +759,12 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   // three taps of a 3-wide window come from three loads for both cells.
   __device__ __forceinline__ PR<T> tap2c(int x, int y, int lx, int ly, int dx, int dy) const {
     static_assert(sizeof(T) == 4 && SW % 2 == 0 && PX % 2 == 0, "tap2c: 4-byte cells, even row stride and pad");
+    const float2 *row = (const float2 *)(s + (ly + HY + dy) * SW + lx + PX);
     const int o = dx & 1, m = (dx - o) / 2;
-    const u64 p = lds_bits<8>::ld(at(lx + 2 * m, ly, 0, dy));
-    if (!o) return PR<T>(__float_as_raw<T>(__uint_as_float((u32)p)), __float_as_raw<T>(__uint_as_float((u32)(p >> 32))));
-    const u64 q = lds_bits<8>::ld(at(lx + 2 * m + 2, ly, 0, dy));
-    return PR<T>(__float_as_raw<T>(__uint_as_float((u32)(p >> 32))), __float_as_raw<T>(__uint_as_float((u32)q)));
+    const float2 p = row[m];
+    if (!o) return PR<T>(__float_as_raw<T>(p.x), __float_as_raw<T>(p.y));
+    const float2 q = row[m + 1];
+    return PR<T>(__float_as_raw<T>(p.y), __float_as_raw<T>(q.x));
   }
   // The taps at (dx, dy) of the byte cells lx .. lx + 3 (lx a multiple of 4, the
   // row stride SW and pad PX multiples of 4, |dx| <= PX), in the interleaved
@@ -819,7 +775,7 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
   // W_m and the odd lanes of W_m+1. Each piece is one byte permute of loaded
   // words, and the pieces of neighbouring offsets are the same expressions.
   __device__ __forceinline__ u32 word(int lx, int ly, int dy, int m) const {
-    return lds_bits<4>::ld(at(lx + 4 * m, ly, 0, dy));
+    return ((const u32 *)(s + (ly + HY + dy) * SW + lx + PX))[m];
   }
   __device__ __forceinline__ u32 tap4_e(int lx, int ly, int dy, int m) const {   // lanes 4m + 2, 4m + 4
     return __byte_perm(q4_even(word(lx, ly, dy, m)), word(lx, ly, dy, m + 1), 0x1412);
@@ -838,14 +794,6 @@ template <class T, int SW, int PX, int HY> struct SmemTap {
     }
   }
 };
-// The tap object of a tile staged at `p` in shared memory. The shared address is
-// taken by a volatile instruction, which stays after the staging wait and the
-// barrier before it, and every load of the tile depends on it.
-template <class T, int SW, int PX, int HY> __device__ __forceinline__ SmemTap<T, SW, PX, HY> make_smem_tap(const void *p) {
-  u32 a;
-  asm volatile("{\n\t.reg .u64 t;\n\tcvta.to.shared.u64 t, %1;\n\tcvt.u32.u64 %0, t;\n\t}" : "=r"(a) : "l"((u64)p));
-  return SmemTap<T, SW, PX, HY>{a};
-}
 
 // ------------------------------------------------------------------ dependent launches
 

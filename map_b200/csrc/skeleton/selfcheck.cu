@@ -22,7 +22,7 @@ extern "C" __global__ void __launch_bounds__(256) selfcheck_focal(const __grid_c
       tma_load_2d(smem, &a.tm[0], bar, t.x0 - 4, t.y0 - 1);
     }
     if (!mbar_wait_bounded(bar, 0, 1u << 14)) { skel_fail(a.err, ERR_TMA_TIMEOUT); return; }
-    const auto f = make_smem_tap<float, 72, 4, 1>(smem);
+    const SmemTap<float, 72, 4, 1> f{(const float *)smem};
     const int x = t.x0 + threadIdx.x % 64, y = t.y0 + threadIdx.x / 64;
     str<float>(a.out[0], x, y, f.tap(x, y, threadIdx.x % 64, threadIdx.x / 64, -1, 1));
   } else {
