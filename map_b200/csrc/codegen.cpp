@@ -1298,6 +1298,17 @@ std::string fnv_hex(const std::string &s) {
 // cells per CTA of NT threads; each thread owns TH*TW/NT cells of one column,
 // issues all of its input loads first (memory-level parallelism), then
 // evaluates the fused expression and stores the outputs.
+// run_tile by linear tile index (the batched dispatcher's work items): the tile's
+// coordinates from the index, then the tile's code
+static std::string run_tile_by_index(int TW, int TH) {
+  std::ostringstream s;
+  s << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
+    << "                                         bool gdesc) {\n"
+    << "  return run_tile_t(a, tile_of<" << TW << ", " << TH << ">(a.g, tile), smem, bar, phase, gdesc);\n"
+    << "}\n";
+  return s.str();
+}
+
 static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap) {
   KernelPlan &P = G.plan;
   const int TW = P.tile_w, TH = P.tile_h, NT = P.threads, R = TH * TW / NT;
@@ -1337,9 +1348,8 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << "__device__ __forceinline__ void compute_cellr(const Args &a, const In &in, int x, int y" << G.out_params(false)
          << ") {\n" << G.center_loads(true) << G.body(false) << G.out_assigns() << "}\n";
   }
-  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
-       << "                                         bool gdesc) {\n"
-       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n";
+  body << "__device__ __forceinline__ bool run_tile_t(const Args &a, const Tile t, unsigned char *smem, u64 *bar,\n"
+       << "                                           u32 &phase, bool gdesc) {\n";
   if (vec) {
     std::ostringstream align;
     align << "(t.x0 * " << es << ")";
@@ -1407,12 +1417,14 @@ static void gen_local(Gen &G, std::ostringstream &body, std::ostringstream &wrap
        << "  }\n"
        << "  return true;\n"
        << "}\n";
-  // launched as a dependent launch: no global access before griddep_wait
+  body << run_tile_by_index(TW, TH);
+  // launched as a dependent launch over the region's tiles in two dimensions:
+  // no global access before griddep_wait
   wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  u32 phase = 0;\n"
        << "  griddep_launch();\n"
        << "  griddep_wait();\n"
-       << "  run_tile(a, blockIdx.x, nullptr, nullptr, phase, false);\n"
+       << "  run_tile_t(a, tile_at<" << TW << ", " << TH << ">(a.g, blockIdx.x, blockIdx.y), nullptr, nullptr, phase, false);\n"
        << "}\n";
 }
 
@@ -1684,9 +1696,8 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     loop_edge = e.str();
   }
   // gdesc: the Args (and their tensor maps) live in global memory (batched dispatch)
-  body << "__device__ __forceinline__ bool run_tile(const Args &a, int tile, unsigned char *smem, u64 *bar, u32 &phase,\n"
-       << "                                         bool gdesc) {\n"
-       << "  const Tile t = tile_of<" << TW << ", " << TH << ">(a.g, tile);\n";
+  body << "__device__ __forceinline__ bool run_tile_t(const Args &a, const Tile t, unsigned char *smem, u64 *bar,\n"
+       << "                                           u32 &phase, bool gdesc) {\n";
   if (use_tma) {
     size_t total = 0;
     for (auto &t : P.tma) total += (size_t)t.box_w * t.box_h * dt_size(t.dtype);
@@ -1780,6 +1791,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     body << "    const GatherTap<" << ty << "> f" << k << "{a.in[" << G.rin.at(staged_nodes[k]) << "], &a.g};\n";
   }
   body << loop.str() << "  }\n  return true;\n}\n";
+  body << run_tile_by_index(TW, TH);
   wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT;
   if (tune.minb > 0) wrap << ", " << tune.minb;
   wrap << ") KNAME(const __grid_constant__ Args a) {\n"
@@ -1793,11 +1805,11 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
          << "  griddep_launch();\n"
          << "  __syncthreads();\n"
          << "  griddep_wait();\n"
-         << "  run_tile(a, blockIdx.x, smem, bar, phase, false);\n";
+         << "  run_tile_t(a, tile_at<" << TW << ", " << TH << ">(a.g, blockIdx.x, blockIdx.y), smem, bar, phase, false);\n";
   else
     wrap << "  griddep_launch();\n"
          << "  griddep_wait();\n"
-         << "  run_tile(a, blockIdx.x, smem, nullptr, phase, false);\n";
+         << "  run_tile_t(a, tile_at<" << TW << ", " << TH << ">(a.g, blockIdx.x, blockIdx.y), smem, nullptr, phase, false);\n";
   wrap << "}\n";
   if (!use_tma) P.tma.clear();
 }

@@ -276,15 +276,24 @@ void CudaEnv::launch(const KernelHandle &k, int grid, int block, size_t smem, CU
 // griddepcontrol.wait (map_common.cuh griddep_wait) before it touches global
 // memory, which waits for the previous grid to complete and its writes to be
 // visible. Used for the generated Local / Focal kernels, which all do.
-void CudaEnv::launch_pdl(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args) {
-  if (grid <= 0) return;
+void CudaEnv::launch_2d(const KernelHandle &k, int gx, int gy, int block, size_t smem, CUstream_st *stream, void *args) {
+  if (gx <= 0 || gy <= 0) return;
+  void *params[] = {args};
+  drv_check(g_drv.launchKernel(reinterpret_cast<CUfunction>(k.fn), (unsigned)gx, (unsigned)gy, 1, (unsigned)block, 1, 1,
+                               (unsigned)smem, reinterpret_cast<CUstream>(stream), params, nullptr),
+            "cuLaunchKernel");
+  launches_++;
+}
+
+void CudaEnv::launch_pdl(const KernelHandle &k, int grid, int gy, int block, size_t smem, CUstream_st *stream, void *args) {
+  if (grid <= 0 || gy <= 0) return;
   void *params[] = {args};
   CUlaunchAttribute attr;
   attr.id = CU_LAUNCH_ATTRIBUTE_PROGRAMMATIC_STREAM_SERIALIZATION;
   attr.value.programmaticStreamSerializationAllowed = 1;
   CUlaunchConfig cfg = {};
   cfg.gridDimX = (unsigned)grid;
-  cfg.gridDimY = 1;
+  cfg.gridDimY = (unsigned)gy;
   cfg.gridDimZ = 1;
   cfg.blockDimX = (unsigned)block;
   cfg.blockDimY = 1;

@@ -42,8 +42,10 @@ class CudaEnv {
   KernelHandle kernel(const std::string &source, const std::string &name, size_t dyn_smem);
   void launch(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args, size_t args_size);
   void launch_cluster(const KernelHandle &k, int grid, int block, int cluster, size_t smem, CUstream_st *stream, void *args);
-  // programmatic dependent launch (the kernel waits with griddepcontrol.wait)
-  void launch_pdl(const KernelHandle &k, int grid, int block, size_t smem, CUstream_st *stream, void *args);
+  // a grid of gx x gy CTAs (the Local / Focal kernels: the region's tiles)
+  void launch_2d(const KernelHandle &k, int gx, int gy, int block, size_t smem, CUstream_st *stream, void *args);
+  // programmatic dependent launch of gx x gy CTAs (the kernel waits with griddepcontrol.wait)
+  void launch_pdl(const KernelHandle &k, int gx, int gy, int block, size_t smem, CUstream_st *stream, void *args);
   int occupancy(const KernelHandle &k, int block, size_t smem);   // resident CTAs per SM
   // Writes `value` (elem_size bytes: 1, 2 or 4) into every element of a width x
   // height 2-D array; false (nothing done) for other element sizes.

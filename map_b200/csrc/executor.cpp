@@ -319,6 +319,10 @@ std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const 
   return a;
 }
 
+// Largest grid height of a launch (CUDA's limit on gridDim.y): taller regions of
+// Local / Focal tiles are launched in pieces of this many tile rows.
+constexpr int kMaxGridY = 65535;
+
 Executor &Executor::get() {
   static Executor e;
   return e;
@@ -607,11 +611,19 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
       z.slots += grid;
       (void)nz;
     } else {
-      // Local / Focal kernels wait for their predecessor in the kernel
-      // (griddep_wait), so they are launched as dependent launches
-      auto a = build_args(g, K, rx0, ry0, rx1, ry1, 0, 0);
-      if (rt.dependent_launch && focal_tune().pdl) env.launch_pdl(kh, tiles, K.threads, K.smem_bytes, (CUstream_st *)st, a.data());
-      else env.launch(kh, tiles, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+      // Local / Focal kernels run one CTA per tile on a tx x ty grid (regions of
+      // more than kMaxGridY tile rows in vertical pieces) and wait for their
+      // predecessor in the kernel (griddep_wait), so they are dependent launches
+      for (int y = ry0; y < ry1; y += kMaxGridY * K.tile_h) {
+        const int ye = std::min(ry1, y + kMaxGridY * K.tile_h);
+        const int pty = (ye - y + K.tile_h - 1) / K.tile_h;
+        auto a = build_args(g, K, rx0, y, rx1, ye, 0, 0);
+        if (rt.dependent_launch && focal_tune().pdl)
+          env.launch_pdl(kh, tx, pty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data());
+        else
+          env.launch_2d(kh, tx, pty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data());
+      }
+      (void)ty;
     }
   };
 
@@ -970,11 +982,14 @@ void Executor::evaluate_rows(const std::vector<Node *> &targets_in, const std::v
       const Group &g = *gp;
       const KernelPlan &K = P.plans[g.id];
       const int ry0 = std::max(0, y0 - R.need[&g]), ry1 = std::min(H, y1 + R.need[&g]);
-      const int tx = (W + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+      const int tx = (W + K.tile_w - 1) / K.tile_w;
       KernelHandle kh = env.kernel(K.source, K.kname, K.smem_bytes);
       uint64_t aux[4] = {0, 0, 0, 0};
-      auto a = pack_args(g, K, get, bufs, 0, ry0, W, ry1, aux);
-      env.launch(kh, tx * ty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+      for (int y = ry0; y < ry1; y += kMaxGridY * K.tile_h) {
+        const int ye = std::min(ry1, y + kMaxGridY * K.tile_h);
+        auto a = pack_args(g, K, get, bufs, 0, y, W, ye, aux);
+        env.launch_2d(kh, tx, (ye - y + K.tile_h - 1) / K.tile_h, K.threads, K.smem_bytes, (CUstream_st *)st, a.data());
+      }
     }
     for (auto &c : copies) {
       const DevRaster &r = bufs.at(c.second);
@@ -1131,11 +1146,15 @@ bool Executor::evaluate_streamed(const Prepared &P, const std::vector<Node *> &t
         const Group &g = *gp;
         const KernelPlan &K = P.plans[g.id];
         const int ry0 = std::max(0, y0 - need[&g]), ry1 = std::min(H, y1 + need[&g]);
-        const int tx = (W + K.tile_w - 1) / K.tile_w, ty = (ry1 - ry0 + K.tile_h - 1) / K.tile_h;
+        const int tx = (W + K.tile_w - 1) / K.tile_w;
         KernelHandle kh = env.kernel(K.source, K.kname, K.smem_bytes);
         uint64_t aux[4] = {0, 0, 0, 0};
-        auto a = pack_args(g, K, get, bufs, 0, ry0, W, ry1, aux);
-        env.launch(kh, tx * ty, K.threads, K.smem_bytes, (CUstream_st *)st, a.data(), a.size());
+        for (int y = ry0; y < ry1; y += kMaxGridY * K.tile_h) {
+          const int ye = std::min(ry1, y + kMaxGridY * K.tile_h);
+          auto a = pack_args(g, K, get, bufs, 0, y, W, ye, aux);
+          env.launch_2d(kh, tx, (ye - y + K.tile_h - 1) / K.tile_h, K.threads, K.smem_bytes, (CUstream_st *)st,
+                        a.data());
+        }
       }
       cuda_check(cudaEventRecord(bs.ev_comp[sidx], st), "cudaEventRecord");
       cuda_check(cudaStreamWaitEvent(bs.down, bs.ev_comp[sidx], 0), "cudaStreamWaitEvent");

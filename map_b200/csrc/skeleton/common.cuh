@@ -887,6 +887,17 @@ template <int TW, int TH> __device__ __forceinline__ Tile tile_of(const Geom &g,
   return r;
 }
 
+// Tile (tx, ty) of the region, for launches whose grid is the region's tiles in
+// two dimensions (no division to recover the tile's coordinates)
+template <int TW, int TH> __device__ __forceinline__ Tile tile_at(const Geom &g, int tx, int ty) {
+  Tile r;
+  r.x0 = g.rx0 + tx * TW;
+  r.y0 = g.ry0 + ty * TH;
+  r.xe = min(r.x0 + TW, g.rx1);
+  r.ye = min(r.y0 + TH, g.ry1);
+  return r;
+}
+
 // Whether the tile plus its halo lies inside the raster (so TMA staging with no
 // border handling serves every tap).
 template <int TW, int TH> __device__ __forceinline__ bool tile_interior(const Geom &g, const Tile &t, int hx, int hy) {
