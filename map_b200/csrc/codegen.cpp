@@ -683,23 +683,45 @@ struct Gen {
     // finite taps, NaN otherwise); the x sum starts from it, so a non-finite
     // such tap makes x, hence x^2 + y^2, NaN (the sign of a zero x does not
     // change the result)
-    s << T << " " << v << "_xc = " << T << "(0.0f);";
+    // The terms of each sum in order: (tap, weight), the zero-weight taps
+    // first (x sum only).
+    std::vector<std::pair<std::string, double>> terms[2];
     for (int i1 = -hy; i1 <= hy; i1++)
       for (int i0 = -hx; i0 <= hx; i0++) {
         const int k = (i1 + hy) * mw + (i0 + hx);
-        if (var_as_f64(f.xc->mask[k]) == 0.0 && var_as_f64(f.yc->mask[k]) == 0.0)
-          s << " " << v << "_xc = " << fma << tapv(i0, i1) << ", 0.0f, " << v << "_xc);";
+        if (var_as_f64(f.xc->mask[k]) == 0.0 && var_as_f64(f.yc->mask[k]) == 0.0) terms[0].push_back({tapv(i0, i1), 0.0});
       }
     for (int c = 0; c < 2; c++) {
       Node *cv = c ? f.yc : f.xc;
-      const std::string acc = v + (c ? "_yc" : "_xc");
-      if (c) s << " " << T << " " << acc << " = " << T << "(0.0f);";
       for (int i1 = -hy; i1 <= hy; i1++)
         for (int i0 = -hx; i0 <= hx; i0++) {
           const double w = var_as_f64(cv->mask[(i1 + hy) * mw + (i0 + hx)]);
-          if (w == 0.0) continue;
-          s << " " << acc << " = " << fma << tapv(i0, i1) << ", " << fl((float)w) << ", " << acc << ");";
+          if (w != 0.0) terms[c].push_back({tapv(i0, i1), w});
         }
+    }
+    for (int c = 0; c < 2; c++) {
+      const std::string acc = v + (c ? "_yc" : "_xc");
+      std::vector<std::pair<std::string, double>> &t = terms[c];
+      // A sum from +0 whose first non-zero term has weight +-1: that term is
+      // exact, so it becomes the addend of the fused multiply-add before it (a
+      // zero-weight tap) or after it (the next term), one instruction fewer.
+      // Only the sign of a zero partial sum can differ, which changes neither
+      // x^2 + y^2, nor the tests x != 0 and y < 0, nor the result.
+      size_t nz = 0;
+      while (nz < t.size() && t[nz].second == 0.0) nz++;
+      if (!pair && nz < t.size() && std::fabs(t[nz].second) == 1.0 && t.size() >= 2) {
+        const std::string lead = (t[nz].second < 0 ? "-" : "") + t[nz].first;
+        const size_t with = nz > 0 ? 0 : 1;   // the term that takes it as its addend
+        s << " " << T << " " << acc << " = " << fma << t[with].first << ", " << fl((float)t[with].second) << ", " << lead
+          << ");";
+        for (size_t j = 0; j < t.size(); j++)
+          if (j != with && j != nz)
+            s << " " << acc << " = " << fma << t[j].first << ", " << fl((float)t[j].second) << ", " << acc << ");";
+        continue;
+      }
+      s << " " << T << " " << acc << " = " << T << "(0.0f);";
+      for (const auto &e : t)
+        s << " " << acc << " = " << fma << e.first << ", " << fl((float)e.second) << ", " << acc << ");";
     }
     s << " " << T << " " << v << "_q; " << T << " " << v << " = map_shade_fast(" << v << "_xc, " << v << "_yc, "
       << fl(shades[i].cz) << ", " << fl(f.szks) << ", " << fl(f.kks) << ", " << fl(f.S0) << ", " << fl(f.dS) << ", "

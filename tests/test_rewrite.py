@@ -174,19 +174,26 @@ def test_fast_form_equals_general_form_replay():
     V = np.array([[-1, -2, -1], [0, 0, 0], [1, 2, 1]], f32)
     xl = O.conv_f32(d, H, (128, 128), 0)
     yl = O.conv_f32(d, V, (128, 128), 0)
-    # the fast sums: fma(tap, w, acc) over non-zero weights, from +0
+    # the fast sums as emitted: fma(tap, w, acc) over the non-zero weights, the
+    # first (weight -1, exact) the addend of the fma before it (the centre tap
+    # times 0, x sum) or after it (y sum)
     p = np.pad(d, 1, mode="symmetric")      # interior cells only are compared below
-    def fast_sum(m):
-        acc = np.zeros(d.shape, f32)
-        for i1 in range(3):
-            for i0 in range(3):
-                if m[i1, i0] != 0:
-                    acc = fma32(p[i1:i1 + d.shape[0], i0:i0 + d.shape[1]], m[i1, i0], acc)
+    def tap(i1, i0):
+        return p[i1:i1 + d.shape[0], i0:i0 + d.shape[1]]
+    def fast_sum(m, lead_with_centre):
+        nz = [(i1, i0) for i1 in range(3) for i0 in range(3) if m[i1, i0] != 0]
+        assert m[nz[0]] == -1
+        if lead_with_centre:
+            acc, rest = fma32(tap(1, 1), f32(0), -tap(*nz[0])), nz[1:]
+        else:
+            acc, rest = fma32(tap(*nz[1]), m[nz[1]], -tap(*nz[0])), nz[2:]
+        for i1, i0 in rest:
+            acc = fma32(tap(i1, i0), m[i1, i0], acc)
         return acc
-    xc, yc = fast_sum(H), fast_sum(V)
+    xc, yc = fast_sum(H, True), fast_sum(V, False)
     inner = (slice(1, -1), slice(1, -1))
-    assert np.array_equal(xc[inner].view(np.uint32), xl[inner].view(np.uint32))
-    assert np.array_equal(yc[inner].view(np.uint32), yl[inner].view(np.uint32))
+    # equal values (a zero sum may carry the other sign)
+    assert np.array_equal(xc[inner], xl[inner]) and np.array_equal(yc[inner], yl[inner])
     general = replay_shade((xl * f32(0.125)).astype(f32), (yl * f32(0.125)).astype(f32), k)
     # fast: q = fma(xc, xc, yc*yc) + 0; choice by arithmetic; constants scaled
     q = fma32(xc, xc, (yc * yc).astype(f32))
