@@ -709,7 +709,7 @@ struct Gen {
       // x^2 + y^2, nor the tests x != 0 and y < 0, nor the result.
       size_t nz = 0;
       while (nz < t.size() && t[nz].second == 0.0) nz++;
-      if (!pair && nz < t.size() && std::fabs(t[nz].second) == 1.0 && t.size() >= 2) {
+      if (!pair && focal_tune().fmerge && nz < t.size() && std::fabs(t[nz].second) == 1.0 && t.size() >= 2) {
         const std::string lead = (t[nz].second < 0 ? "-" : "") + t[nz].first;
         const size_t with = nz > 0 ? 0 : 1;   // the term that takes it as its addend
         s << " " << T << " " << acc << " = " << fma << t[with].first << ", " << fl((float)t[with].second) << ", " << lead
@@ -2557,6 +2557,7 @@ const FocalTune &focal_tune() {
         else if (k == "fpair") r.fpair = v;
         else if (k == "cpair") r.cpair = v;
         else if (k == "fflag") r.fflag = v;
+        else if (k == "fmerge") r.fmerge = v;
       }
       i = j + 1;
     }

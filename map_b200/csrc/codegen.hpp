@@ -80,6 +80,8 @@ struct FocalTune {
   int cpair = 0;                    // pairs of cells (x, x + 1) of one row instead of (y, y + 1) of one column
   int fflag = 0;                    // fast form's non-finite record: comparison (0) or unsigned maximum (1, measured
                                     // 2.5% slower: a dependent chain through the record)
+  int fmerge = 1;                   // fast form: the exact leading term of a derivative sum as the addend of the
+                                    // neighbouring fused multiply-add (0: every sum from +0)
 };
 const FocalTune &focal_tune();
 
