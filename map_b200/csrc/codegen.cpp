@@ -1815,7 +1815,8 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   body << loop.str() << "  }\n  return true;\n}\n";
   body << run_tile_by_index(TW, TH);
   wrap << "extern \"C\" __global__ void __launch_bounds__(" << NT;
-  if (tune.minb > 0) wrap << ", " << tune.minb;
+  const int minb = tune.minb > 0 ? tune.minb : G.plan.min_blocks;
+  if (minb > 0) wrap << ", " << minb;
   wrap << ") KNAME(const __grid_constant__ Args a) {\n"
        << "  extern __shared__ __align__(128) unsigned char smem[];\n"
        << "  u32 phase = 0;\n";
@@ -2594,6 +2595,7 @@ KernelPlan generate_kernel(const Group &g, TileCfg cfg) {
   P.threads = cfg.nt;
   P.tile_w = cfg.tw;
   P.tile_h = cfg.th;
+  P.min_blocks = cfg.minb;
   Gen G(g, P);
   G.classify();
   std::string src;

@@ -28,6 +28,7 @@ struct TmaSpec {
 // Tile shape of the Local / Focal / Zonal skeletons: TW x TH cells per CTA of NT threads.
 struct TileCfg {
   int tw = 64, th = 32, nt = 256;
+  int minb = 0;   // focal kernels: minimum resident CTAs per SM in the launch bounds (0: none)
 };
 bool tile_cfg_valid(const TileCfg &c);
 // Whether a focal group's interior tiles compute four byte cells of a row per
@@ -54,6 +55,7 @@ struct KernelPlan {
   std::vector<TmaSpec> tma;
   int threads = 256;
   int tile_w = 64, tile_h = 32;
+  int min_blocks = 0;   // minimum resident CTAs per SM in the launch bounds (0: none)
   int halo_x = 0, halo_y = 0;
   size_t smem_bytes = 0;
   int aux_count = 0;

@@ -353,10 +353,13 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
       if (focal_fast_shade(*g)) {
         // fast hillshade form: 64 x 64 tiles of 256 threads, 16 rows per thread
         // (532 Gcells/s at 16384^2, against 530 for 32 x 128 of 256 threads and
-        // 513 for 32 x 128 of 128, the same box, with per-thread store addresses)
+        // 513 for 32 x 128 of 128, the same box, with per-thread store addresses),
+        // registers capped for 6 resident CTAs per SM (533 against 521 with the
+        // 5 that 48 registers allow, the same box)
         cfg.tw = 64;
         cfg.th = 64;
         cfg.nt = 256;
+        cfg.minb = 6;
       }
       const FocalTune &ft = focal_tune();
       if (ft.nt) cfg.nt = ft.nt;
