@@ -76,8 +76,12 @@ ma_Node *ma_radialScan(ma_Node *node, int type, ma_Array coord);                
 ma_Node *ma_spreadScan(ma_Node *node, ma_Node *dir, int type);                   /* front/bindings.hpp:77 */
 ma_Node *ma_stats(ma_Node *node);                                                /* front/bindings.hpp:79 */
 ma_Node *ma_barrier(ma_Node *node);                                              /* front/bindings.hpp:80 */
-/* Symbolic loops: the reference declares them but has no task to run them
- * (runtime/task/Task.cpp:38-84); here they record an "unsupported" error. */
+/* Symbolic loops: the reference captures a Python `while` over a raster
+ * condition through these entries (python/map.py:234-330, assembled by
+ * runtime/Runtime.cpp:156-311) but has no task to run the loop
+ * (runtime/task/Task.cpp:38-84). Here the Python module runs such loops itself,
+ * one evaluation per iteration with the loop-carried rasters kept resident by
+ * ma_materialize; these capture entries record an "unsupported" error. */
 void ma_loopStart(void);                                                         /* front/bindings.hpp:86 */
 void ma_loopCond(ma_Node *cond);                                                 /* front/bindings.hpp:87 */
 void ma_loopBody(void);                                                          /* front/bindings.hpp:88 */
@@ -224,6 +228,15 @@ int ma_toHost(ma_Node *node, void *dst, size_t bytes);
  * With async != 0 the call returns once the work is enqueued on the library's
  * stream (see ma_stream / ma_sync). Returns 0 on success. */
 int ma_toDevice(ma_Node *node, void *dptr, long long pitch, int async);
+/* Evaluate the `num` nodes of `vec` in one evaluation and write to out[i] a
+ * node that holds the value of vec[i]: a 2-D raster kept in a device buffer
+ * the library owns (freed, stream-ordered, once the node is unreferenced and
+ * ma_collectGarbage runs), a scalar (D0) as a constant. Device inputs holding a
+ * whole raster and constants come back as they are. The returned nodes carry
+ * no reference of their own (ma_increaseRef them to keep them). This keeps the
+ * loop-carried values of a while-loop resident between iterations, so each
+ * iteration evaluates only its own body. Returns 0 on success. */
+int ma_materialize(ma_Node **vec, int num, ma_Node **out);
 /* Evaluate several nodes; async as above (scalar results always synchronise). */
 int ma_evalAsync(ma_Node **vec, int num);
 int ma_sync(void);

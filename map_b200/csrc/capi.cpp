@@ -311,7 +311,9 @@ ma_Node *ma_barrier(ma_Node *node) {
   return node_call([&] { return Runtime::get().barrier(checked(node)); });
 }
 
-static void loops_unsupported() { fail("symbolic loops are not supported (the reference cannot execute them either)"); }
+static void loops_unsupported() {
+  fail("symbolic loop capture entries are not supported: the Python module runs while-loops itself (ma_materialize)");
+}
 void ma_loopStart(void) { loops_unsupported(); }
 void ma_loopCond(ma_Node *) { loops_unsupported(); }
 void ma_loopBody(void) { loops_unsupported(); }
@@ -483,6 +485,16 @@ int ma_toDevice(ma_Node *node, void *dptr, long long pitch, int async) {
     s.dev = dptr;
     s.dev_pitch = pitch;
     Executor::get().evaluate({}, {s}, async != 0);
+    return 0;
+  });
+}
+
+int ma_materialize(ma_Node **vec, int num, ma_Node **out) {
+  return int_call([&] {
+    std::vector<Node *> v = node_vec(vec, num);
+    if (!out) throw MapError("materialize: null output array");
+    std::vector<Node *> r = Executor::get().materialize(v);
+    for (int i = 0; i < num; i++) out[i] = MN(r[i]);
     return 0;
   });
 }

@@ -7,6 +7,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
+#include <cstdlib>
+#include <mutex>
 #include <chrono>
 #include <functional>
 #include <cstring>
@@ -413,6 +416,91 @@ std::shared_ptr<Executor::Prepared> Executor::prepare_cached(const std::vector<N
   e.epoch = rt.epoch;
   e.used = ++cache_tick_;
   return P;
+}
+
+namespace {
+// Set by an exit handler registered at the first materialisation (so it runs
+// before the runtime's and the device environment's destructors): buffers of
+// nodes destroyed during process teardown are left to the driver.
+std::atomic<bool> g_exiting{false};
+std::once_flag g_exit_hook;
+}  // namespace
+
+DevData::~DevData() {
+  if (!owned || ptr == nullptr || g_exiting.load()) return;
+  try {
+    CudaEnv &env = CudaEnv::get();
+    if (env.device_ready()) cudaFreeAsync(ptr, (cudaStream_t)env.stream());
+  } catch (...) {
+  }
+}
+
+std::vector<Node *> Executor::materialize(const std::vector<Node *> &nodes) {
+  Runtime &rt = Runtime::get();
+  std::lock_guard<std::recursive_mutex> lk(rt.mtx);
+  std::call_once(g_exit_hook, [] { std::atexit([] { g_exiting.store(true); }); });
+  std::vector<Node *> out(nodes.size(), nullptr);
+  std::vector<Node *> d0;
+  std::vector<Sink> sinks;
+  struct Held { Node *node; void *ptr; long long pitch; };
+  std::vector<Held> held;
+  std::unordered_map<Node *, size_t> slot;   // a node given twice is evaluated once
+  for (size_t i = 0; i < nodes.size(); i++) {
+    Node *n = nodes[i];
+    if (!rt.owns(n)) throw MapError("materialize: unknown node");
+    if (n->meta.numdim == D0) {
+      d0.push_back(n);
+      continue;
+    }
+    if (n->meta.numdim != D2) throw MapError("materialize: only D0 and D2 rasters are supported");
+    if (n->kind == K_CONSTANT || (n->kind == K_DEVIN && n->dev->rows == 0)) {
+      out[i] = n;
+      continue;
+    }
+    if (slot.count(n)) continue;
+    CudaEnv &env = CudaEnv::get();
+    env.ensure_device();
+    Held h{n, nullptr, pitch_for(n->meta.W(), n->meta.dtype)};
+    const cudaError_t e = cudaMallocAsync(&h.ptr, (size_t)h.pitch * n->meta.H(), (cudaStream_t)env.stream());
+    if (e != cudaSuccess) {
+      for (const Held &o : held) cudaFreeAsync(o.ptr, (cudaStream_t)env.stream());
+      cuda_check(e, "cudaMallocAsync(materialize)");
+    }
+    slot[n] = held.size();
+    held.push_back(h);
+    Sink s;
+    s.node = n;
+    s.dev = h.ptr;
+    s.dev_pitch = h.pitch;
+    sinks.push_back(s);
+  }
+  if (!d0.empty() || !sinks.empty()) {
+    try {
+      evaluate(d0, sinks);
+    } catch (...) {
+      for (const Held &o : held) cudaFreeAsync(o.ptr, (cudaStream_t)CudaEnv::get().stream());
+      throw;
+    }
+  }
+  std::vector<Node *> made(held.size(), nullptr);
+  for (size_t k = 0; k < held.size(); k++) {
+    const Held &h = held[k];
+    Node *m = rt.dev_input(h.ptr, h.pitch, h.node->meta.ds, h.node->meta.dtype, h.node->meta.bs);
+    m->dev->owned = true;
+    m->meta.memorder = h.node->meta.memorder;
+    made[k] = m;
+  }
+  for (size_t i = 0; i < nodes.size(); i++) {
+    Node *n = nodes[i];
+    if (out[i]) continue;
+    if (n->meta.numdim == D0) {
+      if (!n->has_value) throw MapError("materialize: a scalar was not computed");
+      out[i] = rt.constant(n->value, Arr2(), n->meta.dtype, n->meta.memorder, Arr2());
+    } else {
+      out[i] = made[slot.at(n)];
+    }
+  }
+  return out;
 }
 
 std::vector<std::string> Executor::compile_only(const std::vector<Node *> &targets, bool compile) {

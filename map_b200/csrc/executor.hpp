@@ -97,6 +97,12 @@ class Executor {
   // Rows beyond [y0, y1) (above and below, clipped to the raster) that
   // evaluate_rows reads from the inputs of `targets`.
   int row_margin(const std::vector<Node *> &targets);
+  // Evaluates `nodes` in one evaluation and returns, for each, a node that
+  // holds its value: a D2 result in a device buffer the library owns (freed
+  // with the returned node), a D0 result as a constant. Device inputs holding a
+  // whole raster and constants are returned as they are. Loop-carried values
+  // of a while-loop stay resident this way between iterations.
+  std::vector<Node *> materialize(const std::vector<Node *> &nodes);
   // Fusion + code generation + compilation only (no device needed).
   std::vector<std::string> compile_only(const std::vector<Node *> &targets, bool compile);
   std::string describe_groups(const std::vector<Node *> &targets);

@@ -46,12 +46,19 @@ struct HostData {
 };
 
 struct DevData {
-  void *ptr = nullptr;    // caller-owned device memory (address of raster row `row0`)
+  void *ptr = nullptr;    // device memory (address of raster row `row0`), caller-owned unless `owned`
   long long pitch = 0;    // bytes between rows
   // Row band: the memory holds raster rows row0 .. row0 + rows - 1 only
   // (rows == 0: the whole raster). Such an input is evaluated by row ranges
   // (Executor::evaluate_rows) that read no row outside the band.
   int row0 = 0, rows = 0;
+  // The library allocated the memory (Executor::materialize) and frees it,
+  // stream-ordered, with the last node that holds it.
+  bool owned = false;
+  DevData() = default;
+  DevData(const DevData &) = delete;
+  DevData &operator=(const DevData &) = delete;
+  ~DevData();
 };
 
 struct Node {

@@ -10,8 +10,10 @@
 # Differences from the reference module:
 #  * Python 3: `/` maps to __truediv__, `__bool__` replaces `__nonzero__`;
 #  * errors raise MapError with the library's message instead of asserting;
-#  * symbolic while-loops (python/map.py:234-330) raise MapError, as the
-#    reference runtime cannot execute them either;
+#  * while-loops over raster tests (python/map.py:234-330) are run by this
+#    module, one evaluation per iteration with loop-carried rasters kept
+#    resident, where the reference only captures them (its runtime has no task
+#    to execute them);
 #  * extensions at the end: NumPy in/out, border and launch-mode switches,
 #    device-resident inputs, flow direction / accumulation and viewshed helpers.
 ##
@@ -234,7 +236,36 @@ class Raster:
         raise MapError("unsupported neighbour access")
 
     def __bool__(self):
-        raise MapError("symbolic while-loops over rasters are not supported")
+        # Truth value of a scalar (D0) raster, evaluated. In the test of a
+        # `while` statement whose source file is readable, the whole loop runs
+        # here instead (_run_while: the reference's hook for symbolic loops,
+        # python/map.py:234-330) and the value returned makes the test false.
+        if _lib.ma_numdim(self) != D0:
+            raise MapError("the truth value of a 2-D raster is ambiguous: reduce it to a scalar (D0) raster first, "
+                           "e.g. with zmax or zor")
+        replay = getattr(_loop_tls, "replay", None)
+        if replay is not None:
+            return replay.answer(self)
+        if getattr(_loop_tls, "truth", 0) > 0:
+            return _truth_of(self)
+        frame = _sys._getframe(1)
+        loop = _while_at(frame)
+        if loop is None:
+            return _truth_of(self)
+        # A raster asked for later in the same evaluation of the test (a larger
+        # instruction offset than the request that ran the loop) belongs to the
+        # test the loop's answer ends: its own truth, no second loop.
+        done = _loop_tls.__dict__.setdefault("done", {})
+        key = (id(frame), frame.f_code.co_filename, loop.lineno)
+        last = done.pop(key, None)
+        if last is not None and frame.f_lasti > last:
+            done[key] = last
+            return _truth_of(self)
+        r = _run_while(loop, frame)
+        if len(done) > 64:
+            done.clear()
+        done[key] = frame.f_lasti
+        return r
 
     __hash__ = object.__hash__
 
@@ -361,6 +392,258 @@ for _sym, _bt in zip(BinaryTypeSym, BinaryTypeVal):
 # Python 2 spelling of the division operator, kept for callers that use it
 Raster.__div__ = Raster.__truediv__
 Raster.__rdiv__ = Raster.__rtruediv__
+
+## While-loops over rasters (python/map.py:234-330, runtime/Runtime.cpp:156-311)
+#
+# When Python asks for the truth value of a raster in a `while` test, the
+# reference re-reads the loop's source from the caller's file (inspect + ast),
+# runs the body twice symbolically to find the loop-carried values and builds
+# Loop nodes, which its runtime has no task to execute. Here the same hook runs
+# the loop: the test and the body, compiled from the caller's file, are
+# evaluated in the caller's namespace, one evaluation per iteration. Every
+# raster the body assigns (loop-carried) and every raster the loop reads but
+# does not assign (invariant) is kept resident through materialize(), so an
+# iteration evaluates only its own body, the test's reduction fused with it.
+# Afterwards the caller's variables hold the last iteration's values and the
+# hook returns the truth value that makes the caller's test false (found by
+# replaying the test), so Python leaves the loop (and runs its `else` clause).
+# `break`, `continue`, `return` and `yield` directly in such a body are not
+# supported; the test is evaluated more than once and should have no side
+# effects. Without a readable source (interactive input, exec of a string) a
+# raster test is just evaluated each time Python asks: the loop runs in
+# Python, correct but recomputing the loop's history at every test.
+
+import ast as _ast
+import linecache as _linecache
+import sys as _sys
+import threading as _threading
+
+_loop_tls = _threading.local()
+_tree_cache = {}
+
+
+def _truth_of(r):
+    _lib.ma_eval(ct.cast((Node * 1)(r._node), ct.POINTER(Node)), 1)
+    return bool(_lib.ma_value(r).value())
+
+
+def _file_tree(filename, module_globals):
+    lines = _linecache.getlines(filename, module_globals)
+    if not lines:
+        return None
+    text = "".join(lines)
+    key = (filename, hash(text))
+    tree = _tree_cache.get(key)
+    if tree is None:
+        try:
+            tree = _ast.parse(text, filename)
+        except SyntaxError:
+            return None
+        if len(_tree_cache) > 32:
+            _tree_cache.clear()
+        _tree_cache[key] = tree
+    return tree
+
+
+def _while_at(frame):
+    """The innermost `while` statement of the frame's file whose test spans the
+    frame's current line, or None."""
+    filename = frame.f_code.co_filename
+    if filename.startswith("<"):
+        return None
+    tree = _file_tree(filename, frame.f_globals)
+    if tree is None:
+        return None
+    line = frame.f_lineno
+    best = None
+    for node in _ast.walk(tree):
+        if isinstance(node, _ast.While) and node.test.lineno <= line <= node.test.end_lineno:
+            if best is None or node.lineno > best.lineno:
+                best = node
+    return best
+
+
+def _target_names(t, out):
+    if isinstance(t, _ast.Name):
+        out.add(t.id)
+    elif isinstance(t, (_ast.Tuple, _ast.List)):
+        for e in t.elts:
+            _target_names(e, out)
+    elif isinstance(t, _ast.Starred):
+        _target_names(t.value, out)
+    elif isinstance(t, (_ast.Subscript, _ast.Attribute)):   # x[m] = v updates the raster x in place
+        _target_names(t.value, out)
+
+
+def _loop_names(loop):
+    """(names the body assigns, names the test or body reads)."""
+    assigned, read = set(), set()
+    for stmt in loop.body:
+        for n in _ast.walk(stmt):
+            if isinstance(n, (_ast.Assign,)):
+                for t in n.targets:
+                    _target_names(t, assigned)
+            elif isinstance(n, (_ast.AugAssign, _ast.AnnAssign, _ast.NamedExpr)):
+                _target_names(n.target, assigned)
+            elif isinstance(n, (_ast.For, _ast.AsyncFor, _ast.comprehension)):
+                _target_names(n.target, assigned)
+            elif isinstance(n, (_ast.With, _ast.AsyncWith)):
+                for it in n.items:
+                    if it.optional_vars is not None:
+                        _target_names(it.optional_vars, assigned)
+            elif isinstance(n, _ast.Delete):
+                for t in n.targets:
+                    _target_names(t, assigned)
+    for n in _ast.walk(loop.test):
+        if isinstance(n, _ast.NamedExpr):
+            _target_names(n.target, assigned)
+    for part in [loop.test] + loop.body:
+        for n in _ast.walk(part):
+            if isinstance(n, _ast.Name) and isinstance(n.ctx, _ast.Load):
+                read.add(n.id)
+    return assigned, read
+
+
+def _check_body(loop):
+    def visit(node, in_loop):
+        for c in _ast.iter_child_nodes(node):
+            if isinstance(c, (_ast.FunctionDef, _ast.AsyncFunctionDef, _ast.Lambda, _ast.ClassDef)):
+                continue
+            if isinstance(c, (_ast.Return, _ast.Yield, _ast.YieldFrom, _ast.Await)) or (
+                    not in_loop and isinstance(c, (_ast.Break, _ast.Continue))):
+                raise MapError("line %d: %s inside a while-loop over rasters is not supported"
+                               % (c.lineno, type(c).__name__.lower()))
+            visit(c, in_loop or isinstance(c, (_ast.For, _ast.AsyncFor, _ast.While)))
+    for stmt in loop.body:
+        visit(_ast.Module(body=[stmt], type_ignores=[]), False)
+
+
+def _swap_nodes(rasters):
+    """Replaces, in place, the node of each raster by one holding its value
+    (one evaluation for all)."""
+    uniq = []
+    seen = set()
+    for r in rasters:
+        if id(r) not in seen:
+            seen.add(id(r))
+            uniq.append(r)
+    if not uniq:
+        return
+    n = len(uniq)
+    arr = (Node * n)(*[r._node for r in uniq])
+    out = (Node * n)()
+    _lib.ma_materialize(arr, n, out)
+    for r, m in zip(uniq, out):
+        m = m.value if isinstance(m, Node) else m
+        if m != r._node.value:
+            tmp = Raster(Node(m))                      # a reference to the new node
+            r._node, tmp._node = tmp._node, r._node
+            del tmp                                    # releases the old one
+
+
+class _Replay:
+    """Answers raster truth requests while the test is replayed after the loop:
+    the first one (the raster whose truth started the loop) with `first`, later
+    ones with their evaluated truth; names read before the first request see
+    their values from before the loop, as Python's own evaluation of the test
+    did."""
+
+    def __init__(self, first):
+        self.first = first
+        self.switched = False
+        self.given = {}            # a raster asked again (the value of `a and b`) gets the same answer
+
+    def answer(self, r):
+        if id(r) in self.given:
+            return self.given[id(r)][1]
+        if not self.switched:
+            self.switched = True
+            v = self.first
+        else:
+            v = _truth_of(r)
+        self.given[id(r)] = (r, v)
+        return v
+
+
+class _ReplayScope:
+    def __init__(self, replay, before, lookup):
+        self.replay, self.before, self.lookup = replay, before, lookup
+
+    def __getitem__(self, name):
+        if not self.replay.switched and name in self.before:
+            return self.before[name]
+        return self.lookup(name)
+
+
+def _run_while(loop, frame):
+    _check_body(loop)
+    filename = frame.f_code.co_filename
+    test_code = compile(_ast.Expression(body=loop.test), filename, "eval")
+    body_code = compile(_ast.Module(body=loop.body, type_ignores=[]), filename, "exec")
+    g = frame.f_globals
+    scope = frame.f_locals            # the module namespace at module level, else the frame's locals
+    module_level = scope is g
+    assigned, read = _loop_names(loop)
+    missing = object()
+
+    def lookup(name):
+        if name in scope:
+            return scope[name]
+        if name in g:
+            return g[name]
+        if hasattr(_builtins, name):
+            return getattr(_builtins, name)
+        raise KeyError(name)
+
+    def get(name):
+        try:
+            return lookup(name)
+        except KeyError:
+            return missing
+
+    test_names = {n.id for n in _ast.walk(loop.test) if isinstance(n, _ast.Name)}
+    before = {n: get(n) for n in test_names}
+    before = {k: v for k, v in before.items() if v is not missing}
+    _swap_nodes([v for v in (get(n) for n in sorted(read - assigned)) if isinstance(v, Raster)])
+    try:
+        while True:
+            _loop_tls.truth = getattr(_loop_tls, "truth", 0) + 1
+            try:
+                t = _builtins.eval(test_code, g, scope)
+            finally:
+                _loop_tls.truth -= 1
+            carried = [v for v in (get(n) for n in sorted(assigned)) if isinstance(v, Raster)]
+            if isinstance(t, Raster):
+                if _lib.ma_numdim(t) != D0:
+                    raise MapError("line %d: the while test is a 2-D raster: reduce it to a scalar (D0) raster first"
+                                   % loop.test.lineno)
+                _swap_nodes([t] + carried)
+                go = bool(_lib.ma_value(t).value())
+            else:
+                _swap_nodes(carried)
+                go = bool(t)
+            del t, carried
+            _lib.ma_collectGarbage()
+            if not go:
+                break
+            _builtins.exec(body_code, g, scope)
+    finally:
+        if not module_level and _sys.version_info < (3, 13):
+            ct.pythonapi.PyFrame_LocalsToFast(ct.py_object(frame), ct.c_int(0))
+    for first in (False, True):
+        replay = _Replay(first)
+        _loop_tls.replay = replay
+        try:
+            t = _builtins.eval(test_code, g, _ReplayScope(replay, before, lookup))
+            if isinstance(t, Raster):            # the test itself: Python asks for its truth
+                t = replay.answer(t)
+        finally:
+            _loop_tls.replay = None
+        if not t:
+            return first
+    raise MapError("line %d: the while test stays true after the loop ended (a test with side effects?)"
+                   % loop.test.lineno)
+
 
 ## Standalone functions
 
@@ -757,6 +1040,28 @@ def to_device(raster, ptr, pitch, sync=True):
     _lib.ma_toDevice(raster, ct.c_void_p(ptr), pitch, 0 if sync else 1)
 
 
+def materialize(*rasters):
+    """Evaluates the rasters in one evaluation and returns, for each, a raster
+    holding its value: 2-D results stay in device memory the library owns
+    (released with the returned raster), scalars become constants."""
+    out = []
+    for r in rasters:
+        c = Raster(r._node)
+        out.append(c)
+    _swap_nodes(out)
+    return out
+
+
+def node_count():
+    """Nodes the runtime holds (after collect_garbage: the live ones)."""
+    return _lib.ma_nodeCount()
+
+
+def collect_garbage():
+    """Drops the nodes no raster refers to, with the device memory they own."""
+    _lib.ma_collectGarbage()
+
+
 def set_border(mode):
     _lib.ma_setBorder(mode)
 
@@ -1022,6 +1327,9 @@ _sig('ma_fromHost', [ct.c_void_p, Array, ct.c_int, Array, ct.c_int], Node)
 _sig('ma_fromDevice', [ct.c_void_p, ct.c_longlong, Array, ct.c_int, Array], Node)
 _sig('ma_toHost', [Raster, ct.c_void_p, ct.c_size_t], ct.c_int)
 _sig('ma_toDevice', [Raster, ct.c_void_p, ct.c_longlong, ct.c_int], ct.c_int)
+_sig('ma_materialize', [ct.POINTER(Node), ct.c_int, ct.POINTER(Node)], ct.c_int)
+_sig('ma_collectGarbage', [], None)
+_sig('ma_nodeCount', [], ct.c_int, check=False)
 _sig('ma_sync', [], ct.c_int)
 _sig('ma_stream', [], ct.c_void_p)
 _sig('ma_lastLaunchCount', [], ct.c_int, check=False)

@@ -48,7 +48,7 @@ def test_errors_are_reported_not_fatal(M):
         M._lib.ma_unary(M.Raster(), M.SIN)
     with pytest.raises(M.MapError):
         M.read("/nonexistent/file.bin")
-    with pytest.raises(M.MapError, match="symbolic loops"):
+    with pytest.raises(M.MapError, match="symbolic loop capture"):
         M._lib.ma_loopStart()
     # the error state clears on the next successful call
     r = M.zeros([8, 8])
