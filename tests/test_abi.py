@@ -96,7 +96,7 @@ def test_scalar_graph_evaluates_on_host(M):
     assert M.value(c) == np.float32(np.sqrt(np.float32(7 * 2.5 + 1)))
 
 
-def test_symbolic_while_is_rejected(M):
+def test_truth_of_a_2d_raster_is_rejected(M):
     r = M.zeros([4, 4])
-    with pytest.raises(M.MapError):
+    with pytest.raises(M.MapError, match="2-D raster"):
         bool(r)
