@@ -455,12 +455,22 @@ def _while_at(frame):
     if tree is None:
         return None
     line = frame.f_lineno
-    best = None
-    for node in _ast.walk(tree):
-        if isinstance(node, _ast.While) and node.test.lineno <= line <= node.test.end_lineno:
-            if best is None or node.lineno > best.lineno:
-                best = node
-    return best
+    spans = _while_spans.get(id(tree))
+    if spans is None or spans[0] is not tree:
+        tests = [n for n in _ast.walk(tree) if isinstance(n, _ast.While)]
+        spans = (tree, {})
+        for n in tests:
+            for l in range(n.test.lineno, n.test.end_lineno + 1):
+                b = spans[1].get(l)
+                if b is None or n.lineno > b.lineno:       # the innermost statement
+                    spans[1][l] = n
+        if len(_while_spans) > 32:
+            _while_spans.clear()
+        _while_spans[id(tree)] = spans
+    return spans[1].get(line)
+
+
+_while_spans = {}   # id(tree) -> (tree, {line: innermost while statement whose test spans it})
 
 
 def _target_names(t, out):
