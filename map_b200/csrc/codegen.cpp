@@ -1481,15 +1481,32 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     t.halo_y = hy;
     P.tma.push_back(t);
   }
+  // opt-in output tile store: the single output's TW x TH tile staged after the inputs
+  if (focal_tune().tstore && nst > 0 && G.outk.size() == 1) {
+    Node *o = G.outk.begin()->first;
+    const int es = (int)dt_size(o->meta.dtype);
+    if ((TW * es) % 16 == 0) {
+      TmaSpec t;
+      t.in_index = G.outk.begin()->second;
+      t.dtype = o->meta.dtype;
+      t.box_w = TW;
+      t.box_h = TH;
+      off = (off + 127) / 128 * 128;
+      t.smem_off = off;
+      off += (size_t)TW * TH * es;
+      P.tma_out.push_back(t);
+    }
+  }
   off = (off + 15) / 16 * 16;
   const size_t bar_off = off;
   bool use_tma = nst > 0 && hx <= 16 && hy <= 16;
   for (auto &t : P.tma)
     if (t.box_w > 256 || t.box_h > 256) use_tma = false;
   if (use_tma && off + 16 > 200 * 1024) use_tma = false;
+  if (!use_tma) P.tma_out.clear();
   P.smem_bytes = use_tma ? off + 16 : 0;
   P.bar_off = bar_off;
-  body << G.args_struct(use_tma ? nst : 0, false) << G.shade_decls();
+  body << G.args_struct(use_tma ? nst + (int)P.tma_out.size() : 0, false) << G.shade_decls();
   body << "template <";
   for (int k = 0; k < nst; k++) body << (k ? ", " : "") << "class F" << k;
   body << ">\n__device__ __forceinline__ void focal_cell(const Args &a";
@@ -1654,12 +1671,32 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
               << "      " << callr.str() << ";\n"
               << "    }\n";
     if (flagged) loop_full << "    }\n";
+    // output tile store (opt-in; whole-raster outputs, full tiles): the results
+    // go to the staging tile, then one thread stores it with one TMA copy
+    const bool tstore = !P.tma_out.empty() && !pair && !cpair;
+    if (tstore) {
+      const TmaSpec &to = P.tma_out[0];
+      const std::string ty = G.T(G.outk.begin()->first);
+      loop_full << "    if (a.aux[2] != 0 && t.xe == t.x0 + " << TW << " && t.ye == t.y0 + " << TH << ") {\n"
+                << "      " << ty << " *os = (" << ty << " *)(smem + " << to.smem_off << ");\n"
+                << "#pragma unroll\n"
+                << "      for (int k = 0; k < " << R << "; k++) os[(ly0 + k) * " << TW << " + lx] = r0[k];\n"
+                << "      fence_proxy_async();\n"
+                << "      __syncthreads();\n"
+                << "      if (threadIdx.x == 0) {\n"
+                << "        tma_store_2d(&a.tm[" << nst << "], os, t.x0, t.y0 - a.g.oy);\n"
+                << "        bulk_commit_group();\n"
+                << "        bulk_wait_group_read0();\n"
+                << "      }\n"
+                << "    } else {\n";
+    }
     loop_full << bases.str()
               << "#pragma unroll\n"
               << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
               << "      const int y = t.y0 + ly0 + k;\n"
               << outs.str()
               << "    }\n";
+    if (tstore) loop_full << "    }\n";
   } else {
     loop_full << unroll
               << "    for (int k = 0; k < " << R << "; k += " << step << ") {\n"
@@ -1834,7 +1871,10 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
          << "  griddep_wait();\n"
          << "  run_tile_t(a, tile_at<" << TW << ", " << TH << ">(a.g, blockIdx.x, blockIdx.y), smem, nullptr, phase, false);\n";
   wrap << "}\n";
-  if (!use_tma) P.tma.clear();
+  if (!use_tma) {
+    P.tma.clear();
+    P.tma_out.clear();
+  }
 }
 
 static std::string gen_zonal(Gen &G) {
@@ -2559,6 +2599,7 @@ const FocalTune &focal_tune() {
         else if (k == "cpair") r.cpair = v;
         else if (k == "fflag") r.fflag = v;
         else if (k == "fmerge") r.fmerge = v;
+        else if (k == "tstore") r.tstore = v;
       }
       i = j + 1;
     }

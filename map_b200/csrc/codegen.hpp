@@ -53,6 +53,9 @@ struct KernelPlan {
   std::vector<Node *> scalars;      // a.s[k]
   std::vector<Node *> zonal;        // reductions, in partial-slot order
   std::vector<TmaSpec> tma;
+  // Output tile stores (focal, opt-in): in_index is the output's index, the
+  // staging tile sits at smem_off, the tensor maps follow the inputs' maps.
+  std::vector<TmaSpec> tma_out;
   int threads = 256;
   int tile_w = 64, tile_h = 32;
   int min_blocks = 0;   // minimum resident CTAs per SM in the launch bounds (0: none)
@@ -84,6 +87,8 @@ struct FocalTune {
                                     // 2.5% slower: a dependent chain through the record)
   int fmerge = 1;                   // fast form: the exact leading term of a derivative sum as the addend of the
                                     // neighbouring fused multiply-add (0: every sum from +0)
+  int tstore = 0;                   // interior tiles of single-output focal groups store their results through
+                                    // shared memory with one TMA tile store (1) instead of one global store per cell
 };
 const FocalTune &focal_tune();
 

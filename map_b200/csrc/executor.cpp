@@ -268,7 +268,8 @@ std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &
 
 std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
                                      std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
-                                     const uint64_t aux[4], const std::unordered_map<const Node *, Variant> *scalars) {
+                                     const uint64_t aux[4], const std::unordered_map<const Node *, Variant> *scalars,
+                                     bool out_maps) {
   CudaEnv &env = CudaEnv::get();
   std::vector<unsigned char> a(K.args_size, 0);
   int32_t oy = 0;
@@ -318,7 +319,23 @@ std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const 
   std::memcpy(a.data() + K.off_geom, geom, sizeof geom);
   uint64_t errp = (uint64_t)(uintptr_t)env.err_word();
   std::memcpy(a.data() + K.off_err, &errp, 8);
-  std::memcpy(a.data() + K.off_aux, aux, 4 * sizeof(uint64_t));
+  uint64_t ax[4] = {aux[0], aux[1], aux[2], aux[3]};
+  // output tile stores: maps over the whole output rasters, after the inputs' maps
+  bool omaps = out_maps && !K.tma_out.empty();
+  for (size_t j = 0; omaps && j < K.tma_out.size(); j++) {
+    const TmaSpec &t = K.tma_out[j];
+    const DevRaster &r = bufs.at(K.out_rasters[t.in_index]);
+    if (((uintptr_t)r.ptr & 15) != 0 || (r.pitch & 15) != 0 || r.rows != 0) {
+      omaps = false;
+      break;
+    }
+    alignas(64) unsigned char desc[128];
+    env.encode_tma_2d(desc, r.dtype, r.ptr, (uint64_t)r.W, (uint64_t)r.H, (uint64_t)r.pitch, (uint32_t)t.box_w,
+                      (uint32_t)t.box_h);
+    std::memcpy(a.data() + K.off_tm + 128 * (K.tma.size() + j), desc, 128);
+  }
+  if (!K.tma_out.empty()) ax[2] = omaps ? 1 : 0;
+  std::memcpy(a.data() + K.off_aux, ax, 4 * sizeof(uint64_t));
   return a;
 }
 
@@ -679,7 +696,7 @@ void Executor::evaluate(const std::vector<Node *> &targets_in, const std::vector
   auto build_args = [&](const Group &g, const KernelPlan &K, int rx0, int ry0, int rx1, int ry1, uint64_t aux0,
                         uint64_t aux1) {
     uint64_t aux[4] = {aux0, aux1, 0, 0};
-    return pack_args(g, K, get, bufs, rx0, ry0, rx1, ry1, aux);
+    return pack_args(g, K, get, bufs, rx0, ry0, rx1, ry1, aux, nullptr, true);
   };
 
   auto ensure_outputs = [&](const Group &g, const KernelPlan &K) {

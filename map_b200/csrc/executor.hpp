@@ -63,10 +63,13 @@ std::vector<PlainJob> plain_schedule(const std::vector<std::unique_ptr<Group>> &
 // Packs the kernel argument struct of plan K for a launch over region
 // [rx0,rx1) x [ry0,ry1); rasters are looked up with `get` (inputs) and in `bufs` (outputs).
 // `scalars`, when given, overrides the values of scalar argument nodes.
+// `out_maps`: the outputs are whole rasters at their own base addresses, so a
+// plan with output tile stores (K.tma_out) gets their tensor maps and aux[2] = 1.
 std::vector<unsigned char> pack_args(const Group &g, const KernelPlan &K, const std::function<DevRaster &(Node *)> &get,
                                      std::unordered_map<Node *, DevRaster> &bufs, int rx0, int ry0, int rx1, int ry1,
                                      const uint64_t aux[4],
-                                     const std::unordered_map<const Node *, Variant> *scalars = nullptr);
+                                     const std::unordered_map<const Node *, Variant> *scalars = nullptr,
+                                     bool out_maps = false);
 
 // Every node `targets` depend on (themselves included), in id (= topological) order.
 std::vector<Node *> collect_nodes(const std::vector<Node *> &targets);

@@ -872,6 +872,19 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const TmaDesc *tmap, u64 
       : "memory");
 }
 
+// Tile store from shared memory to the tensor the map describes, at element
+// (x, y): x times the element size a multiple of 16 bytes, y >= 0; cells outside
+// the tensor's extent are not written. Threads fence their shared-memory
+// writes (fence_proxy_async) and synchronise before one thread issues it, and
+// that thread waits until the copy has read shared memory before the CTA ends.
+__device__ __forceinline__ void tma_store_2d(const TmaDesc *tmap, const void *src, int x, int y) {
+  asm volatile("cp.async.bulk.tensor.2d.global.shared::cta.tile.bulk_group [%0, {%1, %2}], [%3];" ::"l"((u64)tmap),
+               "r"(x), "r"(y), "r"(smem_u32(src))
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit_group() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_group_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+
 // ------------------------------------------------------------------ tiles
 
 // Tile t of the launch region: origin and the end of the computed cells.
