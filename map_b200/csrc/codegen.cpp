@@ -1481,8 +1481,12 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
     t.halo_y = hy;
     P.tma.push_back(t);
   }
-  // opt-in output tile store: the single output's TW x TH tile staged after the inputs
-  if (focal_tune().tstore && nst > 0 && G.outk.size() == 1) {
+  // output tile store: the single output's TW x TH tile staged after the inputs
+  // (by default for the fast hillshade form, whose interior tiles keep their
+  // results in registers one cell per thread step, the form the store serves)
+  const FocalTune &ft0 = focal_tune();
+  if (nst > 0 && G.outk.size() == 1 &&
+      (ft0.tstore >= 2 || (ft0.tstore == 1 && G.any_fast() && !ft0.fpair && !ft0.cpair))) {
     Node *o = G.outk.begin()->first;
     const int es = (int)dt_size(o->meta.dtype);
     if ((TW * es) % 16 == 0) {
