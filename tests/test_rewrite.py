@@ -208,3 +208,22 @@ def test_fast_form_equals_general_form_replay():
     r = (1.0 / np.sqrt(v.astype(np.float64))).astype(f32)
     fast = (fma32(f32(k["sz"] / 8), num, k["cz"]) * r).astype(f32)
     assert np.array_equal(fast[inner].view(np.uint32), general[inner].view(np.uint32))
+
+
+def test_fast_form_kernel_shape(R):
+    """The fast hillshade kernel: 64 x 64 tiles of 256 threads with registers
+    capped for 6 CTAs per SM, interior tiles stored by one TMA tile store
+    (whole-raster outputs; the per-cell stores stay for the other paths). Other
+    focal kernels keep their per-cell stores and launch bounds."""
+    import re
+    M = R
+    d = M.from_numpy(np.zeros((512, 512), np.float32), bs=[256, 256])
+    src = M.generated_source(W.hillshade(d))
+    assert re.search(r"__launch_bounds__\(256, 6\) map_focal_", src)
+    assert "tma_store_2d(&a.tm[1], os, t.x0, t.y0 - a.g.oy);" in src
+    assert "a.aux[2] != 0 && t.xe == t.x0 + 64 && t.ye == t.y0 + 64" in src
+    assert "str_out_row<float>(ob0, op0, k, r0[k]);" in src        # the fallback path
+    other = M.generated_source(M.convolve(d, [[1, 2, 1], [2, 4, 2], [1, 2, 1]]) * 0.0625)
+    assert "tma_store_2d" not in other and "__launch_bounds__(128) map_focal_" in other
+    life = M.generated_source(W.life_step(M.from_numpy(np.zeros((256, 256), np.uint8), bs=[128, 128])))
+    assert "tma_store_2d" not in life
