@@ -595,6 +595,23 @@ def _run_while(loop, frame):
     module_level = scope is g
     assigned, read = _loop_names(loop)
     missing = object()
+    # in a function, a name the body assigns that is not one of the function's
+    # variables is declared global there: the body's stores go to its module
+    # (a namespace frame, such as a module, a class body or an outer loop's
+    # body, keeps its stores in its own mapping)
+    co = frame.f_code
+    own = set(co.co_varnames) | set(co.co_cellvars) | set(co.co_freevars)
+    function = bool(co.co_flags & 0x1)   # CO_OPTIMIZED: the frame of a function
+    to_module = {n for n in assigned if n not in own} if function and not module_level else set()
+
+    def flush_globals():
+        for n in to_module:
+            try:
+                if n in scope:
+                    g[n] = scope[n]
+                    del scope[n]
+            except (KeyError, TypeError):
+                pass
 
     def lookup(name):
         if name in scope:
@@ -637,8 +654,10 @@ def _run_while(loop, frame):
             if not go:
                 break
             _builtins.exec(body_code, g, scope)
+            flush_globals()
     finally:
-        if not module_level and _sys.version_info < (3, 13):
+        flush_globals()
+        if function and _sys.version_info < (3, 13):   # 3.13 frames' locals write through
             ct.pythonapi.PyFrame_LocalsToFast(ct.py_object(frame), ct.c_int(0))
     for first in (False, True):
         replay = _Replay(first)

@@ -157,3 +157,45 @@ def test_module_level_loop_and_source_less_fallback(tmp_path):
     r = subprocess.run([sys.executable, str(script)], capture_output=True, text=True, timeout=120, env=env)
     assert r.returncode == 0, r.stderr
     assert r.stdout.split() == ["12", "4", "6"]
+
+
+_G = None
+
+
+def test_global_and_nonlocal_names_assigned_in_the_loop(L):
+    global _G
+    _G = L.zeros(dt=L.S32)
+
+    def bump():
+        global _G
+        n = 0
+        while _G < 5:
+            _G = _G + 1
+            n += 1
+        return n
+
+    assert bump() == 5 and L.value(_G) == 5
+
+    def outer():
+        c = L.zeros(dt=L.S32)
+
+        def inner():
+            nonlocal c
+            while c < 3:
+                c = c + 1
+
+        inner()
+        return L.value(c)
+
+    assert outer() == 3
+
+
+def test_loop_in_a_method_and_tuple_assignment(L):
+    class Acc:
+        def run(self, k):
+            a, b = L.zeros(dt=L.S32), L.ones(dt=L.S32)
+            while b < k:
+                a, b = b, a + b          # Fibonacci
+            return L.value(a), L.value(b)
+
+    assert Acc().run(50) == (34, 55)
