@@ -495,7 +495,7 @@ def _loop_names(loop):
                     _target_names(t, assigned)
             elif isinstance(n, (_ast.AugAssign, _ast.AnnAssign, _ast.NamedExpr)):
                 _target_names(n.target, assigned)
-            elif isinstance(n, (_ast.For, _ast.AsyncFor, _ast.comprehension)):
+            elif isinstance(n, (_ast.For, _ast.AsyncFor)):      # (comprehension variables do not persist)
                 _target_names(n.target, assigned)
             elif isinstance(n, (_ast.With, _ast.AsyncWith)):
                 for it in n.items:
