@@ -179,6 +179,28 @@ inline Variant value(const Raster &r) {
   detail::check();
   return Variant(v);
 }
+/* The truth value of a scalar (D0) raster, evaluated: the test of a loop over
+ * rasters (the reference captures Python `while` loops, python/map.py:234-330,
+ * but cannot run them). */
+inline bool truth(const Raster &r) {
+  if (r.numdim() != D0) throw Error("map: the truth value of a 2-D raster is ambiguous: reduce it first");
+  eval({r});
+  return value(r).get() != 0.0;
+}
+/* Evaluates the rasters in one evaluation and makes each hold its value
+ * (ma_materialize): 2-D rasters stay in device memory the library owns, scalars
+ * become constants, and the nodes no raster refers to are dropped. A loop
+ * keeps its loop-carried rasters resident this way, so an iteration evaluates
+ * only its own body:
+ *   while (map::truth(d > 0)) { y = step(x); d = zsum(y - x); x = y; map::materialize({&x, &d}); } */
+inline void materialize(std::initializer_list<Raster *> list) {
+  std::vector<ma_Node *> in, out(list.size(), nullptr);
+  for (Raster *r : list) in.push_back(r->node);
+  if (ma_materialize(in.data(), (int)in.size(), out.data()) != 0) throw Error(ma_lastError());
+  size_t i = 0;
+  for (Raster *r : list) *r = Raster(out[i++]);
+  ma_collectGarbage();
+}
 inline Raster read(const std::string &path) { return Raster(ma_read(path.c_str())); }
 inline int write(const Raster &r, const std::string &path) {
   int e = ma_write(r.node, path.c_str());

@@ -80,6 +80,18 @@ int main(int argc, char **argv) {
       std::fputs(buf.data(), stdout);
       return 0;
     }
+    if (argc >= 2 && std::string(argv[1]) == "loop") {
+      // a scalar loop with its carried rasters materialised every iteration
+      Raster x = zeros(DataSize(), S32);
+      int k = 0;
+      while (truth(x < Variant((int32_t)10))) {
+        x = x + Variant((int32_t)3);
+        materialize({&x});
+        k++;
+      }
+      std::printf("%d %d %d\n", (int)value(x).get(), k, ma_nodeCount());
+      return 0;
+    }
     if (argc >= 6 && std::string(argv[1]) == "eval") {
       const int W = std::atoi(argv[3]), H = std::atoi(argv[4]);
       const size_t n = (size_t)W * H;
@@ -106,6 +118,6 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "map error: %s\n", e.what());
     return 3;
   }
-  std::fprintf(stderr, "usage: frontend_programs source W H | eval in.f32 W H out\n");
+  std::fprintf(stderr, "usage: frontend_programs source W H | eval in.f32 W H out | loop\n");
   return 1;
 }

@@ -39,6 +39,12 @@ def test_cpp_hillshade_builds_the_same_kernels_as_python(M, program):
     assert "map_focal_" in got
 
 
+def test_cpp_scalar_loop_with_materialize(program):
+    out = subprocess.run([program, "loop"], check=True, capture_output=True, text=True).stdout.split()
+    assert out[:2] == ["12", "4"]
+    assert int(out[2]) < 16          # the loop's history is dropped as it goes
+
+
 @pytest.mark.gpu
 def test_cpp_programs_match_python_results(M, program, tmp_path):
     h, w = 240, 310
