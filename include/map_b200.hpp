@@ -192,7 +192,7 @@ inline bool truth(const Raster &r) {
  * become constants, and the nodes no raster refers to are dropped. A loop
  * keeps its loop-carried rasters resident this way, so an iteration evaluates
  * only its own body:
- *   while (map::truth(d > 0)) { y = step(x); d = zsum(y - x); x = y; map::materialize({&x, &d}); } */
+ *   while (map::truth(d > 0)) { y = step(x); d = zonalSum(y - x); x = y; map::materialize({&x, &d}); } */
 inline void materialize(std::initializer_list<Raster *> list) {
   std::vector<ma_Node *> in, out(list.size(), nullptr);
   for (Raster *r : list) in.push_back(r->node);
