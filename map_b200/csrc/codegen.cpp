@@ -1485,7 +1485,7 @@ static void gen_focal(Gen &G, std::ostringstream &body, std::ostringstream &wrap
   // (by default for the fast hillshade form, whose interior tiles keep their
   // results in registers one cell per thread step, the form the store serves)
   const FocalTune &ft0 = focal_tune();
-  if (nst > 0 && G.outk.size() == 1 &&
+  if (P.tile_store && nst > 0 && G.outk.size() == 1 &&
       (ft0.tstore >= 2 || (ft0.tstore == 1 && G.any_fast() && !ft0.fpair && !ft0.cpair))) {
     Node *o = G.outk.begin()->first;
     const int es = (int)dt_size(o->meta.dtype);
@@ -2641,6 +2641,7 @@ KernelPlan generate_kernel(const Group &g, TileCfg cfg) {
   P.tile_w = cfg.tw;
   P.tile_h = cfg.th;
   P.min_blocks = cfg.minb;
+  P.tile_store = cfg.tile_store;
   Gen G(g, P);
   G.classify();
   std::string src;

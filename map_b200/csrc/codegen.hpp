@@ -29,6 +29,10 @@ struct TmaSpec {
 struct TileCfg {
   int tw = 64, th = 32, nt = 256;
   int minb = 0;   // focal kernels: minimum resident CTAs per SM in the launch bounds (0: none)
+  // focal kernels of the executor's own launches: interior tiles may store a
+  // single output with one TMA tile store (FocalTune::tstore says for which
+  // groups); the batched and serving dispatchers keep per-cell stores
+  bool tile_store = false;
 };
 bool tile_cfg_valid(const TileCfg &c);
 // Whether a focal group's interior tiles compute four byte cells of a row per
@@ -59,6 +63,7 @@ struct KernelPlan {
   int threads = 256;
   int tile_w = 64, tile_h = 32;
   int min_blocks = 0;   // minimum resident CTAs per SM in the launch bounds (0: none)
+  bool tile_store = false;   // TileCfg::tile_store
   int halo_x = 0, halo_y = 0;
   size_t smem_bytes = 0;
   int aux_count = 0;

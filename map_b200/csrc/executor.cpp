@@ -391,6 +391,7 @@ Executor::Prepared Executor::prepare(const std::vector<Node *> &targets, const s
       if (ft.ltw) cfg.tw = ft.ltw;
       if (ft.lth) cfg.th = ft.lth;
     }
+    cfg.tile_store = g->skeleton == SK_FOCAL;   // whole-raster launches: the output tile store where it applies
     P.plans[g->id] = generate_kernel(*g, cfg);
     if (compile && seen.insert(P.plans[g->id].source).second) {
       const std::string *src = &P.plans[g->id].source;
