@@ -585,15 +585,28 @@ class _ReplayScope:
         return self.lookup(name)
 
 
+_loop_code = {}   # id(while statement) -> (statement, test code, body code, names assigned, names read)
+
+
+def _compiled(loop, filename):
+    c = _loop_code.get(id(loop))
+    if c is None or c[0] is not loop:
+        _check_body(loop)
+        assigned, read = _loop_names(loop)
+        c = (loop, compile(_ast.Expression(body=loop.test), filename, "eval"),
+             compile(_ast.Module(body=loop.body, type_ignores=[]), filename, "exec"), assigned, read)
+        if len(_loop_code) > 256:
+            _loop_code.clear()
+        _loop_code[id(loop)] = c
+    return c
+
+
 def _run_while(loop, frame):
-    _check_body(loop)
     filename = frame.f_code.co_filename
-    test_code = compile(_ast.Expression(body=loop.test), filename, "eval")
-    body_code = compile(_ast.Module(body=loop.body, type_ignores=[]), filename, "exec")
+    _, test_code, body_code, assigned, read = _compiled(loop, filename)
     g = frame.f_globals
     scope = frame.f_locals            # the module namespace at module level, else the frame's locals
     module_level = scope is g
-    assigned, read = _loop_names(loop)
     missing = object()
     # in a function, a name the body assigns that is not one of the function's
     # variables is declared global there: the body's stores go to its module
