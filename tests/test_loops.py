@@ -199,3 +199,17 @@ def test_loop_in_a_method_and_tuple_assignment(L):
             return L.value(a), L.value(b)
 
     assert Acc().run(50) == (34, 55)
+
+
+def test_materialize_constants_pass_through_and_device_errors_are_reported(L):
+    """A constant raster comes back as it is (nothing to evaluate); a computed
+    2-D raster needs the device: without one the error is reported and the
+    library stays usable."""
+    a = L.zeros([8, 8], dt=L.S32, bs=[8, 8])
+    (b,) = L.materialize(a)
+    assert b._node.value == a._node.value
+    import torch
+    if not torch.cuda.is_available():
+        with pytest.raises(L.MapError):
+            L.materialize(a + 1)
+    assert L.value(L.materialize(L.zeros(dt=L.S32) + 2)[0]) == 2
