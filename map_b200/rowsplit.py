@@ -215,3 +215,69 @@ def zone_stats_allreduce(count, vmin, vmax, vsum, dist):
     dist.all_reduce(s, op=dist.ReduceOp.SUM)
     out_dev = count.device
     return c.to(out_dev), key_f32(-kmin).to(out_dev), key_f32(kmax).to(out_dev), s.to(out_dev)
+
+
+# ---- whole-raster reductions across ranks (the zonal skeleton's D0 results)
+
+SUM, PROD, AND, OR, MAX, MIN = 1, 2, 3, 4, 6, 7   # the map module's reduction codes (python/map.py:85)
+
+
+def f64_key(x):
+    """Order-preserving int64 key of float64 values: a < b as floats exactly
+    when key(a) < key(b) (-0 below +0; NaN excluded)."""
+    import torch
+    i = x.contiguous().view(torch.int64)
+    return torch.where(i >= 0, i, -(i & 0x7FFFFFFFFFFFFFFF) - 1)
+
+
+def key_f64(k):
+    """Inverse of f64_key."""
+    import torch
+    lo = torch.iinfo(torch.int64).min
+    return torch.where(k >= 0, k, (-k - 1) | lo).view(torch.float64)
+
+
+def zonal_allreduce(value, red, dist, bits=None, signed=True):
+    """Combines every rank's reduction of its own rows (a Python number, such
+    as M.value(M.zsum(band)) over the rank's own rows) into the whole raster's,
+    on every rank; `red` is the map module's reduction code (zsum SUM, zprod
+    PROD, zmax MAX, zmin MIN, rAND, rOR). Integers combine exactly in int64
+    (wrapped to a `bits`-wide signed or unsigned type when given, as the
+    raster type's arithmetic wraps);
+    float sums and products combine in float64, so they agree with a
+    one-device evaluation to that type's rounding; float MAX and MIN travel as
+    order-preserving integer keys and are exact and independent of the rank
+    order; rAND / rOR are the MIN / MAX of the ranks' truth values."""
+    import torch
+    if dist is None:
+        return value
+    integer = isinstance(value, (bool, int)) and not isinstance(value, float)
+    if red in (AND, OR):
+        t = torch.tensor([1 if value else 0], dtype=torch.int64)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN if red == AND else dist.ReduceOp.MAX)
+        return bool(t.item())
+    if red in (MAX, MIN):
+        if integer:
+            t = torch.tensor([int(value)], dtype=torch.int64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX if red == MAX else dist.ReduceOp.MIN)
+            return int(t.item())
+        k = f64_key(torch.tensor([float(value)], dtype=torch.float64))
+        if red == MIN:
+            k = -k
+        dist.all_reduce(k, op=dist.ReduceOp.MAX)
+        return float(key_f64(k if red == MAX else -k).item())
+    if red not in (SUM, PROD):
+        raise ValueError("zonal_allreduce: unknown reduction %r" % (red,))
+    op = dist.ReduceOp.SUM if red == SUM else dist.ReduceOp.PRODUCT
+    if integer:
+        t = torch.tensor([int(value)], dtype=torch.int64)
+        dist.all_reduce(t, op=op)
+        v = int(t.item())
+        if bits:
+            v &= (1 << bits) - 1
+            if signed and v >= 1 << (bits - 1):
+                v -= 1 << bits
+        return v
+    t = torch.tensor([float(value)], dtype=torch.float64)
+    dist.all_reduce(t, op=op)
+    return float(t.item())

@@ -85,6 +85,37 @@ def zones(rank, world, dist):
             "sum_rel": float(np.max(np.abs(s.numpy() - ref["sum64"]) / np.abs(ref["sum64"])))}
 
 
+def zonal(rank, world, dist):
+    """Whole-raster reductions of a row-split raster: each rank reduces its own
+    rows, zonal_allreduce combines them."""
+    H, W = 257, 311
+    val = synth.lognormal_f32(H, W, seed=45).astype(np.float64)
+    val[3, 4] = -7.25
+    ints = (np.arange(H * W, dtype=np.int64).reshape(H, W) * 2654435761) % 1000003 - 500000
+    small = (ints % 3 + 1).astype(np.int64)
+    sp = RS.RowSplit(H, W, rank, world, margin=0)
+    mine = slice(sp.y0, sp.y1)
+    res = {}
+    s = RS.zonal_allreduce(float(val[mine].sum()), RS.SUM, dist)
+    res["fsum_rel"] = abs(s - float(val.sum())) / abs(float(val.sum()))
+    res["fmax"] = RS.zonal_allreduce(float(val[mine].max()), RS.MAX, dist) == float(val.max())
+    res["fmin"] = RS.zonal_allreduce(float(val[mine].min()), RS.MIN, dist) == float(val.min())
+    res["isum"] = RS.zonal_allreduce(int(ints[mine].sum()), RS.SUM, dist) == int(ints.sum())
+    res["imax"] = RS.zonal_allreduce(int(ints[mine].max()), RS.MAX, dist) == int(ints.max())
+    res["imin"] = RS.zonal_allreduce(int(ints[mine].min()), RS.MIN, dist) == int(ints.min())
+    tot = 1
+    for v in small[:, :2].ravel():
+        tot = (tot * int(v)) & 0xFFFFFFFF
+    want = tot - (1 << 32) if tot >= 1 << 31 else tot
+    p = 1
+    for v in small[mine, :2].ravel():
+        p = (p * int(v)) & 0xFFFFFFFF
+    res["iprod_wrapped"] = RS.zonal_allreduce(p, RS.PROD, dist, bits=32) == want
+    res["and"] = RS.zonal_allreduce(bool((ints[mine] != 0).all()), RS.AND, dist) == bool((ints != 0).all())
+    res["or"] = RS.zonal_allreduce(bool((ints[mine] == 7).any()), RS.OR, dist) == bool((ints == 7).any())
+    return res
+
+
 def engine(rank, world, dist, kind, border):
     """The same split with each rank's rows computed by the engine on the GPU
     (ma_fromDeviceRows / ma_evalRows); rank 0 compares with a one-process
@@ -131,6 +162,8 @@ def main():
             res = hill(rank, world, dist, int(mode[4:]))
         elif mode.startswith("life"):
             res = life(rank, world, dist, int(mode[4:]))
+        elif mode == "zonal":
+            res = zonal(rank, world, dist)
         else:
             res = zones(rank, world, dist)
         print(json.dumps(dict(res, rank=rank)), flush=True)

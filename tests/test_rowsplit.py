@@ -5,7 +5,8 @@ point-to-point send / recv into each rank's own buffer, rows computed per rank
 evaluation. Hillshade under the three border rules and Game of Life over 100
 generations (halo of 4 rows exchanged every 4 generations) are bit-identical;
 per-zone count / min / max are bit-identical and sums agree to float64
-rounding."""
+rounding; whole-raster reductions (zsum, zprod, zmax, zmin, rAND, rOR)
+combined across ranks are exact for integers and float max / min."""
 import json
 import os
 import socket
@@ -65,6 +66,18 @@ def test_zone_stats_allreduce(world):
     for r in range(world):
         assert outs[r]["count"] and outs[r]["min"] and outs[r]["max"], outs[r]
         assert outs[r]["sum_rel"] < 1e-12
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_whole_raster_reductions_allreduce(world):
+    """zsum / zprod / zmax / zmin / rAND / rOR of a row-split raster: each
+    rank's reduction of its own rows combined on every rank. Integer results
+    and float max / min are exact, float sums agree to float64 rounding."""
+    outs = _run("zonal", world)
+    for r in range(world):
+        o = outs[r]
+        assert all(o[k] for k in ("fmax", "fmin", "isum", "imax", "imin", "iprod_wrapped", "and", "or")), o
+        assert o["fsum_rel"] < 1e-12
 
 
 def test_band_rows_partition():
