@@ -248,10 +248,11 @@ def zonal_allreduce(value, red, dist, bits=None, signed=True):
     one-device evaluation to that type's rounding; float MAX and MIN travel as
     order-preserving integer keys and are exact and independent of the rank
     order; rAND / rOR are the MIN / MAX of the ranks' truth values."""
+    import numbers
     import torch
     if dist is None:
         return value
-    integer = isinstance(value, (bool, int)) and not isinstance(value, float)
+    integer = isinstance(value, numbers.Integral)       # Python or NumPy integers (bool included)
     if red in (AND, OR):
         t = torch.tensor([1 if value else 0], dtype=torch.int64)
         dist.all_reduce(t, op=dist.ReduceOp.MIN if red == AND else dist.ReduceOp.MAX)
