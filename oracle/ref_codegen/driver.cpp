@@ -6,7 +6,7 @@
 // reference fuse, generate and print its OpenCL kernels (the stand-in OpenCL of
 // stubs.cpp runs nothing).
 //
-// usage: ref_codegen hill|life|wsum <work dir>
+// usage: ref_codegen hill|life|wsum|stats|view <work dir>
 //        ref_codegen binwrite <path> <W> <H> <BS> <dtype>
 //        ref_codegen binread <path> <out>
 #include "front/bindings.hpp"
@@ -156,7 +156,7 @@ int main(int argc, char **argv) {
     return bin_write(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]));
   if (argc >= 4 && std::string(argv[1]) == "binread") return bin_read(argv[2], argv[3]);
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s hill|life|wsum <work dir>\n", argv[0]);
+    std::fprintf(stderr, "usage: %s hill|life|wsum|stats|view <work dir>\n", argv[0]);
     return 2;
   }
   const std::string what = argv[1], dir = argv[2];
@@ -186,11 +186,58 @@ int main(int argc, char **argv) {
     o = bin(o, bin(fconst(0.3), r[2], MUL), ADD);
     o = bin(o, bin(r[3], fconst(0.4), MUL), ADD);
     out = bin(o, iconst(0), ADD);
+  } else if (what == "stats") {
+    // python/stats.py:12-35 (N = prod(datasize) is a Python int, 1.0/N a float)
+    write_bin(dir + "/dem.bin", 512, 512, 256, F32);
+    Node *dem = ma_read((dir + "/dem.bin").c_str());
+    const int N = 512 * 512;
+    Node *maxv = ma_zonalReduc(dem, MAX), *minv = ma_zonalReduc(dem, MIN);
+    Node *rang = bin(maxv, minv, SUB);
+    Node *mean = bin(ma_zonalReduc(dem, SUM), iconst(N), DIV);
+    Node *geom = bin(ma_zonalReduc(dem, PROD), fconst(1.0 / N), POW);
+    Node *harm = bin(iconst(N), ma_zonalReduc(bin(fconst(1.0), dem, DIV), SUM), DIV);
+    Node *quam = un(bin(ma_zonalReduc(bin(dem, iconst(2), POW), SUM), iconst(N), DIV), SQRT);
+    Node *cubm = un(bin(ma_zonalReduc(bin(dem, iconst(3), POW), SUM), iconst(N), DIV), CBRT);
+    Node *dev = bin(bin(dem, mean, SUB), iconst(2), POW);
+    Node *std_ = un(bin(ma_zonalReduc(dev, SUM), iconst(N), DIV), SQRT);
+    Node *norm = bin(bin(dev, minv, SUB), rang, DIV);
+    Node *nstd = un(bin(ma_zonalReduc(norm, SUM), iconst(N), DIV), SQRT);
+    Node *all[] = {maxv, minv, rang, mean, geom, harm, quam, cubm, std_, nstd};
+    for (Node *n : all) ma_increaseRef(n);
+    std::fflush(stdout);
+    ma_eval(all, 10);
+    std::fflush(stdout);
+    for (Node *n : all) ma_decreaseRef(n);
+    return 0;
+  } else if (what == "view") {
+    // python/view.py:17-43 with observer (100, 150) and h = 10.0
+    write_bin(dir + "/dem.bin", 512, 512, 256, F32);
+    Node *dem = ma_read((dir + "/dem.bin").c_str());
+    Node *norm = bin(bin(dem, ma_zonalReduc(dem, MIN), SUB),
+                     bin(ma_zonalReduc(dem, MAX), ma_zonalReduc(dem, MIN), SUB), DIV);
+    const int ox = 100, oy = 150;
+    const double h = 10.0;
+    Node *shift = bin(norm, fconst(h), SUB);
+    Node *x = bin(iconst(ox), ma_index(norm, D1), SUB);
+    Node *y = bin(iconst(oy), ma_index(norm, D2), SUB);
+    Node *dist = un(bin(bin(bin(x, x, MUL), bin(y, y, MUL), ADD), fconst(0.0), ADD), SQRT);
+    Node *slope = bin(shift, dist, DIV);
+    Node *maxr = ma_radialScan(slope, MAX, Coord{ox, oy});
+    Node *view = bin(bin(bin(maxr, dist, MUL), fconst(h), ADD), norm, SUB);
+    std::vector<VariantType> f;
+    for (double v : {1.0 / 16, 1.0 / 8, 1.0 / 16, 1.0 / 8, 1.0 / 4, 1.0 / 8, 1.0 / 16, 1.0 / 8, 1.0 / 16})
+      f.push_back(VariantType((float)v));
+    Node *soft = ma_convolution(view, f.data(), 9, DataSize{3, 3});
+    VariantType zero = VariantType(0.0f);
+    Node *zeros = ma_constant(zero, DataSize{512, 512}, F32, ROW + BLK, BlockSize{256, 256});
+    out = ma_conditional(bin(soft, fconst(0.1), LT), dem, zeros);
   } else {
     std::fprintf(stderr, "unknown program %s\n", what.c_str());
     return 2;
   }
   ma_increaseRef(out);
   std::fflush(stdout);
-  return ma_write(out, (dir + "/out.bin").c_str());
+  const int rc = ma_write(out, (dir + "/out.bin").c_str());
+  ma_decreaseRef(out);
+  return rc;
 }

@@ -2,7 +2,8 @@
 
 tests/golden/ref_kernel_facts.json holds facts of the OpenCL kernels that the
 reference's runtime generates for the example programs (hill.py, life.py,
-wsum.py), and of the scalar values it launches them with, produced by running
+wsum.py, stats.py, view.py), and of the scalar values it launches them with,
+produced by running
 the reference's DAG, fusion compiler and kernel generators built from its own
 sources (oracle/ref_codegen: build_ref_codegen.py, dump_kernels.py). These
 tests check that the oracle's restatement (oracle/oracle.c) performs the same
@@ -198,3 +199,83 @@ def test_bin_files_written_here_read_by_the_reference(M, tmp_path, w, h, bs, dty
     assert (W, H, b0, b1) == (w, h) + tuple(bs)
     assert mo == M.ROW + M.BLK and dt == M._dt_of_np[np.dtype(dtype).name]
     assert np.array_equal(np.frombuffer(body, dtype=dtype).reshape(h, w), a)
+
+
+def test_stats_reductions_as_the_reference_generates_them(facts, M):
+    """stats.py (python/stats.py:12-35): the reference's two zonal kernels
+    reduce with these neutral values and operators (util/ReductionType.cpp),
+    compute 1.0 / dem, dem ** 2 and dem ** 3 as pow with an integer exponent,
+    and in the second pass (dem - mean) ** 2 and (dev - minv) / rang; the
+    engine's kernels for the same script start from the same neutral values
+    and compute the same operations."""
+    first, second = facts["stats"]
+    assert first["statements"][4:] == ["t4f = t1f / t0f", "t5f = pow(t0f,t2i)", "t6f = pow(t0f,t3i)"]
+    assert [(a["type"], a["value"]) for a in first["scalar_args"]] == [("float", 1.0), ("int", 2), ("int", 3)]
+    assert first["zonal"] == [{"atomic": "MAX", "tree": "max", "neutral": "-INFINITY"},
+                              {"atomic": "MIN", "tree": "min", "neutral": "INFINITY"},
+                              {"atomic": "SUM", "tree": "+", "neutral": "0"},
+                              {"atomic": "PROD", "tree": "*", "neutral": "1"}] + \
+        [{"atomic": "SUM", "tree": "+", "neutral": "0"}] * 3
+    assert second["statements"][5:] == ["t5f = t0f - t3f", "t6f = pow(t5f,t4i)", "t7f = t6f - t1f", "t8f = t7f / t2f"]
+    assert [z["atomic"] for z in second["zonal"]] == ["SUM", "SUM"]
+    import re
+    src = M.generated_source(*W_stats(M).values())
+    for red, neutral in ((6, "__int_as_float(0xff800000)"), (7, "__int_as_float(0x7f800000)"), (1, "0x0p+0f"),
+                         (2, "0x1p+0f")):
+        acc = re.search(r"(acc\d+) = RedOp<%d, float>" % red, src).group(1)
+        assert re.search(r"float %s = %s;" % (acc, re.escape(neutral)), src), (red, neutral)
+    assert re.search(r"= \(float\)\(\(\(float\)0x1p\+0f\) / i0\);", src)           # 1.0 / dem in float32
+    assert len(re.findall(r"powf\(\(float\)\(\w+\), \(float\)\(\(\(s32\)2\)\)\)", src)) == 2   # dem ** 2, dev
+    assert len(re.findall(r"powf\(\(float\)\(\w+\), \(float\)\(\(\(s32\)3\)\)\)", src)) == 1
+
+
+def W_stats(M):
+    import numpy as np
+    from map_b200 import workloads as W
+    return W.stats(M.from_numpy(np.ones((512, 512), np.float32), bs=[256, 256]))
+
+
+def test_viewshed_chain_as_the_reference_generates_it(facts):
+    """view.py (python/view.py:17-43): the reference's radial kernel computes
+    the normalised DEM, the observer distance with S64 integer differences and
+    squares (x*x + y*y), converted to F32 by the + 0.0, its square root, the
+    slope, the radial max guarded by isfinite, and the view; the restatement
+    the tests use (tests/test_gpu_scan.py slope_from_observer, oracle.c
+    orc_radial_f32) follows those steps, checked here by evaluating the
+    reference's statements literally in NumPy against it."""
+    import importlib.util
+    import numpy as np
+    radial = [k for k in facts["view"] if k["guards"]][0]
+    assert radial["guards"] == ["isfinite(t19f)"]
+    st = radial["statements"]
+    assert st[7:] == ["t7f = t0f - t1f", "t8f = t7f / t2f", "t9f = t8f - t3f", "t10l = BC0*BS0+bc0", "t11l = t4i - t10l",
+                      "t12l = BC1*BS1+bc1", "t13l = t5i - t12l", "t14l = t13l * t13l", "t15l = t11l * t11l",
+                      "t16l = t15l + t14l", "t17f = t16l + t6f", "t18f = sqrt(t17f)", "t19f = t9f / t18f",
+                      "t20f = LIT_F32(t21f[gc+1],t21f[gc])", "t20f = max(t20f, t19f)", "t22f = t20f * t18f",
+                      "t23f = t22f + t3f", "t24f = t23f - t8f"]
+    args = radial["scalar_args"]
+    assert [a["type"] for a in args] == ["float", "float", "float", "int", "int", "float"]
+    assert args[2]["bits"] == "41200000" and [args[3]["value"], args[4]["value"]] == [100, 150]
+    assert args[5]["bits"] == "00000000"
+    # the reference's statements, literally, on a small normalised raster
+    rng = np.random.default_rng(3)
+    h, w, ox, oy, hh = 37, 53, 11, 29, np.float32(10.0)
+    norm = rng.random((h, w)).astype(np.float32)
+    t10 = np.arange(w, dtype=np.int64)[None, :]
+    t12 = np.arange(h, dtype=np.int64)[:, None]
+    t11, t13 = np.int64(ox) - t10, np.int64(oy) - t12
+    t16 = t11 * t11 + t13 * t13
+    t17 = (t16.astype(np.float32) + np.float32(0.0)).astype(np.float32)
+    t18 = np.sqrt(t17)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        t19 = ((norm - hh) / t18).astype(np.float32)
+    spec = importlib.util.spec_from_file_location("gpu_scan", os.path.join(ROOT, "tests", "test_gpu_scan.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    slope, dist = mod.slope_from_observer(norm, [ox, oy], 10.0)
+    assert np.array_equal(dist.view(np.uint32), t18.view(np.uint32))
+    assert np.array_equal(slope.view(np.uint32), t19.view(np.uint32))
+    focal = [k for k in facts["view"] if k["masks"]][0]
+    assert list(focal["masks"].values()) == [[[0.0625, 0.125, 0.0625], [0.125, 0.25, 0.125], [0.0625, 0.125, 0.0625]]]
+    assert focal["statements"][-2:] == ["t7u8 = t0f < t5f", "t8f = (t7u8) ? t3f : t6f"]    # con(soft < 0.1, dem, 0)
+    assert focal["scalar_args"] == [{"type": "float", "value": np.float32(0.1).item(), "bits": "3dcccccd"}]
