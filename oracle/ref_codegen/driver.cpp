@@ -6,7 +6,7 @@
 // reference fuse, generate and print its OpenCL kernels (the stand-in OpenCL of
 // stubs.cpp runs nothing).
 //
-// usage: ref_codegen hill|life|wsum|stats|view <work dir>
+// usage: ref_codegen hill|life|wsum|stats|view|percent <work dir>
 //        ref_codegen binwrite <path> <W> <H> <BS> <dtype>
 //        ref_codegen binread <path> <out>
 #include "front/bindings.hpp"
@@ -156,7 +156,7 @@ int main(int argc, char **argv) {
     return bin_write(argv[2], std::atoi(argv[3]), std::atoi(argv[4]), std::atoi(argv[5]), std::atoi(argv[6]));
   if (argc >= 4 && std::string(argv[1]) == "binread") return bin_read(argv[2], argv[3]);
   if (argc < 3) {
-    std::fprintf(stderr, "usage: %s hill|life|wsum|stats|view <work dir>\n", argv[0]);
+    std::fprintf(stderr, "usage: %s hill|life|wsum|stats|view|percent <work dir>\n", argv[0]);
     return 2;
   }
   const std::string what = argv[1], dir = argv[2];
@@ -209,6 +209,15 @@ int main(int argc, char **argv) {
     std::fflush(stdout);
     for (Node *n : all) ma_decreaseRef(n);
     return 0;
+  } else if (what == "percent") {
+    // FocalPercent (front/Raster.cpp:438-447): percentage (AGE) and percentile
+    // (ILE) of an F32 raster over a 3 x 3 window, summed into one output
+    write_bin(dir + "/dem.bin", 512, 512, 256, F32);
+    Node *dem = ma_read((dir + "/dem.bin").c_str());
+    std::vector<VariantType> m(9, VariantType(1.0f));
+    Node *age = ma_focalPercent(dem, m.data(), 9, DataSize{3, 3}, AGE);
+    Node *ile = ma_focalPercent(dem, m.data(), 9, DataSize{3, 3}, ILE);
+    out = bin(age, ile, ADD);
   } else if (what == "view") {
     // python/view.py:17-43 with observer (100, 150) and h = 10.0
     write_bin(dir + "/dem.bin", 512, 512, 256, F32);

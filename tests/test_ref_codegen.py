@@ -279,3 +279,31 @@ def test_viewshed_chain_as_the_reference_generates_it(facts):
     assert list(focal["masks"].values()) == [[[0.0625, 0.125, 0.0625], [0.125, 0.25, 0.125], [0.0625, 0.125, 0.0625]]]
     assert focal["statements"][-2:] == ["t7u8 = t0f < t5f", "t8f = (t7u8) ? t3f : t6f"]    # con(soft < 0.1, dem, 0)
     assert focal["scalar_args"] == [{"type": "float", "value": np.float32(0.1).item(), "bits": "3dcccccd"}]
+
+
+def test_focal_percent_as_the_reference_generates_it(facts):
+    """FocalPercent (front/Raster.cpp:438-447, runtime/skeleton/FocalSkeleton.cpp:
+    375-403) as the reference generates it cannot run: its halo sizes are
+    empty (`int H0 = ;`), its window loops start at the centre (0 .. 2h), its
+    divisor lacks parentheses ((H0*2+1)*H1*2+1 instead of the window size), it
+    compares against the centre value before loading it (the load follows the
+    core), and its Predictor asserts on the node. The oracle keeps what the
+    kernel states -- `==` for percentage, `>` for percentile, a count in the
+    argument's type from 0, divided after the loop -- over the window centred
+    on the cell, by the window size, against the cell's own value."""
+    import numpy as np
+    from oracle import oracle as O
+    (k,) = facts["percent"]
+    assert k["halo"] == ["int H0 = ;", "int H1 = ;"]
+    assert k["loop_headers"] == ["for (int i1=0; i1<3; i1++)", "for (int i0=0; i0<3; i0++)"] * 2
+    assert k["focal_loops"] == ["t0f += (t1f == t2f[tap(i0,i1)])", "t3f += (t1f > t2f[tap(i0,i1)])"]
+    assert k["scalings"] == ["t0f /= (H0*2+1)*H1*2+1", "t3f /= (H0*2+1)*H1*2+1"]
+    assert k["statements"][:3] == ["t0f = 0", "t3f = 0", "t1f = LOAD_L_F32(IN_6)"]
+    a = np.random.default_rng(1).integers(0, 3, (20, 30)).astype(np.float32)
+    p = np.pad(a, 1)
+    win = np.stack([p[i:i + 20, j:j + 30] for i in range(3) for j in range(3)])
+    for typ, cmp in ((1, np.equal), (2, np.greater)):
+        want = (cmp(a[None], win).astype(np.float32).sum(axis=0) / np.float32(9)).astype(np.float32)
+        got = O.focal_percent(a, 1, 1, typ, (64, 64), border=2)
+        inner = (slice(1, -1), slice(1, -1))
+        assert np.array_equal(got[inner], want[inner])
